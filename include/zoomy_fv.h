@@ -1,0 +1,195 @@
+/*
+ * zoomy_fv.h — C ABI of libzoomyfv.so, the sm_100a implementation of
+ * zoomy-amrex's per-level finite-volume right-hand side and SSP-RK2 time step.
+ *
+ * The reference runs this path as AMReX C++ (Source/ZoomyAmr.cpp +
+ * Source/make_rhs.H) inside a compiled executable that zoomy_amrex/run_case.py
+ * launches as a subprocess. This library replaces that executable's hot loop
+ * with an in-process call: the caller (Python via ctypes, or any C caller)
+ * owns every device buffer, the library owns only a small handle.
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 = OK, <0 = error
+ *    (zfv_last_error() returns the message). No C++ exception crosses this ABI.
+ *  - State arrays are structure-of-arrays, component-major, x fastest:
+ *    Q[n][j][i], element (i,j,n) at Q + n*ny*nx + j*nx + i, i in [0,nx),
+ *    j in [0,ny). This is Array4's (i,j,k,n) order with no ghost cells:
+ *    ghost cells are never stored; they are rebuilt inside each kernel's
+ *    tile load (mirror + Model::boundary_conditions).
+ *  - Element type: double for ZFV_PREC_FP64, float for ZFV_PREC_FP32.
+ *  - All device work is enqueued on the given stream (cudaStream_t passed as
+ *    void*; NULL = legacy default stream). Functions never synchronize unless
+ *    their comment says so.
+ *  - A handle is used by one host thread at a time.
+ */
+#ifndef ZOOMY_FV_H
+#define ZOOMY_FV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZFV_MAX_PARAMS 16
+
+/* Compiled model families (the Model::/Numerics:: pair a handle runs). */
+enum {
+    ZFV_MODEL_SWE1D = 1,   /* shallow water, 1 horizontal dim: Q=[b,h,hu],    aux 4 */
+    ZFV_MODEL_SWE2D = 2    /* shallow water, 2 horizontal dims: Q=[b,h,hu,hv], aux 7 */
+};
+
+/* Arithmetic form. */
+enum {
+    ZFV_PREC_FP64 = 0      /* the plain form: FP64 everywhere, bit-compatible with the CPU path */
+};
+
+/* Status flags (bitwise OR) reported by zfv_get_status(). */
+enum {
+    ZFV_FLAG_NONFINITE_DT   = 1,   /* the CFL reduction produced a non-finite dt            */
+    ZFV_FLAG_MOOD_REDO      = 2,   /* a step was redone at order 1 (positivity = mood)      */
+    ZFV_FLAG_DONE           = 4    /* time >= time_end or step >= max_step: kernels idle   */
+};
+
+/*
+ * Solver configuration. Field meanings follow the reference's inputs deck
+ * (ZoomyAmr.cpp:27-83 reads it; build.py:55-120 writes it) and its
+ * generated MarchConstants.H (zoomy_amrex/_constants.py:59-88).
+ */
+typedef struct zfv_config {
+    int model;              /* ZFV_MODEL_*                                          */
+    int precision;          /* ZFV_PREC_*                                           */
+    int nx, ny;             /* amr.n_cell (ny = 1 for 1-D models)                   */
+    double prob_lo[2];      /* geometry.prob_lo                                     */
+    double prob_hi[2];      /* geometry.prob_hi                                     */
+    int spatial_order;      /* solver.spatial_order: 1 (PCM, 1 stage) or 2 (MUSCL/minmod, SSP-RK2) */
+    int well_balanced;      /* solver.well_balanced: Audusse hydrostatic reconstruction */
+    int implicit_source;    /* solver.implicit_source: point-implicit source after each stage */
+    int clamp_positivity;   /* solver.clamp_positivity: h<0 -> 0 in UpdateState    */
+    int positivity_mood;    /* solver.positivity == "mood": whole-step order-1 redo */
+    double cfl;             /* solver.cfl (pure safety factor)                      */
+    double dtmin, dtmax;    /* solver.dtmin / solver.dtmax                          */
+    double time_end;        /* solver.time_end                                      */
+    int max_step;           /* solver.max_step (<0: no cap)                         */
+    int cfl_dimension;      /* ZoomyConstants::c_cfl_dimension (= d)                */
+    int cfl_degree_factor;  /* ZoomyConstants::c_cfl_degree_factor (= 2k+1)         */
+    int bc_tag[4];          /* bc.x_lo, bc.x_hi, bc.y_lo, bc.y_hi resolved to the
+                               index in Model::get_boundary_tags()                  */
+    int n_params;           /* Model::n_parameters                                  */
+    double params[ZFV_MAX_PARAMS]; /* p_mat: Model::default_parameters() + params.* */
+} zfv_config;
+
+/* Device-side run status (read back by zfv_get_status; one 64-byte record). */
+typedef struct zfv_status {
+    double time;            /* simulated time reached                               */
+    double dt;              /* dt of the NEXT step (already clamped to time_end)    */
+    double mass;            /* sum(h) * dx * dy after the last completed step       */
+    double max_inv;         /* max over cells, dirs of |lambda|/dx of the last reduction */
+    int64_t step;           /* completed steps                                      */
+    uint32_t flags;         /* ZFV_FLAG_*                                           */
+    uint32_t mood_redos;    /* number of steps redone at order 1                    */
+    uint32_t pad[4];
+} zfv_status;
+
+typedef struct zfv_handle zfv_handle;
+
+/* Last error message of the calling thread ("" if none). */
+const char* zfv_last_error(void);
+
+/* Library build identification, e.g. "zoomyfv sm_100a fp64". */
+const char* zfv_version(void);
+
+/*
+ * Create a solver handle for one level.
+ * Replaces the ZoomyAmr constructor's deck parsing and parameter setup
+ * (Source/ZoomyAmr.cpp:27-107). Validates the configuration; no device work.
+ */
+int zfv_create(const zfv_config* cfg, zfv_handle** out);
+int zfv_destroy(zfv_handle* h);
+
+/* Model shape: number of state rows, aux rows, parameters and space dims. */
+int zfv_model_info(int model, int* n_q, int* n_aux, int* n_params, int* dimension);
+
+/*
+ * Bytes of caller-provided device scratch a handle needs (stage buffer,
+ * reduction partials and the device-side status record). The scratch must
+ * stay valid and unmodified between calls that share a run.
+ */
+size_t zfv_scratch_bytes(const zfv_handle* h);
+
+/*
+ * Initialise the device status record in scratch (time = 0, step = 0, flags
+ * cleared) and compute the first dt from (Q, aux) exactly as
+ * ZoomyAmr::ComputeDt does (Source/ZoomyAmr.cpp:448-515), reading the aux
+ * as stored (the reference's first ComputeDt sees the aux that
+ * init_solution wrote, before any UpdateState).
+ */
+int zfv_begin(zfv_handle* h, const void* Q, const void* aux, void* scratch, void* stream);
+
+/*
+ * ZoomyAmr::UpdateState (Source/ZoomyAmr.cpp:293-334) on every cell:
+ * Model::update_variables, optional h>=0 clamp, Model::update_aux_variables.
+ * Q and aux are updated in place.
+ */
+int zfv_update_state(zfv_handle* h, void* Q, void* aux, double time, void* stream);
+
+/*
+ * ZoomyAmr::ComputeDt (Source/ZoomyAmr.cpp:448-515) on (Q, aux) as stored.
+ * Writes the un-clamped-to-time_end dt and max_inv into the status record.
+ */
+int zfv_compute_dt(zfv_handle* h, const void* Q, const void* aux, void* scratch, void* stream);
+
+/*
+ * Up to n_steps iterations of ZoomyAmr::Evolve's loop body
+ * (Source/ZoomyAmr.cpp:782-810) for a single level: TimeStep's dt clamp to
+ * time_end (733-749), Advance (538-731: SSP-RK2 stages, implicit source,
+ * Heun combine, MOOD redo, final UpdateState), time/step bookkeeping and the
+ * mass sum (517-536). dt, time and the stop test live on the device, so the
+ * call enqueues work without synchronizing; steps past the stop condition
+ * are no-ops. Q is advanced in place; aux is written at the end of the call
+ * (aux = Model::update_aux_variables of the final state).
+ */
+int zfv_evolve(zfv_handle* h, void* Q, void* aux, void* scratch, int n_steps, void* stream);
+
+/*
+ * One explicit right-hand side as compute_cell_rhs / assemble_cell_rhs
+ * compute it (Source/make_rhs.H:234-290, 346-399) for the given stage
+ * state: UpdateState + ghost fill + RHS. Writes rhs[n][j][i]. Validation
+ * entry: the stepping kernels fuse this work and never store the RHS.
+ */
+int zfv_rhs(zfv_handle* h, const void* Q, const void* aux, void* rhs, double time, void* stream);
+
+/*
+ * Ghost fill as FillPatch + FillPhysicalBC_mf leave it
+ * (Source/ZoomyAmr.cpp:258-277, 342-443), after UpdateState: writes the
+ * grown arrays Qg[n][ny+2g][nx+2g], auxg[n][ny+2g][nx+2g] with g = ng
+ * (ng = 1 at order 1, 2 at order 2; in 1-D models only x ghosts are
+ * filled, as in the reference). Validation entry for the tile loaders.
+ */
+int zfv_fill_ghosts(zfv_handle* h, const void* Q, const void* aux, void* Qg, void* auxg,
+                    double time, void* stream);
+
+/* Sum(h) * dx * dy into the status record's mass field (ZoomyAmr.cpp:517-536). */
+int zfv_total_mass(zfv_handle* h, const void* Q, void* scratch, void* stream);
+
+/*
+ * Copy the device status record to *out. Synchronizes the stream.
+ */
+int zfv_get_status(zfv_handle* h, const void* scratch, zfv_status* out, void* stream);
+
+/*
+ * Per-step log written by zfv_evolve: for step s (1-based) entry s-1 holds
+ * {dt, time, mass} — the fields of the reference's "Step n dt: time: mass:"
+ * line (ZoomyAmr.cpp:804-809). The log keeps the last zfv_log_capacity()
+ * steps (ring buffer). Synchronizes the stream.
+ */
+int zfv_log_capacity(const zfv_handle* h);
+int zfv_read_log(zfv_handle* h, const void* scratch, double* out3, int max_entries,
+                 int64_t* first_step, int* n_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZOOMY_FV_H */
