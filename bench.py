@@ -1,0 +1,353 @@
+"""Benchmark: cell-updates/s of the SSP-RK2 step on 4096^2 shallow water with
+wet/dry, Manning friction (point-implicit) and well-balancing.
+
+One "step" is one full SSP-RK2 step (two fused stage kernels) over the whole
+4096 x 4096 grid. Inputs are synthetic (seeded): 16 Gaussian bumps as
+bathymetry, still water at eta = 1 m plus a 0.3 m Gaussian hump, reflective
+walls, Manning n = 0.03, dry threshold 1e-6 m.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU runs are independent replicas (one level per GPU, no data-path
+collective); the time is the max over ranks and the value the sum of cell
+updates over all ranks divided by it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s FP32-batched vs FP64 plain at stated error; HBM GB/s; adj/fwd"
+UNIT = "cell-updates/s"
+SEED = 2026
+N_DEFAULT = 4096
+DOMAIN = 100.0
+
+# Algorithmic HBM bytes per cell-update of the FP64 SWE step with a static bed:
+# stage 1 reads b,h,hu,hv and writes h,hu,hv (7 x 8 B); stage 2 reads
+# b,h*,hu*,hv* and Q^n h,hu,hv and writes h,hu,hv (10 x 8 B).
+BYTES_PER_CELL_STEP_FP64 = 136
+
+# DRAM bytes per cell per step of the two k_stage launches, from
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (profiles/k_stage_swe2d_fp64.md).
+NCU_TRAFFIC_PER_CELL_STEP_FP64 = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=N_DEFAULT, help="cells per side")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_fields(n: int, seed: int = SEED, rows: slice | None = None):
+    """Config-2 initial state (n x n over [0,100]^2): returns Q0 (4, ny, n), aux0 (7, ny, n)."""
+    rng = np.random.default_rng(seed)
+    cx, cy = rng.uniform(0, DOMAIN, 16), rng.uniform(0, DOMAIN, 16)
+    amp, wid = rng.uniform(0.2, 1.5, 16), rng.uniform(2.0, 10.0, 16)
+    hx, hy, hw = rng.uniform(0, DOMAIN), rng.uniform(0, DOMAIN), rng.uniform(2.0, 10.0)
+    dx = DOMAIN / n
+    x = (np.arange(n) + 0.5) * dx
+    ys = x if rows is None else x[rows]
+    ny = len(ys)
+    b = np.zeros((ny, n))
+    for k in range(16):
+        gx = np.exp(-((x - cx[k]) ** 2) / (2 * wid[k] ** 2))
+        gy = np.exp(-((ys - cy[k]) ** 2) / (2 * wid[k] ** 2))
+        b += amp[k] * np.outer(gy, gx)
+    eta = 1.0 + 0.3 * np.outer(np.exp(-((ys - hy) ** 2) / (2 * hw ** 2)),
+                               np.exp(-((x - hx) ** 2) / (2 * hw ** 2)))
+    h = np.maximum(eta - b, 0.0)
+    Q0 = np.zeros((4, ny, n))
+    Q0[0], Q0[1] = b, h
+    aux0 = np.zeros((7, ny, n))
+    aux0[1] = np.where(x < 0.5 * DOMAIN, 2.0, 1.0)[None, :]   # init_solution on aux
+    return Q0, aux0
+
+
+def workload_config(n: int, ny: int | None = None, y_extent: float | None = None):
+    from zoomy_amrex_b200._abi import ZFV_MODEL_SWE2D, make_config
+    ny = n if ny is None else ny
+    ye = DOMAIN if y_extent is None else y_extent
+    return make_config(ZFV_MODEL_SWE2D, n, ny, (0.0, 0.0), (DOMAIN, ye), spatial_order=2,
+                       well_balanced=True, implicit_source=True, clamp_positivity=False,
+                       cfl=0.45, dtmin=1e-7, dtmax=1.0, time_end=1e30, max_step=-1,
+                       bc=("wall",) * 4, params={"n_m": 0.03, "h_floor": 1e-6, "eps": 1e-24})
+
+
+def config_desc(n, K):
+    return {"workload": f"swe2d_{n}x{n}_wetdry_manning_implicit_wb_order2", "nx": n, "ny": n,
+            "n_q": 4, "spatial_order": 2, "scheme": "MUSCL-minmod + path-conservative Rusanov, SSP-RK2",
+            "implicit_source": True, "well_balanced": True, "bc": "wall", "cfl": 0.45,
+            "steps_timed": K, "l2": "inputs larger than L2 (state 4 x 8 B x n^2)"}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return None
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5], parts[6], parts[7], parts[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        sm = sorted(r[0] for r in rows)
+        reasons = set()
+        for r in rows:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), r[2:]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_sample(kind: str, n: int, rows: int = 256, min_seconds: float = 10.0, max_steps: int = 40):
+    """The CPU implementation on a strip of the same workload (first `rows` rows
+    of the n x n grid, same cells and data, walls on the strip edges)."""
+    from oracle.oracle import Oracle
+    o = Oracle(kind)
+    threads = o.max_threads()
+    Q0, A0 = workload_fields(n, rows=slice(0, rows))
+    cfg = workload_config(n, ny=rows, y_extent=DOMAIN * rows / n)
+    cfg.max_step = 1
+    t0 = time.perf_counter()
+    Q, A, _, _, _, _ = o.run(cfg, Q0, A0)          # warm-up + calibration step
+    one = time.perf_counter() - t0
+    steps = int(max(1, min(max_steps, min_seconds / max(one, 1e-6))))
+    cfg.max_step = steps
+    t0 = time.perf_counter()
+    Q, A, _, _, _, _ = o.run(cfg, Q, A)            # `steps` steps in one Evolve call
+    el = time.perf_counter() - t0
+    return {"value": n * rows * steps / el, "unit": UNIT, "cores": threads,
+            "kind": "reference" if kind == "ref" else "port",
+            "sample": f"{steps} SSP-RK2 steps on rows 0..{rows - 1} of the {n}x{n} grid "
+                      f"({n * rows} cells), OpenMP over rows, FP64"}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def run_reference(args, ws, rank):
+    """Reference arm: the reference's CPU path (make_rhs.H via oracle/_ref, or
+    the restatement when the reference build is absent) on the host cores."""
+    if rank != 0:
+        return
+    from oracle.oracle import LIB_REF
+    kind = "ref" if LIB_REF.exists() else "oracle"
+    from oracle.oracle import Oracle
+    o = Oracle(kind)
+    n, rows = args.n, 64
+    Q0, A0 = workload_fields(n, rows=slice(0, rows))
+    cfg = workload_config(n, ny=rows, y_extent=DOMAIN * rows / n)
+    cfg.max_step = max(1, args.warmup)
+    Q, A, _, _, _, _ = o.run(cfg, Q0, A0)          # warm-up steps
+    cfg.max_step = args.steps
+    t0 = time.perf_counter()
+    Q, A, _, _, _, _ = o.run(cfg, Q, A)            # K steps in one Evolve call
+    el = time.perf_counter() - t0
+    v = n * rows * args.steps / el
+    sample = (f"each step: 1 SSP-RK2 step on rows 0..{rows - 1} of the {n}x{n} grid ({n * rows} cells), "
+              f"{'reference make_rhs.H' if kind == 'ref' else 'oracle restatement'}, FP64, OpenMP")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_desc(n, args.steps),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": o.max_threads(),
+                             "kind": "reference" if kind == "ref" else "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    from zoomy_amrex_b200.build import build
+    if rank == 0 or ws == 1:
+        build()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    from zoomy_amrex_b200.level import Level
+
+    n = args.n
+    cells = n * n
+    Q0, A0 = workload_fields(n)
+    cfg = workload_config(n)
+    lev = Level(cfg, Q0, A0, device=f"cuda:{local}")
+    stream = lev.stream
+    lev.begin()
+    for _ in range(max(3, args.warmup)):
+        lev.evolve(1)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if ws == 1:
+            return v
+        import torch.distributed as dist
+        t = torch.tensor([v], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    K = args.steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        barrier(); torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            lev.evolve(K)
+            e1.record(stream)
+        torch.cuda.synchronize(); barrier()
+    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(ms)
+    st = lev.status()
+    assert not st["done"] and np.isfinite(st["dt"]), st
+    value = cells * K * ws / (ms * 1e-3)
+
+    # per-step device time of the fused stage pair (the dominant kernel)
+    step_s = ms * 1e-3 / K
+    peak, peak_kind = measured_peak()
+    achieved = cells * BYTES_PER_CELL_STEP_FP64 / step_s / 1e9
+    traffic = (None if NCU_TRAFFIC_PER_CELL_STEP_FP64 is None
+               else NCU_TRAFFIC_PER_CELL_STEP_FP64 * cells / 2)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                "kernel": "k_stage (stage-1 + stage-2 launches per step)",
+                "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_FP64,
+                "traffic_per": "launch"}
+    lev.close()
+
+    # end to end through the public Level API with host buffers: pinned H2D of
+    # the initial state, K steps, D2H of the final state, all inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        Qh = torch.from_numpy(Q0).pin_memory()
+        Ah = torch.from_numpy(A0).pin_memory()
+        Qout = torch.empty_like(Qh).pin_memory()
+        lev2 = Level(cfg, Q0, A0, device=f"cuda:{local}")
+        torch.cuda.synchronize(); barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(lev2.stream):
+            f0.record(lev2.stream)
+            lev2.Q.copy_(Qh, non_blocking=True)
+            lev2.aux.copy_(Ah, non_blocking=True)
+            lev2.begin()
+            lev2.evolve(K)
+            Qout.copy_(lev2.Q, non_blocking=True)
+            f1.record(lev2.stream)
+        torch.cuda.synchronize(); barrier()
+        ms2 = max_over_ranks(f0.elapsed_time(f1))
+        lev2.close()
+        e2e = {"value": cells * K * ws / (ms2 * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": (Qh.numel() + Ah.numel()) * 8 / K,
+               "d2h_bytes_per_step": Qout.numel() * 8 / K,
+               "note": "one run of K steps through Level: pinned H2D of (Q, aux), begin (first dt), "
+                       "K device-driven steps, D2H of Q"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle.oracle import LIB_REF
+        try:
+            cpu = cpu_sample("ref" if LIB_REF.exists() else "oracle", n)
+        except Exception as e:   # the baseline is reported, not required
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
+                "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(config_desc(n, K), parallelism=f"replicas x{ws}" if ws > 1 else "single GPU"),
+                "forms": {"fp64_plain": value, "fp32_chosen": None},
+                "hbm_gbs": achieved,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": 2 * K, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -100,6 +100,10 @@ const char* zfv_last_error(void);
 /* Library build identification, e.g. "zoomyfv sm_100a fp64". */
 const char* zfv_version(void);
 
+/* sizeof(zfv_config) and sizeof(zfv_status) as compiled, for binding checks. */
+size_t zfv_sizeof_config(void);
+size_t zfv_sizeof_status(void);
+
 /*
  * Create a solver handle for one level.
  * Replaces the ZoomyAmr constructor's deck parsing and parameter setup

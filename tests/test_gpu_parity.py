@@ -1,0 +1,242 @@
+"""sm_100a kernels against the CPU oracle, through the C ABI.
+
+FP64 with --fmad=false on the GPU and -ffp-contract=off on the CPU evaluate
+the same IEEE operations in the same order, so state, aux, step count, time
+and dt are required to match BITWISE; the mass (a reduction whose summation
+order differs) to 1e-13 relative.
+"""
+import numpy as np
+import pytest
+
+from cases import GOLDEN_CASES, golden_setup, setup
+from zoomy_amrex_b200.models import SWE
+
+pytestmark = pytest.mark.gpu
+
+
+def run_gpu(cfg, Q0, A0, use_graph=False, chunk=16):
+    from zoomy_amrex_b200.level import Level
+    lev = Level(cfg, Q0, A0)
+    try:
+        st = lev.run(chunk=chunk, use_graph=use_graph)
+        return lev.Q.cpu().numpy(), lev.aux.cpu().numpy(), st, lev.log()
+    finally:
+        lev.close()
+
+
+def assert_same_run(cfg, Q0, A0, oracle, use_graph=False):
+    Qo, Ao, n, t, logo, _ = oracle.run(cfg, Q0, A0)
+    Qg, Ag, st, logg = run_gpu(cfg, Q0, A0, use_graph=use_graph)
+    assert st["step"] == n, (st["step"], n)
+    assert st["time"] == t
+    bad = np.argwhere(Qg != Qo)
+    assert bad.size == 0, f"{len(bad)} state values differ, first {bad[:3].tolist()}, max {np.abs(Qg - Qo).max():.3e}"
+    assert np.array_equal(Ag, Ao), f"aux max diff {np.abs(Ag - Ao).max():.3e}"
+    k = min(len(logo), len(logg))
+    assert np.array_equal(logg[-k:, :2], logo[-k:, :2]), "dt/time sequence differs"
+    np.testing.assert_allclose(logg[-k:, 2], logo[-k:, 2], rtol=1e-13, atol=0)
+    return Qg, Ag, st
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN_CASES))
+def test_golden_cases_bitwise_vs_oracle(cuda, oracle, name):
+    assert_same_run(*golden_setup(name), oracle)
+
+
+def _bumps(x, seed, n=6, lo=0.0, hi=10.0, amp=(0.2, 1.2), width=(0.5, 2.0)):
+    rng = np.random.default_rng(seed)
+    b = np.zeros(x.shape[1])
+    for _ in range(n):
+        cx, cy = rng.uniform(lo, hi, 2)
+        a, w = rng.uniform(*amp), rng.uniform(*width)
+        b += a * np.exp(-((x[0] - cx) ** 2 + (x[1] - cy) ** 2) / (2 * w * w))
+    return b
+
+
+def wetdry_ic(seed, eta0=1.0, hump=0.3, moving=False):
+    def ic(x):
+        b = _bumps(x, seed)
+        rng = np.random.default_rng(seed + 1)
+        cx, cy = rng.uniform(2, 8, 2)
+        eta = eta0 + hump * np.exp(-((x[0] - cx) ** 2 + (x[1] - cy) ** 2) / 2.0)
+        h = np.maximum(eta - b, 0.0)
+        hu = h * rng.uniform(-0.1, 0.1, h.shape) if moving else np.zeros_like(h)
+        hv = h * rng.uniform(-0.1, 0.1, h.shape) if moving else np.zeros_like(h)
+        return np.array([b, h, hu, hv])
+    return ic
+
+
+def dambreak_2d(x):
+    h = np.where(x[0] < 0.5, 2.0, 1.0)
+    z = np.zeros_like(h)
+    return np.array([z, h, z, z])
+
+
+CASES_2D = {
+    # config 1: 100x100 dam break, order 2, cfl 0.45 (Exec/inputs), extrapolation, t=0.1
+    "dambreak_o2": (SWE(2, "extrapolation", None),
+                    dict(dimension=2, domain=[0, 1, 0, 1], n_cells=[100, 100], spatial_order=2,
+                         cfl=0.45, time_end=0.1, dtmax=0.1)),
+    "dambreak_o2_clamp": (SWE(2, "extrapolation", None),
+                          dict(dimension=2, domain=[0, 1, 0, 1], n_cells=[100, 100], spatial_order=2,
+                               cfl=0.45, time_end=0.1, dtmax=0.1, clamp_positivity=True)),
+    "wetdry_wb_manning_o2": (SWE(2, "wall", wetdry_ic(3), parameters={"n_m": 0.03}),
+                             dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[48, 40],
+                                  spatial_order=2, cfl=0.9, time_end=1e30, max_step=40,
+                                  well_balanced=True, implicit_source=True)),
+    "wetdry_moving_o2_mixed_bc": (SWE(2, {"West": "wall", "East": "extrapolation", "South": "extrapolation",
+                                          "North": "wall"}, wetdry_ic(5, moving=True),
+                                      parameters={"n_m": 0.05}),
+                                  dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[33, 17],
+                                       spatial_order=2, cfl=0.9, time_end=1e30, max_step=30,
+                                       well_balanced=True, implicit_source=False)),
+    "wetdry_o1_impl": (SWE(2, "wall", wetdry_ic(7, moving=True), parameters={"n_m": 0.03}),
+                       dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[37, 29], spatial_order=1,
+                            cfl=0.9, time_end=1e30, max_step=25, well_balanced=True,
+                            implicit_source=True)),
+    "tiny_7x5_o2": (SWE(2, "wall", wetdry_ic(11, moving=True)),
+                    dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[7, 5], spatial_order=2,
+                         cfl=0.9, time_end=1e30, max_step=20, well_balanced=True)),
+    "strip_65x2_o2": (SWE(2, "extrapolation", wetdry_ic(13, moving=True)),
+                      dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[65, 2], spatial_order=2,
+                           cfl=0.9, time_end=1e30, max_step=10)),
+}
+
+
+def ritter_o2(x):
+    h = np.where(x[0] < 5.0, 0.005, 0.0)
+    z = np.zeros_like(h)
+    return np.array([z, h, z])
+
+
+def bump_1d(x):
+    b = 0.3 * np.exp(-((x[0] - 4.0) ** 2)) + 0.8 * np.exp(-((x[0] - 7.0) ** 2) * 4)
+    h = np.maximum(0.9 - b, 0.0)
+    return np.array([b, h, 0.02 * h])
+
+
+CASES_1D = {
+    "ritter_o2": (SWE(1, "swashes", ritter_o2),
+                  dict(dimension=1, domain=[0, 10], n_cells=129, spatial_order=2, cfl=0.9, time_end=2.0)),
+    "bump_wall_wb_impl_o2": (SWE(1, "wall", bump_1d, parameters={"n_m": 0.04}),
+                             dict(dimension=1, domain=[0, 10], n_cells=200, spatial_order=2, cfl=0.9,
+                                  time_end=1e30, max_step=60, well_balanced=True, implicit_source=True)),
+    "bump_o1_explicit_manning": (SWE(1, {"West": "wall", "East": "extrapolation"}, bump_1d,
+                                     parameters={"n_m": 0.04}),
+                                 dict(dimension=1, domain=[0, 10], n_cells=301, spatial_order=1,
+                                      cfl=0.9, time_end=1e30, max_step=40, well_balanced=True)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES_2D))
+def test_2d_cases_bitwise_vs_oracle(cuda, oracle, name):
+    assert_same_run(*setup(*CASES_2D[name]), oracle)
+
+
+@pytest.mark.parametrize("name", sorted(CASES_1D))
+def test_1d_cases_bitwise_vs_oracle(cuda, oracle, name):
+    assert_same_run(*setup(*CASES_1D[name]), oracle)
+
+
+def test_graph_replay_is_bitwise_eager(cuda, oracle):
+    cfg, Q0, A0 = setup(*CASES_2D["wetdry_wb_manning_o2"])
+    a = run_gpu(cfg, Q0, A0, use_graph=False)
+    b = run_gpu(cfg, Q0, A0, use_graph=True)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("dim", [1, 2])
+def test_ghost_fill_bitwise(cuda, oracle, order, dim):
+    """FillPatch + FillPhysicalBC_mf (ZoomyAmr.cpp:342-443): mirror indices,
+    x-first corners, wall reflection, identity aux BC."""
+    import torch
+    from zoomy_amrex_b200.level import Level
+    if dim == 2:
+        model, s = CASES_2D["wetdry_moving_o2_mixed_bc"]
+    else:
+        model, s = CASES_1D["bump_o1_explicit_manning"]
+    s = dict(s, spatial_order=order)
+    cfg, Q0, A0 = setup(model, s)
+    rng = np.random.default_rng(0)
+    A0 = A0 + rng.uniform(0, 1, A0.shape)       # carried aux rows must pass through unchanged
+    Qg_o, Ag_o = oracle.fill_ghosts(cfg, Q0, A0, 0.25)
+    lev = Level(cfg, Q0, A0)
+    Qg, Ag = lev.fill_ghosts(0.25)
+    torch.cuda.synchronize()
+    Qg, Ag = Qg.cpu().numpy(), Ag.cpu().numpy()
+    lev.close()
+    if dim == 1:   # only the j = 0 row (and its x ghosts) holds data in a 1-D run
+        ng = Qg.shape[1] // 2
+        Qg, Ag, Qg_o, Ag_o = (a[:, ng:ng + 1, :] for a in (Qg, Ag, Qg_o, Ag_o))
+    assert np.array_equal(Qg, Qg_o)
+    assert np.array_equal(Ag, Ag_o)
+
+
+@pytest.mark.parametrize("name", ["dambreak_o2", "wetdry_wb_manning_o2", "wetdry_o1_impl"])
+def test_rhs_bitwise(cuda, oracle, name):
+    """One stage's RHS (make_rhs.H:346-399) from a moving, partly dry state."""
+    import torch
+    from zoomy_amrex_b200.level import Level
+    cfg, Q0, A0 = setup(*CASES_2D[name])
+    Q1, A1, _, _, _, _ = oracle.run(cfg, Q0, A0, max_steps=3)   # a non-trivial state
+    for impl in (0, 1):
+        cfg.implicit_source = impl
+        R_o = oracle.rhs(cfg, Q1, A1, 0.5)
+        lev = Level(cfg, Q1, A1)
+        R = lev.rhs(0.5)
+        torch.cuda.synchronize()
+        R = R.cpu().numpy()
+        lev.close()
+        assert np.array_equal(R, R_o), f"max diff {np.abs(R - R_o).max():.3e}"
+
+
+def test_compute_dt_and_mass(cuda, oracle):
+    from zoomy_amrex_b200.level import Level
+    cfg, Q0, A0 = setup(*CASES_2D["wetdry_moving_o2_mixed_bc"])
+    Q1, A1, _, _, _, _ = oracle.run(cfg, Q0, A0, max_steps=4)
+    dt_o, mi_o = oracle.compute_dt(cfg, Q1, A1)
+    lev = Level(cfg, Q1, A1)
+    lev.begin()
+    dt, mi = lev.compute_dt()
+    m = lev.total_mass()
+    lev.close()
+    assert dt == dt_o and mi == mi_o
+    dx = (cfg.prob_hi[0] - cfg.prob_lo[0]) / cfg.nx
+    dy = (cfg.prob_hi[1] - cfg.prob_lo[1]) / cfg.ny
+    np.testing.assert_allclose(m, Q1[1].sum() * (dx * dy), rtol=1e-13)
+
+
+def test_first_dt_uses_stored_aux(cuda, oracle):
+    """ZoomyAmr::Evolve's first ComputeDt reads the aux init_solution wrote
+    (hinv = 0), not an updated one: a moving start must reproduce that."""
+    cfg, Q0, A0 = setup(*CASES_2D["wetdry_o1_impl"])
+    Qo, Ao, n, t, logo, _ = oracle.run(cfg, Q0, A0, max_steps=1)
+    from zoomy_amrex_b200.level import Level
+    lev = Level(cfg, Q0, A0)
+    lev.begin()
+    lev.evolve(1)
+    log = lev.log()
+    lev.close()
+    assert log[0, 0] == logo[0, 0]
+
+
+def test_update_state_bitwise(cuda, oracle):
+    import torch
+    from zoomy_amrex_b200.level import Level
+    cfg, Q0, A0 = setup(*CASES_2D["wetdry_moving_o2_mixed_bc"])
+    cfg.clamp_positivity = 1
+    Q0 = Q0.copy(); Q0[1, 3, 3] = -1e-3          # a negative depth for the clamp
+    Qo, Ao = oracle.update_state(cfg, Q0, A0, 0.0)
+    lev = Level(cfg, Q0, A0)
+    lev.update_state(0.0)
+    torch.cuda.synchronize()
+    assert np.array_equal(lev.Q.cpu().numpy(), Qo) and np.array_equal(lev.aux.cpu().numpy(), Ao)
+    lev.close()
+
+
+def test_run_is_deterministic(cuda):
+    cfg, Q0, A0 = setup(*CASES_2D["dambreak_o2"])
+    a = run_gpu(cfg, Q0, A0)
+    b = run_gpu(cfg, Q0, A0)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[3], b[3])

@@ -1,0 +1,87 @@
+"""The reference's test suite (tests/test_swe_*.py, test_wb_lake_at_rest.py,
+test_parity_numpy.py, test_parallel_two_ranks.py), run through this package's
+public entry points (HyperbolicSolver.solve / run_case) on the GPU and checked
+the way the reference checks itself: np.allclose against the golden (Q, Qaux)
+(tests/refs.py:301-312) plus each test's physical assertions."""
+import pathlib
+
+import numpy as np
+import pytest
+
+from cases import CFL_1D, CFL_2D, GOLDEN_CASES, gaussian_pulse_2d, lake_at_rest_ic, ritter_ic, stoker_ic
+from zoomy_amrex_b200.models import SME, SWE
+from zoomy_amrex_b200.run_case import run_case
+from zoomy_amrex_b200.solvers import HyperbolicSolver
+
+pytestmark = pytest.mark.gpu
+GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
+
+
+def check(name, Q, Qaux):   # tests/refs.py:check
+    ref = np.load(GOLDEN / f"{name}.npz")
+    assert np.allclose(Q, ref["Q"]), f"{name}.Q: max|diff| {np.abs(Q - ref['Q']).max():.3e}"
+    assert np.allclose(Qaux, ref["Qaux"]), f"{name}.Qaux: max|diff| {np.abs(Qaux - ref['Qaux']).max():.3e}"
+
+
+def march(model, settings, t_end, cfl):
+    r = run_case(model, dict(settings, time_end=t_end, cfl=cfl))
+    return r.Q, r.Qaux
+
+
+ONE_D = {"dimension": 1, "domain": [0.0, 10.0], "n_cells": 100, "spatial_order": 1,
+         "output_snapshots": 1, "max_level": 0}
+
+
+def test_stoker_wet(cuda):
+    Q, Qaux = march(SME(level=0, dimension=2, bc="swashes", initial_conditions=stoker_ic), ONE_D, 1.0, CFL_1D)
+    assert np.isfinite(Q).all()
+    assert Q[1].min() > 0.0
+    assert np.abs(Q[2]).max() > 0.0
+    check("stoker_wet", Q, Qaux)
+
+
+def test_ritter_dry(cuda):
+    Q, Qaux = march(SME(level=0, dimension=2, bc="swashes", initial_conditions=ritter_ic), ONE_D, 1.0, CFL_1D)
+    assert np.isfinite(Q).all()
+    assert Q[1].min() >= 0.0
+    assert Q[1].max() > 0.0
+    check("ritter_dry", Q, Qaux)
+
+
+def test_lake_at_rest_over_bump(cuda):
+    Q, Qaux = march(SME(level=0, dimension=2, bc="wall", initial_conditions=lake_at_rest_ic),
+                    dict(ONE_D, well_balanced=True), 1.0, CFL_1D)
+    eta = Q[0] + Q[1]
+    u = Q[2] / np.maximum(Q[1], 1e-300)
+    assert np.isfinite(Q).all()
+    assert np.abs(eta - eta.mean()).max() < 1e-12
+    assert np.abs(u).max() < 1e-12
+    check("wb_lake", Q, Qaux)
+
+
+def test_swe_2d_pulse(cuda):
+    solver = HyperbolicSolver(CFL=CFL_2D, order=1, well_balanced=False)
+    r = solver.solve(SME(level=0, dimension=3, bc="extrapolation", initial_conditions=gaussian_pulse_2d),
+                     {"domain": [-1.0, 1.0, -1.0, 1.0], "n_cells": [32, 32]},
+                     {"time_end": 0.1, "output": {"snapshots": 1}})
+    Q = r.Q
+    assert np.isfinite(Q).all() and Q[1].min() > 0.0
+    assert np.abs(Q[2]).max() > 0.0 and np.abs(Q[3]).max() > 0.0
+    check("swe_2d", Q, r.Qaux)
+
+
+@pytest.mark.parametrize("n_cells", [100, 200])
+def test_numpy_parity_goldens(cuda, n_cells):
+    Q, Qaux = march(SME(level=0, dimension=2, bc="swashes", initial_conditions=stoker_ic),
+                    dict(ONE_D, n_cells=n_cells), 0.5, CFL_1D)
+    check(f"parity_numpy_n{n_cells}", Q, Qaux)
+
+
+def test_two_rank_golden_and_box_invariance(cuda):
+    """The reference asserts 1 rank == 2 ranks bitwise; one GPU level is one
+    box, and the result equals the 2-rank golden bitwise."""
+    Q, Qaux = march(SME(level=0, dimension=2, bc="swashes", initial_conditions=stoker_ic),
+                    dict(ONE_D, n_cells=128), 0.5, CFL_1D)
+    ref = np.load(GOLDEN / "parallel_2rank.npz")
+    assert np.abs(Q - ref["Q"]).max() == 0.0
+    assert np.abs(Qaux - ref["Qaux"]).max() == 0.0

@@ -1,0 +1,80 @@
+"""The CPU oracle against the reference's golden data and assertions.
+
+The reference suite compares each run to tests/refs/<name>.npz with
+np.allclose (tests/refs.py:301-312) and asserts physical properties per test;
+both are applied here to the oracle, which the GPU path is then checked
+against. The oracle is also checked bitwise against the reference's own
+make_rhs.H (oracle/_ref) on the same driver.
+"""
+import numpy as np
+import pytest
+
+from cases import GOLDEN_CASES, golden_setup
+
+GOLDEN = __import__("pathlib").Path(__file__).resolve().parent / "golden"
+
+
+def golden(name):
+    return np.load(GOLDEN / f"{name}.npz")
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN_CASES))
+@pytest.mark.parametrize("face_based", [True, False])
+def test_oracle_matches_reference_golden(oracle, name, face_based):
+    cfg, Q0, A0 = golden_setup(name)
+    Q, A, n, t, log, _ = oracle.run(cfg, Q0, A0, face_based=face_based)
+    g = golden(name)
+    assert np.allclose(Q, g["Q"]), f"{name}.Q: max|diff| {np.abs(Q - g['Q']).max():.3e}"
+    assert np.allclose(A, g["Qaux"]), f"{name}.Qaux: max|diff| {np.abs(A - g['Qaux']).max():.3e}"
+    # far tighter than allclose: the restated model is fitted to the last bits
+    assert np.abs(Q - g["Q"]).max() <= 2e-15 * max(1.0, np.abs(g["Q"]).max())
+    assert t == cfg.time_end
+
+
+def test_stoker_properties(oracle):    # tests/test_swe_stoker_wet.py:36-41
+    Q, _, _, _, _, _ = oracle.run(*golden_setup("stoker_wet"))
+    assert np.isfinite(Q).all() and Q[1].min() > 0.0 and np.abs(Q[2]).max() > 0.0
+
+
+def test_ritter_properties(oracle):    # tests/test_swe_ritter_dry.py
+    Q, _, _, _, _, _ = oracle.run(*golden_setup("ritter_dry"))
+    assert np.isfinite(Q).all() and Q[1].min() >= 0.0 and Q[1].max() > 0.0
+
+
+def test_lake_at_rest_properties(oracle):   # tests/test_wb_lake_at_rest.py:94-103
+    Q, _, _, _, _, _ = oracle.run(*golden_setup("wb_lake"))
+    eta = Q[0] + Q[1]
+    u = Q[2] / np.maximum(Q[1], 1e-300)
+    assert np.abs(eta - eta.mean()).max() < 1e-12
+    assert np.abs(u).max() < 1e-12
+
+
+def test_swe_2d_properties(oracle):     # tests/test_swe_2d.py:145-151
+    Q, _, _, _, _, _ = oracle.run(*golden_setup("swe_2d"))
+    assert np.isfinite(Q).all() and Q[1].min() > 0.0
+    assert np.abs(Q[2]).max() > 0.0 and np.abs(Q[3]).max() > 0.0
+
+
+def test_exact_goldens_are_bitwise(oracle):
+    """Where the oracle reproduces the reference bit for bit, keep it that way."""
+    for name in ("ritter_dry", "parity_numpy_n100", "parallel_2rank"):
+        Q, A, _, _, _, _ = oracle.run(*golden_setup(name))
+        g = golden(name)
+        assert np.array_equal(Q, g["Q"]) and np.array_equal(A, g["Qaux"]), name
+
+
+def test_decomposition_free_two_rank_golden(oracle):
+    """test_parallel_two_ranks.py:283-296: 1 rank == 2 ranks bitwise; the
+    2-rank golden is reproduced exactly by the single-box oracle."""
+    Q, A, _, _, _, _ = oracle.run(*golden_setup("parallel_2rank"))
+    g = golden("parallel_2rank")
+    assert np.abs(Q - g["Q"]).max() == 0.0 and np.abs(A - g["Qaux"]).max() == 0.0
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN_CASES))
+def test_oracle_equals_reference_make_rhs(oracle, ref_oracle, name):
+    """The restated make_rhs.H is bitwise the reference's make_rhs.H."""
+    cfg, Q0, A0 = golden_setup(name)
+    a = oracle.run(cfg, Q0, A0)
+    b = ref_oracle.run(cfg, Q0, A0)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]

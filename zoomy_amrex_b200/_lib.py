@@ -1,0 +1,62 @@
+"""Load libzoomyfv.so and declare the C ABI of include/zoomy_fv.h.
+
+There is no CPU fallback: if the library is missing or cannot be loaded the
+import of the solver fails with the reason.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+from ._abi import zfv_config, zfv_status
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "lib" / "libzoomyfv.so"
+
+_lib = None
+
+SYMBOLS = ("zfv_last_error", "zfv_version", "zfv_sizeof_config", "zfv_sizeof_status", "zfv_model_info", "zfv_create", "zfv_destroy",
+           "zfv_scratch_bytes", "zfv_begin", "zfv_update_state", "zfv_compute_dt", "zfv_evolve",
+           "zfv_rhs", "zfv_fill_ghosts", "zfv_total_mass", "zfv_get_status", "zfv_log_capacity",
+           "zfv_read_log")
+
+
+class ZfvError(RuntimeError):
+    pass
+
+
+def lib():
+    """The loaded library (built on first use if the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ZfvError(f"{LIB_PATH} is not built; run `python -m zoomy_amrex_b200.build`")
+    L = C.CDLL(str(LIB_PATH))
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    L.zfv_last_error.restype = C.c_char_p
+    L.zfv_version.restype = C.c_char_p
+    L.zfv_sizeof_config.restype = C.c_size_t
+    L.zfv_sizeof_status.restype = C.c_size_t
+    L.zfv_model_info.argtypes = [i, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+    L.zfv_create.argtypes = [C.POINTER(zfv_config), C.POINTER(vp)]
+    L.zfv_destroy.argtypes = [vp]
+    L.zfv_scratch_bytes.argtypes = [vp]
+    L.zfv_scratch_bytes.restype = C.c_size_t
+    L.zfv_begin.argtypes = [vp, vp, vp, vp, vp]
+    L.zfv_update_state.argtypes = [vp, vp, vp, d, vp]
+    L.zfv_compute_dt.argtypes = [vp, vp, vp, vp, vp]
+    L.zfv_evolve.argtypes = [vp, vp, vp, vp, i, vp]
+    L.zfv_rhs.argtypes = [vp, vp, vp, vp, d, vp]
+    L.zfv_fill_ghosts.argtypes = [vp, vp, vp, vp, vp, d, vp]
+    L.zfv_total_mass.argtypes = [vp, vp, vp, vp]
+    L.zfv_get_status.argtypes = [vp, vp, C.POINTER(zfv_status), vp]
+    L.zfv_log_capacity.argtypes = [vp]
+    L.zfv_read_log.argtypes = [vp, vp, C.POINTER(d), i, C.POINTER(C.c_int64), C.POINTER(i), vp]
+    _lib = L
+    return L
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = lib().zfv_last_error().decode(errors="replace")
+        raise ZfvError(f"{what} failed ({rc}): {msg}")

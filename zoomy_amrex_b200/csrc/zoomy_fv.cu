@@ -1,0 +1,436 @@
+// libzoomyfv.so: the C ABI of include/zoomy_fv.h over the sm_100a kernels.
+//
+// Build (see zoomy_amrex_b200/build.py):
+//   nvcc -gencode arch=compute_100a,code=sm_100a -O3 --fmad=false -std=c++17
+//        -Xcompiler -fPIC -shared ...
+// --fmad=false matches the reference's CUDA build (build.py:33-41) and keeps
+// the FP64 arithmetic bitwise equal to the CPU build of the same expressions.
+#include <cstdio>
+#include <cstring>
+#include <cstdarg>
+#include <new>
+#include <memory>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "zoomy_fv.h"
+#include "swe.H"
+#include "fv_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return 0;
+    return fail(-3, "%s: %s", what, cudaGetErrorString(e));
+}
+
+constexpr size_t kAlign = 256;
+size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+constexpr int kLogCap = 4096;     // per-step log ring buffer entries
+constexpr int kReduceNT = 256;
+constexpr int kReduceBlocksMax = 1184;   // 8 x 148 SMs
+
+// Scratch layout (offsets from the caller's scratch base).
+struct ScratchLayout {
+    size_t state = 0;        // DevState
+    size_t partials = 0;     // 2 doubles per block
+    size_t log = 0;          // 3 doubles per entry
+    size_t stage = 0;        // nq state planes (SSP-RK2 stage / order-1 ping-pong)
+    size_t total = 0;
+};
+
+// Per-model runner: owns the kernel instantiations for one Model/Numerics pair.
+struct Runner {
+    virtual ~Runner() = default;
+    virtual int setup() = 0;
+    virtual int n_blocks_stage() const = 0;
+    virtual int begin(const void* Q, const void* A, char* scratch, cudaStream_t s) = 0;
+    virtual int update_state(void* Q, void* A, double time, cudaStream_t s) = 0;
+    virtual int compute_dt(const void* Q, const void* A, char* scratch, cudaStream_t s) = 0;
+    virtual int total_mass(const void* Q, char* scratch, cudaStream_t s) = 0;
+    virtual int evolve(void* Q, void* A, char* scratch, int n, cudaStream_t s) = 0;
+    virtual int rhs(const void* Q, void* out, double time, cudaStream_t s) = 0;
+    virtual int fill_ghosts(const void* Q, const void* A, void* Qg, void* Ag, double time,
+                            cudaStream_t s) = 0;
+};
+
+}  // namespace
+
+struct zfv_handle {
+    zfv_config cfg;
+    ScratchLayout lay;
+    std::unique_ptr<Runner> run;
+};
+
+namespace {
+
+template <class Model, class Numerics, int TX, int TY>
+struct RunnerT final : Runner {
+    static constexpr int NP = Model::n_parameters;
+    static constexpr int nq = Model::n_dof_q;
+    using PL = zfv::LevelParams<double, NP>;
+
+    zfv_handle* h;
+    PL L;
+    dim3 grid, block;
+
+    explicit RunnerT(zfv_handle* hh) : h(hh) {
+        const zfv_config& c = h->cfg;
+        std::memset(&L, 0, sizeof L);
+        L.nx = c.nx; L.ny = c.ny;
+        L.plane = (long long)c.nx * c.ny;
+        L.dx = (c.prob_hi[0] - c.prob_lo[0]) / c.nx;
+        L.dy = (c.prob_hi[1] - c.prob_lo[1]) / c.ny;
+        L.plox = c.prob_lo[0]; L.ploy = c.prob_lo[1];
+        for (int k = 0; k < NP; ++k) L.p[k] = c.params[k];
+        for (int s = 0; s < 4; ++s) L.bc_tag[s] = c.bc_tag[s];
+        L.clamp = c.clamp_positivity && !c.positivity_mood;   // ZoomyAmr.cpp:303
+        L.well_balanced = c.well_balanced;
+        L.implicit_source = c.implicit_source;
+        L.cfl = c.cfl; L.dtmin = c.dtmin; L.dtmax = c.dtmax; L.time_end = c.time_end;
+        L.max_step = c.max_step;
+        L.cfl_dimension = c.cfl_dimension; L.cfl_degree_factor = c.cfl_degree_factor;
+        grid = dim3((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY, 1);
+        block = dim3(TX * TY, 1, 1);
+    }
+
+    int n_blocks_stage() const override { return int(grid.x * grid.y); }
+
+    template <int ORDER, int MODE, bool WB, bool IMPL>
+    static auto kfn() { return &zfv::k_stage<Model, Numerics, ORDER, MODE, WB, IMPL, TX, TY>; }
+
+    template <int ORDER, int MODE, bool WB, bool IMPL>
+    int set_smem() {
+        using Sh = zfv::TileShape<Model, ORDER, TX, TY>;
+        return cuda_check(cudaFuncSetAttribute(kfn<ORDER, MODE, WB, IMPL>(),
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               int(Sh::smem_bytes)),
+                          "cudaFuncSetAttribute");
+    }
+
+    template <int ORDER, bool WB, bool IMPL>
+    int setup_combo() {
+        int rc = 0;
+        rc |= set_smem<ORDER, zfv::MODE_RHS, WB, IMPL>();
+        if constexpr (ORDER == 2) {
+            rc |= set_smem<ORDER, zfv::MODE_S1, WB, IMPL>();
+            rc |= set_smem<ORDER, zfv::MODE_S2, WB, IMPL>();
+        } else {
+            rc |= set_smem<ORDER, zfv::MODE_ONE, WB, IMPL>();
+        }
+        return rc;
+    }
+
+    // Runtime flags -> compile-time instantiation.
+    template <class F>
+    int with_combo(F&& f) {
+        const zfv_config& c = h->cfg;
+        const bool wb = c.well_balanced != 0, im = c.implicit_source != 0;
+        if (c.spatial_order == 2) {
+            if (wb) return im ? f.template operator()<2, true, true>() : f.template operator()<2, true, false>();
+            return im ? f.template operator()<2, false, true>() : f.template operator()<2, false, false>();
+        }
+        if (wb) return im ? f.template operator()<1, true, true>() : f.template operator()<1, true, false>();
+        return im ? f.template operator()<1, false, true>() : f.template operator()<1, false, false>();
+    }
+
+    struct SetupF {
+        RunnerT* r;
+        template <int O, bool W, bool I> int operator()() { return r->template setup_combo<O, W, I>(); }
+    };
+    int setup() override { return with_combo(SetupF{this}); }
+
+    zfv::DevState* st(char* scratch) const { return reinterpret_cast<zfv::DevState*>(scratch + h->lay.state); }
+    double* partials(char* scratch) const { return reinterpret_cast<double*>(scratch + h->lay.partials); }
+    double* log3(char* scratch) const { return reinterpret_cast<double*>(scratch + h->lay.log); }
+    double* stage(char* scratch) const { return reinterpret_cast<double*>(scratch + h->lay.stage); }
+
+    int reduce_blocks() const {
+        long long need = (L.plane + kReduceNT - 1) / kReduceNT;
+        return int(need < kReduceBlocksMax ? (need > 0 ? need : 1) : kReduceBlocksMax);
+    }
+
+    int begin(const void* Q, const void* A, char* scratch, cudaStream_t s) override {
+        zfv::k_begin<<<1, 1, 0, s>>>(st(scratch), L);
+        zfv::k_reduce<Model, Numerics, kReduceNT, 0, true><<<reduce_blocks(), kReduceNT, 0, s>>>(
+            (const double*)Q, (const double*)A, L, st(scratch), partials(scratch));
+        return cuda_check(cudaGetLastError(), "zfv_begin launch");
+    }
+
+    int update_state(void* Q, void* A, double time, cudaStream_t s) override {
+        const int nb = int((L.plane + 255) / 256);
+        zfv::k_update_state<Model><<<nb, 256, 0, s>>>((double*)Q, (double*)A, L, time);
+        return cuda_check(cudaGetLastError(), "zfv_update_state launch");
+    }
+
+    int compute_dt(const void* Q, const void* A, char* scratch, cudaStream_t s) override {
+        zfv::k_reduce<Model, Numerics, kReduceNT, 0, false><<<reduce_blocks(), kReduceNT, 0, s>>>(
+            (const double*)Q, (const double*)A, L, st(scratch), partials(scratch));
+        return cuda_check(cudaGetLastError(), "zfv_compute_dt launch");
+    }
+
+    int total_mass(const void* Q, char* scratch, cudaStream_t s) override {
+        zfv::k_reduce<Model, Numerics, kReduceNT, 1, false><<<reduce_blocks(), kReduceNT, 0, s>>>(
+            (const double*)Q, nullptr, L, st(scratch), partials(scratch));
+        return cuda_check(cudaGetLastError(), "zfv_total_mass launch");
+    }
+
+    template <int ORDER, int MODE, bool WB, bool IMPL>
+    void launch(const double* qin, const double* qbed, const double* qold, double* qout,
+                char* scratch, cudaStream_t s, double time_arg = 0.0) {
+        using Sh = zfv::TileShape<Model, ORDER, TX, TY>;
+        auto kernel = kfn<ORDER, MODE, WB, IMPL>();
+        kernel<<<grid, block, Sh::smem_bytes, s>>>(
+            qin, qbed, qold, qout, L, scratch ? st(scratch) : nullptr,
+            scratch ? partials(scratch) : nullptr, scratch ? log3(scratch) : nullptr,
+            scratch ? kLogCap : 0, time_arg);
+    }
+
+    struct EvolveF {
+    RunnerT* r; double* Q; double* Q1; char* scratch; int n; cudaStream_t s; bool sbed;
+    template <int O, bool W, bool I> int operator()() {
+        bool in_q1 = false;
+        for (int k = 0; k < n; ++k) {
+            if constexpr (O == 2) {
+                r->template launch<2, zfv::MODE_S1, W, I>(Q, Q, nullptr, Q1, scratch, s);
+                r->template launch<2, zfv::MODE_S2, W, I>(Q1, Q, Q, Q, scratch, s);
+            } else {
+                double* src = in_q1 ? Q1 : Q;
+                double* dst = in_q1 ? Q : Q1;
+                r->template launch<1, zfv::MODE_ONE, W, I>(src, Q, nullptr, dst, scratch, s);
+                in_q1 = !in_q1;
+            }
+        }
+        if (in_q1) {   // order-1 ping-pong ended in the stage buffer: copy the state back
+            const size_t pb = size_t(r->L.plane) * sizeof(double);
+            const int n0 = sbed ? 1 : 0;
+            cudaError_t e = cudaMemcpyAsync(Q + n0 * r->L.plane, Q1 + n0 * r->L.plane,
+                                            pb * (nq - n0), cudaMemcpyDeviceToDevice, s);
+            if (e != cudaSuccess) return cuda_check(e, "zfv_evolve copy-back");
+        }
+        return cuda_check(cudaGetLastError(), "zfv_evolve launch");
+    }
+    };
+
+    int evolve(void* Qv, void* Av, char* scratch, int n, cudaStream_t s) override {
+        double* Q = (double*)Qv;
+        double* Q1 = stage(scratch);
+        const bool sbed = zfv::static_bed<Model>::value;
+        int rc = with_combo(EvolveF{this, Q, Q1, scratch, n, s, sbed});
+        if (rc) return rc;
+        const int nb = int((L.plane + 255) / 256);
+        zfv::k_aux_from_state<Model><<<nb, 256, 0, s>>>(Q, (double*)Av, L, st(scratch));
+        return cuda_check(cudaGetLastError(), "zfv_evolve aux launch");
+    }
+
+    struct RhsF {
+        RunnerT* r; const double* Q; double* out; double time; cudaStream_t s;
+        template <int O, bool W, bool I> int operator()() {
+            r->template launch<O, zfv::MODE_RHS, W, I>(Q, Q, nullptr, out, nullptr, s, time);
+            return cuda_check(cudaGetLastError(), "zfv_rhs launch");
+        }
+    };
+
+    int rhs(const void* Q, void* out, double time, cudaStream_t s) override {
+        return with_combo(RhsF{this, (const double*)Q, (double*)out, time, s});
+    }
+
+    int fill_ghosts(const void* Q, const void* A, void* Qg, void* Ag, double time,
+                    cudaStream_t s) override {
+        const int ng = (h->cfg.spatial_order == 2) ? 2 : 1;
+        const long long gp = (long long)(L.nx + 2 * ng) * (L.ny + 2 * ng);
+        const int nb = int((gp + 255) / 256);
+        zfv::k_fill_ghosts<Model><<<nb, 256, 0, s>>>((const double*)Q, (const double*)A,
+                                                    (double*)Qg, (double*)Ag, L, ng, time);
+        return cuda_check(cudaGetLastError(), "zfv_fill_ghosts launch");
+    }
+};
+
+int model_shape(int model, int* nq, int* na, int* np, int* dim) {
+    switch (model) {
+    case ZFV_MODEL_SWE1D:
+        *nq = zb::SWE<double, 1>::n_dof_q; *na = zb::SWE<double, 1>::n_dof_qaux;
+        *np = zb::SWE<double, 1>::n_parameters; *dim = 1; return 0;
+    case ZFV_MODEL_SWE2D:
+        *nq = zb::SWE<double, 2>::n_dof_q; *na = zb::SWE<double, 2>::n_dof_qaux;
+        *np = zb::SWE<double, 2>::n_parameters; *dim = 2; return 0;
+    default: return -1;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* zfv_last_error(void) { return g_err.c_str(); }
+
+const char* zfv_version(void) { return "zoomyfv 0.1 sm_100a fp64"; }
+
+size_t zfv_sizeof_config(void) { return sizeof(zfv_config); }
+size_t zfv_sizeof_status(void) { return sizeof(zfv_status); }
+
+int zfv_model_info(int model, int* n_q, int* n_aux, int* n_params, int* dimension) {
+    int a, b, c, d;
+    if (model_shape(model, &a, &b, &c, &d) != 0) return fail(-1, "unknown model id %d", model);
+    if (n_q) *n_q = a;
+    if (n_aux) *n_aux = b;
+    if (n_params) *n_params = c;
+    if (dimension) *dimension = d;
+    return 0;
+}
+
+int zfv_create(const zfv_config* cfg, zfv_handle** out) {
+    g_err.clear();
+    if (!cfg || !out) return fail(-1, "zfv_create: null argument");
+    *out = nullptr;
+    int nq, na, np, dim;
+    if (model_shape(cfg->model, &nq, &na, &np, &dim) != 0)
+        return fail(-1, "zfv_create: unknown model id %d", cfg->model);
+    if (cfg->precision != ZFV_PREC_FP64)
+        return fail(-1, "zfv_create: unsupported precision %d", cfg->precision);
+    if (cfg->nx < 1 || cfg->ny < 1) return fail(-1, "zfv_create: bad grid %d x %d", cfg->nx, cfg->ny);
+    if (dim == 1 && cfg->ny != 1) return fail(-1, "zfv_create: 1-D model needs ny == 1 (got %d)", cfg->ny);
+    if ((long long)cfg->nx * cfg->ny > (1LL << 31))
+        return fail(-1, "zfv_create: grid too large for one level (%lld cells)", (long long)cfg->nx * cfg->ny);
+    if (cfg->spatial_order != 1 && cfg->spatial_order != 2)
+        return fail(-1, "zfv_create: spatial_order must be 1 or 2 (got %d)", cfg->spatial_order);
+    {
+        // Every ghost layer must mirror onto a valid cell (ZoomyAmr.cpp:399-406);
+        // with fewer cells than ghost layers the reference mirrors a ghost onto
+        // another ghost, which has no defined value.
+        const int ng = (cfg->spatial_order == 2) ? 2 : 1;
+        if (cfg->nx < ng || (dim == 2 && cfg->ny < ng))
+            return fail(-1, "zfv_create: order %d needs at least %d cells per direction (grid %d x %d)",
+                        cfg->spatial_order, ng, cfg->nx, cfg->ny);
+    }
+    if (cfg->positivity_mood && cfg->spatial_order == 2)
+        return fail(-2, "zfv_create: positivity = mood is not implemented in this build");
+    if (cfg->n_params != np)
+        return fail(-1, "zfv_create: model takes %d parameters, config has %d", np, cfg->n_params);
+    if (!(cfg->prob_hi[0] > cfg->prob_lo[0]) || !(cfg->prob_hi[1] > cfg->prob_lo[1]))
+        return fail(-1, "zfv_create: empty domain");
+    if (cfg->cfl_dimension < 1 || cfg->cfl_degree_factor < 1)
+        return fail(-1, "zfv_create: march constants must be >= 1");
+    for (int s = 0; s < 4; ++s)
+        if (cfg->bc_tag[s] < 0 || cfg->bc_tag[s] >= 2)
+            return fail(-1, "zfv_create: bc tag %d on side %d is not declared by the model", cfg->bc_tag[s], s);
+
+    zfv_handle* h = new (std::nothrow) zfv_handle();
+    if (!h) return fail(-4, "zfv_create: out of host memory");
+    h->cfg = *cfg;
+    switch (cfg->model) {
+    case ZFV_MODEL_SWE1D:
+        h->run.reset(new RunnerT<zb::SWE<double, 1>, zb::SWENumerics<double, 1>, 128, 1>(h)); break;
+    case ZFV_MODEL_SWE2D:
+        h->run.reset(new RunnerT<zb::SWE<double, 2>, zb::SWENumerics<double, 2>, 32, 8>(h)); break;
+    }
+    const size_t plane_bytes = size_t(cfg->nx) * cfg->ny * sizeof(double);
+    const int nblk = std::max(h->run->n_blocks_stage(), kReduceBlocksMax);
+    ScratchLayout& L = h->lay;
+    L.state = 0;
+    L.partials = align_up(sizeof(zfv::DevState));
+    L.log = L.partials + align_up(sizeof(double) * 2 * nblk);
+    L.stage = L.log + align_up(sizeof(double) * 3 * kLogCap);
+    L.total = L.stage + align_up(plane_bytes * nq);
+    int rc = h->run->setup();
+    if (rc) { delete h; return rc; }
+    *out = h;
+    return 0;
+}
+
+int zfv_destroy(zfv_handle* h) {
+    delete h;
+    return 0;
+}
+
+size_t zfv_scratch_bytes(const zfv_handle* h) { return h ? h->lay.total : 0; }
+
+int zfv_begin(zfv_handle* h, const void* Q, const void* aux, void* scratch, void* stream) {
+    if (!h || !Q || !aux || !scratch) return fail(-1, "zfv_begin: null argument");
+    return h->run->begin(Q, aux, (char*)scratch, (cudaStream_t)stream);
+}
+
+int zfv_update_state(zfv_handle* h, void* Q, void* aux, double time, void* stream) {
+    if (!h || !Q || !aux) return fail(-1, "zfv_update_state: null argument");
+    return h->run->update_state(Q, aux, time, (cudaStream_t)stream);
+}
+
+int zfv_compute_dt(zfv_handle* h, const void* Q, const void* aux, void* scratch, void* stream) {
+    if (!h || !Q || !aux || !scratch) return fail(-1, "zfv_compute_dt: null argument");
+    return h->run->compute_dt(Q, aux, (char*)scratch, (cudaStream_t)stream);
+}
+
+int zfv_evolve(zfv_handle* h, void* Q, void* aux, void* scratch, int n_steps, void* stream) {
+    if (!h || !Q || !aux || !scratch) return fail(-1, "zfv_evolve: null argument");
+    if (n_steps < 0) return fail(-1, "zfv_evolve: negative step count");
+    return h->run->evolve(Q, aux, (char*)scratch, n_steps, (cudaStream_t)stream);
+}
+
+int zfv_rhs(zfv_handle* h, const void* Q, const void* aux, void* rhs, double time, void* stream) {
+    if (!h || !Q || !rhs) return fail(-1, "zfv_rhs: null argument");
+    (void)aux;
+    return h->run->rhs(Q, rhs, time, (cudaStream_t)stream);
+}
+
+int zfv_fill_ghosts(zfv_handle* h, const void* Q, const void* aux, void* Qg, void* auxg,
+                    double time, void* stream) {
+    if (!h || !Q || !aux || !Qg || !auxg) return fail(-1, "zfv_fill_ghosts: null argument");
+    return h->run->fill_ghosts(Q, aux, Qg, auxg, time, (cudaStream_t)stream);
+}
+
+int zfv_total_mass(zfv_handle* h, const void* Q, void* scratch, void* stream) {
+    if (!h || !Q || !scratch) return fail(-1, "zfv_total_mass: null argument");
+    return h->run->total_mass(Q, (char*)scratch, (cudaStream_t)stream);
+}
+
+int zfv_get_status(zfv_handle* h, const void* scratch, zfv_status* out, void* stream) {
+    if (!h || !scratch || !out) return fail(-1, "zfv_get_status: null argument");
+    static_assert(sizeof(zfv_status) == 64, "zfv_status is 64 bytes");
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = cuda_check(cudaMemcpyAsync(out, (const char*)scratch + h->lay.state, sizeof(zfv_status),
+                                        cudaMemcpyDeviceToHost, s), "zfv_get_status copy");
+    if (rc) return rc;
+    return cuda_check(cudaStreamSynchronize(s), "zfv_get_status sync");
+}
+
+int zfv_log_capacity(const zfv_handle* h) { return h ? kLogCap : 0; }
+
+int zfv_read_log(zfv_handle* h, const void* scratch, double* out3, int max_entries,
+                 int64_t* first_step, int* n_out, void* stream) {
+    if (!h || !scratch || !out3 || !first_step || !n_out) return fail(-1, "zfv_read_log: null argument");
+    zfv_status stt;
+    int rc = zfv_get_status(h, scratch, &stt, stream);
+    if (rc) return rc;
+    const long long steps = stt.step;
+    const long long avail = steps < kLogCap ? steps : kLogCap;
+    const long long n = avail < max_entries ? avail : max_entries;
+    const long long first = steps - n;   // 0-based index of the first returned step
+    static thread_local double ring[3 * kLogCap];
+    rc = cuda_check(cudaMemcpyAsync(ring, (const char*)scratch + h->lay.log, sizeof(double) * 3 * kLogCap,
+                                    cudaMemcpyDeviceToHost, (cudaStream_t)stream), "zfv_read_log copy");
+    if (rc) return rc;
+    rc = cuda_check(cudaStreamSynchronize((cudaStream_t)stream), "zfv_read_log sync");
+    if (rc) return rc;
+    for (long long k = 0; k < n; ++k) {
+        const long long s = first + k;
+        std::memcpy(out3 + 3 * k, ring + 3 * (s % kLogCap), 3 * sizeof(double));
+    }
+    *first_step = first + 1;
+    *n_out = int(n);
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,174 @@
+"""One refinement level on one B200: PyTorch tensors + a libzoomyfv handle.
+
+This is the in-process replacement for the part of the reference's AMReX
+executable that a zoomy_amrex run spends its time in: the level data
+(Q, Qaux: ZoomyAmr.H:81-84) live in HBM as component-major torch tensors, and
+each call enqueues SSP-RK2 steps whose dt, time and stop test stay on the
+device (ZoomyAmr::Evolve's loop, ZoomyAmr.cpp:782-810). The host reads the run
+status only when asked.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._abi import MODELS, zfv_config, zfv_status
+
+_DTYPE = torch.float64
+
+
+def _ptr(t: torch.Tensor) -> int:
+    return t.data_ptr()
+
+
+class Level:
+    """A single-level solver state on ``device``.
+
+    Q:   (n_q, ny, nx) float64, rows [b, h, hu, (hv)]
+    aux: (n_aux, ny, nx) float64, last row hinv
+    """
+
+    def __init__(self, cfg: zfv_config, Q0, aux0, device: str | torch.device = "cuda:0",
+                 stream: torch.cuda.Stream | None = None):
+        if not torch.cuda.is_available():
+            raise _lib.ZfvError("zoomy_amrex_b200 needs a CUDA device (no CPU fallback)")
+        self.cfg = cfg
+        self.info = MODELS[cfg.model]
+        self.device = torch.device(device)
+        L = _lib.lib()
+        h = C.c_void_p()
+        _lib.check(L.zfv_create(C.byref(cfg), C.byref(h)), "zfv_create")
+        self._h = h
+        nq, na = self.info["n_q"], self.info["n_aux"]
+        shape_q, shape_a = (nq, cfg.ny, cfg.nx), (na, cfg.ny, cfg.nx)
+        self.Q = self._as_tensor(Q0, shape_q)
+        self.aux = self._as_tensor(aux0, shape_a)
+        nbytes = int(L.zfv_scratch_bytes(h))
+        self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        self.stream = stream if stream is not None else torch.cuda.current_stream(self.device)
+        self._graph = None
+        self._graph_steps = 0
+
+    def _as_tensor(self, a, shape):
+        t = torch.as_tensor(np.asarray(a) if not torch.is_tensor(a) else a)
+        t = t.to(device=self.device, dtype=_DTYPE).reshape(shape).contiguous().clone()
+        return t
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _s(self):
+        return C.c_void_p(self.stream.cuda_stream)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._graph = None
+            _lib.lib().zfv_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- the reference's driver entry points -------------------------------------
+    def begin(self):
+        """Reset time/step and compute the first dt from (Q, aux) as stored."""
+        _lib.check(_lib.lib().zfv_begin(self._h, _ptr(self.Q), _ptr(self.aux), _ptr(self.scratch),
+                                        self._s()), "zfv_begin")
+
+    def evolve(self, n_steps: int):
+        """Enqueue up to n_steps time steps (no host synchronization)."""
+        _lib.check(_lib.lib().zfv_evolve(self._h, _ptr(self.Q), _ptr(self.aux), _ptr(self.scratch),
+                                         int(n_steps), self._s()), "zfv_evolve")
+
+    def capture(self, n_steps: int):
+        """Capture `evolve(n_steps)` into a CUDA graph for replay()."""
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(self.stream):
+            with torch.cuda.graph(g, stream=self.stream):
+                _lib.check(_lib.lib().zfv_evolve(self._h, _ptr(self.Q), _ptr(self.aux),
+                                                 _ptr(self.scratch), int(n_steps),
+                                                 C.c_void_p(torch.cuda.current_stream().cuda_stream)),
+                           "zfv_evolve (capture)")
+        self._graph, self._graph_steps = g, int(n_steps)
+        return g
+
+    def replay(self):
+        if self._graph is None:
+            raise RuntimeError("capture() first")
+        with torch.cuda.stream(self.stream):
+            self._graph.replay()
+
+    def status(self) -> dict:
+        st = zfv_status()
+        _lib.check(_lib.lib().zfv_get_status(self._h, _ptr(self.scratch), C.byref(st), self._s()),
+                   "zfv_get_status")
+        return dict(time=st.time, dt=st.dt, mass=st.mass, max_inv=st.max_inv, step=int(st.step),
+                    flags=int(st.flags), done=bool(st.flags & 4), mood_redos=int(st.mood_redos))
+
+    def run(self, max_steps: int | None = None, chunk: int = 64, use_graph: bool = False) -> dict:
+        """Evolve until time_end / max_step (or max_steps), syncing once per chunk."""
+        self.begin()
+        done_steps = 0
+        while True:
+            n = chunk if max_steps is None else min(chunk, max_steps - done_steps)
+            if n <= 0:
+                break
+            if use_graph:
+                if self._graph is None or self._graph_steps != n:
+                    self.capture(n)
+                self.replay()
+            else:
+                self.evolve(n)
+            done_steps += n
+            st = self.status()
+            if st["done"]:
+                break
+        return self.status()
+
+    def log(self) -> np.ndarray:
+        """(steps, 3) array of (dt, time, mass) per completed step (last 4096 kept)."""
+        L = _lib.lib()
+        cap = int(L.zfv_log_capacity(self._h))
+        out = (C.c_double * (3 * cap))()
+        first = C.c_int64(0); n = C.c_int(0)
+        _lib.check(L.zfv_read_log(self._h, _ptr(self.scratch), out, cap, C.byref(first), C.byref(n),
+                                  self._s()), "zfv_read_log")
+        return np.frombuffer(out, dtype=np.float64, count=3 * n.value).reshape(n.value, 3).copy()
+
+    # -- validation entries -------------------------------------------------------
+    def rhs(self, time: float = 0.0) -> torch.Tensor:
+        out = torch.empty_like(self.Q)
+        _lib.check(_lib.lib().zfv_rhs(self._h, _ptr(self.Q), _ptr(self.aux), _ptr(out), float(time),
+                                      self._s()), "zfv_rhs")
+        return out
+
+    def fill_ghosts(self, time: float = 0.0):
+        ng = 2 if self.cfg.spatial_order == 2 else 1
+        nq, na = self.info["n_q"], self.info["n_aux"]
+        Qg = torch.empty((nq, self.cfg.ny + 2 * ng, self.cfg.nx + 2 * ng), dtype=_DTYPE, device=self.device)
+        Ag = torch.empty((na, self.cfg.ny + 2 * ng, self.cfg.nx + 2 * ng), dtype=_DTYPE, device=self.device)
+        _lib.check(_lib.lib().zfv_fill_ghosts(self._h, _ptr(self.Q), _ptr(self.aux), _ptr(Qg), _ptr(Ag),
+                                              float(time), self._s()), "zfv_fill_ghosts")
+        return Qg, Ag
+
+    def update_state(self, time: float = 0.0):
+        _lib.check(_lib.lib().zfv_update_state(self._h, _ptr(self.Q), _ptr(self.aux), float(time),
+                                               self._s()), "zfv_update_state")
+
+    def compute_dt(self) -> tuple[float, float]:
+        _lib.check(_lib.lib().zfv_compute_dt(self._h, _ptr(self.Q), _ptr(self.aux), _ptr(self.scratch),
+                                             self._s()), "zfv_compute_dt")
+        st = self.status()
+        return st["dt"], st["max_inv"]
+
+    def total_mass(self) -> float:
+        _lib.check(_lib.lib().zfv_total_mass(self._h, _ptr(self.Q), _ptr(self.scratch), self._s()),
+                   "zfv_total_mass")
+        return self.status()["mass"]
