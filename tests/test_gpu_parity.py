@@ -89,7 +89,7 @@ CASES_2D = {
                                       parameters={"n_m": 0.05}),
                                   dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[33, 17],
                                        spatial_order=2, cfl=0.9, time_end=1e30, max_step=30,
-                                       well_balanced=True, implicit_source=False)),
+                                       well_balanced=True, implicit_source=True)),
     "wetdry_o1_impl": (SWE(2, "wall", wetdry_ic(7, moving=True), parameters={"n_m": 0.03}),
                        dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[37, 29], spatial_order=1,
                             cfl=0.9, time_end=1e30, max_step=25, well_balanced=True,
@@ -136,6 +136,19 @@ def test_2d_cases_bitwise_vs_oracle(cuda, oracle, name):
 @pytest.mark.parametrize("name", sorted(CASES_1D))
 def test_1d_cases_bitwise_vs_oracle(cuda, oracle, name):
     assert_same_run(*setup(*CASES_1D[name]), oracle)
+
+
+def test_explicit_friction_blow_up_is_reproduced(cuda, oracle):
+    """Explicit Manning friction on thin films is unstable (make_rhs.H:411-416
+    explains why the reference moved to the point-implicit source); the GPU
+    must follow the oracle through the blow-up value for value, NaNs included."""
+    model, s = CASES_2D["wetdry_moving_o2_mixed_bc"]
+    cfg, Q0, A0 = setup(model, dict(s, implicit_source=False, max_step=12))
+    Qo, Ao, n, t, _, _ = oracle.run(cfg, Q0, A0)
+    Qg, Ag, st, _ = run_gpu(cfg, Q0, A0)
+    assert np.isnan(Qo).any() and st["step"] == n
+    assert np.array_equal(np.isnan(Qg), np.isnan(Qo))
+    assert np.array_equal(Qg, Qo, equal_nan=True)
 
 
 def test_graph_replay_is_bitwise_eager(cuda, oracle):

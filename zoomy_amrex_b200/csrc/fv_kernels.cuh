@@ -31,16 +31,22 @@ enum StageMode : int {
     MODE_ONE = 3    // order 1: single stage + final UpdateState + reduction
 };
 
-template <class Model, int ORDER, int TX, int TY>
+// Face records in shared memory hold make_rhs.H:310-315's components
+// (flux, D+, D-, h*_L, h*_R) for the rows the step evolves: with a static bed
+// (and outside the RHS validation mode) the bed row is skipped.
+template <class Model, int ORDER, int TX, int TY, bool SKIPB>
 struct TileShape {
     static constexpr int dim = Model::dimension;
     static constexpr int nq = Model::n_dof_q;
+    static constexpr int n0 = SKIPB ? 1 : 0;               // first evolved row
+    static constexpr int NQE = nq - n0;
     static constexpr int G = (ORDER == 2) ? 2 : 1;        // ZoomyAmr.H:152 nghost()
     static constexpr int GY = (dim == 2) ? G : 0;
     static constexpr int RW = TX + 2 * G;
     static constexpr int RH = TY + 2 * GY;
-    static constexpr int NFC = 3 * nq + 2;                 // make_rhs.H:315 n_face_comp
+    static constexpr int NFC = 3 * NQE + 2;                // make_rhs.H:315 n_face_comp
     static constexpr int NT = TX * TY;
+    static constexpr int min_blocks = (dim == 2) ? 3 : 2;
     static constexpr size_t q_elems = size_t(nq) * RH * RW;
     static constexpr size_t fx_elems = size_t(TY) * (TX + 1) * NFC;
     static constexpr size_t fy_elems = (dim == 2) ? size_t(TY + 1) * TX * NFC : 0;
@@ -125,19 +131,19 @@ __device__ __forceinline__ void finish_step(double m, double s, double* red, dou
 }
 
 template <class Model, class Numerics, int ORDER, int MODE, bool WB, bool IMPL, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY)
+__global__ void __launch_bounds__(TX * TY, (Model::dimension == 2) ? 3 : 2)
 k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
         const double* __restrict__ qold, double* __restrict__ qout,
         LevelParams<double, Model::n_parameters> L, DevState* st,
         double* __restrict__ partials, double* __restrict__ log3, int log_cap, double time_arg)
 {
-    using Sh = TileShape<Model, ORDER, TX, TY>;
+    constexpr bool sbed = static_bed<Model>::value;
+    using Sh = TileShape<Model, ORDER, TX, TY, sbed && MODE != MODE_RHS>;
     using T = ModelTypes<Model>;
     using R = double;
-    constexpr int nq = Sh::nq, dim = Sh::dim;
+    constexpr int nq = Sh::nq, dim = Sh::dim, n0 = Sh::n0, NQE = Sh::NQE;
     constexpr int G = Sh::G, GY = Sh::GY, RW = Sh::RW, RH = Sh::RH, NFC = Sh::NFC, NT = Sh::NT;
     constexpr bool pure = aux_pure<Model>::value;
-    constexpr bool sbed = static_bed<Model>::value;
     static_assert(pure, "the fused stage kernel needs Model::zb_aux_pure");
 
     extern __shared__ __align__(16) double smem[];
@@ -238,11 +244,13 @@ k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
     };
     auto store_face = [&](double* F, typename T::VQ const& fl, typename T::V2Q const& fc, R hl, R hr) {
 #pragma unroll
-        for (int n = 0; n < nq; ++n) F[n] = fl(n, 0);
-#pragma unroll
-        for (int n = 0; n < 2 * nq; ++n) F[nq + n] = fc(n, 0);
-        F[3 * nq] = hl;
-        F[3 * nq + 1] = hr;
+        for (int n = n0; n < nq; ++n) {
+            F[n - n0] = fl(n, 0);                 // flux
+            F[NQE + n - n0] = fc(n, 0);           // D+
+            F[2 * NQE + n - n0] = fc(nq + n, 0);  // D-
+        }
+        F[3 * NQE] = hl;
+        F[3 * NQE + 1] = hr;
     };
     // x-face f sits between cells f-1 and f of row jj (local row ly)
     auto x_face = [&](int f, int jj, int ly, double* F) {
@@ -299,19 +307,21 @@ k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
         for (int n = 0; n < nq; ++n) S(n, 0) = R(0.0);
         if constexpr (!IMPL) S = Model::source(qc, ac, p, time, X);
         typename T::VQ rhs;
+        if constexpr (n0 == 1) rhs(0, 0) = R(0.0);   // static bed: never used
 #pragma unroll
-        for (int n = 0; n < nq; ++n) {
-            const R Fx = -(FxR[n] - FxL[n]) - FxR[2 * nq + n] - FxL[nq + n];
+        for (int n = n0; n < nq; ++n) {
+            const int k = n - n0;
+            const R Fx = -(FxR[k] - FxL[k]) - FxR[2 * NQE + k] - FxL[NQE + k];
             R Fy = R(0.0);
-            if constexpr (dim == 2) Fy = -(FyR[n] - FyL[n]) - FyR[2 * nq + n] - FyL[nq + n];
+            if constexpr (dim == 2) Fy = -(FyR[k] - FyL[k]) - FyR[2 * NQE + k] - FyL[NQE + k];
             rhs(n, 0) = Fx / L.dx + Fy / L.dy;
             if constexpr (!IMPL) rhs(n, 0) += S(n, 0);
         }
         if constexpr (WB) {
             const R g = p(0, 0);
-            rhs(kIdxH + 1, 0) += R(0.5) * g * (FxR[3 * nq] * FxR[3 * nq] - FxL[3 * nq + 1] * FxL[3 * nq + 1]) / L.dx;
+            rhs(kIdxH + 1, 0) += R(0.5) * g * (FxR[3 * NQE] * FxR[3 * NQE] - FxL[3 * NQE + 1] * FxL[3 * NQE + 1]) / L.dx;
             if constexpr (dim == 2)
-                rhs(kIdxH + 2, 0) += R(0.5) * g * (FyR[3 * nq] * FyR[3 * nq] - FyL[3 * nq + 1] * FyL[3 * nq + 1]) / L.dy;
+                rhs(kIdxH + 2, 0) += R(0.5) * g * (FyR[3 * NQE] * FyR[3 * NQE] - FyL[3 * NQE + 1] * FyL[3 * NQE + 1]) / L.dy;
         }
         const long long c = (long long)j * nx + i;
         if constexpr (MODE == MODE_RHS) {

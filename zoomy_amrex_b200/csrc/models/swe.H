@@ -27,7 +27,8 @@
 // neither fluxed nor dissipated (b is constant in time); the bed
 // non-conservative product uses the exact integral of g h along the straight
 // path, g (hL + hR)/2 (bR - bL); Manning friction is
-// S = -g n^2 u |u| / max(h, h_floor)^(1/3) with u = hu * hinv.
+// S = -g n^2 u |u| max(h, h_floor)^(-1/3) with u = hu * hinv, the power taken
+// by zb::inv_cbrt_pos so that it is bitwise the same on CPU and GPU.
 #pragma once
 #include <vector>
 #include <string>
@@ -122,7 +123,7 @@ struct SWE
         return J;   // the printer emits all zeros here (to_amrex.py:475-480)
     }
 
-    // Friction factor c = g n^2 |u| / max(h, h_floor)^(1/3), so S_m = -c * u_m.
+    // Friction factor k = g n^2 max(h, h_floor)^(-1/3); S_m = -k u_m |u|.
     static PORTABLE_FN AMREX_FORCE_INLINE R speed(VQ const& Q, R hinv) {
         R ux = Q(2, 0) * hinv;
         if constexpr (DIM == 2) {
@@ -139,7 +140,7 @@ struct SWE
         const R g = p(swe_g, 0), nm = p(swe_n_m, 0);
         const R hinv = Qaux(i_hinv, 0);
         const R m = amrex::max(Q(1, 0), p(swe_h_floor, 0));
-        const R k = g * nm * nm / cbrt_pos(m);
+        const R k = g * nm * nm * inv_cbrt_pos(m);
         const R sp = speed(Q, hinv);
         S(2, 0) = g * p(swe_ex, 0) * Q(1, 0) - k * (Q(2, 0) * hinv) * sp;
         if constexpr (DIM == 2)
@@ -157,11 +158,11 @@ struct SWE
         const R h = Q(1, 0);
         const R hf = p(swe_h_floor, 0);
         const R m = amrex::max(h, hf);
-        const R cr = cbrt_pos(m);
-        const R k = g * nm * nm / cr;
-        // d/dh of m^(-1/3) = -(1/3) m^(-4/3) * Heaviside(h - h_floor, 1/2)
+        const R ic = inv_cbrt_pos(m);
+        const R k = g * nm * nm * ic;
+        // d/dh of m^(-1/3) = -(1/3) m^(-4/3) * Heaviside(h - h_floor, 1/2), m^(-1) = ic^3
         const R heav = (h - hf > R(0)) ? R(1) : ((h - hf < R(0)) ? R(0) : R(0.5));
-        const R dk_dh = -g * nm * nm / (R(3) * m * cr) * heav;
+        const R dk_dh = -k * (ic * ic * ic) * R(1.0 / 3.0) * heav;
         const R sp = speed(Q, hinv);
         const R ux = Q(2, 0) * hinv;
         if constexpr (DIM == 1) {
@@ -171,8 +172,9 @@ struct SWE
         } else {
             const R uy = Q(3, 0) * hinv;
             // d|u|/dhu = ux hinv / |u|, d|u|/dhv = uy hinv / |u| (0 at rest)
-            const R dsp_x = (sp > R(0)) ? ux * hinv / sp : R(0);
-            const R dsp_y = (sp > R(0)) ? uy * hinv / sp : R(0);
+            const R rsp = (sp > R(0)) ? R(1) / sp : R(0);
+            const R dsp_x = ux * hinv * rsp;
+            const R dsp_y = uy * hinv * rsp;
             J(2 * n + 1, 0) = g * p(swe_ex, 0) - dk_dh * ux * sp;
             J(2 * n + 2, 0) = -k * (hinv * sp + ux * dsp_x);
             J(2 * n + 3, 0) = -k * (ux * dsp_y);
@@ -191,7 +193,7 @@ struct SWE
         const R g = p(swe_g, 0), nm = p(swe_n_m, 0);
         const R hinv = Qaux(i_hinv, 0);
         const R m = amrex::max(Q(1, 0), p(swe_h_floor, 0));
-        const R k = g * nm * nm / cbrt_pos(m);
+        const R k = g * nm * nm * inv_cbrt_pos(m);
         const R sp = speed(Q, hinv);
         // S_m = -k q_m hinv |u| with |u| = |hinv| |q|, so dS_m/dhinv = -2 k q_m |u|
         J(2 * na + i_hinv, 0) = -k * R(2) * Q(2, 0) * sp;

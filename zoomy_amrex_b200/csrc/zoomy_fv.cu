@@ -112,9 +112,12 @@ struct RunnerT final : Runner {
     template <int ORDER, int MODE, bool WB, bool IMPL>
     static auto kfn() { return &zfv::k_stage<Model, Numerics, ORDER, MODE, WB, IMPL, TX, TY>; }
 
+    template <int ORDER, int MODE>
+    using ShapeOf = zfv::TileShape<Model, ORDER, TX, TY, zfv::static_bed<Model>::value && MODE != zfv::MODE_RHS>;
+
     template <int ORDER, int MODE, bool WB, bool IMPL>
     int set_smem() {
-        using Sh = zfv::TileShape<Model, ORDER, TX, TY>;
+        using Sh = ShapeOf<ORDER, MODE>;
         return cuda_check(cudaFuncSetAttribute(kfn<ORDER, MODE, WB, IMPL>(),
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                int(Sh::smem_bytes)),
@@ -191,7 +194,7 @@ struct RunnerT final : Runner {
     template <int ORDER, int MODE, bool WB, bool IMPL>
     void launch(const double* qin, const double* qbed, const double* qold, double* qout,
                 char* scratch, cudaStream_t s, double time_arg = 0.0) {
-        using Sh = zfv::TileShape<Model, ORDER, TX, TY>;
+        using Sh = ShapeOf<ORDER, MODE>;
         auto kernel = kfn<ORDER, MODE, WB, IMPL>();
         kernel<<<grid, block, Sh::smem_bytes, s>>>(
             qin, qbed, qold, qout, L, scratch ? st(scratch) : nullptr,

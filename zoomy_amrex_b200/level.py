@@ -48,7 +48,9 @@ class Level:
         self.aux = self._as_tensor(aux0, shape_a)
         nbytes = int(L.zfv_scratch_bytes(h))
         self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
-        self.stream = stream if stream is not None else torch.cuda.current_stream(self.device)
+        # A dedicated stream: CUDA graphs cannot be captured on the default stream.
+        self.stream = stream if stream is not None else torch.cuda.Stream(self.device)
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
         self._graph = None
         self._graph_steps = 0
 
@@ -90,6 +92,7 @@ class Level:
     def capture(self, n_steps: int):
         """Capture `evolve(n_steps)` into a CUDA graph for replay()."""
         g = torch.cuda.CUDAGraph()
+        self.stream.synchronize()
         with torch.cuda.stream(self.stream):
             with torch.cuda.graph(g, stream=self.stream):
                 _lib.check(_lib.lib().zfv_evolve(self._h, _ptr(self.Q), _ptr(self.aux),
@@ -143,8 +146,13 @@ class Level:
         return np.frombuffer(out, dtype=np.float64, count=3 * n.value).reshape(n.value, 3).copy()
 
     # -- validation entries -------------------------------------------------------
+    def sync(self):
+        """Wait for this level's stream (host reads of Q/aux need it)."""
+        self.stream.synchronize()
+
     def rhs(self, time: float = 0.0) -> torch.Tensor:
         out = torch.empty_like(self.Q)
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
         _lib.check(_lib.lib().zfv_rhs(self._h, _ptr(self.Q), _ptr(self.aux), _ptr(out), float(time),
                                       self._s()), "zfv_rhs")
         return out
@@ -154,6 +162,7 @@ class Level:
         nq, na = self.info["n_q"], self.info["n_aux"]
         Qg = torch.empty((nq, self.cfg.ny + 2 * ng, self.cfg.nx + 2 * ng), dtype=_DTYPE, device=self.device)
         Ag = torch.empty((na, self.cfg.ny + 2 * ng, self.cfg.nx + 2 * ng), dtype=_DTYPE, device=self.device)
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
         _lib.check(_lib.lib().zfv_fill_ghosts(self._h, _ptr(self.Q), _ptr(self.aux), _ptr(Qg), _ptr(Ag),
                                               float(time), self._s()), "zfv_fill_ghosts")
         return Qg, Ag
