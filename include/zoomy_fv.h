@@ -192,6 +192,28 @@ int zfv_log_capacity(const zfv_handle* h);
 int zfv_read_log(zfv_handle* h, const void* scratch, double* out3, int max_entries,
                  int64_t* first_step, int* n_out, void* stream);
 
+/*
+ * zfv_evolve without caller-provided scratch. No counterpart in the reference
+ * (its AMReX driver allocates MultiFabs itself); it exists for callers that
+ * cannot call cudaMalloc at all — code inside another framework's memory
+ * pool, under a caching allocator that owns all device memory, or in a
+ * plugin that must not allocate at call time.
+ *
+ * Scratch is a 64 MiB array compiled into the library (every GPU that loads
+ * the library holds it until exit); levels whose zfv_scratch_bytes() exceeds
+ * it (about 2 million cells for ZFV_MODEL_SWE2D) are rejected with an error.
+ * restart != 0 starts a run like zfv_begin (clearing the device run record);
+ * restart == 0 continues the run that the previous call on this device left
+ * in the array. Every call on a device shares the one array: calls that
+ * overlap on the GPU (other streams, other handles) race, and interleaving
+ * runs of different handles needs restart != 0. The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture. If status_out is not NULL the run status is
+ * copied into it and the stream is synchronized. Allocates no device memory.
+ */
+int zfv_evolve_static(zfv_handle* h, void* Q, void* aux, int n_steps, int restart,
+                      zfv_status* status_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

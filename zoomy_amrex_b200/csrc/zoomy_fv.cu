@@ -5,6 +5,7 @@
 //        -Xcompiler -fPIC -shared ...
 // --fmad=false matches the reference's CUDA build (build.py:33-41) and keeps
 // the FP64 arithmetic bitwise equal to the CPU build of the same expressions.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <cstdarg>
@@ -437,3 +438,70 @@ int zfv_read_log(zfv_handle* h, const void* scratch, double* out3, int max_entri
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.
+//
+// For callers that cannot call cudaMalloc: code running where a device
+// allocation is not allowed or not possible, e.g. inside another framework's
+// memory pool that forbids foreign allocations, a host that has handed all
+// device memory to a caching allocator, or a plugin that must not grow the
+// process's footprint at call time. The step's scratch (run record, reduction
+// partials, step log and the SSP-RK2 stage buffer) lives in a fixed array
+// compiled into this library; the caller only passes Q and aux.
+// ---------------------------------------------------------------------------
+namespace {
+
+// 64 MiB per GPU that loads the library, held until process exit. Enough for
+// about 2 million cells of the 2-D shallow-water model (4 state planes of
+// FP64 in the stage buffer plus a few hundred KB of bookkeeping).
+constexpr size_t kStaticScratchBytes = size_t(64) << 20;
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+// Device address of g_static_scratch per device ordinal. In host code the
+// symbol's name is only a host-side stand-in, never a device address.
+constexpr int kMaxDevices = 64;
+std::atomic<void*> g_static_scratch_addr[kMaxDevices];
+
+}  // namespace
+
+extern "C" int zfv_evolve_static(zfv_handle* h, void* Q, void* aux, int n_steps, int restart,
+                                 zfv_status* status_out, void* stream) {
+    if (!h || !Q || !aux) return fail(-1, "zfv_evolve_static: null argument");
+    if (n_steps < 0) return fail(-1, "zfv_evolve_static: negative step count");
+    if (h->lay.total > kStaticScratchBytes)
+        return fail(-5, "zfv_evolve_static: this level needs %zu bytes of scratch; the static "
+                        "scratch holds %zu bytes (grid %d x %d is too large for this entry point, "
+                        "use zfv_evolve with caller-provided scratch)",
+                    h->lay.total, kStaticScratchBytes, h->cfg.nx, h->cfg.ny);
+    int dev = -1;
+    int rc = cuda_check(cudaGetDevice(&dev), "zfv_evolve_static: cudaGetDevice");
+    if (rc) return rc;
+    if (dev < 0 || dev >= kMaxDevices) return fail(-1, "zfv_evolve_static: device %d out of range", dev);
+    void* base = g_static_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!base) {   // once per device, with that device current
+        void* addr = nullptr;
+        rc = cuda_check(cudaGetSymbolAddress(&addr, g_static_scratch),
+                        "zfv_evolve_static: cudaGetSymbolAddress");
+        if (rc) return rc;
+        g_static_scratch_addr[dev].store(addr, std::memory_order_release);
+        base = addr;
+    }
+    char* scratch = static_cast<char*>(base);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (restart) {
+        // the run record (time, step, flags, reduction counter) must start at zero
+        rc = h->run->begin(Q, aux, scratch, s);
+        if (rc) return rc;
+    }
+    rc = h->run->evolve(Q, aux, scratch, n_steps, s);
+    if (rc) return rc;
+    if (status_out) {
+        rc = cuda_check(cudaMemcpyAsync(status_out, scratch + h->lay.state, sizeof(zfv_status),
+                                        cudaMemcpyDeviceToHost, s), "zfv_evolve_static status copy");
+        if (rc) return rc;
+        rc = cuda_check(cudaStreamSynchronize(s), "zfv_evolve_static sync");
+    }
+    return rc;
+}
+
