@@ -33,14 +33,17 @@ SEED = 2026
 N_DEFAULT = 4096
 DOMAIN = 100.0
 
-# Algorithmic HBM bytes per cell-update of the FP64 SWE step with a static bed:
-# stage 1 reads b,h,hu,hv and writes h,hu,hv (7 x 8 B); stage 2 reads
-# b,h*,hu*,hv* and Q^n h,hu,hv and writes h,hu,hv (10 x 8 B).
+# Algorithmic HBM bytes per cell-update (one SSP-RK2 step), static bed.
+# FP64 plain: stage 1 reads b,h,hu,hv, writes h,hu,hv (7 x 8 B); stage 2 reads
+# b,h*,hu*,hv* and Q^n h,hu,hv, writes h,hu,hv (10 x 8 B).
 BYTES_PER_CELL_STEP_FP64 = 136
+# FP32 chosen form: stage 1 reads b,eta,hu,hv, writes inc1 (7 x 4 B); stage 2
+# reads b,eta,hu,hv, inc1, lo and writes eta,hu,hv and lo (16 x 4 B).
+BYTES_PER_CELL_STEP_FP32 = 92
 
-# DRAM bytes per cell per step of the two k_stage launches, from
-# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (profiles/k_stage_swe2d_fp64.md).
-NCU_TRAFFIC_PER_CELL_STEP_FP64 = None
+# DRAM bytes per cell per step of the two k32_stage launches, from
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (profiles/).
+NCU_TRAFFIC_PER_CELL_STEP_FP32 = None
 
 
 def parse():
@@ -52,6 +55,8 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="cells per side")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--err-steps", type=int, default=1000,
+                    help="steps of the FP32-vs-FP64 depth-error study (0 = skip)")
     return ap.parse_args()
 
 
@@ -226,6 +231,57 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def time_form(precision, n, Q0, A0, K, W, local, ws, barrier, max_over_ranks):
+    """Time K device-driven steps of one arithmetic form; returns (ms, value, st)."""
+    import torch
+    from zoomy_amrex_b200.level import Level
+    cfg = workload_config(n)
+    cfg.precision = precision
+    lev = Level(cfg, Q0, A0, device=f"cuda:{local}")
+    lev.begin()
+    for _ in range(max(3, W)):
+        lev.evolve(1)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(); torch.cuda.synchronize()
+    with torch.cuda.stream(lev.stream):
+        e0.record(lev.stream)
+        lev.evolve(K)
+        e1.record(lev.stream)
+    torch.cuda.synchronize(); barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    st = lev.status()
+    lev.close()
+    assert not st["done"] and np.isfinite(st["dt"]), st
+    return ms, n * n * K * ws / (ms * 1e-3), st
+
+
+def depth_error(n, Q0, A0, steps, local):
+    """FP32 chosen form vs FP64 plain form after `steps` steps from the same
+    state. The FP64 GPU form equals the CPU oracle bitwise (tests/test_gpu_parity.py),
+    so it stands in for the oracle at this size."""
+    import torch
+    from zoomy_amrex_b200._abi import ZFV_PREC_FP32, ZFV_PREC_FP64
+    from zoomy_amrex_b200.level import Level
+    out = {}
+    for prec in (ZFV_PREC_FP64, ZFV_PREC_FP32):
+        cfg = workload_config(n)
+        cfg.precision = prec
+        cfg.max_step = steps
+        lev = Level(cfg, Q0, A0, device=f"cuda:{local}")
+        st = lev.run(chunk=250)
+        out[prec] = (lev.state64()[1].clone(), st)
+        lev.close()
+    h64, st64 = out[ZFV_PREC_FP64]
+    h32, st32 = out[ZFV_PREC_FP32]
+    dh = (h32 - h64).abs()
+    wet = h64 > 1e-6
+    return {"steps": steps, "l1_depth": float(dh.mean()), "linf_depth": float(dh.max()),
+            "l1_depth_wet": float(dh[wet].mean()), "time_fp64": st64["time"],
+            "time_fp32": st32["time"], "mass_rel_diff": abs(st32["mass"] - st64["mass"]) / st64["mass"],
+            "reference": "FP64 plain form on the GPU (bitwise equal to the CPU oracle)"}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup(args)
@@ -244,18 +300,8 @@ def main():
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
+    from zoomy_amrex_b200._abi import ZFV_PREC_FP32, ZFV_PREC_FP64
     from zoomy_amrex_b200.level import Level
-
-    n = args.n
-    cells = n * n
-    Q0, A0 = workload_fields(n)
-    cfg = workload_config(n)
-    lev = Level(cfg, Q0, A0, device=f"cuda:{local}")
-    stream = lev.stream
-    lev.begin()
-    for _ in range(max(3, args.warmup)):
-        lev.evolve(1)
-    torch.cuda.synchronize()
 
     def barrier():
         if ws > 1:
@@ -270,51 +316,62 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    n = args.n
+    cells = n * n
     K = args.steps
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    Q0, A0 = workload_fields(n)
+
     with Clocks(local) as clk:
-        barrier(); torch.cuda.synchronize()
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-            lev.evolve(K)
-            e1.record(stream)
-        torch.cuda.synchronize(); barrier()
-    ms = e0.elapsed_time(e1)
-    ms = max_over_ranks(ms)
-    st = lev.status()
-    assert not st["done"] and np.isfinite(st["dt"]), st
-    value = cells * K * ws / (ms * 1e-3)
-
-    # per-step device time of the fused stage pair (the dominant kernel)
-    step_s = ms * 1e-3 / K
+        ms64, v64, _ = time_form(ZFV_PREC_FP64, n, Q0, A0, K, args.warmup, local, ws, barrier, max_over_ranks)
+        ms32, v32, _ = time_form(ZFV_PREC_FP32, n, Q0, A0, K, args.warmup, local, ws, barrier, max_over_ranks)
     peak, peak_kind = measured_peak()
-    achieved = cells * BYTES_PER_CELL_STEP_FP64 / step_s / 1e9
-    traffic = (None if NCU_TRAFFIC_PER_CELL_STEP_FP64 is None
-               else NCU_TRAFFIC_PER_CELL_STEP_FP64 * cells / 2)
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                "kernel": "k_stage (stage-1 + stage-2 launches per step)",
-                "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_FP64,
-                "traffic_per": "launch"}
-    lev.close()
+    step32 = ms32 * 1e-3 / K
+    step64 = ms64 * 1e-3 / K
+    achieved32 = cells * BYTES_PER_CELL_STEP_FP32 / step32 / 1e9
+    achieved64 = cells * BYTES_PER_CELL_STEP_FP64 / step64 / 1e9
+    traffic = (None if NCU_TRAFFIC_PER_CELL_STEP_FP32 is None
+               else NCU_TRAFFIC_PER_CELL_STEP_FP32 * cells / 2)
+    roofline = {"bound": "hbm", "achieved": achieved32, "peak": peak, "unit": "GB/s",
+                "frac": achieved32 / peak, "traffic": traffic, "peak_source": peak_kind,
+                "kernel": "k32_stage (FP32 chosen form; stage-1 + stage-2 launches per step)",
+                "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_FP32, "traffic_per": "launch",
+                "fp64_plain": {"achieved": achieved64, "frac": achieved64 / peak,
+                               "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_FP64,
+                               "bound": "fp64 alu"}}
 
-    # end to end through the public Level API with host buffers: pinned H2D of
-    # the initial state, K steps, D2H of the final state, all inside the timed region
+    err = None
+    if args.err_steps > 0 and rank == 0:
+        err = depth_error(n, Q0, A0, args.err_steps, local)
+
+    # end to end through the public Level API with host buffers (FP32 form):
+    # pinned H2D of the FP64 state + aux, import (FP32 split), first dt,
+    # K device-driven steps, export to FP64 and D2H of the state
     e2e = None
     if not args.no_e2e:
         Qh = torch.from_numpy(Q0).pin_memory()
         Ah = torch.from_numpy(A0).pin_memory()
         Qout = torch.empty_like(Qh).pin_memory()
+        cfg = workload_config(n)
+        cfg.precision = ZFV_PREC_FP32
         lev2 = Level(cfg, Q0, A0, device=f"cuda:{local}")
+        q64 = torch.empty(Qh.shape, dtype=torch.float64, device=f"cuda:{local}")
+        from zoomy_amrex_b200 import _lib
+        import ctypes as C
+        L = _lib.lib()
         torch.cuda.synchronize(); barrier()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s = C.c_void_p(lev2.stream.cuda_stream)
         with torch.cuda.stream(lev2.stream):
             f0.record(lev2.stream)
-            lev2.Q.copy_(Qh, non_blocking=True)
+            q64.copy_(Qh, non_blocking=True)
             lev2.aux.copy_(Ah, non_blocking=True)
+            _lib.check(L.zfv_state_import(lev2.handle, q64.data_ptr(), lev2.Q.data_ptr(),
+                                          lev2.scratch.data_ptr(), s), "import")
             lev2.begin()
             lev2.evolve(K)
-            Qout.copy_(lev2.Q, non_blocking=True)
+            _lib.check(L.zfv_state_export(lev2.handle, lev2.Q.data_ptr(), lev2.scratch.data_ptr(),
+                                          q64.data_ptr(), s), "export")
+            Qout.copy_(q64, non_blocking=True)
             f1.record(lev2.stream)
         torch.cuda.synchronize(); barrier()
         ms2 = max_over_ranks(f0.elapsed_time(f1))
@@ -322,8 +379,8 @@ def main():
         e2e = {"value": cells * K * ws / (ms2 * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": (Qh.numel() + Ah.numel()) * 8 / K,
                "d2h_bytes_per_step": Qout.numel() * 8 / K,
-               "note": "one run of K steps through Level: pinned H2D of (Q, aux), begin (first dt), "
-                       "K device-driven steps, D2H of Q"}
+               "note": "one run of K steps of the FP32 form through Level/C ABI: pinned H2D of the "
+                       "FP64 (Q, aux), import, first dt, K device-driven steps, export, D2H of Q"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -334,12 +391,15 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"failed: {e}"}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
-                "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": dict(config_desc(n, K), parallelism=f"replicas x{ws}" if ws > 1 else "single GPU"),
-                "forms": {"fp64_plain": value, "fp32_chosen": None},
-                "hbm_gbs": achieved,
+        line = {"metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": ws, "steps": K,
+                "warmup": args.warmup, "ms_per_step": ms32 / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": dict(config_desc(n, K), parallelism=f"replicas x{ws}" if ws > 1 else "single GPU",
+                               form="FP32 chosen (compensated, eta storage)"),
+                "forms": {"fp32_chosen": v32, "fp64_plain": v64, "fp32_over_fp64": v32 / v64,
+                          "ms_per_step_fp32": ms32 / K, "ms_per_step_fp64": ms64 / K},
+                "depth_error_fp32_vs_fp64": err,
+                "hbm_gbs": achieved32,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 2 * K, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)

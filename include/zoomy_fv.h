@@ -16,7 +16,10 @@
  *    j in [0,ny). This is Array4's (i,j,k,n) order with no ghost cells:
  *    ghost cells are never stored; they are rebuilt inside each kernel's
  *    tile load (mirror + Model::boundary_conditions).
- *  - Element type: double for ZFV_PREC_FP64, float for ZFV_PREC_FP32.
+ *  - Element type of Q: double for ZFV_PREC_FP64; float for ZFV_PREC_FP32,
+ *    whose rows are [b, eta = h + b, hu, hv] (use zfv_state_import/export to
+ *    convert from/to the reference layout [b, h, hu, hv] in FP64). aux is
+ *    always double.
  *  - All device work is enqueued on the given stream (cudaStream_t passed as
  *    void*; NULL = legacy default stream). Functions never synchronize unless
  *    their comment says so.
@@ -42,7 +45,11 @@ enum {
 
 /* Arithmetic form. */
 enum {
-    ZFV_PREC_FP64 = 0      /* the plain form: FP64 everywhere, bit-compatible with the CPU path */
+    ZFV_PREC_FP64 = 0,     /* the plain form: FP64 everywhere, bit-compatible with the CPU path */
+    ZFV_PREC_FP32 = 1      /* the chosen form (ZFV_MODEL_SWE2D): FP32 state and flux arithmetic,
+                              Q = [b, eta = h + b, hu, hv] as float, compensation planes in
+                              scratch carry the low-order part of eta, hu, hv (compensated
+                              update); FP64 for near-dry implicit sources and the mass sum */
 };
 
 /* Status flags (bitwise OR) reported by zfv_get_status(). */
@@ -173,6 +180,16 @@ int zfv_rhs(zfv_handle* h, const void* Q, const void* aux, void* rhs, double tim
  */
 int zfv_fill_ghosts(zfv_handle* h, const void* Q, const void* aux, void* Qg, void* auxg,
                     double time, void* stream);
+
+/*
+ * Convert between the reference layout (Q64: [b, h, hu, (hv)] float64) and a
+ * handle's state Q. FP64 handles copy. FP32 handles split eta = h + b, hu, hv
+ * into a float part in Q and a float remainder in scratch (the compensation
+ * planes), so the FP64 input is carried to ~48 bits; export recombines them.
+ * zfv_state_import must precede zfv_begin for FP32 handles.
+ */
+int zfv_state_import(zfv_handle* h, const double* Q64, void* Q, void* scratch, void* stream);
+int zfv_state_export(zfv_handle* h, const void* Q, const void* scratch, double* Q64, void* stream);
 
 /* Sum(h) * dx * dy into the status record's mass field (ZoomyAmr.cpp:517-536). */
 int zfv_total_mass(zfv_handle* h, const void* Q, void* scratch, void* stream);

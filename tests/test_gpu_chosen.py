@@ -1,0 +1,144 @@
+"""The FP32 chosen form (ZFV_PREC_FP32) against the FP64 oracle.
+
+The chosen form is the same scheme evaluated in FP32 with a compensated
+update, so it is compared to the FP64 oracle by error norms, not bitwise:
+L1 / Linf of the depth after a number of steps, plus the properties the form
+is built for — an exactly well-balanced lake at rest, FP64-accurate mass.
+"""
+import numpy as np
+import pytest
+
+from cases import setup
+from zoomy_amrex_b200._abi import ZFV_PREC_FP32
+from zoomy_amrex_b200.models import SWE
+from zoomy_amrex_b200.settings import config_from_settings
+
+pytestmark = pytest.mark.gpu
+
+
+def bumps(seed, n_b=8, hump=0.3, eta0=1.0, wet_everywhere=False, moving=False):
+    def ic(x):
+        rng = np.random.default_rng(seed)
+        b = np.zeros(x.shape[1])
+        for _ in range(n_b):
+            cx, cy = rng.uniform(0, 100, 2)
+            a, w = rng.uniform(0.2, 1.5), rng.uniform(2.0, 10.0)
+            b += a * np.exp(-((x[0] - cx) ** 2 + (x[1] - cy) ** 2) / (2 * w * w))
+        e0 = b.max() + 0.5 if wet_everywhere else eta0
+        hx, hy = rng.uniform(20, 80, 2)
+        eta = e0 + hump * np.exp(-((x[0] - hx) ** 2 + (x[1] - hy) ** 2) / (2 * 5.0 ** 2))
+        h = np.maximum(eta - b, 0.0)
+        hu = 0.05 * h * np.sin(x[1] / 7.0) if moving else np.zeros_like(h)
+        hv = -0.05 * h * np.cos(x[0] / 9.0) if moving else np.zeros_like(h)
+        return np.array([b, h, hu, hv])
+    return ic
+
+
+def _settings(n, steps, **kw):
+    s = dict(dimension=2, domain=[0, 100, 0, 100], n_cells=[n, n], spatial_order=2, cfl=0.45,
+             time_end=1e30, max_step=steps, well_balanced=True, implicit_source=True)
+    s.update(kw)
+    return s
+
+
+def run_fp32(model, settings):
+    from zoomy_amrex_b200.level import Level
+    cfg64, Q0, A0 = setup(model, settings)
+    cfg = config_from_settings(model, settings, precision=ZFV_PREC_FP32)
+    lev = Level(cfg, Q0, A0)
+    try:
+        st = lev.run(chunk=32)
+        return lev.state64().cpu().numpy(), lev.aux.cpu().numpy(), st, lev.log(), (cfg64, Q0, A0)
+    finally:
+        lev.close()
+
+
+def test_lake_at_rest_is_exact_in_fp32(cuda):
+    """Config 2's lake-at-rest variant (still water over the bumps, no hump),
+    fully wet, order 2, Manning implicit: u stays exactly zero (the FP32 bound
+    required is 1e-6) and eta does not move."""
+    model = SWE(2, "wall", bumps(3, hump=0.0, wet_everywhere=True), parameters={"n_m": 0.03})
+    Q, _, st, _, (cfg, Q0, A0) = run_fp32(model, _settings(96, 200))
+    assert st["step"] == 200
+    u = np.abs(Q[2:]) / np.maximum(Q[1], 1e-300)
+    assert u.max() < 1e-6
+    assert np.abs(Q[2:]).max() == 0.0
+    assert np.abs((Q[0] + Q[1]) - (Q0[0] + Q0[1])).max() < 1e-12
+
+
+def test_lake_at_rest_with_dry_islands_order1(cuda):
+    """With emerging bumps (dry islands) the reference scheme is exactly
+    well-balanced at order 1 (Audusse); so is the FP32 form."""
+    model = SWE(2, "wall", bumps(5, hump=0.0), parameters={"n_m": 0.03})
+    s = _settings(64, 100, spatial_order=1)
+    from zoomy_amrex_b200.level import Level
+    cfg64, Q0, A0 = setup(model, s)
+    assert (Q0[1] == 0).any()
+    # the FP32 form runs the SSP-RK2 path only: check the FP64 form here and the
+    # FP32 form at order 2 on the fully wet lake above
+    lev = Level(cfg64, Q0, A0)
+    lev.run(chunk=50)
+    Q = lev.Q.cpu().numpy()
+    lev.close()
+    assert np.abs(Q[2:]).max() < 1e-12
+
+
+@pytest.mark.parametrize("moving", [False, True])
+def test_fp32_depth_error_vs_fp64_oracle(cuda, oracle, moving):
+    """L1 / Linf depth error of the chosen form after 150 steps of a wet/dry
+    hump over bumps (Manning implicit, WB, walls, order 2)."""
+    model = SWE(2, "wall", bumps(7, moving=moving), parameters={"n_m": 0.03})
+    s = _settings(80, 150)
+    Q32, A32, st, log32, (cfg, Q0, A0) = run_fp32(model, s)
+    Qo, Ao, n, t, logo, _ = oracle.run(cfg, Q0, A0)
+    assert st["step"] == n == 150
+    assert abs(st["time"] - t) <= 1e-6 * t
+    dh = np.abs(Q32[1] - Qo[1])
+    l1, linf = dh.mean(), dh.max()
+    print(f"[fp32 vs fp64 oracle] moving={moving}: L1 {l1:.3e} Linf {linf:.3e} "
+          f"mom {np.abs(Q32[2:] - Qo[2:]).max():.3e} dt-time {abs(st['time'] - t):.3e}")
+    assert l1 <= 1e-6, l1
+    assert linf <= 1e-4, linf
+    assert np.abs(Q32[2:] - Qo[2:]).max() <= 1e-4
+    # dry cells agree on being dry
+    assert ((Q32[1] <= 1e-6) == (Qo[1] <= 1e-6)).mean() > 0.999
+
+
+def test_fp32_mass_is_conserved_with_walls(cuda):
+    model = SWE(2, "wall", bumps(9, moving=True), parameters={"n_m": 0.03})
+    Q, _, st, log, (cfg, Q0, A0) = run_fp32(model, _settings(72, 120))
+    dx = dy = 100.0 / 72
+    # the FP32 form's initial mass: depth measured from its FP32 bed
+    b32 = Q0[0].astype(np.float32).astype(np.float64)
+    m0 = ((Q0[1] + Q0[0]) - b32).sum() * dx * dy
+    m = log[:, 2]
+    assert np.abs(m - m0).max() / m0 < 1e-10
+    assert abs(Q[1].sum() * dx * dy - m0) / m0 < 1e-10
+    assert abs(m0 - Q0[1].sum() * dx * dy) / m0 < 1e-7
+
+
+def test_fp32_import_export_round_trip(cuda):
+    import torch
+    from zoomy_amrex_b200.level import Level
+    model = SWE(2, "wall", bumps(11, moving=True))
+    s = _settings(40, 1)
+    cfg64, Q0, A0 = setup(model, s)
+    cfg = config_from_settings(model, s, precision=ZFV_PREC_FP32)
+    lev = Level(cfg, Q0, A0)
+    back = lev.state64().cpu().numpy()
+    lev.close()
+    b32 = Q0[0].astype(np.float32).astype(np.float64)
+    assert np.array_equal(back[0], b32)
+    # eta = h + b is carried as float + float remainder (~48 bits)
+    eta0, eta = Q0[0] + Q0[1], back[0] + back[1]
+    assert np.abs(eta - eta0).max() <= 1e-13 * max(1.0, np.abs(eta0).max())
+    # the depth is measured from the FP32 bed: within half an FP32 ulp of b
+    assert np.abs(back[1] - Q0[1]).max() <= 6e-8 * max(1.0, np.abs(Q0[0]).max())
+    assert np.abs(back[2:] - Q0[2:]).max() <= 1e-14
+
+
+def test_fp32_runs_are_deterministic(cuda):
+    model = SWE(2, "wall", bumps(13, moving=True), parameters={"n_m": 0.03})
+    a = run_fp32(model, _settings(48, 40))
+    b = run_fp32(model, _settings(48, 40))
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[3], b[3])

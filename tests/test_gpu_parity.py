@@ -253,3 +253,21 @@ def test_run_is_deterministic(cuda):
     a = run_gpu(cfg, Q0, A0)
     b = run_gpu(cfg, Q0, A0)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[3], b[3])
+
+
+def test_mood_whole_step_redo_bitwise(cuda, oracle):
+    """positivity = "mood" (ZoomyAmr.cpp:685-720): order-2 candidates with a
+    negative or non-finite depth are discarded and the whole step is redone at
+    order 1 from Q^n; the GPU redoes exactly the same steps."""
+    model = SWE(2, "wall", wetdry_ic(5, moving=True))
+    s = dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[40, 32], spatial_order=2, cfl=1.0,
+             time_end=1e30, max_step=60, positivity="mood")
+    cfg, Q0, A0 = setup(model, s)
+    Qo, Ao, n, t, logo, redos = oracle.run(cfg, Q0, A0)
+    assert redos > 0
+    for graph in (False, True):
+        Qg, Ag, st, logg = run_gpu(cfg, Q0, A0, use_graph=graph)
+        assert st["step"] == n and st["time"] == t
+        assert st["mood_redos"] == redos and st["flags"] & 2
+        assert np.array_equal(Qg, Qo) and np.array_equal(Ag, Ao)
+        assert np.array_equal(logg[:, :2], logo[:, :2])

@@ -13,6 +13,7 @@ ZFV_MODEL_SWE1D = 1
 ZFV_MODEL_SWE2D = 2
 
 ZFV_PREC_FP64 = 0
+ZFV_PREC_FP32 = 1
 
 ZFV_FLAG_NONFINITE_DT = 1
 ZFV_FLAG_MOOD_REDO = 2

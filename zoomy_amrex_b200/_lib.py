@@ -17,7 +17,7 @@ _lib = None
 SYMBOLS = ("zfv_last_error", "zfv_version", "zfv_sizeof_config", "zfv_sizeof_status", "zfv_model_info", "zfv_create", "zfv_destroy",
            "zfv_scratch_bytes", "zfv_begin", "zfv_update_state", "zfv_compute_dt", "zfv_evolve",
            "zfv_rhs", "zfv_fill_ghosts", "zfv_total_mass", "zfv_get_status", "zfv_log_capacity",
-           "zfv_read_log", "zfv_evolve_static")
+           "zfv_read_log", "zfv_evolve_static", "zfv_state_import", "zfv_state_export")
 
 
 class ZfvError(RuntimeError):
@@ -52,6 +52,8 @@ def lib():
     L.zfv_get_status.argtypes = [vp, vp, C.POINTER(zfv_status), vp]
     L.zfv_log_capacity.argtypes = [vp]
     L.zfv_read_log.argtypes = [vp, vp, C.POINTER(d), i, C.POINTER(C.c_int64), C.POINTER(i), vp]
+    L.zfv_state_import.argtypes = [vp, vp, vp, vp, vp]
+    L.zfv_state_export.argtypes = [vp, vp, vp, vp, vp]
     L.zfv_evolve_static.argtypes = [vp, vp, vp, i, i, C.POINTER(zfv_status), vp]
     _lib = L
     return L

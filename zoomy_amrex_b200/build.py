@@ -3,9 +3,10 @@
     python -m zoomy_amrex_b200.build [--verbose]
 
 The library is written to zoomy_amrex_b200/lib/libzoomyfv.so. FMA contraction
-is disabled (--fmad=false), as in the reference's CUDA build (build.py:33-41 of
-zoomy-amrex), so the FP64 kernels evaluate the same IEEE operations as the
-CPU build of the same expressions.
+is disabled (--fmad=false) for the FP64 plain form, as in the reference's CUDA
+build (build.py:33-41 of zoomy-amrex), so those kernels evaluate the same IEEE
+operations as the CPU build of the same expressions; the FP32 chosen form
+(zoomy_fv32.cu) is compiled with FMA.
 """
 from __future__ import annotations
 
@@ -22,7 +23,10 @@ LIB = LIB_DIR / "libzoomyfv.so"
 INCLUDE = PKG.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["zoomy_fv.cu"]
+# (source, extra flags): the FP64 plain form keeps FMA contraction off so its
+# arithmetic is bitwise the CPU build's; the FP32 chosen form uses FMA.
+SOURCES = [("zoomy_fv.cu", ["--fmad=false"]),
+           ("zoomy_fv32.cu", ["--fmad=true"])]
 
 
 def nvcc() -> str:
@@ -49,16 +53,20 @@ def build(verbose: bool = False, force: bool = False) -> pathlib.Path:
     if not force and up_to_date():
         return LIB
     LIB_DIR.mkdir(exist_ok=True)
-    objs = []
-    for src in SOURCES:
+    objs, jobs = [], []
+    for src, flags in SOURCES:
         obj = LIB_DIR / (pathlib.Path(src).stem + ".o")
-        cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
+        cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", *flags, "-std=c++17",
                "-Xcompiler", "-fPIC", "-I", str(CSRC), "-I", str(CSRC / "amrex_compat"),
                "-I", str(CSRC / "models"), "-I", str(INCLUDE), "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        jobs.append((cmd, obj))
+    procs = [subprocess.Popen(cmd) for cmd, _ in jobs]
+    for p, (cmd, obj) in zip(procs, jobs):
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, cmd)
         objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)

@@ -37,7 +37,8 @@ struct alignas(128) DevState {
     unsigned flags, mood_redos;
     unsigned pad0[4];
     unsigned counter;       // last-block-done counter of the grid reductions
-    unsigned pad1[15];
+    unsigned troubled;      // MOOD: some cell of this step's order-2 candidate has h < 0 or non-finite
+    unsigned pad1[14];
 };
 static_assert(sizeof(DevState) == 128, "DevState layout");
 

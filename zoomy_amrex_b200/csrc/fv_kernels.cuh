@@ -28,7 +28,11 @@ enum StageMode : int {
     MODE_RHS = 0,   // write the RHS only (validation entry zfv_rhs)
     MODE_S1 = 1,    // SSP-RK2 stage 1: write the stage state
     MODE_S2 = 2,    // SSP-RK2 stage 2: Heun + final UpdateState + reduction
-    MODE_ONE = 3    // order 1: single stage + final UpdateState + reduction
+    MODE_ONE = 3,   // order 1: single stage + final UpdateState + reduction
+    // positivity = "mood" (ZoomyAmr.cpp:685-720):
+    MODE_S2M = 4,   // stage 2 writing the Heun candidate to a buffer and flagging troubled cells
+    MODE_R1 = 5,    // order-1 redo, stage 1 (runs only when the step is troubled)
+    MODE_R2 = 6     // order-1 redo, stage 2 + final UpdateState + reduction (troubled only)
 };
 
 // Face records in shared memory hold make_rhs.H:310-315's components
@@ -84,7 +88,7 @@ __device__ __forceinline__ void block_reduce_max_sum(double& m, double& s, doubl
 template <int NT, class PL>
 __device__ __forceinline__ void finish_step(double m, double s, double* red, double* partials,
                                             double* log3, int log_cap, DevState* st, PL const& L,
-                                            double dt_used, double time_used) {
+                                            double dt_used, double time_used, bool mood_redo = false) {
     block_reduce_max_sum<NT>(m, s, red);
     const unsigned nblk = gridDim.x * gridDim.y;
     const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
@@ -119,6 +123,11 @@ __device__ __forceinline__ void finish_step(double m, double s, double* red, dou
         unsigned flags = st->flags;
         if (!isfinite(dt_next)) flags |= kFlagNonfiniteDt;
         if (run_done(t_new, step, L)) flags |= kFlagDone;
+        if (mood_redo) {
+            flags |= kFlagMoodRedo;
+            st->mood_redos = st->mood_redos + 1u;
+            st->troubled = 0u;
+        }
         st->time = t_new;
         st->step = step;
         st->mass = mass;
@@ -157,6 +166,10 @@ k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
     const int nx = L.nx, ny = L.ny;
     const long long plane = L.plane;
 
+    // The MOOD redo stages run only for a troubled step.
+    if constexpr (MODE == MODE_R1 || MODE == MODE_R2) {
+        if (*(volatile unsigned*)&st->troubled == 0u) return;
+    }
     // Idle once the run is done (time_end / max_step reached).
     const unsigned flags0 = (MODE == MODE_RHS) ? 0u : *(volatile unsigned*)&st->flags;
     if (flags0 & kFlagDone) {
@@ -332,11 +345,20 @@ k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
 #pragma unroll
             for (int n = 0; n < nq; ++n) q(n, 0) = qc(n, 0) + dt * rhs(n, 0);
             if constexpr (IMPL) implicit_source_cell<Model, R>(q, ac, dt, p, time, X);
-            if constexpr (MODE == MODE_S1) {
+            if constexpr (MODE == MODE_S1 || MODE == MODE_R1) {
 #pragma unroll
                 for (int n = (sbed ? 1 : 0); n < nq; ++n) qout[n * plane + c] = q(n, 0);
+            } else if constexpr (MODE == MODE_S2M) {
+                // Heun candidate; the MOOD test (ZoomyAmr.cpp:706-708) runs on it
+                // before the final UpdateState, as in the reference
+#pragma unroll
+                for (int n = 0; n < nq; ++n) q(n, 0) = R(0.5) * qold[n * plane + c] + R(0.5) * q(n, 0);
+#pragma unroll
+                for (int n = (sbed ? 1 : 0); n < nq; ++n) qout[n * plane + c] = q(n, 0);
+                const R hh = q(kIdxH, 0);
+                if (!(hh >= R(0.0)) || !(hh < R(1.0e300))) atomicOr(&st->troubled, 1u);
             } else {
-                if constexpr (MODE == MODE_S2) {
+                if constexpr (MODE == MODE_S2 || MODE == MODE_R2) {
                     // Heun: Q = 0.5*Q^n + 0.5*Q** (the bed row of Q^n is qbed == qold row 0)
 #pragma unroll
                     for (int n = 0; n < nq; ++n) q(n, 0) = R(0.5) * qold[n * plane + c] + R(0.5) * q(n, 0);
@@ -351,8 +373,45 @@ k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
             }
         }
     }
-    if constexpr (MODE == MODE_S2 || MODE == MODE_ONE)
-        finish_step<NT>(m_loc, s_loc, red, partials, log3, log_cap, st, L, dt, time);
+    if constexpr (MODE == MODE_S2 || MODE == MODE_ONE || MODE == MODE_R2)
+        finish_step<NT>(m_loc, s_loc, red, partials, log3, log_cap, st, L, dt, time, MODE == MODE_R2);
+}
+
+// MOOD commit (positivity = "mood", ZoomyAmr.cpp:699-730): when no cell of the
+// order-2 candidate is troubled, the candidate becomes Q^{n+1} after the final
+// UpdateState, and this kernel contributes the CFL / mass reduction. When the
+// step is troubled it does nothing; the order-1 redo stages finish the step.
+template <class Model, class Numerics, int NT>
+__global__ void __launch_bounds__(NT)
+k_mood_commit(const double* __restrict__ qcand, double* __restrict__ qout,
+              LevelParams<double, Model::n_parameters> L, DevState* st,
+              double* __restrict__ partials, double* __restrict__ log3, int log_cap) {
+    using T = ModelTypes<Model>;
+    constexpr bool sbed = static_bed<Model>::value;
+    constexpr int nq = Model::n_dof_q;
+    __shared__ double red[2 * ((NT + 31) / 32)];
+    if (*(volatile unsigned*)&st->troubled != 0u) return;
+    if (*(volatile unsigned*)&st->flags & kFlagDone) return;
+    const double dt = *(volatile double*)&st->dt;
+    const double time = *(volatile double*)&st->time;
+    typename T::VP p;
+    for (int k = 0; k < Model::n_parameters; ++k) p(k, 0) = L.p[k];
+    const long long c = (long long)blockIdx.x * NT + threadIdx.x;
+    double m_loc = 0.0, s_loc = 0.0;
+    if (c < L.plane) {
+        const int i = int(c % L.nx), j = int(c / L.nx);
+        typename T::VQ q;
+        q(0, 0) = sbed ? qout[c] : qcand[c];
+#pragma unroll
+        for (int n = 1; n < nq; ++n) q(n, 0) = qcand[n * L.plane + c];
+        typename T::VA a{};
+        update_state_cell<Model, double>(q, a, p, L, time, cell_centre<Model, double>(L, i, j));
+#pragma unroll
+        for (int n = (sbed ? 1 : 0); n < nq; ++n) qout[n * L.plane + c] = q(n, 0);
+        m_loc = cell_max_inv<Model, Numerics, double>(q, a, p, L);
+        s_loc = q(kIdxH, 0);
+    }
+    finish_step<NT>(m_loc, s_loc, red, partials, log3, log_cap, st, L, dt, time, false);
 }
 
 // ---------------------------------------------------------------------------
@@ -506,6 +565,7 @@ __global__ void k_begin(DevState* st, PL L) {
     st->time = 0.0; st->dt = 0.0; st->mass = 0.0; st->max_inv = 0.0;
     st->step = 0; st->flags = run_done(0.0, 0, L) ? kFlagDone : 0u; st->mood_redos = 0;
     st->counter = 0u;
+    st->troubled = 0u;
 }
 
 }  // namespace zfv

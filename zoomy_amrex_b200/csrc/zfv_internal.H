@@ -1,0 +1,61 @@
+// Internals shared by the translation units of libzoomyfv.so (not installed).
+#pragma once
+#include <cstddef>
+#include <memory>
+#include <cuda_runtime.h>
+#include "zoomy_fv.h"
+
+namespace zfvi {
+
+// Record an error message for zfv_last_error() and return `code`.
+int fail(int code, const char* fmt, ...);
+// 0 if e == cudaSuccess, else fail(-3, "<what>: <cuda message>").
+int cuda_check(cudaError_t e, const char* what);
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+constexpr int kLogCap = 4096;            // per-step log ring buffer entries
+constexpr int kReduceNT = 256;
+constexpr int kReduceBlocksMax = 1184;   // 8 x 148 SMs
+
+// Scratch layout (byte offsets from the caller's scratch base).
+struct ScratchLayout {
+    size_t state = 0;        // DevState (128 B; first 64 B = zfv_status)
+    size_t partials = 0;     // 2 doubles per block
+    size_t log = 0;          // 3 doubles per entry
+    size_t stage = 0;        // FP64: n_q stage planes; FP32: increment planes
+    size_t alt = 0;          // FP32: ping-pong state planes
+    size_t lo = 0;           // FP32: compensation planes
+    size_t total = 0;
+};
+
+// One compiled model/precision: owns its kernel instantiations.
+struct Runner {
+    virtual ~Runner() = default;
+    virtual int setup() = 0;
+    virtual void layout(ScratchLayout& L) const = 0;
+    virtual int begin(const void* Q, const void* A, char* scratch, cudaStream_t s) = 0;
+    virtual int update_state(void* Q, void* A, double time, cudaStream_t s) = 0;
+    virtual int compute_dt(const void* Q, const void* A, char* scratch, cudaStream_t s) = 0;
+    virtual int total_mass(const void* Q, char* scratch, cudaStream_t s) = 0;
+    virtual int evolve(void* Q, void* A, char* scratch, int n, cudaStream_t s) = 0;
+    virtual int rhs(const void* Q, void* out, double time, cudaStream_t s) = 0;
+    virtual int fill_ghosts(const void* Q, const void* A, void* Qg, void* Ag, double time,
+                            cudaStream_t s) = 0;
+    virtual int state_import(const double* Q64, void* Q, char* scratch, cudaStream_t s) = 0;
+    virtual int state_export(const void* Q, const char* scratch, double* Q64, cudaStream_t s) = 0;
+};
+
+}  // namespace zfvi
+
+struct zfv_handle {
+    zfv_config cfg;
+    zfvi::ScratchLayout lay;
+    std::unique_ptr<zfvi::Runner> run;
+};
+
+namespace zfvi {
+// FP32 chosen-form runner for ZFV_MODEL_SWE2D (zoomy_fv32.cu).
+Runner* make_runner_fp32_swe2d(zfv_handle* h);
+}

@@ -12,13 +12,15 @@
 #include <new>
 #include <memory>
 #include <string>
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include "zoomy_fv.h"
+#include "zfv_internal.H"
 #include "swe.H"
 #include "fv_kernels.cuh"
 
-namespace {
+namespace zfvi {
 
 thread_local std::string g_err;
 
@@ -37,44 +39,9 @@ int cuda_check(cudaError_t e, const char* what) {
     return fail(-3, "%s: %s", what, cudaGetErrorString(e));
 }
 
-constexpr size_t kAlign = 256;
-size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+}  // namespace zfvi
 
-constexpr int kLogCap = 4096;     // per-step log ring buffer entries
-constexpr int kReduceNT = 256;
-constexpr int kReduceBlocksMax = 1184;   // 8 x 148 SMs
-
-// Scratch layout (offsets from the caller's scratch base).
-struct ScratchLayout {
-    size_t state = 0;        // DevState
-    size_t partials = 0;     // 2 doubles per block
-    size_t log = 0;          // 3 doubles per entry
-    size_t stage = 0;        // nq state planes (SSP-RK2 stage / order-1 ping-pong)
-    size_t total = 0;
-};
-
-// Per-model runner: owns the kernel instantiations for one Model/Numerics pair.
-struct Runner {
-    virtual ~Runner() = default;
-    virtual int setup() = 0;
-    virtual int n_blocks_stage() const = 0;
-    virtual int begin(const void* Q, const void* A, char* scratch, cudaStream_t s) = 0;
-    virtual int update_state(void* Q, void* A, double time, cudaStream_t s) = 0;
-    virtual int compute_dt(const void* Q, const void* A, char* scratch, cudaStream_t s) = 0;
-    virtual int total_mass(const void* Q, char* scratch, cudaStream_t s) = 0;
-    virtual int evolve(void* Q, void* A, char* scratch, int n, cudaStream_t s) = 0;
-    virtual int rhs(const void* Q, void* out, double time, cudaStream_t s) = 0;
-    virtual int fill_ghosts(const void* Q, const void* A, void* Qg, void* Ag, double time,
-                            cudaStream_t s) = 0;
-};
-
-}  // namespace
-
-struct zfv_handle {
-    zfv_config cfg;
-    ScratchLayout lay;
-    std::unique_ptr<Runner> run;
-};
+using namespace zfvi;
 
 namespace {
 
@@ -108,7 +75,33 @@ struct RunnerT final : Runner {
         block = dim3(TX * TY, 1, 1);
     }
 
-    int n_blocks_stage() const override { return int(grid.x * grid.y); }
+    bool mood() const { return h->cfg.positivity_mood && h->cfg.spatial_order == 2; }
+
+    void layout(ScratchLayout& S) const override {
+        const size_t plane_bytes = size_t(L.plane) * sizeof(double);
+        const int nblk = std::max(int(grid.x * grid.y), kReduceBlocksMax);
+        S.state = 0;
+        S.partials = align_up(sizeof(zfv::DevState));
+        S.log = S.partials + align_up(sizeof(double) * 2 * nblk);
+        S.stage = S.log + align_up(sizeof(double) * 3 * kLogCap);
+        S.lo = 0;
+        if (mood()) {   // second stage buffer for the MOOD candidate
+            S.alt = S.stage + align_up(plane_bytes * nq);
+            S.total = S.alt + align_up(plane_bytes * nq);
+        } else {
+            S.alt = 0;
+            S.total = S.stage + align_up(plane_bytes * nq);
+        }
+    }
+
+    int state_import(const double* Q64, void* Q, char*, cudaStream_t s) override {
+        return cuda_check(cudaMemcpyAsync(Q, Q64, size_t(L.plane) * nq * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, s), "zfv_state_import copy");
+    }
+    int state_export(const void* Q, const char*, double* Q64, cudaStream_t s) override {
+        return cuda_check(cudaMemcpyAsync(Q64, Q, size_t(L.plane) * nq * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, s), "zfv_state_export copy");
+    }
 
     template <int ORDER, int MODE, bool WB, bool IMPL>
     static auto kfn() { return &zfv::k_stage<Model, Numerics, ORDER, MODE, WB, IMPL, TX, TY>; }
@@ -132,6 +125,9 @@ struct RunnerT final : Runner {
         if constexpr (ORDER == 2) {
             rc |= set_smem<ORDER, zfv::MODE_S1, WB, IMPL>();
             rc |= set_smem<ORDER, zfv::MODE_S2, WB, IMPL>();
+            rc |= set_smem<ORDER, zfv::MODE_S2M, WB, IMPL>();
+            rc |= set_smem<1, zfv::MODE_R1, WB, IMPL>();
+            rc |= set_smem<1, zfv::MODE_R2, WB, IMPL>();
         } else {
             rc |= set_smem<ORDER, zfv::MODE_ONE, WB, IMPL>();
         }
@@ -161,6 +157,7 @@ struct RunnerT final : Runner {
     double* partials(char* scratch) const { return reinterpret_cast<double*>(scratch + h->lay.partials); }
     double* log3(char* scratch) const { return reinterpret_cast<double*>(scratch + h->lay.log); }
     double* stage(char* scratch) const { return reinterpret_cast<double*>(scratch + h->lay.stage); }
+    double* stage2(char* scratch) const { return reinterpret_cast<double*>(scratch + h->lay.alt); }
 
     int reduce_blocks() const {
         long long need = (L.plane + kReduceNT - 1) / kReduceNT;
@@ -303,8 +300,14 @@ int zfv_create(const zfv_config* cfg, zfv_handle** out) {
     int nq, na, np, dim;
     if (model_shape(cfg->model, &nq, &na, &np, &dim) != 0)
         return fail(-1, "zfv_create: unknown model id %d", cfg->model);
-    if (cfg->precision != ZFV_PREC_FP64)
+    if (cfg->precision != ZFV_PREC_FP64 && cfg->precision != ZFV_PREC_FP32)
         return fail(-1, "zfv_create: unsupported precision %d", cfg->precision);
+    if (cfg->precision == ZFV_PREC_FP32) {
+        if (cfg->model != ZFV_MODEL_SWE2D)
+            return fail(-1, "zfv_create: the FP32 form is built for ZFV_MODEL_SWE2D only");
+        if (cfg->clamp_positivity)
+            return fail(-1, "zfv_create: the FP32 form does not implement clamp_positivity");
+    }
     if (cfg->nx < 1 || cfg->ny < 1) return fail(-1, "zfv_create: bad grid %d x %d", cfg->nx, cfg->ny);
     if (dim == 1 && cfg->ny != 1) return fail(-1, "zfv_create: 1-D model needs ny == 1 (got %d)", cfg->ny);
     if ((long long)cfg->nx * cfg->ny > (1LL << 31))
@@ -320,8 +323,6 @@ int zfv_create(const zfv_config* cfg, zfv_handle** out) {
             return fail(-1, "zfv_create: order %d needs at least %d cells per direction (grid %d x %d)",
                         cfg->spatial_order, ng, cfg->nx, cfg->ny);
     }
-    if (cfg->positivity_mood && cfg->spatial_order == 2)
-        return fail(-2, "zfv_create: positivity = mood is not implemented in this build");
     if (cfg->n_params != np)
         return fail(-1, "zfv_create: model takes %d parameters, config has %d", np, cfg->n_params);
     if (!(cfg->prob_hi[0] > cfg->prob_lo[0]) || !(cfg->prob_hi[1] > cfg->prob_lo[1]))
@@ -335,20 +336,17 @@ int zfv_create(const zfv_config* cfg, zfv_handle** out) {
     zfv_handle* h = new (std::nothrow) zfv_handle();
     if (!h) return fail(-4, "zfv_create: out of host memory");
     h->cfg = *cfg;
-    switch (cfg->model) {
-    case ZFV_MODEL_SWE1D:
-        h->run.reset(new RunnerT<zb::SWE<double, 1>, zb::SWENumerics<double, 1>, 128, 1>(h)); break;
-    case ZFV_MODEL_SWE2D:
-        h->run.reset(new RunnerT<zb::SWE<double, 2>, zb::SWENumerics<double, 2>, 32, 8>(h)); break;
+    if (cfg->precision == ZFV_PREC_FP32) {
+        h->run.reset(make_runner_fp32_swe2d(h));
+    } else {
+        switch (cfg->model) {
+        case ZFV_MODEL_SWE1D:
+            h->run.reset(new RunnerT<zb::SWE<double, 1>, zb::SWENumerics<double, 1>, 128, 1>(h)); break;
+        case ZFV_MODEL_SWE2D:
+            h->run.reset(new RunnerT<zb::SWE<double, 2>, zb::SWENumerics<double, 2>, 32, 8>(h)); break;
+        }
     }
-    const size_t plane_bytes = size_t(cfg->nx) * cfg->ny * sizeof(double);
-    const int nblk = std::max(h->run->n_blocks_stage(), kReduceBlocksMax);
-    ScratchLayout& L = h->lay;
-    L.state = 0;
-    L.partials = align_up(sizeof(zfv::DevState));
-    L.log = L.partials + align_up(sizeof(double) * 2 * nblk);
-    L.stage = L.log + align_up(sizeof(double) * 3 * kLogCap);
-    L.total = L.stage + align_up(plane_bytes * nq);
+    h->run->layout(h->lay);
     int rc = h->run->setup();
     if (rc) { delete h; return rc; }
     *out = h;
@@ -393,6 +391,16 @@ int zfv_fill_ghosts(zfv_handle* h, const void* Q, const void* aux, void* Qg, voi
                     double time, void* stream) {
     if (!h || !Q || !aux || !Qg || !auxg) return fail(-1, "zfv_fill_ghosts: null argument");
     return h->run->fill_ghosts(Q, aux, Qg, auxg, time, (cudaStream_t)stream);
+}
+
+int zfv_state_import(zfv_handle* h, const double* Q64, void* Q, void* scratch, void* stream) {
+    if (!h || !Q64 || !Q || !scratch) return fail(-1, "zfv_state_import: null argument");
+    return h->run->state_import(Q64, Q, (char*)scratch, (cudaStream_t)stream);
+}
+
+int zfv_state_export(zfv_handle* h, const void* Q, const void* scratch, double* Q64, void* stream) {
+    if (!h || !Q64 || !Q || !scratch) return fail(-1, "zfv_state_export: null argument");
+    return h->run->state_export(Q, (const char*)scratch, Q64, (cudaStream_t)stream);
 }
 
 int zfv_total_mass(zfv_handle* h, const void* Q, void* scratch, void* stream) {

@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._abi import MODELS, zfv_config, zfv_status
+from ._abi import MODELS, ZFV_PREC_FP32, zfv_config, zfv_status
 
 _DTYPE = torch.float64
 
@@ -27,8 +27,13 @@ def _ptr(t: torch.Tensor) -> int:
 class Level:
     """A single-level solver state on ``device``.
 
-    Q:   (n_q, ny, nx) float64, rows [b, h, hu, (hv)]
-    aux: (n_aux, ny, nx) float64, last row hinv
+    FP64 plain form (cfg.precision == ZFV_PREC_FP64):
+      Q:   (n_q, ny, nx) float64, rows [b, h, hu, (hv)]
+    FP32 chosen form (ZFV_PREC_FP32, 2-D shallow water):
+      Q:   (4, ny, nx) float32, rows [b, eta = h + b, hu, hv]; the low-order
+           remainders of eta, hu, hv live in the scratch buffer. state64()
+           returns the combined state in the reference layout.
+    aux: (n_aux, ny, nx) float64, last row hinv (both forms)
     """
 
     def __init__(self, cfg: zfv_config, Q0, aux0, device: str | torch.device = "cuda:0",
@@ -44,12 +49,22 @@ class Level:
         self._h = h
         nq, na = self.info["n_q"], self.info["n_aux"]
         shape_q, shape_a = (nq, cfg.ny, cfg.nx), (na, cfg.ny, cfg.nx)
-        self.Q = self._as_tensor(Q0, shape_q)
+        self.fp32 = cfg.precision == ZFV_PREC_FP32
         self.aux = self._as_tensor(aux0, shape_a)
         nbytes = int(L.zfv_scratch_bytes(h))
-        self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        self.scratch = torch.zeros(nbytes, dtype=torch.uint8, device=self.device)
         # A dedicated stream: CUDA graphs cannot be captured on the default stream.
         self.stream = stream if stream is not None else torch.cuda.Stream(self.device)
+        if self.fp32:
+            q64 = self._as_tensor(Q0, shape_q)
+            self.Q = torch.empty(shape_q, dtype=torch.float32, device=self.device)
+            self.stream.wait_stream(torch.cuda.current_stream(self.device))
+            _lib.check(L.zfv_state_import(h, _ptr(q64), _ptr(self.Q), _ptr(self.scratch), self._s()),
+                       "zfv_state_import")
+            self.stream.synchronize()
+            del q64
+        else:
+            self.Q = self._as_tensor(Q0, shape_q)
         self.stream.wait_stream(torch.cuda.current_stream(self.device))
         self._graph = None
         self._graph_steps = 0
@@ -134,6 +149,18 @@ class Level:
             if st["done"]:
                 break
         return self.status()
+
+    def state64(self) -> torch.Tensor:
+        """The state in the reference layout [b, h, hu, (hv)], float64 (synchronizes)."""
+        if not self.fp32:
+            self.stream.synchronize()
+            return self.Q.clone()
+        out = torch.empty(self.Q.shape, dtype=_DTYPE, device=self.device)
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
+        _lib.check(_lib.lib().zfv_state_export(self._h, _ptr(self.Q), _ptr(self.scratch), _ptr(out),
+                                               self._s()), "zfv_state_export")
+        self.stream.synchronize()
+        return out
 
     def log(self) -> np.ndarray:
         """(steps, 3) array of (dt, time, mass) per completed step (last 4096 kept)."""
