@@ -204,10 +204,22 @@ struct RunnerT final : Runner {
     RunnerT* r; double* Q; double* Q1; char* scratch; int n; cudaStream_t s; bool sbed;
     template <int O, bool W, bool I> int operator()() {
         bool in_q1 = false;
+        const bool mood = r->mood();
+        double* Q2 = mood ? r->stage2(scratch) : nullptr;
         for (int k = 0; k < n; ++k) {
             if constexpr (O == 2) {
                 r->template launch<2, zfv::MODE_S1, W, I>(Q, Q, nullptr, Q1, scratch, s);
-                r->template launch<2, zfv::MODE_S2, W, I>(Q1, Q, Q, Q, scratch, s);
+                if (!mood) {
+                    r->template launch<2, zfv::MODE_S2, W, I>(Q1, Q, Q, Q, scratch, s);
+                } else {
+                    // ZoomyAmr.cpp:699-720: candidate, then commit or whole-step order-1 redo
+                    r->template launch<2, zfv::MODE_S2M, W, I>(Q1, Q, Q, Q2, scratch, s);
+                    const int nb = int((r->L.plane + kReduceNT - 1) / kReduceNT);
+                    zfv::k_mood_commit<Model, Numerics, kReduceNT><<<nb, kReduceNT, 0, s>>>(
+                        Q2, Q, r->L, r->st(scratch), r->partials(scratch), r->log3(scratch), kLogCap);
+                    r->template launch<1, zfv::MODE_R1, W, I>(Q, Q, nullptr, Q1, scratch, s);
+                    r->template launch<1, zfv::MODE_R2, W, I>(Q1, Q, Q, Q, scratch, s);
+                }
             } else {
                 double* src = in_q1 ? Q1 : Q;
                 double* dst = in_q1 ? Q : Q1;

@@ -166,214 +166,11 @@ __device__ __forceinline__ void manning_implicit(T h, T u, T v, T hinv, T dt, T 
 
 enum Mode { S1 = 1, S2 = 2 };
 
-template <int TX, int TY, int ORDER>
-struct Shape {
-    static constexpr int G = (ORDER == 2) ? 2 : 1;
-    static constexpr int RW = TX + 2 * G, RH = TY + 2 * G, NT = TX * TY;
-    static constexpr size_t q_elems = size_t(4) * RH * RW;
-    static constexpr size_t fx_elems = size_t(TY) * (TX + 1) * NFC;
-    static constexpr size_t fy_elems = size_t(TY + 1) * TX * NFC;
-    static constexpr size_t smem_bytes = (q_elems + fx_elems + fy_elems) * sizeof(float);
-};
+}  // namespace zfv32
 
-// One SSP-RK2 stage on a TX x TY tile.
-//  S1: state X (eta, hu, hv planes) + bed -> writes inc1 = the stage-1 increment.
-//  S2: stage state X + inc1 -> writes Y = FP32 part of Q^{n+1}, lo in place;
-//      reduction for the next dt and the mass.
-template <int ORDER, int MODE, bool WB, bool IMPL, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY, 3)
-k32_stage(const float* __restrict__ bed, const float* __restrict__ X, const float* __restrict__ inc_in,
-          float* __restrict__ inc_out, float* __restrict__ Y, float* __restrict__ lo, Params L,
-          zfv::DevState* st, double* __restrict__ partials, double* __restrict__ log3, int log_cap)
-{
-    using Sh = Shape<TX, TY, ORDER>;
-    constexpr int G = Sh::G, RW = Sh::RW, RH = Sh::RH, NT = Sh::NT;
-    extern __shared__ __align__(16) float smf[];
-    float* sB = smf;
-    float* sE = sB + RH * RW;
-    float* sU = sE + RH * RW;
-    float* sV = sU + RH * RW;
-    float* sFx = smf + Sh::q_elems;
-    float* sFy = sFx + Sh::fx_elems;
-    __shared__ double red[2 * ((NT + 31) / 32)];
+#include "fv32_sweep.cuh"
 
-    const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int nx = L.nx, ny = L.ny;
-    const long long plane = L.plane;
-
-    if (*(volatile unsigned*)&st->flags & zfv::kFlagDone) {
-        if constexpr (MODE == S2) {   // keep the state in the output buffer of this step
-            for (int k = tid; k < TX * TY; k += NT) {
-                const int i = x0 + k % TX, j = y0 + k / TX;
-                if (i < nx && j < ny) {
-                    const long long c = (long long)j * nx + i;
-                    Y[c] = X[c]; Y[plane + c] = X[plane + c]; Y[2 * plane + c] = X[2 * plane + c];
-                }
-            }
-        }
-        return;
-    }
-    const double dtd = *(volatile double*)&st->dt;
-    const double time = *(volatile double*)&st->time;
-    const float dt = float(dtd);
-
-    // 1. tile + halo (stage-2 state = X + inc1)
-    for (int k = tid; k < RW * RH; k += NT) {
-        const int lx = k % RW, ly = k / RW;
-        const int gi = x0 - G + lx, gj = y0 - G + ly;
-        if (gi >= 0 && gi < nx && gj >= 0 && gj < ny) {
-            const long long c = (long long)gj * nx + gi;
-            float e = X[c], u = X[plane + c], v = X[2 * plane + c];
-            if constexpr (MODE == S2) {
-                e += inc_in[c]; u += inc_in[plane + c]; v += inc_in[2 * plane + c];
-            }
-            sB[ly * RW + lx] = bed[c];
-            sE[ly * RW + lx] = e;
-            sU[ly * RW + lx] = u;
-            sV[ly * RW + lx] = v;
-        }
-    }
-    __syncthreads();
-
-    // 2. ghost frame: mirror + boundary condition (extrapolation / wall)
-    const bool edge = (x0 - G < 0) || (x0 + TX + G > nx) || (y0 - G < 0) || (y0 + TY + G > ny);
-    if (edge) {
-        for (int k = tid; k < RW * RH; k += NT) {
-            const int lx = k % RW, ly = k / RW;
-            const int gi = x0 - G + lx, gj = y0 - G + ly;
-            if (gi >= 0 && gi < nx && gj >= 0 && gj < ny) continue;
-            if (gi < -G || gi > nx - 1 + G || gj < -G || gj > ny - 1 + G) continue;
-            const zfv::GhostMap<2> gm = zfv::ghost_map<2>(gi, gj, nx, ny);
-            if (gm.bc_side < 0) continue;
-            const int mx = gm.ii - x0 + G, my = gm.jj - y0 + G;
-            if (mx < 0 || mx >= RW || my < 0 || my >= RH) continue;
-            const int src = my * RW + mx, dst = ly * RW + lx;
-            float u = sU[src], v = sV[src];
-            if (L.bc_tag[gm.bc_side] == 1) {   // wall: reflect the normal momentum
-                const float n0 = (gm.normal_dir == 0) ? float(gm.normal_sign) : 0.0f;
-                const float n1 = (gm.normal_dir == 1) ? float(gm.normal_sign) : 0.0f;
-                const float un = u * n0 + v * n1;
-                u = u - 2.0f * un * n0;
-                v = v - 2.0f * un * n1;
-            }
-            sB[dst] = sB[src]; sE[dst] = sE[src]; sU[dst] = u; sV[dst] = v;
-        }
-        __syncthreads();
-    }
-
-    const int tx = tid % TX, ty = tid / TX;
-    const int i = x0 + tx, j = y0 + ty;
-    const int iend = min(x0 + TX, nx), jend = min(y0 + TY, ny);
-    auto ld = [&](int lx, int ly) {
-        const int o = ly * RW + lx;
-        return C4{sB[o], sE[o], sU[o], sV[o]};
-    };
-
-    // 3. faces, each once
-    if (j < jend) {
-        const int ly = ty + G;
-        auto xf = [&](int f, float* out) {
-            const int lx = f - x0 + G;
-            C4 LL{}, RR{};
-            if constexpr (ORDER == 2) { LL = ld(lx - 2, ly); RR = ld(lx + 1, ly); }
-            face<ORDER, 0, WB>(LL, ld(lx - 1, ly), ld(lx, ly), RR, L, out);
-        };
-        if (i <= iend) xf(i, sFx + (ty * (TX + 1) + tx) * NFC);
-        if (tx == TX - 1 && x0 + TX <= iend) xf(x0 + TX, sFx + (ty * (TX + 1) + TX) * NFC);
-    }
-    if (i < iend) {
-        const int lx = tx + G;
-        auto yf = [&](int f, float* out) {
-            const int ly = f - y0 + G;
-            C4 LL{}, RR{};
-            if constexpr (ORDER == 2) { LL = ld(lx, ly - 2); RR = ld(lx, ly + 1); }
-            face<ORDER, 1, WB>(LL, ld(lx, ly - 1), ld(lx, ly), RR, L, out);
-        };
-        if (j <= jend) yf(j, sFy + (ty * TX + tx) * NFC);
-        if (ty == TY - 1 && y0 + TY <= jend) yf(y0 + TY, sFy + (TY * TX + tx) * NFC);
-    }
-    __syncthreads();
-
-    // 4. assemble, update, implicit source, epilogue
-    double m_loc = 0.0, s_loc = 0.0;
-    if (i < nx && j < ny) {
-        const float* FxL = sFx + (ty * (TX + 1) + tx) * NFC;
-        const float* FxR = FxL + NFC;
-        const float* FyL = sFy + (ty * TX + tx) * NFC;
-        const float* FyR = FyL + TX * NFC;
-        const C4 q = ld(tx + G, ty + G);
-        const float h = q.e - q.b;
-        const float hinv = kp_hinv(h, L.eps);
-        // Flux difference and well-balancing bed source are summed BEFORE the
-        // 1/dx scaling: at rest they are exact negatives of each other, and
-        // summing first keeps that exact even when the scaling is fused (FMA).
-        float Ax[3], Ay[3];
-#pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            Ax[n] = -(FxR[n] - FxL[n]) - FxR[6 + n] - FxL[3 + n];
-            Ay[n] = -(FyR[n] - FyL[n]) - FyR[6 + n] - FyL[3 + n];
-        }
-        if constexpr (WB) {
-            Ax[1] += FxR[9] - FxL[10];   // P(h*_L at the right face) - P(h*_R at the left face)
-            Ay[2] += FyR[9] - FyL[10];
-        }
-        float r[3];
-#pragma unroll
-        for (int n = 0; n < 3; ++n) r[n] = Ax[n] * L.rdx + Ay[n] * L.rdy;
-        float inc_e = dt * r[0], inc_u = dt * r[1], inc_v = dt * r[2];
-        if constexpr (!IMPL) {   // explicit source
-            float du, dv;
-            const float m = fmaxf(h, L.hfloor);
-            const float k = L.g * L.nm * L.nm * zb::inv_cbrt_pos(m);
-            const float ux = q.u * hinv, uy = q.v * hinv;
-            const float sp = sqrtf(ux * ux + uy * uy);
-            du = dt * (L.g * L.ex * h - k * ux * sp);
-            dv = dt * (L.g * L.ey * h - k * uy * sp);
-            inc_u += du; inc_v += dv;
-        } else {   // point-implicit, linearised at the explicit update with the stage aux
-            const float he = h + inc_e, ue = q.u + inc_u, ve = q.v + inc_v;
-            if (he < kNearDry) {
-                double du, dv;
-                manning_implicit<double>(double(he), double(ue), double(ve), double(hinv), dtd,
-                                         L.gd, L.exd, L.eyd, L.nmd, L.hfloord, du, dv);
-                inc_u += float(du); inc_v += float(dv);
-            } else {
-                float du, dv;
-                manning_implicit<float>(he, ue, ve, hinv, dt, L.g, L.ex, L.ey, L.nm, L.hfloor, du, dv);
-                inc_u += du; inc_v += dv;
-            }
-        }
-        const long long c = (long long)j * nx + i;
-        if constexpr (MODE == S1) {
-            inc_out[c] = inc_e; inc_out[plane + c] = inc_u; inc_out[2 * plane + c] = inc_v;
-        } else {
-            // Heun with compensation: Q^{n+1} = (hi + lo) + (inc1 + inc2)/2 in FP64
-            const float i1e = inc_in[c], i1u = inc_in[plane + c], i1v = inc_in[2 * plane + c];
-            const double ne = (double(X[c]) + double(lo[c])) + 0.5 * (double(i1e) + double(inc_e));
-            const double nu = (double(X[plane + c]) + double(lo[plane + c])) + 0.5 * (double(i1u) + double(inc_u));
-            const double nv = (double(X[2 * plane + c]) + double(lo[2 * plane + c])) + 0.5 * (double(i1v) + double(inc_v));
-            const float he = float(ne), hu = float(nu), hv = float(nv);
-            Y[c] = he; Y[plane + c] = hu; Y[2 * plane + c] = hv;
-            lo[c] = float(ne - double(he));
-            lo[plane + c] = float(nu - double(hu));
-            lo[2 * plane + c] = float(nv - double(hv));
-            // CFL terms of the new state (ZoomyAmr.cpp:472-487) and its mass (FP64)
-            const float hn = he - q.b;
-            const float hin = kp_hinv(hn, L.eps);
-            const float c0 = sqrtf(L.g * fmaxf(hn, 0.0f));
-            const float evx = (fabsf(hu * hin) + c0) / L.fdx;
-            const float evy = (fabsf(hv * hin) + c0) / L.fdy;
-            float mm_ = 0.0f;
-            if (evx > mm_) mm_ = evx;
-            if (evy > mm_) mm_ = evy;
-            m_loc = double(mm_);
-            s_loc = ne - double(q.b);
-        }
-    }
-    if constexpr (MODE == S2)
-        zfv::finish_step<NT>(m_loc, s_loc, red, partials, log3, log_cap, st, L, dtd, time);
-}
+namespace zfv32 {
 
 // FP64 reference layout [b, h, hu, hv] -> FP32 [b, eta, hu, hv] + remainders.
 __global__ void k32_import(const double* __restrict__ Q64, float* __restrict__ Q, float* __restrict__ lo,
@@ -472,7 +269,7 @@ k32_reduce(const float* __restrict__ Q, const float* __restrict__ lo, const doub
 }
 
 // ---------------------------------------------------------------------------
-template <int TX, int TY>
+template <int NW, int CPT>
 struct Runner32 final : Runner {
     zfv_handle* h;
     Params L;
@@ -494,8 +291,8 @@ struct Runner32 final : Runner {
         for (int s = 0; s < 4; ++s) L.bc_tag[s] = c.bc_tag[s];
         L.cfl = c.cfl; L.dtmin = c.dtmin; L.dtmax = c.dtmax; L.time_end = c.time_end;
         L.max_step = c.max_step; L.cfl_dimension = c.cfl_dimension; L.cfl_degree_factor = c.cfl_degree_factor;
-        grid = dim3((c.nx + TX - 1) / TX, (c.ny + TY - 1) / TY, 1);
-        block = dim3(TX * TY, 1, 1);
+        grid = dim3((c.nx + 30) / 31, (c.ny + NW * CPT - 1) / (NW * CPT), 1);
+        block = dim3(32 * NW, 1, 1);
     }
 
     void layout(ScratchLayout& S) const override {
@@ -510,16 +307,11 @@ struct Runner32 final : Runner {
         S.total = S.lo + align_up(pb * 3);
     }
 
-    template <int O, int M, bool W, bool I>
-    static auto kfn() { return &k32_stage<O, M, W, I, TX, TY>; }
+    template <int M, bool W, bool I>
+    static auto kfn() { return &k32s_stage<2, M, W, I, NW, CPT>; }
 
     template <int O, bool W, bool I>
-    int setup_combo() {
-        const int smem = int(Shape<TX, TY, O>::smem_bytes);
-        int rc = cuda_check(cudaFuncSetAttribute(kfn<O, S1, W, I>(), cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "cudaFuncSetAttribute");
-        rc |= cuda_check(cudaFuncSetAttribute(kfn<O, S2, W, I>(), cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "cudaFuncSetAttribute");
-        return rc;
-    }
+    int setup_combo() { return 0; }
 
     template <class F>
     int with_combo(F&& f) {
@@ -586,14 +378,13 @@ struct Runner32 final : Runner {
 
     template <int O, bool W, bool I>
     void launch_step(float* Qf, float* Xs, float* Ys, char* scratch, cudaStream_t s) {
-        using Sh = Shape<TX, TY, O>;
         const float* bedp = Qf;
-        auto k1 = kfn<O, S1, W, I>();
-        k1<<<grid, block, Sh::smem_bytes, s>>>(bedp, Xs, nullptr, inc(scratch), nullptr, nullptr, L,
-                                                st(scratch), partials(scratch), log3(scratch), kLogCap);
-        auto k2 = kfn<O, S2, W, I>();
-        k2<<<grid, block, Sh::smem_bytes, s>>>(bedp, Xs, inc(scratch), nullptr, Ys, lo(scratch), L,
-                                                st(scratch), partials(scratch), log3(scratch), kLogCap);
+        auto k1 = kfn<S1, W, I>();
+        k1<<<grid, block, 0, s>>>(bedp, Xs, nullptr, inc(scratch), nullptr, nullptr, L,
+                                  st(scratch), partials(scratch), log3(scratch), kLogCap);
+        auto k2 = kfn<S2, W, I>();
+        k2<<<grid, block, 0, s>>>(bedp, Xs, inc(scratch), nullptr, Ys, lo(scratch), L,
+                                  st(scratch), partials(scratch), log3(scratch), kLogCap);
     }
 
     struct EvolveF {
@@ -639,5 +430,5 @@ struct Runner32 final : Runner {
 }  // namespace zfv32
 
 namespace zfvi {
-Runner* make_runner_fp32_swe2d(zfv_handle* h) { return new zfv32::Runner32<32, 8>(h); }
+Runner* make_runner_fp32_swe2d(zfv_handle* h) { return new zfv32::Runner32<4, 16>(h); }
 }
