@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="cells per side")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ensemble-steps", type=int, default=100,
+                    help="steps of the 256-box batched-vs-per-box comparison (0 = skip)")
     ap.add_argument("--err-steps", type=int, default=1000,
                     help="steps of the FP32-vs-FP64 depth-error study (0 = skip)")
     return ap.parse_args()
@@ -256,6 +258,102 @@ def time_form(precision, n, Q0, A0, K, W, local, ws, barrier, max_over_ranks):
     return ms, n * n * K * ws / (ms * 1e-3), st
 
 
+def time_fp32_batched(n, Q0, A0, K, W, local, ws, barrier, max_over_ranks):
+    """The FP32 form through the batch engine (a batch of one level), strip
+    shape picked by the autotuner; K device-driven steps. Returns
+    (ms, value, status, tuning)."""
+    import torch
+    from zoomy_amrex_b200._abi import ZFV_PREC_FP32
+    from zoomy_amrex_b200.autotune import tune
+    from zoomy_amrex_b200.batch import Batch
+    cfg = workload_config(n)
+    cfg.precision = ZFV_PREC_FP32
+    b = Batch([cfg], [Q0], [A0], device=f"cuda:{local}")
+    best, times = tune(b, steps=8, warmup=3)
+    b.load([Q0])                       # tuning advanced the state: start over
+    b.begin()
+    b.evolve(max(3, W))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(); torch.cuda.synchronize()
+    e0.record(b.stream)
+    b.evolve(K)
+    e1.record(b.stream)
+    torch.cuda.synchronize(); barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    st = b.status()[0]
+    b.close()
+    assert not st["done"] and np.isfinite(st["dt"]), st
+    from zoomy_amrex_b200.batch import tile_variants
+    shapes = tile_variants()
+    tuning = {"picked": {"warps": shapes[best][0], "rows_per_warp": shapes[best][1]},
+              "ms_per_step": {f"{shapes[v][0]}x{shapes[v][1]}": t for v, t in times.items()}}
+    return ms, n * n * K * ws / (ms * 1e-3), st, tuning
+
+
+def ensemble_bench(K, W, local, n_inst=256, seed=2027):
+    """256 independent dam breaks on uneven boxes (sides log-uniform in
+    [32, 512]): one CUDA graph of one SSP-RK2 step of the whole batch, replayed
+    K times, against launching the same FP32 kernels box by box (2 launches per
+    box per step)."""
+    import torch
+    from zoomy_amrex_b200.autotune import tune
+    from zoomy_amrex_b200.batch import Batch
+    from zoomy_amrex_b200.level import Level
+    from zoomy_amrex_b200.workloads import dam_break_ensemble
+    ens = dam_break_ensemble(n_inst, seed=seed)
+    cfgs, Q0s, A0s = zip(*ens)
+    cells = sum(c.nx * c.ny for c in cfgs)
+    dev = f"cuda:{local}"
+    b = Batch(cfgs, Q0s, A0s, device=dev)
+    best, times = tune(b, steps=8, warmup=3)
+    b.load(Q0s)
+    b.begin()
+    b.evolve(max(3, W))
+    b.capture(1)
+    b.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(b.stream)
+    for _ in range(K):
+        b.replay()
+    e1.record(b.stream)
+    torch.cuda.synchronize()
+    ms_b = e0.elapsed_time(e1)
+    st = b.status()
+    units = b.units
+    b.close()
+    assert all(np.isfinite(s["dt"]) and not s["done"] for s in st)
+
+    # box by box: every instance its own level, launched in turn each step
+    stream = torch.cuda.Stream(dev)
+    levels = [Level(c, q, a, device=dev, stream=stream) for c, q, a in ens]
+    for lev in levels:
+        lev.begin()
+    for _ in range(max(3, W)):
+        for lev in levels:
+            lev.evolve(1)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(K):
+        for lev in levels:
+            lev.evolve(1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_p = e0.elapsed_time(e1)
+    for lev in levels:
+        lev.close()
+    return {"workload": f"{n_inst} SWE2D dam breaks, sides log-uniform [32,512] (seed {seed}), "
+                        f"own bumps, ratio U(1.2,3.0), walls, Manning 0.03, FP32 form",
+            "cells": cells, "units": units, "steps": K,
+            "batched_graph": {"value": cells * K / (ms_b * 1e-3), "ms_per_step": ms_b / K,
+                              "gpu_launches_per_step": 2},
+            "per_box": {"value": cells * K / (ms_p * 1e-3), "ms_per_step": ms_p / K,
+                        "gpu_launches_per_step": 2 * n_inst},
+            "speedup": ms_p / ms_b,
+            "strip_shape_ms_per_step": {str(v): t for v, t in times.items()}, "picked_variant": best}
+
+
 def depth_error(n, Q0, A0, steps, local):
     """FP32 chosen form vs FP64 plain form after `steps` steps from the same
     state. The FP64 GPU form equals the CPU oracle bitwise (tests/test_gpu_parity.py),
@@ -323,7 +421,8 @@ def main():
 
     with Clocks(local) as clk:
         ms64, v64, _ = time_form(ZFV_PREC_FP64, n, Q0, A0, K, args.warmup, local, ws, barrier, max_over_ranks)
-        ms32, v32, _ = time_form(ZFV_PREC_FP32, n, Q0, A0, K, args.warmup, local, ws, barrier, max_over_ranks)
+        ms32, v32, _, tuning = time_fp32_batched(n, Q0, A0, K, args.warmup, local, ws, barrier,
+                                                 max_over_ranks)
     peak, peak_kind = measured_peak()
     step32 = ms32 * 1e-3 / K
     step64 = ms64 * 1e-3 / K
@@ -333,11 +432,15 @@ def main():
                else NCU_TRAFFIC_PER_CELL_STEP_FP32 * cells / 2)
     roofline = {"bound": "hbm", "achieved": achieved32, "peak": peak, "unit": "GB/s",
                 "frac": achieved32 / peak, "traffic": traffic, "peak_source": peak_kind,
-                "kernel": "k32_stage (FP32 chosen form; stage-1 + stage-2 launches per step)",
+                "kernel": "k32b_stage (FP32 chosen form; stage-1 + stage-2 launches per step)",
                 "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_FP32, "traffic_per": "launch",
                 "fp64_plain": {"achieved": achieved64, "frac": achieved64 / peak,
                                "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_FP64,
                                "bound": "fp64 alu"}}
+
+    ens = None
+    if args.ensemble_steps > 0:
+        ens = ensemble_bench(args.ensemble_steps, args.warmup, local)
 
     err = None
     if args.err_steps > 0 and rank == 0:
@@ -399,6 +502,7 @@ def main():
                 "forms": {"fp32_chosen": v32, "fp64_plain": v64, "fp32_over_fp64": v32 / v64,
                           "ms_per_step_fp32": ms32 / K, "ms_per_step_fp64": ms64 / K},
                 "depth_error_fp32_vs_fp64": err,
+                "autotune": tuning, "ensemble": ens,
                 "hbm_gbs": achieved32,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 2 * K, "clocks": clk.summary()}

@@ -17,9 +17,12 @@
  *    ghost cells are never stored; they are rebuilt inside each kernel's
  *    tile load (mirror + Model::boundary_conditions).
  *  - Element type of Q: double for ZFV_PREC_FP64; float for ZFV_PREC_FP32,
- *    whose rows are [b, eta = h + b, hu, hv] (use zfv_state_import/export to
- *    convert from/to the reference layout [b, h, hu, hv] in FP64). aux is
- *    always double.
+ *    whose rows are [b, eta = h + b, hu, hv]. An FP32 state ping-pongs
+ *    between Q rows 1..3 and a scratch buffer from step to step (the buffer
+ *    in use is recorded on the device), so FP32 states are read only through
+ *    zfv_state_export / zfv_batch_export, which convert to the reference
+ *    layout [b, h, hu, hv] in FP64 and refresh aux's hinv row. aux is always
+ *    double.
  *  - All device work is enqueued on the given stream (cudaStream_t passed as
  *    void*; NULL = legacy default stream). Functions never synchronize unless
  *    their comment says so.
@@ -185,7 +188,10 @@ int zfv_fill_ghosts(zfv_handle* h, const void* Q, const void* aux, void* Qg, voi
  * Convert between the reference layout (Q64: [b, h, hu, (hv)] float64) and a
  * handle's state Q. FP64 handles copy. FP32 handles split eta = h + b, hu, hv
  * into a float part in Q and a float remainder in scratch (the compensation
- * planes), so the FP64 input is carried to ~48 bits; export recombines them.
+ * planes), so the FP64 input is carried to ~48 bits; export recombines them
+ * and writes aux's last row (hinv) for the exported state, the refresh that
+ * FP64 handles do at the end of every zfv_evolve (FP32 stages evaluate hinv
+ * from the face states and never read it).
  * zfv_state_import must precede zfv_begin for FP32 handles.
  */
 int zfv_state_import(zfv_handle* h, const double* Q64, void* Q, void* scratch, void* stream);
@@ -208,6 +214,85 @@ int zfv_get_status(zfv_handle* h, const void* scratch, zfv_status* out, void* st
 int zfv_log_capacity(const zfv_handle* h);
 int zfv_read_log(zfv_handle* h, const void* scratch, double* out3, int max_entries,
                  int64_t* first_step, int* n_out, void* stream);
+
+/*
+ * Batches: many independent FP32 SWE2D levels (the boxes of an AMR level or
+ * the members of an ensemble; each with its own grid, bathymetry, parameters,
+ * boundary conditions, dt, time and stop test) advanced together, one launch
+ * per RK stage for all of them. Replaces the per-box launches of the
+ * reference's MFIter loops (ZoomyAmr.cpp:579-637, one ParallelFor per box per
+ * kernel) for the case where the boxes are independent runs.
+ * All instances must be ZFV_MODEL_SWE2D / ZFV_PREC_FP32 / spatial_order 2 and
+ * share well_balanced and implicit_source.
+ *
+ * zfv_batch_bind registers each instance's Q (4 float planes [b, eta, hu, hv])
+ * and aux (double planes) and the caller's scratch, and uploads the work list
+ * (synchronizes the stream). The bound buffers are used by every later call;
+ * zfv_batch_begin / zfv_batch_evolve enqueue work without synchronizing and can
+ * be captured in a CUDA graph.
+ */
+typedef struct zfv_batch zfv_batch;
+int zfv_batch_create(const zfv_config* cfgs, int n_inst, zfv_batch** out);
+int zfv_batch_destroy(zfv_batch* b);
+size_t zfv_batch_scratch_bytes(const zfv_batch* b);
+int zfv_batch_bind(zfv_batch* b, void* const* Q, double* const* aux, void* scratch, void* stream);
+/* FP64 reference layout [b, h, hu, hv] <-> the bound FP32 states (synchronizes).
+ * Export also refreshes each instance's aux hinv row; a NULL Q64[k] refreshes
+ * only that. */
+int zfv_batch_import(zfv_batch* b, const double* const* Q64, void* stream);
+int zfv_batch_export(zfv_batch* b, double* const* Q64, void* stream);
+/* zfv_begin for every instance (time 0, first dt from the stored aux). */
+int zfv_batch_begin(zfv_batch* b, void* stream);
+/* n_steps SSP-RK2 steps of every instance (an instance past its stop test idles):
+ * exactly two kernel launches per step, whatever the step count before, so a
+ * graph captured from a one-step call can be replayed any number of times. */
+int zfv_batch_evolve(zfv_batch* b, int n_steps, void* stream);
+/* Status records of all instances into out[n_inst] (synchronizes). */
+int zfv_batch_status(zfv_batch* b, zfv_status* out, void* stream);
+/* Work units of the current strip shape. */
+int zfv_batch_units(const zfv_batch* b);
+/*
+ * Strip shapes compiled into the library: (warps per block, cells per thread
+ * in y). zfv_tile_variants writes up to max_n of them and returns how many
+ * exist; zfv_batch_set_variant selects one (the autotuner in
+ * zoomy_amrex_b200/autotune.py measures them and caches the fastest per n_dof_q).
+ */
+int zfv_tile_variants(int* nw, int* cpt, int max_n);
+int zfv_batch_set_variant(zfv_batch* b, int variant, void* stream);
+
+/*
+ * Run record save / restore: the device-side time, dt, step and flags of a
+ * handle's run (zfv_run_state_bytes() bytes, device to device, async). With
+ * the state Q this is everything a run needs to continue: the checkpoint of
+ * the adjoint's checkpoint-and-recompute.
+ */
+size_t zfv_run_state_bytes(void);
+int zfv_save_run_state(zfv_handle* h, const void* scratch, void* dst, void* stream);
+int zfv_load_run_state(zfv_handle* h, void* scratch, const void* src, void* stream);
+
+/*
+ * Adjoint of the FP64 ZFV_MODEL_SWE2D step (spatial_order 2, no clamp, no
+ * MOOD). No counterpart in the reference, which has no derivatives; it
+ * differentiates exactly the map zfv_evolve applies, dt included:
+ *   Y1 = stage(Q^n), Y2 = stage(Y1), Q^{n+1} = (Q^n + Y2)/2, stage = explicit
+ *   flux update then point-implicit source (ZoomyAmr.cpp:538-731,
+ *   make_rhs.H:31-509), dt_n = cfl/(d (2k+1) max_inv(Q^n)) (ZoomyAmr.cpp:448-515).
+ * zfv_adj_record runs n_steps steps exactly as zfv_evolve does (same kernels,
+ * same results) and writes what the reverse needs onto `tape`
+ * (zfv_adj_tape_bytes(h, n_steps) bytes, caller-allocated, device). The run
+ * must not reach its stop test inside the recorded steps.
+ * zfv_adj_step reverses recorded step k: on entry lam (n_q planes, like Q)
+ * holds dL/dQ^{k+1}, on exit dL/dQ^k; grad[0] += dL/dn_m (Manning
+ * coefficient), grad[1] += dL/ddt_k (diagnostic). aux0: the aux whose hinv row
+ * the run's first dt was computed from (pass it for the run's first step, NULL
+ * otherwise: later dts use the state's own hinv). work: zfv_adj_work_bytes(h)
+ * bytes, zero-filled before first use. Neither call synchronizes.
+ */
+size_t zfv_adj_tape_bytes(const zfv_handle* h, int n_steps);
+size_t zfv_adj_work_bytes(const zfv_handle* h);
+int zfv_adj_record(zfv_handle* h, void* Q, void* aux, void* scratch, void* tape, int n_steps, void* stream);
+int zfv_adj_step(zfv_handle* h, const void* tape, int k, void* lam, double* grad, const void* aux0,
+                 void* work, void* stream);
 
 /*
  * zfv_evolve without caller-provided scratch. No counterpart in the reference

@@ -1,0 +1,122 @@
+"""The FP32 batch engine: many independent levels, one launch per stage.
+
+A batch advances every instance exactly as a single FP32 level with the same
+configuration would (the same kernels on the same strips), so per-instance
+results are compared bitwise with single-level runs; the single levels are
+checked against the FP64 oracle in test_gpu_chosen.py.
+"""
+import numpy as np
+import pytest
+
+from zoomy_amrex_b200.workloads import dam_break_ensemble, fp64_twin
+
+pytestmark = pytest.mark.gpu
+
+
+def _single(cfg, Q0, A0, steps_chunk=16):
+    from zoomy_amrex_b200.level import Level
+    lev = Level(cfg, Q0, A0)
+    try:
+        st = lev.run(chunk=steps_chunk)
+        return lev.state64().cpu().numpy(), lev.aux.cpu().numpy(), st, lev.log()
+    finally:
+        lev.close()
+
+
+def _ens(n, seed, side_range=(24, 160), **kw):
+    return dam_break_ensemble(n, seed=seed, side_range=side_range, **kw)
+
+
+def test_batch_equals_single_levels(cuda):
+    """Uneven boxes, own bathymetry / dam ratio / friction / stop step."""
+    from zoomy_amrex_b200.batch import Batch
+    ens = _ens(6, seed=1)
+    for k, (cfg, _, _) in enumerate(ens):
+        cfg.max_step = 20 + 7 * k           # instances stop at different steps
+        cfg.params[3] = 0.01 * (k + 1)      # own Manning n
+    cfgs, Q0s, A0s = zip(*ens)
+    b = Batch(cfgs, Q0s, A0s, variant=0)   # the strip shape of a single FP32 level
+    st = b.run(chunk=16)
+    Qb = [q.cpu().numpy() for q in b.state64()]
+    Ab = [a.cpu().numpy() for a in b.aux]
+    b.close()
+    for k, (cfg, Q0, A0) in enumerate(ens):
+        Qs, As, ss, _ = _single(cfg, Q0, A0)
+        assert st[k]["step"] == ss["step"] == cfg.max_step
+        assert st[k]["time"] == ss["time"]
+        assert np.array_equal(Qb[k], Qs), k
+        assert np.array_equal(Ab[k], As), k
+
+
+def test_batch_graph_replay_equals_eager(cuda):
+    from zoomy_amrex_b200.batch import Batch
+    ens = _ens(5, seed=2)
+    cfgs, Q0s, A0s = zip(*ens)
+    a = Batch(cfgs, Q0s, A0s, variant=0)
+    a.begin(); a.evolve(24)
+    Qa = [q.cpu().numpy() for q in a.state64()]
+    sa = a.status()
+    a.close()
+    g = Batch(cfgs, Q0s, A0s, variant=0)
+    g.begin()
+    g.capture(8)
+    for _ in range(3):
+        g.replay()
+    Qg = [q.cpu().numpy() for q in g.state64()]
+    sg = g.status()
+    g.close()
+    for k in range(len(ens)):
+        assert sa[k]["step"] == sg[k]["step"] == 24
+        assert sa[k]["time"] == sg[k]["time"]
+        assert np.array_equal(Qa[k], Qg[k])
+
+
+def test_batch_strip_variants_agree(cuda):
+    """Every compiled strip shape computes the same cell values; only the
+    order of the per-strip mass partial sums differs."""
+    from zoomy_amrex_b200.batch import Batch, tile_variants
+    ens = _ens(4, seed=3, side_range=(40, 300))
+    cfgs, Q0s, A0s = zip(*ens)
+    ref = None
+    for v in range(len(tile_variants())):
+        b = Batch(cfgs, Q0s, A0s, variant=v)
+        b.begin(); b.evolve(30)
+        Q = [q.cpu().numpy() for q in b.state64()]
+        st = b.status()
+        b.close()
+        if ref is None:
+            ref = (Q, st)
+            continue
+        for k in range(len(ens)):
+            assert st[k]["time"] == ref[1][k]["time"]
+            assert np.array_equal(Q[k], ref[0][k]), (v, k)
+            assert abs(st[k]["mass"] - ref[1][k]["mass"]) <= 1e-13 * abs(ref[1][k]["mass"])
+
+
+def test_batch_depth_error_vs_fp64(cuda, oracle):
+    """Batch members against the FP64 oracle (L1 depth, 60 steps)."""
+    from zoomy_amrex_b200.batch import Batch
+    ens = _ens(3, seed=5, side_range=(32, 96), max_step=60)
+    cfgs, Q0s, A0s = zip(*ens)
+    b = Batch(cfgs, Q0s, A0s)
+    st = b.run(chunk=32)
+    Qb = [q.cpu().numpy() for q in b.state64()]
+    b.close()
+    for k, (cfg, Q0, A0) in enumerate(ens):
+        Qo, _, n, t, _, _ = oracle.run(fp64_twin(cfg), Q0, A0)
+        assert st[k]["step"] == n == 60
+        assert abs(st[k]["time"] - t) <= 1e-6 * t
+        dh = np.abs(Qb[k][1] - Qo[1])
+        print(f"[batch vs fp64 oracle] {cfg.nx}x{cfg.ny}: L1 {dh.mean():.3e} Linf {dh.max():.3e}")
+        assert dh.mean() <= 1e-5     # the FP32 form's L1 depth bound
+        assert dh.max() <= 1e-3
+
+
+def test_batch_rejects_mixed_schemes(cuda):
+    from zoomy_amrex_b200 import _lib
+    from zoomy_amrex_b200.batch import Batch
+    ens = _ens(2, seed=6)
+    ens[1][0].implicit_source = 0
+    cfgs, Q0s, A0s = zip(*ens)
+    with pytest.raises(_lib.ZfvError, match="share well_balanced"):
+        Batch(cfgs, Q0s, A0s)

@@ -17,7 +17,12 @@ _lib = None
 SYMBOLS = ("zfv_last_error", "zfv_version", "zfv_sizeof_config", "zfv_sizeof_status", "zfv_model_info", "zfv_create", "zfv_destroy",
            "zfv_scratch_bytes", "zfv_begin", "zfv_update_state", "zfv_compute_dt", "zfv_evolve",
            "zfv_rhs", "zfv_fill_ghosts", "zfv_total_mass", "zfv_get_status", "zfv_log_capacity",
-           "zfv_read_log", "zfv_evolve_static", "zfv_state_import", "zfv_state_export")
+           "zfv_read_log", "zfv_evolve_static", "zfv_state_import", "zfv_state_export",
+           "zfv_batch_create", "zfv_batch_destroy", "zfv_batch_scratch_bytes", "zfv_batch_bind",
+           "zfv_batch_import", "zfv_batch_export", "zfv_batch_begin", "zfv_batch_evolve",
+           "zfv_batch_status", "zfv_batch_units", "zfv_tile_variants", "zfv_batch_set_variant",
+           "zfv_run_state_bytes", "zfv_save_run_state", "zfv_load_run_state", "zfv_adj_tape_bytes",
+           "zfv_adj_work_bytes", "zfv_adj_record", "zfv_adj_step")
 
 
 class ZfvError(RuntimeError):
@@ -54,7 +59,30 @@ def lib():
     L.zfv_read_log.argtypes = [vp, vp, C.POINTER(d), i, C.POINTER(C.c_int64), C.POINTER(i), vp]
     L.zfv_state_import.argtypes = [vp, vp, vp, vp, vp]
     L.zfv_state_export.argtypes = [vp, vp, vp, vp, vp]
+    pp = C.POINTER(C.c_void_p)
+    L.zfv_batch_create.argtypes = [C.POINTER(zfv_config), i, C.POINTER(vp)]
+    L.zfv_batch_destroy.argtypes = [vp]
+    L.zfv_batch_scratch_bytes.argtypes = [vp]
+    L.zfv_batch_scratch_bytes.restype = C.c_size_t
+    L.zfv_batch_bind.argtypes = [vp, pp, pp, vp, vp]
+    L.zfv_batch_import.argtypes = [vp, pp, vp]
+    L.zfv_batch_export.argtypes = [vp, pp, vp]
+    L.zfv_batch_begin.argtypes = [vp, vp]
+    L.zfv_batch_evolve.argtypes = [vp, i, vp]
+    L.zfv_batch_status.argtypes = [vp, C.POINTER(zfv_status), vp]
+    L.zfv_batch_units.argtypes = [vp]
+    L.zfv_tile_variants.argtypes = [C.POINTER(i), C.POINTER(i), i]
+    L.zfv_batch_set_variant.argtypes = [vp, i, vp]
     L.zfv_evolve_static.argtypes = [vp, vp, vp, i, i, C.POINTER(zfv_status), vp]
+    L.zfv_run_state_bytes.restype = C.c_size_t
+    L.zfv_save_run_state.argtypes = [vp, vp, vp, vp]
+    L.zfv_load_run_state.argtypes = [vp, vp, vp, vp]
+    L.zfv_adj_tape_bytes.argtypes = [vp, i]
+    L.zfv_adj_tape_bytes.restype = C.c_size_t
+    L.zfv_adj_work_bytes.argtypes = [vp]
+    L.zfv_adj_work_bytes.restype = C.c_size_t
+    L.zfv_adj_record.argtypes = [vp, vp, vp, vp, vp, i, vp]
+    L.zfv_adj_step.argtypes = [vp, vp, i, vp, vp, vp, vp, vp]
     _lib = L
     return L
 

@@ -24,9 +24,12 @@ INCLUDE = PKG.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # (source, extra flags): the FP64 plain form keeps FMA contraction off so its
-# arithmetic is bitwise the CPU build's; the FP32 chosen form uses FMA.
+# arithmetic is bitwise the CPU build's; the FP32 chosen form uses FMA and the
+# hardware's approximate FP32 division / square root (its FP64 parts are
+# unaffected by these flags); the adjoint (FP64, checked to tolerances) uses FMA.
 SOURCES = [("zoomy_fv.cu", ["--fmad=false"]),
-           ("zoomy_fv32.cu", ["--fmad=true"])]
+           ("zoomy_fv32.cu", ["--fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
+           ("zoomy_adj.cu", ["--fmad=true"])]
 
 
 def nvcc() -> str:

@@ -1,35 +1,32 @@
-// FP32 chosen form: the warp column-sweep stage kernel.
+// FP32 chosen form: the warp column-sweep stage.
 //
-// Work unit = a strip of 31 owned columns x (NW * CPT) rows. One warp per
-// 31 x CPT sub-strip; lane L holds column x0 + L (lane 31 holds the first
-// column of the next strip, needed only as stencil input and for the right
-// face of lane 30's cell). Each lane walks its CPT rows upward keeping a
-// four-row register window of its column (the y-stencil of MUSCL needs rows
-// j-2..j+1), takes the x-stencil of row j from its neighbours by warp
-// shuffles, and evaluates
-//   * the x-face on its left (the right face of its left neighbour arrives
-//     by a shuffle, so every x-face is evaluated once, 1/32 redundant), and
-//   * the y-face above its cell (the face below is carried over from the
-//     previous row in registers),
-// then assembles its cell. No shared memory and no barriers in the sweep.
+// Work unit ("strip") = 30 owned columns x (NW * CPT) rows, one warp per
+// 30 x CPT sub-strip. Lane L holds column x0 - 1 + L (lanes 1..30 own their
+// column; lane 0 and lane 31 hold the neighbour columns x0 - 1 and x0 + 30).
+// Each lane walks its CPT rows upward and, per row j,
+//   * reconstructs its cell once in x (MUSCL/minmod slopes of b, h, hu, hv,
+//     make_rhs.H:57-75, with the slope of h taken as d(eta) - d(b)) and once in
+//     y (for row j+1, from a register window of its column),
+//   * evaluates the x-face on its left from its left neighbour's right-face
+//     state (one shuffle) and its own left-face state, and the y-face above
+//     its cell from the carried top-face state of row j and the bottom-face
+//     state of row j+1,
+//   * receives the face on its right from lane+1 (one shuffle) and the face
+//     below from the previous row (registers), and assembles its cell.
+// Every face and every slope is evaluated once (plus 1/16 of the x work for
+// the two neighbour columns). No shared memory and no barriers in the sweep.
 //
-// Ghost cells (outside the domain) are produced by `fetch`: the mirror index
-// of ZoomyAmr::FillPhysicalBC_mf (ZoomyAmr.cpp:399-406) with the side's
-// boundary condition (extrapolation copies; a wall reverses the normal
-// momentum), x side first.
+// Ghost cells are produced by fetch(): the mirror index of
+// ZoomyAmr::FillPhysicalBC_mf (ZoomyAmr.cpp:399-406) with the side's boundary
+// condition (extrapolation copies; a wall reverses the normal momentum), x side
+// first; strips whose stencil lies inside the domain skip that logic.
 #pragma once
 
 namespace zfv32 {
 
-struct Strip {            // one work unit (a level may be an element of a batch)
-    int x0, y0;           // first owned column / row
-};
+// Reconstructed state of a cell at one of its faces.
+struct RS { float b, h, e, u, v; };
 
-// State of one cell for the stencil: bed, surface, momenta.
-__device__ __forceinline__ C4 shfl_c4(unsigned mask, const C4& v, int src) {
-    return C4{__shfl_sync(mask, v.b, src), __shfl_sync(mask, v.e, src),
-              __shfl_sync(mask, v.u, src), __shfl_sync(mask, v.v, src)};
-}
 __device__ __forceinline__ C4 shfl_up_c4(const C4& v, int d) {
     return C4{__shfl_up_sync(0xffffffffu, v.b, d), __shfl_up_sync(0xffffffffu, v.e, d),
               __shfl_up_sync(0xffffffffu, v.u, d), __shfl_up_sync(0xffffffffu, v.v, d)};
@@ -38,24 +35,100 @@ __device__ __forceinline__ C4 shfl_down_c4(const C4& v, int d) {
     return C4{__shfl_down_sync(0xffffffffu, v.b, d), __shfl_down_sync(0xffffffffu, v.e, d),
               __shfl_down_sync(0xffffffffu, v.u, d), __shfl_down_sync(0xffffffffu, v.v, d)};
 }
+__device__ __forceinline__ RS shfl_up_rs(const RS& v, int d) {
+    return RS{__shfl_up_sync(0xffffffffu, v.b, d), __shfl_up_sync(0xffffffffu, v.h, d),
+              __shfl_up_sync(0xffffffffu, v.e, d), __shfl_up_sync(0xffffffffu, v.u, d),
+              __shfl_up_sync(0xffffffffu, v.v, d)};
+}
 
-// Stage input of cell (i, j) with ghost handling. S2 reads the stage-2 state
-// X + inc1. Rows/columns more than 2 cells outside the domain are never
-// consumed; they are clamped to a valid address.
-template <int MODE>
+// Per-cell MUSCL reconstruction from (minus, centre, plus) neighbours along one
+// axis: lo = state at the cell's lower face, hi = at its upper face.
+__device__ __forceinline__ void reconstruct(const C4& m, const C4& c, const C4& p, RS& lo, RS& hi) {
+    const float dbm = c.b - m.b, dbp = p.b - c.b;
+    const float dem = c.e - m.e, dep = p.e - c.e;
+    const float gb = mm(dbm, dbp);
+    const float gh = mm(dem - dbm, dep - dbp);
+    const float gu = mm(c.u - m.u, p.u - c.u);
+    const float gv = mm(c.v - m.v, p.v - c.v);
+    const float h = c.e - c.b;
+    const float hb = 0.5f * gb, hh = 0.5f * gh, he = 0.5f * (gh + gb);
+    const float hu = 0.5f * gu, hv = 0.5f * gv;
+    hi = RS{c.b + hb, h + hh, c.e + he, c.u + hu, c.v + hv};
+    lo = RS{c.b - hb, h - hh, c.e - he, c.u - hu, c.v - hv};
+}
+
+struct FaceR {
+    float f0, f1, f2;      // central flux (h, hu, hv)
+    float dp0, dp1, dp2;   // D+
+    float dm0, dm1, dm2;   // D-
+    float pl, pr;          // P(h*_L), P(h*_R)
+};
+
+// One face from its reconstructed left/right states (make_rhs.H:77-131 from
+// the Audusse step on, with the model's flux and D+/- fluctuations).
+template <int DIR, bool WB>
+__device__ __forceinline__ FaceR face_rs(RS a, RS c, const Params& L) {
+    float db = 0.0f;
+    if constexpr (WB) {
+        const float bf = fmaxf(a.b, c.b);
+        const float hsL = fmaxf(0.0f, a.e - bf), hsR = fmaxf(0.0f, c.e - bf);
+        const float sL = (a.h > 0.0f) ? __fdividef(hsL, a.h) : 0.0f;
+        const float sR = (c.h > 0.0f) ? __fdividef(hsR, c.h) : 0.0f;
+        a.u *= sL; a.v *= sL; c.u *= sR; c.v *= sR;
+        a.h = hsL; c.h = hsR;
+    } else {
+        db = c.b - a.b;
+    }
+    const float g = L.g, hg = 0.5f * L.g;
+    const float hiL = kp_hinv(a.h, L.eps), hiR = kp_hinv(c.h, L.eps);
+    const float unL = (DIR == 0) ? a.u : a.v, unR = (DIR == 0) ? c.u : c.v;
+    const float pL = hg * a.h * a.h, pR = hg * c.h * c.h;
+    const float qL = unL * hiL, qR = unR * hiR;          // normal velocities
+    float fuL, fvL, fuR, fvR;
+    if constexpr (DIR == 0) {
+        fuL = a.u * qL + pL;  fvL = a.v * qL;
+        fuR = c.u * qR + pR;  fvR = c.v * qR;
+    } else {
+        fuL = a.u * qL;  fvL = a.v * qL + pL;
+        fuR = c.u * qR;  fvR = c.v * qR + pR;
+    }
+    FaceR F;
+    F.f0 = 0.5f * (unL + unR);
+    F.f1 = 0.5f * (fuL + fuR);
+    F.f2 = 0.5f * (fvL + fvR);
+    const float evL = fabsf(qL) + sqrtf(g * fmaxf(a.h, 0.0f));
+    const float evR = fabsf(qR) + sqrtf(g * fmaxf(c.h, 0.0f));
+    const float hs = 0.5f * fmaxf(evL, evR);
+    const float dh = c.h - a.h, du = c.u - a.u, dv = c.v - a.v;
+    float bu = 0.0f, bv = 0.0f;
+    if constexpr (!WB) {
+        const float Bn = 0.5f * g * (0.5f * (a.h + c.h)) * db;
+        if (DIR == 0) bu = Bn; else bv = Bn;
+    }
+    F.dp0 = hs * dh;       F.dm0 = -hs * dh;
+    F.dp1 = bu + hs * du;  F.dm1 = bu - hs * du;
+    F.dp2 = bv + hs * dv;  F.dm2 = bv - hs * dv;
+    F.pl = pL;
+    F.pr = pR;
+    return F;
+}
+
+// Stage input of cell (i, j). S2 reads the stage-2 state X + inc1.
+template <int MODE, bool INTERIOR>
 __device__ __forceinline__ C4 fetch(const float* __restrict__ bed, const float* __restrict__ X,
                                     const float* __restrict__ inc, const Params& L, int i, int j) {
-    const int nx = L.nx, ny = L.ny;
-    int ii = i, jj = j;
-    int side = -1;
-    if (i < 0) { ii = -1 - i; side = 0; }
-    else if (i > nx - 1) { ii = 2 * (nx - 1) + 1 - i; side = 1; }
-    if (j < 0) { jj = -1 - j; if (side < 0) side = 2; }
-    else if (j > ny - 1) { jj = 2 * (ny - 1) + 1 - j; if (side < 0) side = 3; }
-    ii = min(max(ii, 0), nx - 1);
-    jj = min(max(jj, 0), ny - 1);
-    const long long c = (long long)jj * nx + ii;
     const long long pl = L.plane;
+    int ii = i, jj = j, side = -1;
+    if constexpr (!INTERIOR) {
+        const int nx = L.nx, ny = L.ny;
+        if (i < 0) { ii = -1 - i; side = 0; }
+        else if (i > nx - 1) { ii = 2 * (nx - 1) + 1 - i; side = 1; }
+        if (j < 0) { jj = -1 - j; if (side < 0) side = 2; }
+        else if (j > ny - 1) { jj = 2 * (ny - 1) + 1 - j; if (side < 0) side = 3; }
+        ii = min(max(ii, 0), nx - 1);      // beyond the ghost frame: unused, keep in bounds
+        jj = min(max(jj, 0), ny - 1);
+    }
+    const long long c = (long long)jj * L.nx + ii;
     C4 q;
     q.b = __ldg(bed + c);
     q.e = __ldg(X + c);
@@ -66,101 +139,65 @@ __device__ __forceinline__ C4 fetch(const float* __restrict__ bed, const float* 
         q.u += __ldg(inc + pl + c);
         q.v += __ldg(inc + 2 * pl + c);
     }
-    if (side >= 0 && L.bc_tag[side] == 1) {   // wall: reverse the normal momentum
-        if (side < 2) q.u = -q.u;
-        else q.v = -q.v;
+    if constexpr (!INTERIOR) {
+        if (side >= 0 && L.bc_tag[side] == 1) {   // wall: reverse the normal momentum
+            if (side < 2) q.u = -q.u;
+            else q.v = -q.v;
+        }
     }
     return q;
 }
 
-// Face outputs kept in registers.
-struct FaceR {
-    float f0, f1, f2;      // central flux (h, hu, hv)
-    float dp0, dp1, dp2;   // D+
-    float dm0, dm1, dm2;   // D-
-    float pl, pr;          // P(h*_L), P(h*_R)
-};
-template <int ORDER, int DIR, bool WB>
-__device__ __forceinline__ FaceR face_r(const C4& LL, const C4& Lc, const C4& Rc, const C4& RR,
-                                        const Params& L) {
-    float F[NFC];
-    face<ORDER, DIR, WB>(LL, Lc, Rc, RR, L, F);
-    return FaceR{F[0], F[1], F[2], F[3], F[4], F[5], F[6], F[7], F[8], F[9], F[10]};
-}
-
-template <int ORDER, int MODE, bool WB, bool IMPL, int NW, int CPT>
-__global__ void __launch_bounds__(32 * NW)
-k32s_stage(const float* __restrict__ bed, const float* __restrict__ X, const float* __restrict__ inc_in,
-           float* __restrict__ inc_out, float* __restrict__ Y, float* __restrict__ lo, Params L,
-           zfv::DevState* st, double* __restrict__ partials, double* __restrict__ log3, int log_cap)
-{
-    static_assert(ORDER == 2, "the sweep kernel implements the order-2 (SSP-RK2) path");
-    constexpr int NT = 32 * NW;
-    __shared__ double red[2 * NW];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+// One warp's sub-strip: columns x0-1 .. x0+30 (owned x0 .. x0+29), rows j0 .. j0+CPT-1.
+// Accumulates this lane's CFL max and mass into m_loc / s_loc (stage 2).
+template <int MODE, bool WB, bool IMPL, int CPT, bool INTERIOR>
+__device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const float* __restrict__ X,
+                                            const float* __restrict__ inc_in, float* __restrict__ inc_out,
+                                            float* __restrict__ Y, float* __restrict__ lo, const Params& L,
+                                            int x0, int j0, float dt, double dtd, double& m_loc,
+                                            double& s_loc) {
+    const int lane = threadIdx.x & 31;
     const int nx = L.nx, ny = L.ny;
     const long long pl = L.plane;
-    const int x0 = blockIdx.x * 31;
-    const int i = x0 + lane;
-    const int j0 = blockIdx.y * (NW * CPT) + w * CPT;
+    const int i = x0 - 1 + lane;
+    const bool owns = (lane >= 1) && (lane <= 30) && (i < nx);
+    // extra x-neighbour of the edge lanes: lane 0 needs x0-2, lane 31 needs x0+31
+    const bool has_e = (lane == 0) || (lane == 31);
+    const int xe = (lane == 0) ? x0 - 2 : x0 + 31;
 
-    if (*(volatile unsigned*)&st->flags & zfv::kFlagDone) {
-        if constexpr (MODE == S2) {   // keep the state in this step's output buffer
-            if (lane < 31 && i < nx)
-                for (int r = 0; r < CPT; ++r) {
-                    const int j = j0 + r;
-                    if (j < ny) {
-                        const long long c = (long long)j * nx + i;
-                        Y[c] = X[c]; Y[pl + c] = X[pl + c]; Y[2 * pl + c] = X[2 * pl + c];
-                    }
-                }
-        }
-        return;
-    }
-    const double dtd = *(volatile double*)&st->dt;
-    const double time = *(volatile double*)&st->time;
-    const float dt = float(dtd);
+    // y window of this lane's column: rows j0-1, j0, j0+1 (raw) and the
+    // y-reconstruction of row j0 (its face states below and above)
+    C4 wm = fetch<MODE, INTERIOR>(bed, X, inc_in, L, i, j0 - 2);
+    C4 w0 = fetch<MODE, INTERIOR>(bed, X, inc_in, L, i, j0 - 1);
+    C4 w1 = fetch<MODE, INTERIOR>(bed, X, inc_in, L, i, j0);
+    C4 w2 = fetch<MODE, INTERIOR>(bed, X, inc_in, L, i, j0 + 1);
+    RS lo_m, hi_m, lo_0, hi_0;
+    reconstruct(wm, w0, w1, lo_m, hi_m);     // row j0-1
+    reconstruct(w0, w1, w2, lo_0, hi_0);     // row j0
+    FaceR fb = face_rs<1, WB>(hi_m, lo_0, L);   // face below row j0
+    RS top = hi_0;                           // row j0's state at its upper face
 
-    // column of the extra x-stencil value of this lane: lanes 0/1 hold x0-2 / x0-1,
-    // lane 31 holds x0+32 (the right neighbour of lane 31's column)
-    const int xe = (lane == 0) ? x0 - 2 : (lane == 1) ? x0 - 1 : x0 + 32;
-    const bool has_e = (lane <= 1) || (lane == 31);
-    // a lane whose column lies beyond the ghost frame only feeds unused values
-    const bool col_ok = (i <= nx + 1);
-    const bool owns = (lane < 31) && (i < nx);
-
-    // y window of this lane's column: rows j-2, j-1, j, j+1
-    C4 w0 = fetch<MODE>(bed, X, inc_in, L, i, j0 - 2);
-    C4 w1 = fetch<MODE>(bed, X, inc_in, L, i, j0 - 1);
-    C4 w2 = fetch<MODE>(bed, X, inc_in, L, i, j0);
-    C4 w3 = fetch<MODE>(bed, X, inc_in, L, i, j0 + 1);
-    // face below the first row (between rows j0-1 and j0)
-    FaceR fb = face_r<ORDER, 1, WB>(w0, w1, w2, w3, L);
-
-    double m_loc = 0.0, s_loc = 0.0;
 #pragma unroll 1
     for (int r = 0; r < CPT; ++r) {
         const int j = j0 + r;
-        if (j >= ny) break;                          // uniform across the warp
-        // slide the window: rows j-1 .. j+2
-        w0 = w1; w1 = w2; w2 = w3;
-        w3 = fetch<MODE>(bed, X, inc_in, L, i, j + 2);
-        // face above row j (between rows j and j+1): stencil rows j-1 .. j+2
-        const FaceR ft = face_r<ORDER, 1, WB>(w0, w1, w2, w3, L);
+        if (j >= ny) break;                  // uniform across the warp
+        // row j: w1; rows j-1, j+1: w0, w2; load row j+2
+        const C4 w3 = fetch<MODE, INTERIOR>(bed, X, inc_in, L, i, j + 2);
+        RS lo_1, hi_1;
+        reconstruct(w1, w2, w3, lo_1, hi_1);  // row j+1 in y
+        const FaceR ft = face_rs<1, WB>(top, lo_1, L);   // face above row j
 
-        // x-stencil of row j: own = w1 (row j of column i)
-        const C4 own = w1;
+        // x reconstruction of row j
         C4 ex{};
-        if (has_e) ex = fetch<MODE>(bed, X, inc_in, L, xe, j);
-        const C4 up1 = shfl_up_c4(own, 1), up2 = shfl_up_c4(own, 2), dn1 = shfl_down_c4(own, 1);
-        const C4 e1 = shfl_c4(0xffffffffu, ex, 1);   // x0-1, held by lane 1
-        const C4 cm1 = (lane == 0) ? e1 : up1;       // column i-1
-        const C4 cm2 = (lane <= 1) ? ex : up2;       // column i-2 (lane 0: x0-2, lane 1: x0-1)
-        const C4 cp1 = (lane == 31) ? ex : dn1;      // column i+1
-        // x-face on the left of column i: cells i-2, i-1 | i, i+1
-        const FaceR fl = face_r<ORDER, 0, WB>(cm2, cm1, own, cp1, L);
-        // the face on the right of column i is lane+1's left face
-        FaceR fr;
+        if (has_e) ex = fetch<MODE, INTERIOR>(bed, X, inc_in, L, xe, j);
+        const C4 left = (lane == 0) ? ex : shfl_up_c4(w1, 1);
+        const C4 dn = shfl_down_c4(w1, 1);
+        const C4 right = (lane == 31) ? ex : dn;
+        RS xlo, xhi;
+        reconstruct(left, w1, right, xlo, xhi);
+        const RS lhi = shfl_up_rs(xhi, 1);              // left neighbour's state at our left face
+        const FaceR fl = face_rs<0, WB>(lhi, xlo, L);   // face on the left of column i (lanes >= 1)
+        FaceR fr;                                       // face on the right: lane+1's left face
         fr.f0 = __shfl_down_sync(0xffffffffu, fl.f0, 1);
         fr.f1 = __shfl_down_sync(0xffffffffu, fl.f1, 1);
         fr.f2 = __shfl_down_sync(0xffffffffu, fl.f2, 1);
@@ -169,8 +206,8 @@ k32s_stage(const float* __restrict__ bed, const float* __restrict__ X, const flo
         fr.dm2 = __shfl_down_sync(0xffffffffu, fl.dm2, 1);
         fr.pl = __shfl_down_sync(0xffffffffu, fl.pl, 1);
 
-        if (owns && col_ok) {
-            // make_rhs.H:346-399 with the WB source folded before the 1/dx scaling
+        if (owns) {
+            // make_rhs.H:346-399, the WB bed source folded in before the 1/dx scaling
             float Ax0 = -(fr.f0 - fl.f0) - fr.dm0 - fl.dp0;
             float Ax1 = -(fr.f1 - fl.f1) - fr.dm1 - fl.dp1;
             float Ax2 = -(fr.f2 - fl.f2) - fr.dm2 - fl.dp2;
@@ -184,18 +221,18 @@ k32s_stage(const float* __restrict__ bed, const float* __restrict__ X, const flo
             const float r0 = Ax0 * L.rdx + Ay0 * L.rdy;
             const float r1 = Ax1 * L.rdx + Ay1 * L.rdy;
             const float r2 = Ax2 * L.rdx + Ay2 * L.rdy;
-            const float h = own.e - own.b;
+            const float h = w1.e - w1.b;
             const float hinv = kp_hinv(h, L.eps);
             float inc_e = dt * r0, inc_u = dt * r1, inc_v = dt * r2;
             if constexpr (!IMPL) {
                 const float mh = fmaxf(h, L.hfloor);
                 const float k = L.g * L.nm * L.nm * zb::inv_cbrt_pos(mh);
-                const float ux = own.u * hinv, uy = own.v * hinv;
+                const float ux = w1.u * hinv, uy = w1.v * hinv;
                 const float sp = sqrtf(ux * ux + uy * uy);
                 inc_u += dt * (L.g * L.ex * h - k * ux * sp);
                 inc_v += dt * (L.g * L.ey * h - k * uy * sp);
             } else {
-                const float he = h + inc_e, ue = own.u + inc_u, ve = own.v + inc_v;
+                const float he = h + inc_e, ue = w1.u + inc_u, ve = w1.v + inc_v;
                 if (he < kNearDry) {
                     double du, dv;
                     manning_implicit<double>(double(he), double(ue), double(ve), double(hinv), dtd,
@@ -211,6 +248,7 @@ k32s_stage(const float* __restrict__ bed, const float* __restrict__ X, const flo
             if constexpr (MODE == S1) {
                 inc_out[c] = inc_e; inc_out[pl + c] = inc_u; inc_out[2 * pl + c] = inc_v;
             } else {
+                // compensated Heun update in FP64: Q^{n+1} = (hi + lo) + (inc1 + inc2) / 2
                 const float i1e = __ldg(inc_in + c), i1u = __ldg(inc_in + pl + c), i1v = __ldg(inc_in + 2 * pl + c);
                 const float xe_ = __ldg(X + c), xu = __ldg(X + pl + c), xv = __ldg(X + 2 * pl + c);
                 const double ne = (double(xe_) + double(lo[c])) + 0.5 * (double(i1e) + double(inc_e));
@@ -221,22 +259,31 @@ k32s_stage(const float* __restrict__ bed, const float* __restrict__ X, const flo
                 lo[c] = float(ne - double(he));
                 lo[pl + c] = float(nu - double(hu));
                 lo[2 * pl + c] = float(nv - double(hv));
-                const float hn = he - own.b;
+                // CFL terms of the new state (ZoomyAmr.cpp:472-487) and its FP64 mass
+                const float hn = he - w1.b;
                 const float hin = kp_hinv(hn, L.eps);
                 const float c0 = sqrtf(L.g * fmaxf(hn, 0.0f));
-                const float evx = (fabsf(hu * hin) + c0) / L.fdx;
-                const float evy = (fabsf(hv * hin) + c0) / L.fdy;
+                const float evx = (fabsf(hu * hin) + c0) * L.rfdx;
+                const float evy = (fabsf(hv * hin) + c0) * L.rfdy;
                 float mm_ = 0.0f;
                 if (evx > mm_) mm_ = evx;
                 if (evy > mm_) mm_ = evy;
                 if (double(mm_) > m_loc) m_loc = double(mm_);
-                s_loc = s_loc + (ne - double(own.b));
+                s_loc = s_loc + (ne - double(w1.b));
             }
         }
-        fb = ft;   // the face above row j is the face below row j+1
+        // advance: row j+1 becomes the current row
+        fb = ft;
+        top = hi_1;
+        w0 = w1; w1 = w2; w2 = w3;
     }
-    if constexpr (MODE == S2)
-        zfv::finish_step<NT>(m_loc, s_loc, red, partials, log3, log_cap, st, L, dtd, time);
+}
+
+// Whether a strip's stencil (two ghost layers around its cells and its two
+// neighbour columns) lies inside the domain, so fetch needs no mirroring.
+template <int NW, int CPT>
+__device__ __forceinline__ bool strip_interior(const Params& L, int x0, int y0) {
+    return (x0 - 2 >= 0) && (x0 + 31 <= L.nx - 1) && (y0 - 2 >= 0) && (y0 + NW * CPT + 1 <= L.ny - 1);
 }
 
 }  // namespace zfv32

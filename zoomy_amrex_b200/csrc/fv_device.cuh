@@ -38,7 +38,8 @@ struct alignas(128) DevState {
     unsigned pad0[4];
     unsigned counter;       // last-block-done counter of the grid reductions
     unsigned troubled;      // MOOD: some cell of this step's order-2 candidate has h < 0 or non-finite
-    unsigned pad1[14];
+    unsigned parity;        // FP32 form: which ping-pong buffer holds the state (0 = Q, 1 = alt)
+    unsigned pad1[13];
 };
 static_assert(sizeof(DevState) == 128, "DevState layout");
 

@@ -86,12 +86,29 @@ __device__ __forceinline__ void block_reduce_max_sum(double& m, double& s, doubl
 // Every block writes (max, sum) to partials[blk]; the last block to finish
 // reduces them in block order and advances the run state.
 template <int NT, class PL>
+__device__ __forceinline__ bool finish_step_units(double m, double s, double* red, double* partials,
+                                                  double* log3, int log_cap, DevState* st, PL const& L,
+                                                  double dt_used, double time_used, bool mood_redo,
+                                                  unsigned nblk, unsigned blk);
+
+template <int NT, class PL>
 __device__ __forceinline__ void finish_step(double m, double s, double* red, double* partials,
                                             double* log3, int log_cap, DevState* st, PL const& L,
                                             double dt_used, double time_used, bool mood_redo = false) {
+    finish_step_units<NT>(m, s, red, partials, log3, log_cap, st, L, dt_used, time_used, mood_redo,
+                          gridDim.x * gridDim.y, blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// The same over an explicit set of `nblk` work units (this block is unit
+// `blk`): lets one launch carry several independent runs (a batch), each with
+// its own run record and partials. Returns true in the block that finished
+// the step (the last unit to arrive).
+template <int NT, class PL>
+__device__ __forceinline__ bool finish_step_units(double m, double s, double* red, double* partials,
+                                                  double* log3, int log_cap, DevState* st, PL const& L,
+                                                  double dt_used, double time_used, bool mood_redo,
+                                                  unsigned nblk, unsigned blk) {
     block_reduce_max_sum<NT>(m, s, red);
-    const unsigned nblk = gridDim.x * gridDim.y;
-    const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x;
     __shared__ unsigned s_last;
     if (threadIdx.x == 0) {
         partials[2 * blk] = m;
@@ -101,7 +118,7 @@ __device__ __forceinline__ void finish_step(double m, double s, double* red, dou
         s_last = (prev == nblk - 1) ? 1u : 0u;
     }
     __syncthreads();
-    if (!s_last) return;
+    if (!s_last) return false;
     __threadfence();
     double gm = 0.0, gs = 0.0;
     for (unsigned b = threadIdx.x; b < nblk; b += NT) {
@@ -137,6 +154,7 @@ __device__ __forceinline__ void finish_step(double m, double s, double* red, dou
         st->counter = 0u;
         __threadfence();
     }
+    return true;
 }
 
 template <class Model, class Numerics, int ORDER, int MODE, bool WB, bool IMPL, int TX, int TY>
@@ -144,7 +162,8 @@ __global__ void __launch_bounds__(TX * TY, (Model::dimension == 2) ? 3 : 2)
 k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
         const double* __restrict__ qold, double* __restrict__ qout,
         LevelParams<double, Model::n_parameters> L, DevState* st,
-        double* __restrict__ partials, double* __restrict__ log3, int log_cap, double time_arg)
+        double* __restrict__ partials, double* __restrict__ log3, int log_cap, double time_arg,
+        double* __restrict__ qstar)
 {
     constexpr bool sbed = static_bed<Model>::value;
     using Sh = TileShape<Model, ORDER, TX, TY, sbed && MODE != MODE_RHS>;
@@ -344,6 +363,10 @@ k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
             typename T::VQ q;
 #pragma unroll
             for (int n = 0; n < nq; ++n) q(n, 0) = qc(n, 0) + dt * rhs(n, 0);
+            if (qstar) {   // adjoint tape: the stage state before the implicit source
+#pragma unroll
+                for (int n = n0; n < nq; ++n) qstar[(n - n0) * plane + c] = q(n, 0);
+            }
             if constexpr (IMPL) implicit_source_cell<Model, R>(q, ac, dt, p, time, X);
             if constexpr (MODE == MODE_S1 || MODE == MODE_R1) {
 #pragma unroll

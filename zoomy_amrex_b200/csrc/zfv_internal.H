@@ -30,6 +30,22 @@ struct ScratchLayout {
     size_t total = 0;
 };
 
+// Adjoint tape and work layout of one FP64 SWE2D level (zoomy_adj.cu).
+// Tape, per recorded step: Q^n (4 planes), Y1 (4 planes, bed row unused),
+// q* of stage 1 and of stage 2 (3 planes each: h, hu, hv), and the (time, dt)
+// the step used.
+struct AdjLayout {
+    size_t off_X = 0, off_Y1 = 0, off_qs1 = 0, off_qs2 = 0, off_meta = 0, step_bytes = 0;
+    size_t w_lamq = 0, w_loc = 0, w_lamY1 = 0, w_part = 0, w_amax = 0, w_counter = 0, w_total = 0;
+    int nbA = 0, nbD = 0;       // blocks of the per-cell pass and of the dt pass
+};
+AdjLayout adj_layout(long long plane);
+// Reverse of one recorded step (see fv_adjoint.cuh). `Lp` points to the
+// level's zfv::LevelParams<double, 6>.
+int adj_step_swe2d(const void* Lp, bool wb, bool impl, const AdjLayout& A, const char* tape_step,
+                   double* lam, double* grad, const double* aux0, int n_aux, char* work,
+                   cudaStream_t s);
+
 // One compiled model/precision: owns its kernel instantiations.
 struct Runner {
     virtual ~Runner() = default;
@@ -45,6 +61,14 @@ struct Runner {
                             cudaStream_t s) = 0;
     virtual int state_import(const double* Q64, void* Q, char* scratch, cudaStream_t s) = 0;
     virtual int state_export(const void* Q, const char* scratch, double* Q64, cudaStream_t s) = 0;
+    // Adjoint (FP64 SWE2D, order 2): record n forward steps onto a tape, and
+    // the reverse of recorded step k.
+    virtual int adj_record(void*, void*, char*, char*, int, cudaStream_t) {
+        return fail(-2, "zfv_adj_record: the adjoint is implemented for the FP64 SWE2D form, order 2");
+    }
+    virtual int adj_step(const char*, int, double*, double*, const double*, char*, cudaStream_t) {
+        return fail(-2, "zfv_adj_step: the adjoint is implemented for the FP64 SWE2D form, order 2");
+    }
 };
 
 }  // namespace zfvi

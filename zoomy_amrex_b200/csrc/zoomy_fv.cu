@@ -13,6 +13,7 @@
 #include <memory>
 #include <string>
 #include <algorithm>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "zoomy_fv.h"
@@ -191,13 +192,13 @@ struct RunnerT final : Runner {
 
     template <int ORDER, int MODE, bool WB, bool IMPL>
     void launch(const double* qin, const double* qbed, const double* qold, double* qout,
-                char* scratch, cudaStream_t s, double time_arg = 0.0) {
+                char* scratch, cudaStream_t s, double time_arg = 0.0, double* qstar = nullptr) {
         using Sh = ShapeOf<ORDER, MODE>;
         auto kernel = kfn<ORDER, MODE, WB, IMPL>();
         kernel<<<grid, block, Sh::smem_bytes, s>>>(
             qin, qbed, qold, qout, L, scratch ? st(scratch) : nullptr,
             scratch ? partials(scratch) : nullptr, scratch ? log3(scratch) : nullptr,
-            scratch ? kLogCap : 0, time_arg);
+            scratch ? kLogCap : 0, time_arg, qstar);
     }
 
     struct EvolveF {
@@ -259,6 +260,67 @@ struct RunnerT final : Runner {
 
     int rhs(const void* Q, void* out, double time, cudaStream_t s) override {
         return with_combo(RhsF{this, (const double*)Q, (double*)out, time, s});
+    }
+
+    // -- adjoint (SWE2D, order 2, FP64) ------------------------------------------
+    static constexpr bool kAdj = std::is_same<Model, zb::SWE<double, 2>>::value;
+
+    int adj_check(const char* what) const {
+        const zfv_config& c = h->cfg;
+        if (!kAdj || c.spatial_order != 2)
+            return fail(-2, "%s: the adjoint is implemented for the FP64 SWE2D form, order 2", what);
+        if (c.positivity_mood || c.clamp_positivity)
+            return fail(-2, "%s: the adjoint does not differentiate clamp_positivity / MOOD", what);
+        return 0;
+    }
+
+    struct RecordF {
+        RunnerT* r; double* Q; char* scratch; char* tape; int n; cudaStream_t s;
+        template <int O, bool W, bool I> int operator()() {
+            if constexpr (O != 2) {
+                return fail(-2, "zfv_adj_record: order 2 only");
+            } else {
+                const AdjLayout A = adj_layout(r->L.plane);
+                const size_t pb = size_t(r->L.plane) * sizeof(double);
+                for (int k = 0; k < n; ++k) {
+                    char* t = tape + size_t(k) * A.step_bytes;
+                    double* X = reinterpret_cast<double*>(t + A.off_X);
+                    double* Y1 = reinterpret_cast<double*>(t + A.off_Y1);
+                    double* qs1 = reinterpret_cast<double*>(t + A.off_qs1);
+                    double* qs2 = reinterpret_cast<double*>(t + A.off_qs2);
+                    int rc = cuda_check(cudaMemcpyAsync(X, Q, 4 * pb, cudaMemcpyDeviceToDevice, s),
+                                        "zfv_adj_record state copy");
+                    // (time, dt) of the step about to run: the first two doubles of DevState
+                    if (!rc) rc = cuda_check(cudaMemcpyAsync(t + A.off_meta, r->st(scratch), 2 * sizeof(double),
+                                                             cudaMemcpyDeviceToDevice, s),
+                                             "zfv_adj_record dt copy");
+                    if (rc) return rc;
+                    r->template launch<2, zfv::MODE_S1, W, I>(Q, Q, nullptr, Y1, scratch, s, 0.0, qs1);
+                    r->template launch<2, zfv::MODE_S2, W, I>(Y1, Q, Q, Q, scratch, s, 0.0, qs2);
+                }
+                return cuda_check(cudaGetLastError(), "zfv_adj_record launch");
+            }
+        }
+    };
+
+    int adj_record(void* Q, void* Av, char* scratch, char* tape, int n, cudaStream_t s) override {
+        int rc = adj_check("zfv_adj_record");
+        if (rc) return rc;
+        rc = with_combo(RecordF{this, (double*)Q, scratch, tape, n, s});
+        if (rc) return rc;
+        const int nb = int((L.plane + 255) / 256);
+        zfv::k_aux_from_state<Model><<<nb, 256, 0, s>>>((double*)Q, (double*)Av, L, st(scratch));
+        return cuda_check(cudaGetLastError(), "zfv_adj_record aux launch");
+    }
+
+    int adj_step(const char* tape, int k, double* lam, double* grad, const double* aux0, char* work,
+                 cudaStream_t s) override {
+        int rc = adj_check("zfv_adj_step");
+        if (rc) return rc;
+        const AdjLayout A = adj_layout(L.plane);
+        return adj_step_swe2d(&L, h->cfg.well_balanced != 0, h->cfg.implicit_source != 0, A,
+                              tape + size_t(k) * A.step_bytes, lam, grad, aux0, Model::n_dof_qaux,
+                              work, s);
     }
 
     int fill_ghosts(const void* Q, const void* A, void* Qg, void* Ag, double time,
@@ -358,9 +420,9 @@ int zfv_create(const zfv_config* cfg, zfv_handle** out) {
             h->run.reset(new RunnerT<zb::SWE<double, 2>, zb::SWENumerics<double, 2>, 32, 8>(h)); break;
         }
     }
-    h->run->layout(h->lay);
     int rc = h->run->setup();
     if (rc) { delete h; return rc; }
+    h->run->layout(h->lay);
     *out = h;
     return 0;
 }
@@ -428,6 +490,46 @@ int zfv_get_status(zfv_handle* h, const void* scratch, zfv_status* out, void* st
                                         cudaMemcpyDeviceToHost, s), "zfv_get_status copy");
     if (rc) return rc;
     return cuda_check(cudaStreamSynchronize(s), "zfv_get_status sync");
+}
+
+int zfv_save_run_state(zfv_handle* h, const void* scratch, void* dst, void* stream) {
+    if (!h || !scratch || !dst) return fail(-1, "zfv_save_run_state: null argument");
+    return cuda_check(cudaMemcpyAsync(dst, static_cast<const char*>(scratch) + h->lay.state,
+                                      sizeof(zfv::DevState), cudaMemcpyDeviceToDevice, (cudaStream_t)stream),
+                      "zfv_save_run_state copy");
+}
+
+int zfv_load_run_state(zfv_handle* h, void* scratch, const void* src, void* stream) {
+    if (!h || !scratch || !src) return fail(-1, "zfv_load_run_state: null argument");
+    return cuda_check(cudaMemcpyAsync(static_cast<char*>(scratch) + h->lay.state, src,
+                                      sizeof(zfv::DevState), cudaMemcpyDeviceToDevice, (cudaStream_t)stream),
+                      "zfv_load_run_state copy");
+}
+
+size_t zfv_run_state_bytes(void) { return sizeof(zfv::DevState); }
+
+size_t zfv_adj_tape_bytes(const zfv_handle* h, int n_steps) {
+    if (!h || n_steps < 0) return 0;
+    return adj_layout((long long)h->cfg.nx * h->cfg.ny).step_bytes * size_t(n_steps);
+}
+
+size_t zfv_adj_work_bytes(const zfv_handle* h) {
+    return h ? adj_layout((long long)h->cfg.nx * h->cfg.ny).w_total : 0;
+}
+
+int zfv_adj_record(zfv_handle* h, void* Q, void* aux, void* scratch, void* tape, int n_steps, void* stream) {
+    if (!h || !Q || !aux || !scratch || !tape) return fail(-1, "zfv_adj_record: null argument");
+    if (n_steps < 0) return fail(-1, "zfv_adj_record: negative step count");
+    return h->run->adj_record(Q, aux, static_cast<char*>(scratch), static_cast<char*>(tape), n_steps,
+                              (cudaStream_t)stream);
+}
+
+int zfv_adj_step(zfv_handle* h, const void* tape, int k, void* lam, double* grad, const void* aux0,
+                 void* work, void* stream) {
+    if (!h || !tape || !lam || !grad || !work) return fail(-1, "zfv_adj_step: null argument");
+    if (k < 0) return fail(-1, "zfv_adj_step: negative step index");
+    return h->run->adj_step(static_cast<const char*>(tape), k, static_cast<double*>(lam), grad,
+                            static_cast<const double*>(aux0), static_cast<char*>(work), (cudaStream_t)stream);
 }
 
 int zfv_log_capacity(const zfv_handle* h) { return h ? kLogCap : 0; }

@@ -19,6 +19,9 @@
 //    (h < 1e-3) and in the mass sum.
 // Kernels are compiled with FMA contraction on (this file only).
 #include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "zfv_internal.H"
@@ -34,7 +37,7 @@ struct Params {
     int nx, ny;
     long long plane;
     double dx, dy, plox, ploy;       // FP64 (reductions, dt)
-    float fdx, fdy, rdx, rdy;
+    float fdx, fdy, rdx, rdy, rfdx, rfdy;
     float g, ex, ey, nm, hfloor, eps;
     double gd, exd, eyd, nmd, hfloord, epsd;
     int bc_tag[4];
@@ -61,72 +64,6 @@ __device__ __forceinline__ double kp_hinv_d(double h, double eps) {
     const double h2 = h * h;
     const double x0 = h2 * h2;
     return 1.4142135623730951 * h / sqrt(x0 + fmax(x0, eps));
-}
-
-// Face record: flux (h, hu, hv), D+ (3), D- (3), P(h*_L), P(h*_R).
-constexpr int NFC = 11;
-
-template <int ORDER, int DIR, bool WB>
-__device__ __forceinline__ void face(const C4& LL, const C4& Lc, const C4& Rc, const C4& RR,
-                                     const Params& L, float* __restrict__ F) {
-    float bL, bR, eL, eR, hL, hR, uL, uR, vL, vR;
-    if constexpr (ORDER == 2) {
-        const float db1 = Lc.b - LL.b, db2 = Rc.b - Lc.b, db3 = RR.b - Rc.b;
-        const float de1 = Lc.e - LL.e, de2 = Rc.e - Lc.e, de3 = RR.e - Rc.e;
-        const float gbL = mm(db1, db2), gbR = mm(db2, db3);
-        const float ghL = mm(de1 - db1, de2 - db2), ghR = mm(de2 - db2, de3 - db3);
-        bL = Lc.b + 0.5f * gbL;  bR = Rc.b - 0.5f * gbR;
-        hL = (Lc.e - Lc.b) + 0.5f * ghL;  hR = (Rc.e - Rc.b) - 0.5f * ghR;
-        eL = Lc.e + 0.5f * (ghL + gbL);  eR = Rc.e - 0.5f * (ghR + gbR);
-        uL = Lc.u + 0.5f * mm(Lc.u - LL.u, Rc.u - Lc.u);
-        uR = Rc.u - 0.5f * mm(Rc.u - Lc.u, RR.u - Rc.u);
-        vL = Lc.v + 0.5f * mm(Lc.v - LL.v, Rc.v - Lc.v);
-        vR = Rc.v - 0.5f * mm(Rc.v - Lc.v, RR.v - Rc.v);
-    } else {
-        bL = Lc.b; bR = Rc.b; eL = Lc.e; eR = Rc.e;
-        hL = Lc.e - Lc.b; hR = Rc.e - Rc.b;
-        uL = Lc.u; uR = Rc.u; vL = Lc.v; vR = Rc.v;
-    }
-    float db = 0.0f;
-    if constexpr (WB) {
-        const float bf = fmaxf(bL, bR);
-        const float hsL = fmaxf(0.0f, eL - bf), hsR = fmaxf(0.0f, eR - bf);
-        const float sL = (hL > 0.0f) ? hsL / hL : 0.0f;
-        const float sR = (hR > 0.0f) ? hsR / hR : 0.0f;
-        uL *= sL; vL *= sL; uR *= sR; vR *= sR;
-        hL = hsL; hR = hsR;
-    } else {
-        db = bR - bL;
-    }
-    const float g = L.g, hg = 0.5f * L.g;
-    const float hiL = kp_hinv(hL, L.eps), hiR = kp_hinv(hR, L.eps);
-    const float unL = (DIR == 0) ? uL : vL, unR = (DIR == 0) ? uR : vR;
-    const float pL = hg * hL * hL, pR = hg * hR * hR;
-    float fuL, fvL, fuR, fvR;
-    if constexpr (DIR == 0) {
-        fuL = uL * uL * hiL + pL;  fvL = vL * uL * hiL;
-        fuR = uR * uR * hiR + pR;  fvR = vR * uR * hiR;
-    } else {
-        fuL = uL * vL * hiL;  fvL = vL * vL * hiL + pL;
-        fuR = uR * vR * hiR;  fvR = vR * vR * hiR + pR;
-    }
-    F[0] = 0.5f * (unL + unR);
-    F[1] = 0.5f * (fuL + fuR);
-    F[2] = 0.5f * (fvL + fvR);
-    const float evL = fabsf(unL * hiL) + sqrtf(g * fmaxf(hL, 0.0f));
-    const float evR = fabsf(unR * hiR) + sqrtf(g * fmaxf(hR, 0.0f));
-    const float hs = 0.5f * fmaxf(evL, evR);
-    const float dh = hR - hL, du = uR - uL, dv = vR - vL;
-    float bu = 0.0f, bv = 0.0f;
-    if constexpr (!WB) {
-        const float Bn = g * (0.5f * (hL + hR)) * db;
-        if (DIR == 0) bu = 0.5f * Bn; else bv = 0.5f * Bn;
-    }
-    F[3] = hs * dh;        F[6] = -hs * dh;          // D+ / D-, h
-    F[4] = bu + hs * du;   F[7] = bu - hs * du;      // hu
-    F[5] = bv + hs * dv;   F[8] = bv - hs * dv;      // hv
-    F[9] = pL;
-    F[10] = pR;
 }
 
 // Manning friction S_m = g e_m h - k u_m |u|, k = g n^2 max(h, h_floor)^(-1/3),
@@ -168,206 +105,295 @@ enum Mode { S1 = 1, S2 = 2 };
 
 }  // namespace zfv32
 
-#include "fv32_sweep.cuh"
+#include "fv32_batch.cuh"
 
 namespace zfv32 {
 
-// FP64 reference layout [b, h, hu, hv] -> FP32 [b, eta, hu, hv] + remainders.
-__global__ void k32_import(const double* __restrict__ Q64, float* __restrict__ Q, float* __restrict__ lo,
-                           long long plane) {
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= plane) return;
-    // eta from the FP64 bed: a surface that is constant in FP64 (a lake at rest)
-    // rounds to the same FP32 value in every cell. The FP32 form's depth is
-    // eta - b32, within half an FP32 ulp of b of the FP64 depth.
-    const float b = float(Q64[c]);
-    const double eta = Q64[plane + c] + Q64[c];
-    const double hu = Q64[2 * plane + c], hv = Q64[3 * plane + c];
-    const float e = float(eta), u = float(hu), v = float(hv);
-    Q[c] = b; Q[plane + c] = e; Q[2 * plane + c] = u; Q[3 * plane + c] = v;
-    lo[c] = float(eta - double(e));
-    lo[plane + c] = float(hu - double(u));
-    lo[2 * plane + c] = float(hv - double(v));
+// Compiled strip shapes: (warps per block, rows per warp = cells per thread).
+// A strip is 30 columns x (NW * CPT) rows.
+constexpr int kNumVariants = 4;
+constexpr int kVarNW[kNumVariants] = {4, 4, 8, 2};
+constexpr int kVarCPT[kNumVariants] = {16, 8, 8, 32};
+
+template <class F>
+int with_variant(int v, F&& f) {
+    switch (v) {
+    case 0: return f.template operator()<4, 16>();
+    case 1: return f.template operator()<4, 8>();
+    case 2: return f.template operator()<8, 8>();
+    case 3: return f.template operator()<2, 32>();
+    default: return fail(-1, "unknown strip variant %d", v);
+    }
 }
 
-__global__ void k32_export(const float* __restrict__ Q, const float* __restrict__ lo,
-                           double* __restrict__ Q64, long long plane) {
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= plane) return;
-    const double b = double(Q[c]);
-    const double eta = double(Q[plane + c]) + double(lo[c]);
-    Q64[c] = b;
-    Q64[plane + c] = eta - b;
-    Q64[2 * plane + c] = double(Q[2 * plane + c]) + double(lo[plane + c]);
-    Q64[3 * plane + c] = double(Q[3 * plane + c]) + double(lo[2 * plane + c]);
+Params make_params(const zfv_config& c) {
+    Params L;
+    L.nx = c.nx; L.ny = c.ny; L.plane = (long long)c.nx * c.ny;
+    L.dx = (c.prob_hi[0] - c.prob_lo[0]) / c.nx;
+    L.dy = (c.prob_hi[1] - c.prob_lo[1]) / c.ny;
+    L.plox = c.prob_lo[0]; L.ploy = c.prob_lo[1];
+    L.fdx = float(L.dx); L.fdy = float(L.dy);
+    L.rdx = float(1.0 / L.dx); L.rdy = float(1.0 / L.dy);
+    L.rfdx = 1.0f / L.fdx; L.rfdy = 1.0f / L.fdy;
+    L.gd = c.params[zb::swe_g]; L.exd = c.params[zb::swe_ex]; L.eyd = c.params[zb::swe_ey];
+    L.nmd = c.params[zb::swe_n_m]; L.hfloord = c.params[zb::swe_h_floor]; L.epsd = c.params[zb::swe_eps];
+    L.g = float(L.gd); L.ex = float(L.exd); L.ey = float(L.eyd); L.nm = float(L.nmd);
+    L.hfloor = float(L.hfloord); L.eps = float(L.epsd);
+    for (int s = 0; s < 4; ++s) L.bc_tag[s] = c.bc_tag[s];
+    L.cfl = c.cfl; L.dtmin = c.dtmin; L.dtmax = c.dtmax; L.time_end = c.time_end;
+    L.max_step = c.max_step; L.cfl_dimension = c.cfl_dimension; L.cfl_degree_factor = c.cfl_degree_factor;
+    return L;
 }
 
-// Final aux: hinv of the FP64 state (the carried rows stay untouched).
-__global__ void k32_aux(const float* __restrict__ Q, const float* __restrict__ lo, double* __restrict__ A,
-                        long long plane, int n_aux, double eps) {
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= plane) return;
-    const double h = (double(Q[plane + c]) + double(lo[c])) - double(Q[c]);
-    A[(n_aux - 1) * plane + c] = kp_hinv_d(h, eps);
+int units_of(const zfv_config& c, int v) {
+    const int rows = kVarNW[v] * kVarCPT[v];
+    return ((c.nx + 29) / 30) * ((c.ny + rows - 1) / rows);
+}
+int max_units_of(const zfv_config& c) {
+    int m = 0;
+    for (int v = 0; v < kNumVariants; ++v) m = std::max(m, units_of(c, v));
+    return m;
 }
 
-// ComputeDt on the stored state and aux (WHAT 0, clamped to time_end) or the
-// FP64 mass (WHAT 1).
-template <int NT, int WHAT>
-__global__ void __launch_bounds__(NT)
-k32_reduce(const float* __restrict__ Q, const float* __restrict__ lo, const double* __restrict__ A,
-           int n_aux, Params L, zfv::DevState* st, double* partials) {
-    __shared__ double red[2 * ((NT + 31) / 32)];
-    __shared__ unsigned s_last;
-    const long long plane = L.plane;
-    double m = 0.0, s = 0.0;
-    const long long stride = (long long)gridDim.x * NT;
-    for (long long c = (long long)blockIdx.x * NT + threadIdx.x; c < plane; c += stride) {
-        const double b = double(Q[c]);
-        const double h = (double(Q[plane + c]) + double(lo[c])) - b;
-        if constexpr (WHAT == 0) {
-            const double hinv = A[(n_aux - 1) * plane + c];
-            const double c0 = sqrt(L.gd * fmax(h, 0.0));
-            const double hu = double(Q[2 * plane + c]) + double(lo[plane + c]);
-            const double hv = double(Q[3 * plane + c]) + double(lo[2 * plane + c]);
-            const double ix = (fabs(hu * hinv) + c0) / L.dx, iy = (fabs(hv * hinv) + c0) / L.dy;
-            if (ix > m) m = ix;
-            if (iy > m) m = iy;
-        } else {
-            s = s + h;
+// The batch engine: any number of FP32 SWE2D instances sharing one scheme
+// (order 2, the same well_balanced / implicit_source flags).
+struct BatchCore {
+    static constexpr int n_aux = zb::SWE<double, 2>::n_dof_qaux;
+    std::vector<zfv_config> cfg;
+    int n = 0;
+    bool wb = false, impl = false;
+    int variant = 0;
+    // scratch layout
+    size_t off_desc = 0, off_units = 0, off_status = 0;
+    std::vector<size_t> off_state, off_part, off_log, off_alt, off_inc, off_lo;
+    size_t total = 0;
+    int max_units_total = 0;
+    // bound buffers
+    std::vector<BInst> desc;
+    std::vector<int2> units;
+    char* scratch = nullptr;
+    bool bound = false;
+
+    int init(const zfv_config* cfgs, int count) {
+        if (count < 1) return fail(-1, "zfv_batch_create: empty batch");
+        n = count;
+        cfg.assign(cfgs, cfgs + count);
+        wb = cfg[0].well_balanced != 0;
+        impl = cfg[0].implicit_source != 0;
+        for (auto& c : cfg) {
+            if (c.model != ZFV_MODEL_SWE2D || c.precision != ZFV_PREC_FP32)
+                return fail(-1, "zfv_batch: instances must be ZFV_MODEL_SWE2D / ZFV_PREC_FP32");
+            if (c.spatial_order != 2)
+                return fail(-2, "zfv_batch: the FP32 form implements spatial_order 2 only");
+            if ((c.well_balanced != 0) != wb || (c.implicit_source != 0) != impl)
+                return fail(-1, "zfv_batch: all instances must share well_balanced and implicit_source");
+            if (c.positivity_mood) return fail(-2, "zfv_batch: the FP32 form does not implement MOOD");
+            if (c.clamp_positivity) return fail(-1, "zfv_batch: the FP32 form does not implement clamp_positivity");
+            if (c.nx < 2 || c.ny < 2) return fail(-1, "zfv_batch: order 2 needs at least 2 cells per direction");
+        }
+        size_t o = 0;
+        off_desc = o; o += align_up(sizeof(BInst) * n);
+        max_units_total = 0;
+        for (auto& c : cfg) max_units_total += max_units_of(c);
+        off_units = o; o += align_up(sizeof(int2) * max_units_total);
+        off_status = o; o += align_up(sizeof(zfv::DevState) * n);
+        off_state.resize(n); off_part.resize(n); off_log.resize(n);
+        off_alt.resize(n); off_inc.resize(n); off_lo.resize(n);
+        for (int k = 0; k < n; ++k) {
+            const size_t pb = size_t(cfg[k].nx) * cfg[k].ny * sizeof(float);
+            off_state[k] = o; o += align_up(sizeof(zfv::DevState));
+            off_part[k] = o; o += align_up(sizeof(double) * 2 * max_units_of(cfg[k]));
+            off_log[k] = o; o += align_up(sizeof(double) * 3 * kLogCap);
+            off_inc[k] = o; o += align_up(pb * 3);
+            off_alt[k] = o; o += align_up(pb * 3);
+            off_lo[k] = o; o += align_up(pb * 3);
+        }
+        total = o;
+        desc.resize(n);
+        return 0;
+    }
+
+    void build_units() {
+        units.clear();
+        const int rows = kVarNW[variant] * kVarCPT[variant];
+        for (int k = 0; k < n; ++k) {
+            const int nbx = (cfg[k].nx + 29) / 30, nby = (cfg[k].ny + rows - 1) / rows;
+            desc[k].nbx = nbx;
+            desc[k].nby = nby;
+            for (int u = 0; u < nbx * nby; ++u) units.push_back(make_int2(k, u));
         }
     }
-    zfv::block_reduce_max_sum<NT>(m, s, red);
-    if (threadIdx.x == 0) {
-        partials[2 * blockIdx.x] = m;
-        partials[2 * blockIdx.x + 1] = s;
-        __threadfence();
-        s_last = (atomicAdd(&st->counter, 1u) == gridDim.x - 1) ? 1u : 0u;
+
+    int upload(cudaStream_t s) {
+        build_units();
+        int rc = cuda_check(cudaMemcpyAsync(scratch + off_desc, desc.data(), sizeof(BInst) * n,
+                                            cudaMemcpyHostToDevice, s), "zfv_batch descriptor upload");
+        if (rc) return rc;
+        rc = cuda_check(cudaMemcpyAsync(scratch + off_units, units.data(), sizeof(int2) * units.size(),
+                                        cudaMemcpyHostToDevice, s), "zfv_batch unit upload");
+        if (rc) return rc;
+        return cuda_check(cudaStreamSynchronize(s), "zfv_batch upload sync");
     }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    double gm = 0.0, gs = 0.0;
-    for (unsigned bb = threadIdx.x; bb < gridDim.x; bb += NT) {
-        const double pm = __ldcg(&partials[2 * bb]), ps = __ldcg(&partials[2 * bb + 1]);
-        if (pm > gm) gm = pm;
-        gs = gs + ps;
-    }
-    zfv::block_reduce_max_sum<NT>(gm, gs, red);
-    if (threadIdx.x == 0) {
-        if constexpr (WHAT == 0) {
-            const double dt = zfv::dt_from_max(gm, st->time, L);
-            st->max_inv = gm;
-            st->dt = dt;
-            if (!isfinite(dt)) st->flags |= zfv::kFlagNonfiniteDt;
-        } else {
-            st->mass = gs * (L.dx * L.dy);
+
+    int bind(void* const* Q, double* const* aux, char* scr, cudaStream_t s) {
+        scratch = scr;
+        for (int k = 0; k < n; ++k) {
+            BInst& D = desc[k];
+            std::memset(&D, 0, sizeof D);
+            D.P = make_params(cfg[k]);
+            const long long pl = D.P.plane;
+            float* q = static_cast<float*>(Q[k]);
+            D.bed = q;
+            D.Qs = q + pl;
+            D.alt = reinterpret_cast<float*>(scr + off_alt[k]);
+            D.inc = reinterpret_cast<float*>(scr + off_inc[k]);
+            D.lo = reinterpret_cast<float*>(scr + off_lo[k]);
+            D.aux = aux ? aux[k] : nullptr;
+            D.st = reinterpret_cast<zfv::DevState*>(scr + off_state[k]);
+            D.partials = reinterpret_cast<double*>(scr + off_part[k]);
+            D.log3 = reinterpret_cast<double*>(scr + off_log[k]);
+            D.log_cap = kLogCap;
         }
-        st->counter = 0u;
-        __threadfence();
+        bound = true;
+        return upload(s);
     }
-}
+
+    const BInst* d_desc() const { return reinterpret_cast<const BInst*>(scratch + off_desc); }
+    const int2* d_units() const { return reinterpret_cast<const int2*>(scratch + off_units); }
+    int nunits() const { return int(units.size()); }
+
+    int set_variant(int v, cudaStream_t s) {
+        if (v < 0 || v >= kNumVariants) return fail(-1, "zfv_batch_set_variant: unknown variant %d", v);
+        variant = v;
+        return bound ? upload(s) : 0;
+    }
+
+    struct ImportF {
+        BatchCore* b; cudaStream_t s; bool exp;
+        template <int NW, int CPT> int operator()() {
+            if (exp) k32b_export<NW, CPT><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
+            else k32b_import<NW, CPT><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units());
+            return cuda_check(cudaGetLastError(), "zfv_batch import/export launch");
+        }
+    };
+    int convert(const double* const* q64, bool exp, cudaStream_t s) {
+        for (int k = 0; k < n; ++k) desc[k].q64 = q64[k];
+        int rc = upload(s);
+        if (rc) return rc;
+        rc = with_variant(variant, ImportF{this, s, exp});
+        if (rc) return rc;
+        return cuda_check(cudaStreamSynchronize(s), "zfv_batch import/export sync");
+    }
+
+    struct BeginF {
+        BatchCore* b; cudaStream_t s;
+        template <int NW, int CPT> int operator()() {
+            k32b_init<<<(b->n + 127) / 128, 128, 0, s>>>(b->d_desc(), b->n);
+            k32b_reduce<NW, CPT, 0><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
+            return cuda_check(cudaGetLastError(), "zfv_batch begin launch");
+        }
+    };
+    int begin(cudaStream_t s) { return with_variant(variant, BeginF{this, s}); }
+
+    struct MassF {
+        BatchCore* b; cudaStream_t s;
+        template <int NW, int CPT> int operator()() {
+            k32b_reduce<NW, CPT, 1><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
+            return cuda_check(cudaGetLastError(), "zfv_batch mass launch");
+        }
+    };
+    int mass(cudaStream_t s) { return with_variant(variant, MassF{this, s}); }
+
+    template <bool W, bool I>
+    struct StepF {
+        BatchCore* b; cudaStream_t s; int nsteps;
+        template <int NW, int CPT> int operator()() {
+            const int nu = b->nunits();
+            for (int k = 0; k < nsteps; ++k) {
+                k32b_stage<S1, W, I, NW, CPT><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+                k32b_stage<S2, W, I, NW, CPT><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+            }
+            return cuda_check(cudaGetLastError(), "zfv_batch evolve launch");
+        }
+    };
+    int evolve(int nsteps, cudaStream_t s) {
+        if (wb) return impl ? with_variant(variant, StepF<true, true>{this, s, nsteps})
+                            : with_variant(variant, StepF<true, false>{this, s, nsteps});
+        return impl ? with_variant(variant, StepF<false, true>{this, s, nsteps})
+                    : with_variant(variant, StepF<false, false>{this, s, nsteps});
+    }
+
+    int status(zfv_status* out, cudaStream_t s) {
+        static_assert(sizeof(zfv_status) <= sizeof(zfv::DevState), "status fits the run record");
+        zfv::DevState* dst = reinterpret_cast<zfv::DevState*>(scratch + off_status);
+        k32b_status<<<(n + 127) / 128, 128, 0, s>>>(d_desc(), n, dst);
+        std::vector<zfv::DevState> tmp(n);
+        int rc = cuda_check(cudaMemcpyAsync(tmp.data(), dst, sizeof(zfv::DevState) * n,
+                                            cudaMemcpyDeviceToHost, s), "zfv_batch status copy");
+        if (rc) return rc;
+        rc = cuda_check(cudaStreamSynchronize(s), "zfv_batch status sync");
+        for (int k = 0; k < n; ++k) std::memcpy(&out[k], &tmp[k], sizeof(zfv_status));
+        return rc;
+    }
+};
 
 // ---------------------------------------------------------------------------
-template <int NW, int CPT>
+// Single level (zfv_create with ZFV_PREC_FP32): a batch of one. Q / aux /
+// scratch are bound on first use and re-bound (a synchronous upload) if a
+// later call passes different buffers; keep them fixed across CUDA-graph
+// captured calls.
 struct Runner32 final : Runner {
     zfv_handle* h;
-    Params L;
-    dim3 grid, block;
-    static constexpr int n_aux = zb::SWE<double, 2>::n_dof_qaux;
+    BatchCore core;
+    const void* bq = nullptr; const void* ba = nullptr; const char* bs = nullptr;
 
-    explicit Runner32(zfv_handle* hh) : h(hh) {
-        const zfv_config& c = h->cfg;
-        L.nx = c.nx; L.ny = c.ny; L.plane = (long long)c.nx * c.ny;
-        L.dx = (c.prob_hi[0] - c.prob_lo[0]) / c.nx;
-        L.dy = (c.prob_hi[1] - c.prob_lo[1]) / c.ny;
-        L.plox = c.prob_lo[0]; L.ploy = c.prob_lo[1];
-        L.fdx = float(L.dx); L.fdy = float(L.dy);
-        L.rdx = float(1.0 / L.dx); L.rdy = float(1.0 / L.dy);
-        L.gd = c.params[zb::swe_g]; L.exd = c.params[zb::swe_ex]; L.eyd = c.params[zb::swe_ey];
-        L.nmd = c.params[zb::swe_n_m]; L.hfloord = c.params[zb::swe_h_floor]; L.epsd = c.params[zb::swe_eps];
-        L.g = float(L.gd); L.ex = float(L.exd); L.ey = float(L.eyd); L.nm = float(L.nmd);
-        L.hfloor = float(L.hfloord); L.eps = float(L.epsd);
-        for (int s = 0; s < 4; ++s) L.bc_tag[s] = c.bc_tag[s];
-        L.cfl = c.cfl; L.dtmin = c.dtmin; L.dtmax = c.dtmax; L.time_end = c.time_end;
-        L.max_step = c.max_step; L.cfl_dimension = c.cfl_dimension; L.cfl_degree_factor = c.cfl_degree_factor;
-        grid = dim3((c.nx + 30) / 31, (c.ny + NW * CPT - 1) / (NW * CPT), 1);
-        block = dim3(32 * NW, 1, 1);
-    }
+    explicit Runner32(zfv_handle* hh) : h(hh) {}
 
+    int setup() override { return core.init(&h->cfg, 1); }
     void layout(ScratchLayout& S) const override {
-        const size_t pb = size_t(L.plane) * sizeof(float);
-        const int nblk = std::max(int(grid.x * grid.y), kReduceBlocksMax);
-        S.state = 0;
-        S.partials = align_up(sizeof(zfv::DevState));
-        S.log = S.partials + align_up(sizeof(double) * 2 * nblk);
-        S.stage = S.log + align_up(sizeof(double) * 3 * kLogCap);    // inc1: 3 planes
-        S.alt = S.stage + align_up(pb * 3);                           // ping-pong: 3 planes
-        S.lo = S.alt + align_up(pb * 3);                               // remainders: 3 planes
-        S.total = S.lo + align_up(pb * 3);
+        S.state = core.off_state[0];
+        S.partials = core.off_part[0];
+        S.log = core.off_log[0];
+        S.stage = core.off_inc[0];
+        S.alt = core.off_alt[0];
+        S.lo = core.off_lo[0];
+        S.total = core.total;
     }
-
-    template <int M, bool W, bool I>
-    static auto kfn() { return &k32s_stage<2, M, W, I, NW, CPT>; }
-
-    template <int O, bool W, bool I>
-    int setup_combo() { return 0; }
-
-    template <class F>
-    int with_combo(F&& f) {
-        const zfv_config& c = h->cfg;
-        const bool wb = c.well_balanced != 0, im = c.implicit_source != 0;
-        if (c.spatial_order == 2) {
-            if (wb) return im ? f.template operator()<2, true, true>() : f.template operator()<2, true, false>();
-            return im ? f.template operator()<2, false, true>() : f.template operator()<2, false, false>();
-        }
-        if (wb) return im ? f.template operator()<1, true, true>() : f.template operator()<1, true, false>();
-        return im ? f.template operator()<1, false, true>() : f.template operator()<1, false, false>();
+    int ensure_bound(const void* Q, const void* A, char* scratch, cudaStream_t s) {
+        if (core.bound && Q == bq && A == ba && scratch == bs) return 0;
+        void* qp = const_cast<void*>(Q);
+        double* ap = static_cast<double*>(const_cast<void*>(A));
+        int rc = core.bind(&qp, &ap, scratch, s);
+        if (rc) return rc;
+        bq = Q; ba = A; bs = scratch;
+        return 0;
     }
-
-    struct SetupF {
-        Runner32* r;
-        template <int O, bool W, bool I> int operator()() { return r->template setup_combo<O, W, I>(); }
-    };
-    int setup() override {
-        if (h->cfg.spatial_order == 1) {
-            // order 1 (PCM) is a single forward-Euler stage in the reference
-            // (ZoomyAmr.cpp:677-678); the FP32 form implements the SSP-RK2 path
-            return fail(-2, "zfv_create: the FP32 form implements spatial_order 2 only");
-        }
-        if (h->cfg.positivity_mood) return fail(-2, "zfv_create: the FP32 form does not implement MOOD");
-        return with_combo(SetupF{this});
-    }
-
-    zfv::DevState* st(char* s) const { return reinterpret_cast<zfv::DevState*>(s + h->lay.state); }
-    double* partials(char* s) const { return reinterpret_cast<double*>(s + h->lay.partials); }
-    double* log3(char* s) const { return reinterpret_cast<double*>(s + h->lay.log); }
-    float* inc(char* s) const { return reinterpret_cast<float*>(s + h->lay.stage); }
-    float* alt(char* s) const { return reinterpret_cast<float*>(s + h->lay.alt); }
-    float* lo(char* s) const { return reinterpret_cast<float*>(s + h->lay.lo); }
-    const float* lo(const char* s) const { return reinterpret_cast<const float*>(s + h->lay.lo); }
-
-    int reduce_blocks() const {
-        long long need = (L.plane + kReduceNT - 1) / kReduceNT;
-        return int(need < kReduceBlocksMax ? (need > 0 ? need : 1) : kReduceBlocksMax);
-    }
-
     int begin(const void* Q, const void* A, char* scratch, cudaStream_t s) override {
-        zfv::k_begin<<<1, 1, 0, s>>>(st(scratch), L);
-        k32_reduce<kReduceNT, 0><<<reduce_blocks(), kReduceNT, 0, s>>>(
-            (const float*)Q, lo(scratch), (const double*)A, n_aux, L, st(scratch), partials(scratch));
-        return cuda_check(cudaGetLastError(), "zfv_begin (fp32) launch");
+        int rc = ensure_bound(Q, A, scratch, s);
+        return rc ? rc : core.begin(s);
+    }
+    int evolve(void* Q, void* A, char* scratch, int n, cudaStream_t s) override {
+        int rc = ensure_bound(Q, A, scratch, s);
+        return rc ? rc : core.evolve(n, s);
+    }
+    int total_mass(const void* Q, char* scratch, cudaStream_t s) override {
+        int rc = ensure_bound(Q, ba, scratch, s);
+        return rc ? rc : core.mass(s);
+    }
+    int state_import(const double* Q64, void* Q, char* scratch, cudaStream_t s) override {
+        int rc = ensure_bound(Q, ba, scratch, s);
+        return rc ? rc : core.convert(&Q64, false, s);
+    }
+    int state_export(const void* Q, const char* scratch, double* Q64, cudaStream_t s) override {
+        int rc = ensure_bound(Q, ba, const_cast<char*>(scratch), s);
+        const double* q = Q64;
+        return rc ? rc : core.convert(&q, true, s);
     }
     int update_state(void*, void*, double, cudaStream_t) override {
         return fail(-2, "zfv_update_state: validation entry of the FP64 form only");
     }
-    int compute_dt(const void* Q, const void* A, char* scratch, cudaStream_t s) override {
+    int compute_dt(const void*, const void*, char*, cudaStream_t) override {
         return fail(-2, "zfv_compute_dt: validation entry of the FP64 form only");
-    }
-    int total_mass(const void* Q, char* scratch, cudaStream_t s) override {
-        k32_reduce<kReduceNT, 1><<<reduce_blocks(), kReduceNT, 0, s>>>(
-            (const float*)Q, lo(scratch), nullptr, n_aux, L, st(scratch), partials(scratch));
-        return cuda_check(cudaGetLastError(), "zfv_total_mass (fp32) launch");
     }
     int rhs(const void*, void*, double, cudaStream_t) override {
         return fail(-2, "zfv_rhs: validation entry of the FP64 form only");
@@ -375,60 +401,81 @@ struct Runner32 final : Runner {
     int fill_ghosts(const void*, const void*, void*, void*, double, cudaStream_t) override {
         return fail(-2, "zfv_fill_ghosts: validation entry of the FP64 form only");
     }
-
-    template <int O, bool W, bool I>
-    void launch_step(float* Qf, float* Xs, float* Ys, char* scratch, cudaStream_t s) {
-        const float* bedp = Qf;
-        auto k1 = kfn<S1, W, I>();
-        k1<<<grid, block, 0, s>>>(bedp, Xs, nullptr, inc(scratch), nullptr, nullptr, L,
-                                  st(scratch), partials(scratch), log3(scratch), kLogCap);
-        auto k2 = kfn<S2, W, I>();
-        k2<<<grid, block, 0, s>>>(bedp, Xs, inc(scratch), nullptr, Ys, lo(scratch), L,
-                                  st(scratch), partials(scratch), log3(scratch), kLogCap);
-    }
-
-    struct EvolveF {
-        Runner32* r; float* Qf; char* scratch; int n; cudaStream_t s;
-        template <int O, bool W, bool I> int operator()() {
-            const long long plane = r->L.plane;
-            float* A = Qf + plane;            // eta, hu, hv planes of the caller's Q
-            float* B = r->alt(scratch);
-            bool in_b = false;
-            for (int k = 0; k < n; ++k) {
-                r->template launch_step<O, W, I>(Qf, in_b ? B : A, in_b ? A : B, scratch, s);
-                in_b = !in_b;
-            }
-            if (in_b) {
-                cudaError_t e = cudaMemcpyAsync(A, B, size_t(plane) * 3 * sizeof(float),
-                                                cudaMemcpyDeviceToDevice, s);
-                if (e != cudaSuccess) return cuda_check(e, "zfv_evolve (fp32) copy-back");
-            }
-            return cuda_check(cudaGetLastError(), "zfv_evolve (fp32) launch");
-        }
-    };
-
-    int evolve(void* Qv, void* Av, char* scratch, int n, cudaStream_t s) override {
-        int rc = with_combo(EvolveF{this, (float*)Qv, scratch, n, s});
-        if (rc) return rc;
-        const int nb = int((L.plane + 255) / 256);
-        k32_aux<<<nb, 256, 0, s>>>((const float*)Qv, lo(scratch), (double*)Av, L.plane, n_aux, L.epsd);
-        return cuda_check(cudaGetLastError(), "zfv_evolve (fp32) aux launch");
-    }
-
-    int state_import(const double* Q64, void* Q, char* scratch, cudaStream_t s) override {
-        const int nb = int((L.plane + 255) / 256);
-        k32_import<<<nb, 256, 0, s>>>(Q64, (float*)Q, lo(scratch), L.plane);
-        return cuda_check(cudaGetLastError(), "zfv_state_import (fp32) launch");
-    }
-    int state_export(const void* Q, const char* scratch, double* Q64, cudaStream_t s) override {
-        const int nb = int((L.plane + 255) / 256);
-        k32_export<<<nb, 256, 0, s>>>((const float*)Q, lo(scratch), Q64, L.plane);
-        return cuda_check(cudaGetLastError(), "zfv_state_export (fp32) launch");
-    }
 };
 
 }  // namespace zfv32
 
 namespace zfvi {
-Runner* make_runner_fp32_swe2d(zfv_handle* h) { return new zfv32::Runner32<4, 16>(h); }
+Runner* make_runner_fp32_swe2d(zfv_handle* h) { return new zfv32::Runner32(h); }
 }
+
+// ---------------------------------------------------------------------------
+// Batch C ABI (include/zoomy_fv.h).
+struct zfv_batch {
+    zfv32::BatchCore core;
+};
+
+extern "C" {
+
+int zfv_tile_variants(int* nw, int* cpt, int max_n) {
+    for (int v = 0; v < zfv32::kNumVariants && v < max_n; ++v) {
+        if (nw) nw[v] = zfv32::kVarNW[v];
+        if (cpt) cpt[v] = zfv32::kVarCPT[v];
+    }
+    return zfv32::kNumVariants;
+}
+
+int zfv_batch_create(const zfv_config* cfgs, int n_inst, zfv_batch** out) {
+    if (!cfgs || !out) return fail(-1, "zfv_batch_create: null argument");
+    *out = nullptr;
+    zfv_batch* b = new (std::nothrow) zfv_batch();
+    if (!b) return fail(-4, "zfv_batch_create: out of host memory");
+    const int rc = b->core.init(cfgs, n_inst);
+    if (rc) { delete b; return rc; }
+    *out = b;
+    return 0;
+}
+
+int zfv_batch_destroy(zfv_batch* b) { delete b; return 0; }
+
+size_t zfv_batch_scratch_bytes(const zfv_batch* b) { return b ? b->core.total : 0; }
+
+int zfv_batch_bind(zfv_batch* b, void* const* Q, double* const* aux, void* scratch, void* stream) {
+    if (!b || !Q || !aux || !scratch) return fail(-1, "zfv_batch_bind: null argument");
+    return b->core.bind(Q, aux, static_cast<char*>(scratch), (cudaStream_t)stream);
+}
+
+int zfv_batch_import(zfv_batch* b, const double* const* Q64, void* stream) {
+    if (!b || !Q64 || !b->core.bound) return fail(-1, "zfv_batch_import: bind the batch first");
+    return b->core.convert(Q64, false, (cudaStream_t)stream);
+}
+
+int zfv_batch_export(zfv_batch* b, double* const* Q64, void* stream) {
+    if (!b || !Q64 || !b->core.bound) return fail(-1, "zfv_batch_export: bind the batch first");
+    return b->core.convert(const_cast<const double* const*>(Q64), true, (cudaStream_t)stream);
+}
+
+int zfv_batch_begin(zfv_batch* b, void* stream) {
+    if (!b || !b->core.bound) return fail(-1, "zfv_batch_begin: bind the batch first");
+    return b->core.begin((cudaStream_t)stream);
+}
+
+int zfv_batch_evolve(zfv_batch* b, int n_steps, void* stream) {
+    if (!b || !b->core.bound) return fail(-1, "zfv_batch_evolve: bind the batch first");
+    if (n_steps < 0) return fail(-1, "zfv_batch_evolve: negative step count");
+    return b->core.evolve(n_steps, (cudaStream_t)stream);
+}
+
+int zfv_batch_status(zfv_batch* b, zfv_status* out, void* stream) {
+    if (!b || !out || !b->core.bound) return fail(-1, "zfv_batch_status: bind the batch first");
+    return b->core.status(out, (cudaStream_t)stream);
+}
+
+int zfv_batch_set_variant(zfv_batch* b, int variant, void* stream) {
+    if (!b) return fail(-1, "zfv_batch_set_variant: null batch");
+    return b->core.set_variant(variant, (cudaStream_t)stream);
+}
+
+int zfv_batch_units(const zfv_batch* b) { return b ? b->core.nunits() : 0; }
+
+}  // extern "C"

@@ -30,9 +30,11 @@ class Level:
     FP64 plain form (cfg.precision == ZFV_PREC_FP64):
       Q:   (n_q, ny, nx) float64, rows [b, h, hu, (hv)]
     FP32 chosen form (ZFV_PREC_FP32, 2-D shallow water):
-      Q:   (4, ny, nx) float32, rows [b, eta = h + b, hu, hv]; the low-order
-           remainders of eta, hu, hv live in the scratch buffer. state64()
-           returns the combined state in the reference layout.
+      Q:   (4, ny, nx) float32, rows [b, eta = h + b, hu, hv] at import; steps
+           ping-pong the state between Q and a scratch buffer and keep the
+           low-order remainders of eta, hu, hv in scratch, so the state is
+           read through state64() (the reference layout, FP64), which also
+           refreshes aux's hinv row.
     aux: (n_aux, ny, nx) float64, last row hinv (both forms)
     """
 

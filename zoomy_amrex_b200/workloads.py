@@ -1,0 +1,78 @@
+"""Seeded synthetic inputs for the benchmark workloads.
+
+The reference quotes no public dataset for this path; these generators give
+the shapes and value distributions of its scenarios:
+
+* ``bump_field``: Gaussian-bump bathymetry (centres uniform in the box,
+  amplitudes U(0.2, 1.5) m, widths U(2, 10) m) under still water at eta0 plus
+  an optional Gaussian hump;
+* ``dam_break_ensemble``: independent shallow-water boxes of uneven size
+  (sides log-uniform per axis), each with its own bumps and a dam-break ratio
+  drawn U(1.2, 3.0), as a list of (config, Q0, aux0) for the FP32 batch engine.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from ._abi import ZFV_MODEL_SWE2D, ZFV_PREC_FP32, ZFV_PREC_FP64, make_config
+
+
+def _bumps(rng, n_bumps, x_extent, y_extent, width=(2.0, 10.0)):
+    cx, cy = rng.uniform(0, x_extent, n_bumps), rng.uniform(0, y_extent, n_bumps)
+    amp, wid = rng.uniform(0.2, 1.5, n_bumps), rng.uniform(width[0], width[1], n_bumps)
+    return cx, cy, amp, wid
+
+
+def _bed(xs, ys, bumps):
+    cx, cy, amp, wid = bumps
+    b = np.zeros((len(ys), len(xs)))
+    for k in range(len(cx)):
+        gx = np.exp(-((xs - cx[k]) ** 2) / (2 * wid[k] ** 2))
+        gy = np.exp(-((ys - cy[k]) ** 2) / (2 * wid[k] ** 2))
+        b += amp[k] * np.outer(gy, gx)
+    return b
+
+
+def dam_break_ensemble(n_inst: int = 256, seed: int = 4, side_range=(32, 512), dx: float = 0.1,
+                       n_bumps: int = 6, precision: int = ZFV_PREC_FP32, max_step: int = -1,
+                       time_end: float = 1.0e30, n_m: float = 0.03):
+    """``n_inst`` dam breaks over bumps on boxes of nx x ny cells of size dx.
+
+    Per instance: nx, ny = round(exp(U(log lo, log hi))); bumps with centres in
+    the box, amplitudes U(0.2, 1.5) m and widths U(0.05, 0.2) x the shorter
+    box side; eta = r on the left half and 1 m on the right half with
+    r ~ U(1.2, 3.0); h = max(eta - b, 0); walls; Manning n; order 2,
+    well-balanced, point-implicit source.
+    """
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(side_range[0]), np.log(side_range[1])
+    out = []
+    for _ in range(n_inst):
+        nx, ny = (int(round(np.exp(v))) for v in rng.uniform(lo, hi, 2))
+        ratio = rng.uniform(1.2, 3.0)
+        Lx, Ly = nx * dx, ny * dx
+        s = min(Lx, Ly)
+        bumps = _bumps(rng, n_bumps, Lx, Ly, width=(0.05 * s, 0.2 * s))
+        xs = (np.arange(nx) + 0.5) * dx
+        ys = (np.arange(ny) + 0.5) * dx
+        b = _bed(xs, ys, bumps)
+        eta = np.where(xs < 0.5 * Lx, ratio, 1.0)[None, :]
+        Q0 = np.zeros((4, ny, nx))
+        Q0[0] = b
+        Q0[1] = np.maximum(eta - b, 0.0)
+        aux0 = np.zeros((7, ny, nx))
+        cfg = make_config(ZFV_MODEL_SWE2D, nx, ny, (0.0, 0.0), (Lx, Ly), spatial_order=2,
+                          well_balanced=True, implicit_source=True, cfl=0.45, dtmin=1e-7,
+                          dtmax=1.0, time_end=time_end, max_step=max_step, bc=("wall",) * 4,
+                          params={"n_m": n_m}, precision=precision)
+        out.append((cfg, Q0, aux0))
+    return out
+
+
+def fp64_twin(cfg):
+    """The same configuration in the FP64 plain form."""
+    import ctypes as C
+    c = type(cfg)()
+    C.memmove(C.byref(c), C.byref(cfg), C.sizeof(cfg))
+    c.precision = ZFV_PREC_FP64
+    return c
