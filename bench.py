@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=100,
                     help="steps of the 256-box batched-vs-per-box comparison (0 = skip)")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
+                    help="skip the adjoint timing / gradient checks (1024^2, 200 steps)")
     ap.add_argument("--err-steps", type=int, default=1000,
                     help="steps of the FP32-vs-FP64 depth-error study (0 = skip)")
     return ap.parse_args()
@@ -192,14 +194,14 @@ def cpu_sample(kind: str, n: int, rows: int = 256, min_seconds: float = 10.0, ma
 
 
 def dist_setup(args):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    return ws, rank, local
+    """One process per GPU (torchrun). The reference arm runs on host cores
+    only, so its ranks meet over gloo."""
+    from zoomy_amrex_b200 import replicas
+    ws, rank, local = replicas.world()
+    if args.impl != "reference" and ws > 1:
+        import torch
+        torch.cuda.set_device(local)
+    return replicas.init("gloo" if args.impl == "reference" else "nccl", timeout_s=120)
 
 
 def run_reference(args, ws, rank):
@@ -286,8 +288,9 @@ def time_fp32_batched(n, Q0, A0, K, W, local, ws, barrier, max_over_ranks):
     assert not st["done"] and np.isfinite(st["dt"]), st
     from zoomy_amrex_b200.batch import tile_variants
     shapes = tile_variants()
-    tuning = {"picked": {"warps": shapes[best][0], "rows_per_warp": shapes[best][1]},
-              "ms_per_step": {f"{shapes[v][0]}x{shapes[v][1]}": t for v, t in times.items()}}
+    tuning = {"picked": {"warps": shapes[best][0], "rows_per_warp": shapes[best][1],
+                         "columns_per_lane": shapes[best][2]},
+              "ms_per_step": {f"{shapes[v][0]}x{shapes[v][1]}x{shapes[v][2]}": t for v, t in times.items()}}
     return ms, n * n * K * ws / (ms * 1e-3), st, tuning
 
 
@@ -354,6 +357,113 @@ def ensemble_bench(K, W, local, n_inst=256, seed=2027):
             "strip_shape_ms_per_step": {str(v): t for v, t in times.items()}, "picked_variant": best}
 
 
+def box5(a):
+    """5 x 5 box filter with mirrored edges."""
+    p = np.pad(a, 2, mode="symmetric")
+    out = np.zeros_like(a)
+    for dy in range(5):
+        for dx in range(5):
+            out += p[dy:dy + a.shape[0], dx:dx + a.shape[1]]
+    return out / 25.0
+
+
+def adjoint_bench(local, n=1024, steps=200, every=20, n_dirs=32, eps=1e-6, seed=2028):
+    """Gradients of 0.5 sum (eta_T - eta_obs)^2 after `steps` steps (config-2
+    setup at n x n) w.r.t. the bathymetry, Manning n and the initial h, hu, hv:
+    forward / backward timing, central differences on `n_dirs` seeded
+    directions, and FP64 torch autograd of the tensor restatement on a
+    128 x 128, 40-step case."""
+    import torch
+    from zoomy_amrex_b200.adjoint import evolve_differentiable, forward_only
+    dev = f"cuda:{local}"
+    rng = np.random.default_rng(seed)
+    Q0, A0 = workload_fields(n)
+    cfg = workload_config(n)
+    cfg.time_end = 1e30
+    # observations: the same run over a perturbed bed (N(0, 0.05^2), 5x5 box filter)
+    Qp = Q0.copy()
+    db = box5(rng.normal(0.0, 0.05, Q0[0].shape))
+    eta0 = Q0[0] + Q0[1]
+    Qp[0] = Q0[0] + db
+    Qp[1] = np.maximum(eta0 - Qp[0], 0.0)
+    A = torch.from_numpy(A0).to(dev)
+    QT_obs = forward_only(torch.from_numpy(Qp).to(dev), A, cfg, steps)
+    eta_obs = (QT_obs[0] + QT_obs[1]).detach()
+
+    def loss_of(QT):
+        e = QT[0] + QT[1] - eta_obs
+        return 0.5 * (e * e).sum()
+
+    base = torch.from_numpy(Q0).to(dev)
+    # forward alone (zfv_evolve, no checkpoints)
+    forward_only(base, A, cfg, 3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    forward_only(base, A, cfg, steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_fwd = e0.elapsed_time(e1)
+    # forward with checkpoints + backward
+    q = base.clone().requires_grad_(True)
+    nm = torch.tensor(0.03, dtype=torch.float64, device=dev, requires_grad=True)
+    e0.record()
+    L = loss_of(evolve_differentiable(q, nm, A, cfg, steps, checkpoint_every=every))
+    e1.record()
+    torch.cuda.synchronize()
+    ms_fwd_ck = e0.elapsed_time(e1)
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record()
+    L.backward()
+    b1.record()
+    torch.cuda.synchronize()
+    ms_bwd = b0.elapsed_time(b1)
+    gq, gnm = q.grad.detach(), float(nm.grad)
+    # central differences on seeded directions (wet cells only for h, hu, hv:
+    # a dry cell's depth cannot be perturbed both ways)
+    wet = torch.from_numpy((Q0[1] > 0).astype(np.float64)).to(dev)
+    errs = []
+    for k in range(n_dirs):
+        V = torch.from_numpy(rng.standard_normal(Q0.shape) * 1e-2).to(dev)
+        V[1:] *= wet
+        v_nm = float(rng.standard_normal() * 1e-3)
+        lp = float(loss_of(forward_only(base + eps * V, A, cfg, steps, n_m=0.03 + eps * v_nm)))
+        lm = float(loss_of(forward_only(base - eps * V, A, cfg, steps, n_m=0.03 - eps * v_nm)))
+        fd = (lp - lm) / (2 * eps)
+        an = float((gq * V).sum()) + gnm * v_nm
+        errs.append(abs(fd - an) / max(abs(fd), abs(an), 1e-300))
+    # torch autograd of the tensor restatement (small case)
+    from oracle import torch_swe as T
+    m = 128
+    Qs, As = workload_fields(m)
+    cfg_s = workload_config(m)
+    cfg_s.time_end = 1e30
+    As_t = torch.from_numpy(As).to(dev)
+    obs = (torch.from_numpy(Qs[0] + Qs[1]) + 0.01).to(dev)
+    qa = torch.from_numpy(Qs).to(dev).requires_grad_(True)
+    nma = torch.tensor(0.03, dtype=torch.float64, device=dev, requires_grad=True)
+    QTa = evolve_differentiable(qa, nma, As_t, cfg_s, 40, checkpoint_every=every)
+    (0.5 * ((QTa[0] + QTa[1] - obs) ** 2).sum()).backward()
+    qt = torch.from_numpy(Qs).to(dev).requires_grad_(True)
+    nmt = torch.tensor(0.03, dtype=torch.float64, device=dev, requires_grad=True)
+    p = dict(g=9.81, ex=0.0, ey=0.0, h_floor=1e-6, eps=1e-24)
+    QTt, _ = T.run(qt, As_t[6], nmt, 40, p, DOMAIN / m, DOMAIN / m, (1, 1, 1, 1))
+    (0.5 * ((QTt[0] + QTt[1] - obs) ** 2).sum()).backward()
+    ag_err = float((qa.grad - qt.grad).abs().max() / qt.grad.abs().max())
+    ag_nm = abs(float(nma.grad) - float(nmt.grad)) / abs(float(nmt.grad))
+    return {"workload": f"swe2d_{n}x{n} config-2 setup, loss 0.5 sum(eta_T - eta_obs)^2 after {steps} steps, "
+                        f"eta_obs from a bed + box5(N(0, 0.05^2)) run (seed {seed})",
+            "steps": steps, "checkpoint_every": every,
+            "ms_forward": ms_fwd, "ms_forward_with_checkpoints": ms_fwd_ck, "ms_backward": ms_bwd,
+            "adj_over_fwd": ms_bwd / ms_fwd,
+            "fd": {"directions": n_dirs, "eps": eps, "max_rel_err": max(errs),
+                   "median_rel_err": float(np.median(errs)),
+                   "note": "directions over (b, h, hu, hv, n_m); h, hu, hv perturbed on wet cells"},
+            "torch_autograd": {"case": f"{m}x{m}, 40 steps", "max_rel_err_state": ag_err,
+                               "rel_err_n_m": ag_nm}}
+
+
 def depth_error(n, Q0, A0, steps, local):
     """FP32 chosen form vs FP64 plain form after `steps` steps from the same
     state. The FP64 GPU form equals the CPU oracle bitwise (tests/test_gpu_parity.py),
@@ -386,8 +496,8 @@ def main():
     if args.impl == "reference":
         run_reference(args, ws, rank)
         if ws > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+            from zoomy_amrex_b200 import replicas
+            replicas.finish()
         return
 
     import torch
@@ -396,23 +506,16 @@ def main():
     if rank == 0 or ws == 1:
         build()
     if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+        from zoomy_amrex_b200 import replicas as _r
+        _r.barrier()
     from zoomy_amrex_b200._abi import ZFV_PREC_FP32, ZFV_PREC_FP64
     from zoomy_amrex_b200.level import Level
 
-    def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
+    from zoomy_amrex_b200 import replicas
+    barrier = replicas.barrier
 
     def max_over_ranks(v):
-        if ws == 1:
-            return v
-        import torch.distributed as dist
-        t = torch.tensor([v], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(v, device=f"cuda:{local}")
 
     n = args.n
     cells = n * n
@@ -441,6 +544,9 @@ def main():
     ens = None
     if args.ensemble_steps > 0:
         ens = ensemble_bench(args.ensemble_steps, args.warmup, local)
+    adj = None
+    if args.adjoint and rank == 0:
+        adj = adjoint_bench(local)
 
     err = None
     if args.err_steps > 0 and rank == 0:
@@ -502,15 +608,13 @@ def main():
                 "forms": {"fp32_chosen": v32, "fp64_plain": v64, "fp32_over_fp64": v32 / v64,
                           "ms_per_step_fp32": ms32 / K, "ms_per_step_fp64": ms64 / K},
                 "depth_error_fp32_vs_fp64": err,
-                "autotune": tuning, "ensemble": ens,
+                "autotune": tuning, "ensemble": ens, "adjoint": adj,
                 "hbm_gbs": achieved32,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 2 * K, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
-        dist.destroy_process_group()
+        replicas.finish()
 
 
 if __name__ == "__main__":

@@ -72,33 +72,43 @@ def test_batch_graph_replay_equals_eager(cuda):
 
 
 def test_batch_strip_variants_agree(cuda):
-    """Every compiled strip shape computes the same cell values; only the
-    order of the per-strip mass partial sums differs."""
+    """Strip shapes of the same sweep (scalar, or packed column pairs) compute
+    bitwise the same cell values; only the order of the mass partial sums
+    differs. The packed sweep rounds differently (FP32 pair instructions) and
+    agrees with the scalar one to FP32 accuracy."""
     from zoomy_amrex_b200.batch import Batch, tile_variants
     ens = _ens(4, seed=3, side_range=(40, 300))
     cfgs, Q0s, A0s = zip(*ens)
-    ref = None
-    for v in range(len(tile_variants())):
+    ref = {}
+    for v, (_, _, cols) in enumerate(tile_variants()):
         b = Batch(cfgs, Q0s, A0s, variant=v)
         b.begin(); b.evolve(30)
         Q = [q.cpu().numpy() for q in b.state64()]
         st = b.status()
         b.close()
-        if ref is None:
-            ref = (Q, st)
+        if cols not in ref:
+            ref[cols] = (Q, st)
             continue
         for k in range(len(ens)):
-            assert st[k]["time"] == ref[1][k]["time"]
-            assert np.array_equal(Q[k], ref[0][k]), (v, k)
-            assert abs(st[k]["mass"] - ref[1][k]["mass"]) <= 1e-13 * abs(ref[1][k]["mass"])
+            assert st[k]["time"] == ref[cols][1][k]["time"]
+            assert np.array_equal(Q[k], ref[cols][0][k]), (v, k)
+            assert abs(st[k]["mass"] - ref[cols][1][k]["mass"]) <= 1e-13 * abs(ref[cols][1][k]["mass"])
+    if 2 in ref and 1 in ref:
+        for k in range(len(ens)):
+            dh = np.abs(ref[2][0][k][1] - ref[1][0][k][1])
+            print(f"[packed vs scalar sweep] instance {k}: L1 {dh.mean():.2e} Linf {dh.max():.2e}")
+            assert dh.mean() <= 1e-6 and dh.max() <= 1e-4
+            assert abs(ref[2][1][k]["time"] - ref[1][1][k]["time"]) <= 1e-6 * ref[1][1][k]["time"]
 
 
-def test_batch_depth_error_vs_fp64(cuda, oracle):
-    """Batch members against the FP64 oracle (L1 depth, 60 steps)."""
+@pytest.mark.parametrize("variant", [0, 4])
+def test_batch_depth_error_vs_fp64(cuda, oracle, variant):
+    """Batch members against the FP64 oracle (L1 depth, 60 steps), scalar and
+    packed sweeps."""
     from zoomy_amrex_b200.batch import Batch
-    ens = _ens(3, seed=5, side_range=(32, 96), max_step=60)
+    ens = _ens(3, seed=5, side_range=(32, 130), max_step=60)
     cfgs, Q0s, A0s = zip(*ens)
-    b = Batch(cfgs, Q0s, A0s)
+    b = Batch(cfgs, Q0s, A0s, variant=variant)
     st = b.run(chunk=32)
     Qb = [q.cpu().numpy() for q in b.state64()]
     b.close()
@@ -110,6 +120,31 @@ def test_batch_depth_error_vs_fp64(cuda, oracle):
         print(f"[batch vs fp64 oracle] {cfg.nx}x{cfg.ny}: L1 {dh.mean():.3e} Linf {dh.max():.3e}")
         assert dh.mean() <= 1e-5     # the FP32 form's L1 depth bound
         assert dh.max() <= 1e-3
+
+
+def test_packed_sweep_keeps_lake_at_rest(cuda):
+    """Still water over bumps, fully wet, order 2, WB, implicit Manning: the
+    packed sweep keeps the momenta exactly zero (even and odd row lengths)."""
+    from zoomy_amrex_b200.batch import Batch
+    from zoomy_amrex_b200.workloads import dam_break_ensemble
+    ens = dam_break_ensemble(2, seed=8, side_range=(70, 140))
+    cfgs, Q0s, A0s = [], [], []
+    for k, (c, Q0, A0) in enumerate(ens):
+        Q = Q0.copy()
+        Q[1] = (Q0[0].max() + 0.5) - Q0[0]
+        Q[2:] = 0.0
+        cfgs.append(c); Q0s.append(Q); A0s.append(A0)
+    cfgs[1].nx -= 1 if cfgs[1].nx % 2 == 0 else 0          # one odd row length
+    Q0s[1] = Q0s[1][:, :, :cfgs[1].nx].copy()
+    A0s[1] = A0s[1][:, :, :cfgs[1].nx].copy()
+    cfgs[1].prob_hi[0] = cfgs[1].nx * 0.1
+    b = Batch(cfgs, Q0s, A0s, variant=4)
+    b.begin(); b.evolve(100)
+    Q = [q.cpu().numpy() for q in b.state64()]
+    b.close()
+    for k in range(2):
+        assert np.abs(Q[k][2:]).max() == 0.0, k
+        assert np.abs((Q[k][0] + Q[k][1]) - (Q0s[k][0] + Q0s[k][1])).max() < 1e-12
 
 
 def test_batch_rejects_mixed_schemes(cuda):

@@ -85,3 +85,35 @@ def test_two_rank_golden_and_box_invariance(cuda):
     ref = np.load(GOLDEN / "parallel_2rank.npz")
     assert np.abs(Q - ref["Q"]).max() == 0.0
     assert np.abs(Qaux - ref["Qaux"]).max() == 0.0
+
+
+def test_plotfiles_like_evolve(cuda, oracle, tmp_path):
+    """run_case with an output directory writes AMReX plotfiles where the
+    reference's Evolve does (ZoomyAmr.cpp:782-812): at the start of the first
+    step with time >= k * time_end / snapshots, and after the last step; the
+    last plotfile holds the golden (Q, Qaux), read the way the reference's
+    tests read it (tests/conftest.py:101-108)."""
+    from cases import golden_setup
+    from zoomy_amrex_b200.plotfile import read_plotfile
+    model = SME(level=0, dimension=2, bc="swashes", initial_conditions=stoker_ic)
+    settings = dict(ONE_D, time_end=1.0, cfl=CFL_1D, output_snapshots=7)
+    r = run_case(model, settings, str(tmp_path))
+    plts = sorted(tmp_path.glob("plt_*"))
+    assert [p.name for p in plts] == [f"plt_0{k:05d}" for k in range(len(plts))]
+    H, levels = read_plotfile(plts[-1])
+    arr = levels[0].patches[0].data
+    check("stoker_wet", arr[:3], arr[3:])
+    # expected write times from the oracle's per-step log
+    cfg, Q0, A0 = golden_setup("stoker_wet")
+    _, _, n, t_end, log, _ = oracle.run(cfg, Q0, A0)
+    plot_dt = 1.0 / 7
+    expect, nxt, t = [], 0.0, 0.0
+    for s in range(n):
+        if t >= nxt:
+            expect.append(t)
+            nxt += plot_dt
+        t = log[s, 1]
+    expect.append(t)
+    got = [read_plotfile(p)[0]["time"] for p in plts]
+    assert got == expect
+    assert r.plotfiles and pathlib.Path(r.plotfiles[-1]) == plts[-1]

@@ -20,13 +20,14 @@ from . import _lib
 from ._abi import MODELS, ZFV_MODEL_SWE2D, ZFV_PREC_FP32, zfv_config, zfv_status
 
 
-def tile_variants() -> list[tuple[int, int]]:
-    """The compiled strip shapes as (warps per block, rows per warp)."""
+def tile_variants() -> list[tuple[int, int, int]]:
+    """The compiled strip shapes as (warps per block, rows per warp, columns per lane)."""
     L = _lib.lib()
     nw = (C.c_int * 16)()
     cpt = (C.c_int * 16)()
-    n = int(L.zfv_tile_variants(nw, cpt, 16))
-    return [(nw[k], cpt[k]) for k in range(n)]
+    cols = (C.c_int * 16)()
+    n = int(L.zfv_tile_variants(nw, cpt, cols, 16))
+    return [(nw[k], cpt[k], cols[k]) for k in range(n)]
 
 
 class Batch:
@@ -147,6 +148,7 @@ class Batch:
         """Evolve every instance to its own stop (time_end / max_step)."""
         self.begin()
         done_steps = 0
+        last_steps = -1
         while True:
             n = chunk if max_steps is None else min(chunk, max_steps - done_steps)
             if n <= 0:
@@ -158,8 +160,13 @@ class Batch:
             else:
                 self.evolve(n)
             done_steps += n
-            if all(s["done"] for s in self.status()):
+            st = self.status()
+            if all(s["done"] for s in st):
                 break
+            steps = sum(s["step"] for s in st)
+            if steps <= last_steps:   # the device did not advance: stop, do not spin
+                raise _lib.ZfvError(f"no progress after {done_steps} requested steps")
+            last_steps = steps
         return self.status()
 
     def state64(self) -> list[torch.Tensor]:

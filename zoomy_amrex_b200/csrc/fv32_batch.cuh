@@ -4,8 +4,10 @@
 // parameters, boundary conditions, dt, time and stop test).
 //
 // A block takes work unit `blockIdx.x` = (instance, strip) from the unit
-// table, stages its instance's descriptor in shared memory and runs the
-// warp column sweep (fv32_sweep.cuh) on the strip. The CFL max / mass of an
+// table, stages its instance's descriptor in shared memory and runs a warp
+// column sweep on the strip: one column per lane (fv32_sweep.cuh, strips 30
+// columns wide, PK = 1) or a column pair per lane in packed FP32
+// (fv32_sweep2.cuh, 60 columns, PK = 2). The CFL max / mass of an
 // instance are reduced over that instance's units only: the last of its units
 // to finish advances its run record. A single level is a batch of one.
 //
@@ -16,6 +18,7 @@
 // any number of times; an instance that has stopped is left untouched.
 #pragma once
 #include "fv32_sweep.cuh"
+#include "fv32_sweep2.cuh"
 
 namespace zfv32 {
 
@@ -52,10 +55,11 @@ __device__ __forceinline__ const float* state_in(const BInst& D, unsigned parity
     return parity ? D.alt : D.Qs;
 }
 
-template <int MODE, bool WB, bool IMPL, int NW, int CPT>
+template <int MODE, bool WB, bool IMPL, int NW, int CPT, int PK>
 __global__ void __launch_bounds__(32 * NW)
 k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
 {
+    constexpr int SW = 30 * PK;                  // owned columns per strip
     constexpr int NT = 32 * NW;
     __shared__ double red[2 * NW];
     __shared__ BInst sD;
@@ -64,7 +68,7 @@ k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
     const Params& L = sD.P;
     const int w = threadIdx.x >> 5;
     const int bx = u.y % sD.nbx, by = u.y / sD.nbx;
-    const int x0 = bx * 30, y0 = by * (NW * CPT), j0 = y0 + w * CPT;
+    const int x0 = bx * SW, y0 = by * (NW * CPT), j0 = y0 + w * CPT;
     zfv::DevState* st = sD.st;
     if (*(volatile unsigned*)&st->flags & zfv::kFlagDone) return;   // stopped: state stays put
     const unsigned parity = *(volatile unsigned*)&st->parity;
@@ -75,12 +79,27 @@ k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
     double m_loc = 0.0, s_loc = 0.0;
     const float* inc_in = (MODE == S2) ? sD.inc : nullptr;   // stage 2 reads inc1
     float* inc_out = (MODE == S1) ? sD.inc : nullptr;        // stage 1 writes it
-    if (strip_interior<NW, CPT>(L, x0, y0))
-        sweep_strip<MODE, WB, IMPL, CPT, true>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
-                                               float(dtd), dtd, m_loc, s_loc);
-    else
-        sweep_strip<MODE, WB, IMPL, CPT, false>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
-                                                float(dtd), dtd, m_loc, s_loc);
+    if constexpr (PK == 1) {
+        if (strip_interior<NW, CPT>(L, x0, y0))
+            sweep_strip<MODE, WB, IMPL, CPT, true>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
+                                                   float(dtd), dtd, m_loc, s_loc);
+        else
+            sweep_strip<MODE, WB, IMPL, CPT, false>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
+                                                    float(dtd), dtd, m_loc, s_loc);
+    } else {
+        // 8-byte accesses need an even row length (x0 is even)
+        if (pk::strip_interior2<NW, CPT>(L, x0, y0)) {
+            if ((L.nx & 1) == 0)
+                pk::sweep_strip2<MODE, WB, IMPL, CPT, true, true>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
+                                                                  j0, float(dtd), dtd, m_loc, s_loc);
+            else
+                pk::sweep_strip2<MODE, WB, IMPL, CPT, true, false>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
+                                                                   j0, float(dtd), dtd, m_loc, s_loc);
+        } else {
+            pk::sweep_strip2<MODE, WB, IMPL, CPT, false, false>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
+                                                                j0, float(dtd), dtd, m_loc, s_loc);
+        }
+    }
     if constexpr (MODE == S2) {
         const bool last = zfv::finish_step_units<NT>(m_loc, s_loc, red, sD.partials, sD.log3, sD.log_cap,
                                                       st, L, dtd, time, false, unsigned(sD.nbx * sD.nby),
@@ -93,13 +112,14 @@ k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
 }
 
 // Per-cell helpers over the same unit table: each block covers its strip's
-// owned cells (30 x NW*CPT).
-template <int NW, int CPT, class F>
+// owned cells (30 PK x NW*CPT).
+template <int NW, int CPT, int PK, class F>
 __device__ __forceinline__ void for_strip_cells(const BInst& D, int2 u, F&& f) {
+    constexpr int SW = 30 * PK;
     const int bx = u.y % D.nbx, by = u.y / D.nbx;
-    const int x0 = bx * 30, y0 = by * (NW * CPT);
-    for (int k = threadIdx.x; k < 30 * NW * CPT; k += blockDim.x) {
-        const int i = x0 + k % 30, j = y0 + k / 30;
+    const int x0 = bx * SW, y0 = by * (NW * CPT);
+    for (int k = threadIdx.x; k < SW * NW * CPT; k += blockDim.x) {
+        const int i = x0 + k % SW, j = y0 + k / SW;
         if (i < D.P.nx && j < D.P.ny) f((long long)j * D.P.nx + i);
     }
 }
@@ -107,7 +127,7 @@ __device__ __forceinline__ void for_strip_cells(const BInst& D, int2 u, F&& f) {
 // FP64 reference layout [b, h, hu, hv] -> FP32 [b, eta, hu, hv] in Q plus
 // FP32 remainders: eta = h + b is formed in FP64 and split, so a lake at rest
 // imports as a constant eta. The state is left in Q (parity 0).
-template <int NW, int CPT>
+template <int NW, int CPT, int PK>
 __global__ void k32b_import(const BInst* __restrict__ insts, const int2* __restrict__ units) {
     __shared__ BInst sD;
     const int2 u = units[blockIdx.x];
@@ -116,7 +136,7 @@ __global__ void k32b_import(const BInst* __restrict__ insts, const int2* __restr
     const long long pl = sD.P.plane;
     const double* Q64 = sD.q64;
     float* Qb = const_cast<float*>(sD.bed);
-    for_strip_cells<NW, CPT>(sD, u, [&](long long c) {
+    for_strip_cells<NW, CPT, PK>(sD, u, [&](long long c) {
         const float b = float(Q64[c]);
         const double eta = Q64[pl + c] + Q64[c];
         const double hu = Q64[2 * pl + c], hv = Q64[3 * pl + c];
@@ -130,7 +150,7 @@ __global__ void k32b_import(const BInst* __restrict__ insts, const int2* __restr
 // The state in the reference layout (FP64, depth measured from the FP32 bed),
 // and the aux row hinv of that state (UpdateState's aux refresh; the carried
 // aux rows are untouched).
-template <int NW, int CPT>
+template <int NW, int CPT, int PK>
 __global__ void k32b_export(const BInst* __restrict__ insts, const int2* __restrict__ units, int n_aux) {
     __shared__ BInst sD;
     const int2 u = units[blockIdx.x];
@@ -138,7 +158,7 @@ __global__ void k32b_export(const BInst* __restrict__ insts, const int2* __restr
     const long long pl = sD.P.plane;
     double* Q64 = const_cast<double*>(sD.q64);
     const float* X = state_in(sD, *(volatile unsigned*)&sD.st->parity);
-    for_strip_cells<NW, CPT>(sD, u, [&](long long c) {
+    for_strip_cells<NW, CPT, PK>(sD, u, [&](long long c) {
         const double b = double(sD.bed[c]);
         const double eta = double(X[c]) + double(sD.lo[c]);
         const double h = eta - b;
@@ -165,7 +185,7 @@ __global__ void k32b_init(const BInst* __restrict__ insts, int n) {
 
 // ComputeDt (WHAT 0, clamped to time_end, from the stored aux as the
 // reference's first ComputeDt) or the FP64 mass (WHAT 1), per instance.
-template <int NW, int CPT, int WHAT>
+template <int NW, int CPT, int PK, int WHAT>
 __global__ void __launch_bounds__(32 * NW)
 k32b_reduce(const BInst* __restrict__ insts, const int2* __restrict__ units, int n_aux) {
     constexpr int NT = 32 * NW;
@@ -178,7 +198,7 @@ k32b_reduce(const BInst* __restrict__ insts, const int2* __restrict__ units, int
     const long long pl = L.plane;
     const float* X = state_in(sD, *(volatile unsigned*)&sD.st->parity);
     double m = 0.0, s = 0.0;
-    for_strip_cells<NW, CPT>(sD, u, [&](long long c) {
+    for_strip_cells<NW, CPT, PK>(sD, u, [&](long long c) {
         const double b = double(sD.bed[c]);
         const double h = (double(X[c]) + double(sD.lo[c])) - b;
         if constexpr (WHAT == 0) {

@@ -176,13 +176,15 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
     reconstruct(w0, w1, w2, lo_0, hi_0);     // row j0
     FaceR fb = face_rs<1, WB>(hi_m, lo_0, L);   // face below row j0
     RS top = hi_0;                           // row j0's state at its upper face
+    C4 w3 = fetch<MODE, INTERIOR>(bed, X, inc_in, L, i, j0 + 2);
 
 #pragma unroll 1
     for (int r = 0; r < CPT; ++r) {
         const int j = j0 + r;
         if (j >= ny) break;                  // uniform across the warp
-        // row j: w1; rows j-1, j+1: w0, w2; load row j+2
-        const C4 w3 = fetch<MODE, INTERIOR>(bed, X, inc_in, L, i, j + 2);
+        // row j: w1; rows j-1, j+1, j+2: w0, w2, w3. Row j+3 is loaded one
+        // iteration ahead so its latency overlaps this row's arithmetic.
+        const C4 w4 = (r + 1 < CPT) ? fetch<MODE, INTERIOR>(bed, X, inc_in, L, i, j + 3) : w3;
         RS lo_1, hi_1;
         reconstruct(w1, w2, w3, lo_1, hi_1);  // row j+1 in y
         const FaceR ft = face_rs<1, WB>(top, lo_1, L);   // face above row j
@@ -190,8 +192,10 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
         // x reconstruction of row j
         C4 ex{};
         if (has_e) ex = fetch<MODE, INTERIOR>(bed, X, inc_in, L, xe, j);
-        const C4 left = (lane == 0) ? ex : shfl_up_c4(w1, 1);
+        // every lane takes part in both shuffles (full-mask shuffles), then selects
+        const C4 up = shfl_up_c4(w1, 1);
         const C4 dn = shfl_down_c4(w1, 1);
+        const C4 left = (lane == 0) ? ex : up;
         const C4 right = (lane == 31) ? ex : dn;
         RS xlo, xhi;
         reconstruct(left, w1, right, xlo, xhi);
@@ -275,7 +279,7 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
         // advance: row j+1 becomes the current row
         fb = ft;
         top = hi_1;
-        w0 = w1; w1 = w2; w2 = w3;
+        w0 = w1; w1 = w2; w2 = w3; w3 = w4;
     }
 }
 

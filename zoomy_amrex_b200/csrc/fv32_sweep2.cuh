@@ -1,0 +1,390 @@
+// FP32 chosen form: the paired-column warp sweep (sm_100 packed FP32).
+//
+// The same column sweep as fv32_sweep.cuh, with each lane holding TWO
+// adjacent columns (A = x0-2+2L, B = A+1) and doing their arithmetic as
+// float2 pairs through Blackwell's packed FP32 instructions (FADD2/FMUL2/FFMA2
+// via __fadd2_rn/__fmul2_rn/__ffma2_rn): one instruction advances both
+// columns' reconstruction, faces and update. A strip is 60 owned columns
+// (lanes 1..30); lanes 0 and 31 hold the neighbour column pairs, and, unlike
+// the one-column sweep, need no extra loads (the x-stencil of every face a
+// lane evaluates lies inside the 64 columns the warp holds).
+//
+// Per row a lane
+//   * reconstructs A and B in x (neighbours: lane-1's B, lane+1's A by shuffle)
+//     and the next row in y (register window, as before),
+//   * evaluates, packed, the x-faces left of A and between A and B, and the
+//     y-faces above A and B,
+//   * takes the face right of B from lane+1 (its face left of A),
+//   * assembles, applies the point-implicit Manning update (packed; cells
+//     below h = 1e-3 fall back to the per-cell FP64 solve) and writes.
+// Loads and stores are float2 (8-byte) when the strip is interior and nx is
+// even; otherwise per-element with the ghost-cell mirror of fetch().
+#pragma once
+
+namespace zfv32 {
+namespace pk {
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 s2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+__device__ __forceinline__ float2 mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 neg(float2 a) { return f2(-a.x, -a.y); }
+__device__ __forceinline__ float2 mm(float2 a, float2 b) { return f2(zfv32::mm(a.x, b.x), zfv32::mm(a.y, b.y)); }
+__device__ __forceinline__ float2 fmax2(float2 a, float2 b) { return f2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
+__device__ __forceinline__ float2 fabs2(float2 a) { return f2(fabsf(a.x), fabsf(a.y)); }
+__device__ __forceinline__ float2 sqrt2(float2 a) { return f2(sqrtf(a.x), sqrtf(a.y)); }
+__device__ __forceinline__ float2 rsqrt2(float2 a) { return f2(rsqrtf(a.x), rsqrtf(a.y)); }
+
+struct C42 { float2 b, e, u, v; };          // cells A, B: bed, eta, hu, hv
+struct RS2 { float2 b, h, e, u, v; };       // reconstructed face states of A, B
+
+// KP desingularised 1/h (the model's update_aux_variables), packed.
+__device__ __forceinline__ float2 kp_hinv2(float2 h, float eps) {
+    const float2 h2 = mul(h, h);
+    const float2 x0 = mul(h2, h2);
+    return mul(mul(s2(1.41421356237f), h), rsqrt2(add(x0, fmax2(x0, s2(eps)))));
+}
+
+__device__ __forceinline__ void reconstruct2(const C42& m, const C42& c, const C42& p, RS2& lo, RS2& hi) {
+    const float2 dbm = sub(c.b, m.b), dbp = sub(p.b, c.b);
+    const float2 dem = sub(c.e, m.e), dep = sub(p.e, c.e);
+    const float2 gb = mm(dbm, dbp);
+    const float2 gh = mm(sub(dem, dbm), sub(dep, dbp));
+    const float2 gu = mm(sub(c.u, m.u), sub(p.u, c.u));
+    const float2 gv = mm(sub(c.v, m.v), sub(p.v, c.v));
+    const float2 h = sub(c.e, c.b);
+    const float2 half = s2(0.5f);
+    const float2 hb = mul(half, gb), hh = mul(half, gh), he = mul(half, add(gh, gb));
+    const float2 hu = mul(half, gu), hv = mul(half, gv);
+    hi = RS2{add(c.b, hb), add(h, hh), add(c.e, he), add(c.u, hu), add(c.v, hv)};
+    lo = RS2{sub(c.b, hb), sub(h, hh), sub(c.e, he), sub(c.u, hu), sub(c.v, hv)};
+}
+
+struct Face2 {
+    float2 f0, f1, f2;       // central flux (h, hu, hv)
+    float2 dp0, dp1, dp2;    // D+
+    float2 dm0, dm1, dm2;    // D-
+    float2 pl, pr;           // P(h*_L), P(h*_R)
+};
+
+// Two faces at once from their reconstructed left (a) / right (c) states.
+template <int DIR, bool WB>
+__device__ __forceinline__ Face2 face2(RS2 a, RS2 c, const Params& L) {
+    float2 db = s2(0.0f);
+    if constexpr (WB) {
+        const float2 bf = fmax2(a.b, c.b);
+        const float2 hsL = fmax2(s2(0.0f), sub(a.e, bf)), hsR = fmax2(s2(0.0f), sub(c.e, bf));
+        const float2 sL = f2((a.h.x > 0.0f) ? __fdividef(hsL.x, a.h.x) : 0.0f,
+                             (a.h.y > 0.0f) ? __fdividef(hsL.y, a.h.y) : 0.0f);
+        const float2 sR = f2((c.h.x > 0.0f) ? __fdividef(hsR.x, c.h.x) : 0.0f,
+                             (c.h.y > 0.0f) ? __fdividef(hsR.y, c.h.y) : 0.0f);
+        a.u = mul(a.u, sL); a.v = mul(a.v, sL); c.u = mul(c.u, sR); c.v = mul(c.v, sR);
+        a.h = hsL; c.h = hsR;
+    } else {
+        db = sub(c.b, a.b);
+    }
+    const float2 g = s2(L.g), hg = s2(0.5f * L.g), half = s2(0.5f);
+    const float2 hiL = kp_hinv2(a.h, L.eps), hiR = kp_hinv2(c.h, L.eps);
+    const float2 unL = (DIR == 0) ? a.u : a.v, unR = (DIR == 0) ? c.u : c.v;
+    const float2 pL = mul(mul(hg, a.h), a.h), pR = mul(mul(hg, c.h), c.h);
+    const float2 qL = mul(unL, hiL), qR = mul(unR, hiR);
+    float2 fuL, fvL, fuR, fvR;
+    if constexpr (DIR == 0) {
+        fuL = fma(a.u, qL, pL);  fvL = mul(a.v, qL);
+        fuR = fma(c.u, qR, pR);  fvR = mul(c.v, qR);
+    } else {
+        fuL = mul(a.u, qL);  fvL = fma(a.v, qL, pL);
+        fuR = mul(c.u, qR);  fvR = fma(c.v, qR, pR);
+    }
+    Face2 F;
+    F.f0 = mul(half, add(unL, unR));
+    F.f1 = mul(half, add(fuL, fuR));
+    F.f2 = mul(half, add(fvL, fvR));
+    const float2 evL = add(fabs2(qL), sqrt2(mul(g, fmax2(a.h, s2(0.0f)))));
+    const float2 evR = add(fabs2(qR), sqrt2(mul(g, fmax2(c.h, s2(0.0f)))));
+    const float2 hs = mul(half, fmax2(evL, evR));
+    const float2 dh = sub(c.h, a.h), du = sub(c.u, a.u), dv = sub(c.v, a.v);
+    float2 bu = s2(0.0f), bv = s2(0.0f);
+    if constexpr (!WB) {
+        const float2 Bn = mul(mul(hg, mul(half, add(a.h, c.h))), db);
+        if (DIR == 0) bu = Bn; else bv = Bn;
+    }
+    F.dp0 = mul(hs, dh);      F.dm0 = neg(F.dp0);
+    F.dp1 = fma(hs, du, bu);  F.dm1 = fma(neg(hs), du, bu);
+    F.dp2 = fma(hs, dv, bv);  F.dm2 = fma(neg(hs), dv, bv);
+    F.pl = pL;
+    F.pr = pR;
+    return F;
+}
+
+// Stage input of the column pair (cA, cA+1) in row j.
+template <int MODE, bool INTERIOR, bool VEC>
+__device__ __forceinline__ C42 fetch2(const float* __restrict__ bed, const float* __restrict__ X,
+                                      const float* __restrict__ inc, const Params& L, int cA, int j) {
+    if constexpr (INTERIOR && VEC) {
+        const long long pl = L.plane;
+        const long long c = (long long)j * L.nx + cA;
+        C42 q;
+        q.b = __ldg(reinterpret_cast<const float2*>(bed + c));
+        q.e = __ldg(reinterpret_cast<const float2*>(X + c));
+        q.u = __ldg(reinterpret_cast<const float2*>(X + pl + c));
+        q.v = __ldg(reinterpret_cast<const float2*>(X + 2 * pl + c));
+        if constexpr (MODE == S2) {
+            q.e = add(q.e, __ldg(reinterpret_cast<const float2*>(inc + c)));
+            q.u = add(q.u, __ldg(reinterpret_cast<const float2*>(inc + pl + c)));
+            q.v = add(q.v, __ldg(reinterpret_cast<const float2*>(inc + 2 * pl + c)));
+        }
+        return q;
+    } else {
+        const C4 a = fetch<MODE, INTERIOR>(bed, X, inc, L, cA, j);
+        const C4 b = fetch<MODE, INTERIOR>(bed, X, inc, L, cA + 1, j);
+        return C42{f2(a.b, b.b), f2(a.e, b.e), f2(a.u, b.u), f2(a.v, b.v)};
+    }
+}
+
+// Packed point-implicit Manning update of two cells (FP32; the caller routes
+// near-dry pairs to the per-cell solve). Explicit fallback per cell as in
+// make_rhs.H:501-508.
+__device__ __forceinline__ void manning_implicit2(float2 h, float2 u, float2 v, float2 hinv, float dt,
+                                                  const Params& L, float2& du, float2& dv) {
+    const float2 m = fmax2(h, s2(L.hfloor));
+    // m^(-1/3) from the hardware log2 / exp2 (relative error ~1e-7)
+    const float2 ic = f2(exp2f(-0.333333343f * __log2f(m.x)), exp2f(-0.333333343f * __log2f(m.y)));
+    const float2 k = mul(s2(L.g * L.nm * L.nm), ic);
+    const float2 ux = mul(u, hinv), uy = mul(v, hinv);
+    const float2 sp = sqrt2(fma(ux, ux, mul(uy, uy)));
+    const float2 Su = sub(mul(s2(L.g * L.ex), h), mul(mul(k, ux), sp));
+    const float2 Sv = sub(mul(s2(L.g * L.ey), h), mul(mul(k, uy), sp));
+    const float2 rsp = f2(sp.x > 0.0f ? __frcp_rn(sp.x) : 0.0f, sp.y > 0.0f ? __frcp_rn(sp.y) : 0.0f);
+    const float2 dsx = mul(mul(ux, hinv), rsp), dsy = mul(mul(uy, hinv), rsp);
+    const float2 nk = neg(k), vdt = s2(dt), one = s2(1.0f);
+    const float2 J22 = mul(nk, fma(hinv, sp, mul(ux, dsx))), J23 = mul(nk, mul(ux, dsy));
+    const float2 J32 = mul(nk, mul(uy, dsx)), J33 = mul(nk, fma(hinv, sp, mul(uy, dsy)));
+    const float2 a = fma(neg(vdt), J22, one), b = mul(neg(vdt), J23);
+    const float2 c = mul(neg(vdt), J32), d = fma(neg(vdt), J33, one);
+    const float2 det = sub(mul(a, d), mul(b, c));
+    const float2 r0 = mul(vdt, Su), r1 = mul(vdt, Sv);
+    const float2 rdet = f2(__frcp_rn(det.x), __frcp_rn(det.y));
+    const float2 x0 = mul(sub(mul(r0, d), mul(b, r1)), rdet);
+    const float2 x1 = mul(sub(mul(a, r1), mul(c, r0)), rdet);
+    const bool okx = fabsf(det.x) > 0.0f && isfinite(det.x) && isfinite(x0.x) && isfinite(x1.x);
+    const bool oky = fabsf(det.y) > 0.0f && isfinite(det.y) && isfinite(x0.y) && isfinite(x1.y);
+    du = f2(okx ? x0.x : (isfinite(r0.x) ? r0.x : 0.0f), oky ? x0.y : (isfinite(r0.y) ? r0.y : 0.0f));
+    dv = f2(okx ? x1.x : (isfinite(r1.x) ? r1.x : 0.0f), oky ? x1.y : (isfinite(r1.y) ? r1.y : 0.0f));
+}
+
+__device__ __forceinline__ float2 shfl_up2(float2 v, int d) {
+    return f2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
+}
+
+// One warp's sub-strip of the paired sweep: column pairs x0-2+2L, rows j0 .. j0+CPT-1.
+template <int MODE, bool WB, bool IMPL, int CPT, bool INTERIOR, bool VEC>
+__device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, const float* __restrict__ X,
+                                             const float* __restrict__ inc_in, float* __restrict__ inc_out,
+                                             float* __restrict__ Y, float* __restrict__ lo, const Params& L,
+                                             int x0, int j0, float dt, double dtd, double& m_loc,
+                                             double& s_loc) {
+    const int lane = threadIdx.x & 31;
+    const int nx = L.nx, ny = L.ny;
+    const long long pl = L.plane;
+    const int cA = x0 - 2 + 2 * lane;
+    const bool inner = (lane >= 1) && (lane <= 30);
+    const bool ownA = inner && (cA < nx), ownB = inner && (cA + 1 < nx);
+    const bool vec_io = VEC && INTERIOR;    // both cells in the domain, 8-byte aligned
+
+    C42 wm = fetch2<MODE, INTERIOR, VEC>(bed, X, inc_in, L, cA, j0 - 2);
+    C42 w0 = fetch2<MODE, INTERIOR, VEC>(bed, X, inc_in, L, cA, j0 - 1);
+    C42 w1 = fetch2<MODE, INTERIOR, VEC>(bed, X, inc_in, L, cA, j0);
+    C42 w2 = fetch2<MODE, INTERIOR, VEC>(bed, X, inc_in, L, cA, j0 + 1);
+    RS2 lo_m, hi_m, lo_0, hi_0;
+    reconstruct2(wm, w0, w1, lo_m, hi_m);
+    reconstruct2(w0, w1, w2, lo_0, hi_0);
+    Face2 fb = face2<1, WB>(hi_m, lo_0, L);
+    RS2 top = hi_0;
+    const float2 rdx = s2(L.rdx), rdy = s2(L.rdy), vdt = s2(dt);
+    C42 w3 = fetch2<MODE, INTERIOR, VEC>(bed, X, inc_in, L, cA, j0 + 2);
+
+#pragma unroll 1
+    for (int r = 0; r < CPT; ++r) {
+        const int j = j0 + r;
+        if (j >= ny) break;                  // uniform across the warp
+        // row j+3 is loaded one iteration ahead (latency hidden behind this row)
+        const C42 w4 = (r + 1 < CPT) ? fetch2<MODE, INTERIOR, VEC>(bed, X, inc_in, L, cA, j + 3) : w3;
+        RS2 lo_1, hi_1;
+        reconstruct2(w1, w2, w3, lo_1, hi_1);
+        const Face2 ft = face2<1, WB>(top, lo_1, L);
+
+        // x: A's left neighbour is lane-1's B, B's right neighbour is lane+1's A
+        const float pb = __shfl_up_sync(0xffffffffu, w1.b.y, 1), pe = __shfl_up_sync(0xffffffffu, w1.e.y, 1);
+        const float pu = __shfl_up_sync(0xffffffffu, w1.u.y, 1), pv = __shfl_up_sync(0xffffffffu, w1.v.y, 1);
+        const float nb = __shfl_down_sync(0xffffffffu, w1.b.x, 1), ne = __shfl_down_sync(0xffffffffu, w1.e.x, 1);
+        const float nu = __shfl_down_sync(0xffffffffu, w1.u.x, 1), nv = __shfl_down_sync(0xffffffffu, w1.v.x, 1);
+        const C42 m{f2(pb, w1.b.x), f2(pe, w1.e.x), f2(pu, w1.u.x), f2(pv, w1.v.x)};
+        const C42 p{f2(w1.b.y, nb), f2(w1.e.y, ne), f2(w1.u.y, nu), f2(w1.v.y, nv)};
+        RS2 xlo, xhi;
+        reconstruct2(m, w1, p, xlo, xhi);
+        // left states: (lane-1's B at its upper face, A at its upper face)
+        const RS2 xl{f2(__shfl_up_sync(0xffffffffu, xhi.b.y, 1), xhi.b.x),
+                     f2(__shfl_up_sync(0xffffffffu, xhi.h.y, 1), xhi.h.x),
+                     f2(__shfl_up_sync(0xffffffffu, xhi.e.y, 1), xhi.e.x),
+                     f2(__shfl_up_sync(0xffffffffu, xhi.u.y, 1), xhi.u.x),
+                     f2(__shfl_up_sync(0xffffffffu, xhi.v.y, 1), xhi.v.x)};
+        const Face2 fl = face2<0, WB>(xl, xlo, L);   // faces left of A and between A and B
+        // faces right of A and B: (A|B, lane+1's left-of-A)
+        Face2 fr;
+        fr.f0 = f2(fl.f0.y, __shfl_down_sync(0xffffffffu, fl.f0.x, 1));
+        fr.f1 = f2(fl.f1.y, __shfl_down_sync(0xffffffffu, fl.f1.x, 1));
+        fr.f2 = f2(fl.f2.y, __shfl_down_sync(0xffffffffu, fl.f2.x, 1));
+        fr.dm0 = f2(fl.dm0.y, __shfl_down_sync(0xffffffffu, fl.dm0.x, 1));
+        fr.dm1 = f2(fl.dm1.y, __shfl_down_sync(0xffffffffu, fl.dm1.x, 1));
+        fr.dm2 = f2(fl.dm2.y, __shfl_down_sync(0xffffffffu, fl.dm2.x, 1));
+        fr.pl = f2(fl.pl.y, __shfl_down_sync(0xffffffffu, fl.pl.x, 1));
+
+        if (ownA || ownB) {
+            // make_rhs.H:346-399, WB bed source folded in before the 1/dx scaling
+            float2 Ax0 = sub(sub(neg(sub(fr.f0, fl.f0)), fr.dm0), fl.dp0);
+            float2 Ax1 = sub(sub(neg(sub(fr.f1, fl.f1)), fr.dm1), fl.dp1);
+            float2 Ax2 = sub(sub(neg(sub(fr.f2, fl.f2)), fr.dm2), fl.dp2);
+            float2 Ay0 = sub(sub(neg(sub(ft.f0, fb.f0)), ft.dm0), fb.dp0);
+            float2 Ay1 = sub(sub(neg(sub(ft.f1, fb.f1)), ft.dm1), fb.dp1);
+            float2 Ay2 = sub(sub(neg(sub(ft.f2, fb.f2)), ft.dm2), fb.dp2);
+            if constexpr (WB) {
+                Ax1 = add(Ax1, sub(fr.pl, fl.pr));
+                Ay2 = add(Ay2, sub(ft.pl, fb.pr));
+            }
+            const float2 r0 = fma(Ax0, rdx, mul(Ay0, rdy));
+            const float2 r1 = fma(Ax1, rdx, mul(Ay1, rdy));
+            const float2 r2 = fma(Ax2, rdx, mul(Ay2, rdy));
+            const float2 h = sub(w1.e, w1.b);
+            const float2 hinv = kp_hinv2(h, L.eps);
+            float2 inc_e = mul(vdt, r0), inc_u = mul(vdt, r1), inc_v = mul(vdt, r2);
+            if constexpr (!IMPL) {
+                const float2 mh = fmax2(h, s2(L.hfloor));
+                const float2 k = mul(s2(L.g * L.nm * L.nm),
+                                     f2(zb::inv_cbrt_pos(mh.x), zb::inv_cbrt_pos(mh.y)));
+                const float2 ux = mul(w1.u, hinv), uy = mul(w1.v, hinv);
+                const float2 sp = sqrt2(fma(ux, ux, mul(uy, uy)));
+                inc_u = fma(vdt, sub(mul(s2(L.g * L.ex), h), mul(mul(k, ux), sp)), inc_u);
+                inc_v = fma(vdt, sub(mul(s2(L.g * L.ey), h), mul(mul(k, uy), sp)), inc_v);
+            } else {
+                const float2 he = add(h, inc_e), ue = add(w1.u, inc_u), ve = add(w1.v, inc_v);
+                if (he.x < kNearDry || he.y < kNearDry) {
+                    float du[2], dv[2];
+                    const float hh[2] = {he.x, he.y}, uu[2] = {ue.x, ue.y}, vv[2] = {ve.x, ve.y};
+                    const float hi[2] = {hinv.x, hinv.y};
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        if (hh[k] < kNearDry) {
+                            double a, b;
+                            manning_implicit<double>(double(hh[k]), double(uu[k]), double(vv[k]), double(hi[k]),
+                                                     dtd, L.gd, L.exd, L.eyd, L.nmd, L.hfloord, a, b);
+                            du[k] = float(a); dv[k] = float(b);
+                        } else {
+                            manning_implicit<float>(hh[k], uu[k], vv[k], hi[k], dt, L.g, L.ex, L.ey, L.nm,
+                                                    L.hfloor, du[k], dv[k]);
+                        }
+                    }
+                    inc_u = add(inc_u, f2(du[0], du[1]));
+                    inc_v = add(inc_v, f2(dv[0], dv[1]));
+                } else {
+                    float2 du, dv;
+                    manning_implicit2(he, ue, ve, hinv, dt, L, du, dv);
+                    inc_u = add(inc_u, du);
+                    inc_v = add(inc_v, dv);
+                }
+            }
+            const long long c = (long long)j * nx + cA;
+            if constexpr (MODE == S1) {
+                if (vec_io) {
+                    *reinterpret_cast<float2*>(inc_out + c) = inc_e;
+                    *reinterpret_cast<float2*>(inc_out + pl + c) = inc_u;
+                    *reinterpret_cast<float2*>(inc_out + 2 * pl + c) = inc_v;
+                } else {
+                    if (ownA) { inc_out[c] = inc_e.x; inc_out[pl + c] = inc_u.x; inc_out[2 * pl + c] = inc_v.x; }
+                    if (ownB) { inc_out[c + 1] = inc_e.y; inc_out[pl + c + 1] = inc_u.y; inc_out[2 * pl + c + 1] = inc_v.y; }
+                }
+            } else {
+                // compensated Heun update in FP64, per cell
+                float i1[2][3], xs[2][3], lw[2][3];
+                if (vec_io) {
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        const float2 a = __ldg(reinterpret_cast<const float2*>(inc_in + q * pl + c));
+                        const float2 b = __ldg(reinterpret_cast<const float2*>(X + q * pl + c));
+                        const float2 l = *reinterpret_cast<const float2*>(lo + q * pl + c);
+                        i1[0][q] = a.x; i1[1][q] = a.y; xs[0][q] = b.x; xs[1][q] = b.y; lw[0][q] = l.x; lw[1][q] = l.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        const bool own = k == 0 ? ownA : ownB;
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) {
+                            i1[k][q] = own ? __ldg(inc_in + q * pl + c + k) : 0.0f;
+                            xs[k][q] = own ? __ldg(X + q * pl + c + k) : 0.0f;
+                            lw[k][q] = own ? lo[q * pl + c + k] : 0.0f;
+                        }
+                    }
+                }
+                const float i2[2][3] = {{inc_e.x, inc_u.x, inc_v.x}, {inc_e.y, inc_u.y, inc_v.y}};
+                const float bb[2] = {w1.b.x, w1.b.y};
+                float nf[2][3], nl[2][3];
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    double nd[3];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        nd[q] = (double(xs[k][q]) + double(lw[k][q])) + 0.5 * (double(i1[k][q]) + double(i2[k][q]));
+                        nf[k][q] = float(nd[q]);
+                        nl[k][q] = float(nd[q] - double(nf[k][q]));
+                    }
+                    const bool own = k == 0 ? ownA : ownB;
+                    if (own) {
+                        // CFL terms of the new state (ZoomyAmr.cpp:472-487) and its FP64 mass
+                        const float hn = nf[k][0] - bb[k];
+                        const float hin = kp_hinv(hn, L.eps);
+                        const float c0 = sqrtf(L.g * fmaxf(hn, 0.0f));
+                        const float evx = (fabsf(nf[k][1] * hin) + c0) * L.rfdx;
+                        const float evy = (fabsf(nf[k][2] * hin) + c0) * L.rfdy;
+                        const float mm_ = fmaxf(fmaxf(evx, evy), 0.0f);
+                        if (double(mm_) > m_loc) m_loc = double(mm_);
+                        s_loc = s_loc + (nd[0] - double(bb[k]));
+                    }
+                }
+                if (vec_io) {
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        *reinterpret_cast<float2*>(Y + q * pl + c) = f2(nf[0][q], nf[1][q]);
+                        *reinterpret_cast<float2*>(lo + q * pl + c) = f2(nl[0][q], nl[1][q]);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        if (!(k == 0 ? ownA : ownB)) continue;
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) {
+                            Y[q * pl + c + k] = nf[k][q];
+                            lo[q * pl + c + k] = nl[k][q];
+                        }
+                    }
+                }
+            }
+        }
+        fb = ft;
+        top = hi_1;
+        w0 = w1; w1 = w2; w2 = w3; w3 = w4;
+    }
+    (void)w0;
+}
+
+// Whether a paired strip's stencil lies inside the domain (columns x0-2 ..
+// x0+61, rows y0-2 .. y0+rows+1).
+template <int NW, int CPT>
+__device__ __forceinline__ bool strip_interior2(const Params& L, int x0, int y0) {
+    return (x0 - 2 >= 0) && (x0 + 61 <= L.nx - 1) && (y0 - 2 >= 0) && (y0 + NW * CPT + 1 <= L.ny - 1);
+}
+
+}  // namespace pk
+}  // namespace zfv32

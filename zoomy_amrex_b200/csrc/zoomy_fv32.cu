@@ -109,19 +109,24 @@ enum Mode { S1 = 1, S2 = 2 };
 
 namespace zfv32 {
 
-// Compiled strip shapes: (warps per block, rows per warp = cells per thread).
-// A strip is 30 columns x (NW * CPT) rows.
-constexpr int kNumVariants = 4;
-constexpr int kVarNW[kNumVariants] = {4, 4, 8, 2};
-constexpr int kVarCPT[kNumVariants] = {16, 8, 8, 32};
+// Compiled strip shapes: (warps per block, rows per warp = cells per thread,
+// columns per lane). A strip is 30 * PK columns x (NW * CPT) rows; PK = 2 is
+// the packed-FP32 paired-column sweep.
+constexpr int kNumVariants = 7;
+constexpr int kVarNW[kNumVariants] = {4, 4, 8, 2, 4, 4, 8};
+constexpr int kVarCPT[kNumVariants] = {16, 8, 8, 32, 16, 8, 8};
+constexpr int kVarPK[kNumVariants] = {1, 1, 1, 1, 2, 2, 2};
 
 template <class F>
 int with_variant(int v, F&& f) {
     switch (v) {
-    case 0: return f.template operator()<4, 16>();
-    case 1: return f.template operator()<4, 8>();
-    case 2: return f.template operator()<8, 8>();
-    case 3: return f.template operator()<2, 32>();
+    case 0: return f.template operator()<4, 16, 1>();
+    case 1: return f.template operator()<4, 8, 1>();
+    case 2: return f.template operator()<8, 8, 1>();
+    case 3: return f.template operator()<2, 32, 1>();
+    case 4: return f.template operator()<4, 16, 2>();
+    case 5: return f.template operator()<4, 8, 2>();
+    case 6: return f.template operator()<8, 8, 2>();
     default: return fail(-1, "unknown strip variant %d", v);
     }
 }
@@ -146,8 +151,8 @@ Params make_params(const zfv_config& c) {
 }
 
 int units_of(const zfv_config& c, int v) {
-    const int rows = kVarNW[v] * kVarCPT[v];
-    return ((c.nx + 29) / 30) * ((c.ny + rows - 1) / rows);
+    const int rows = kVarNW[v] * kVarCPT[v], sw = 30 * kVarPK[v];
+    return ((c.nx + sw - 1) / sw) * ((c.ny + rows - 1) / rows);
 }
 int max_units_of(const zfv_config& c) {
     int m = 0;
@@ -215,9 +220,9 @@ struct BatchCore {
 
     void build_units() {
         units.clear();
-        const int rows = kVarNW[variant] * kVarCPT[variant];
+        const int rows = kVarNW[variant] * kVarCPT[variant], sw = 30 * kVarPK[variant];
         for (int k = 0; k < n; ++k) {
-            const int nbx = (cfg[k].nx + 29) / 30, nby = (cfg[k].ny + rows - 1) / rows;
+            const int nbx = (cfg[k].nx + sw - 1) / sw, nby = (cfg[k].ny + rows - 1) / rows;
             desc[k].nbx = nbx;
             desc[k].nby = nby;
             for (int u = 0; u < nbx * nby; ++u) units.push_back(make_int2(k, u));
@@ -270,9 +275,9 @@ struct BatchCore {
 
     struct ImportF {
         BatchCore* b; cudaStream_t s; bool exp;
-        template <int NW, int CPT> int operator()() {
-            if (exp) k32b_export<NW, CPT><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
-            else k32b_import<NW, CPT><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units());
+        template <int NW, int CPT, int PK> int operator()() {
+            if (exp) k32b_export<NW, CPT, PK><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
+            else k32b_import<NW, CPT, PK><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units());
             return cuda_check(cudaGetLastError(), "zfv_batch import/export launch");
         }
     };
@@ -287,9 +292,9 @@ struct BatchCore {
 
     struct BeginF {
         BatchCore* b; cudaStream_t s;
-        template <int NW, int CPT> int operator()() {
+        template <int NW, int CPT, int PK> int operator()() {
             k32b_init<<<(b->n + 127) / 128, 128, 0, s>>>(b->d_desc(), b->n);
-            k32b_reduce<NW, CPT, 0><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
+            k32b_reduce<NW, CPT, PK, 0><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
             return cuda_check(cudaGetLastError(), "zfv_batch begin launch");
         }
     };
@@ -297,8 +302,8 @@ struct BatchCore {
 
     struct MassF {
         BatchCore* b; cudaStream_t s;
-        template <int NW, int CPT> int operator()() {
-            k32b_reduce<NW, CPT, 1><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
+        template <int NW, int CPT, int PK> int operator()() {
+            k32b_reduce<NW, CPT, PK, 1><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
             return cuda_check(cudaGetLastError(), "zfv_batch mass launch");
         }
     };
@@ -307,11 +312,11 @@ struct BatchCore {
     template <bool W, bool I>
     struct StepF {
         BatchCore* b; cudaStream_t s; int nsteps;
-        template <int NW, int CPT> int operator()() {
+        template <int NW, int CPT, int PK> int operator()() {
             const int nu = b->nunits();
             for (int k = 0; k < nsteps; ++k) {
-                k32b_stage<S1, W, I, NW, CPT><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
-                k32b_stage<S2, W, I, NW, CPT><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+                k32b_stage<S1, W, I, NW, CPT, PK><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+                k32b_stage<S2, W, I, NW, CPT, PK><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
             }
             return cuda_check(cudaGetLastError(), "zfv_batch evolve launch");
         }
@@ -417,10 +422,11 @@ struct zfv_batch {
 
 extern "C" {
 
-int zfv_tile_variants(int* nw, int* cpt, int max_n) {
+int zfv_tile_variants(int* nw, int* cpt, int* cols, int max_n) {
     for (int v = 0; v < zfv32::kNumVariants && v < max_n; ++v) {
         if (nw) nw[v] = zfv32::kVarNW[v];
         if (cpt) cpt[v] = zfv32::kVarCPT[v];
+        if (cols) cols[v] = zfv32::kVarPK[v];
     }
     return zfv32::kNumVariants;
 }

@@ -136,6 +136,7 @@ class Level:
         """Evolve until time_end / max_step (or max_steps), syncing once per chunk."""
         self.begin()
         done_steps = 0
+        last_step = -1
         while True:
             n = chunk if max_steps is None else min(chunk, max_steps - done_steps)
             if n <= 0:
@@ -150,6 +151,9 @@ class Level:
             st = self.status()
             if st["done"]:
                 break
+            if st["step"] <= last_step:   # the device did not advance: stop, do not spin
+                raise _lib.ZfvError(f"no progress after {done_steps} requested steps: status {st}")
+            last_step = st["step"]
         return self.status()
 
     def state64(self) -> torch.Tensor:
