@@ -289,8 +289,8 @@ def time_fp32_batched(n, Q0, A0, K, W, local, ws, barrier, max_over_ranks):
     from zoomy_amrex_b200.batch import tile_variants
     shapes = tile_variants()
     tuning = {"picked": {"warps": shapes[best][0], "rows_per_warp": shapes[best][1],
-                         "columns_per_lane": shapes[best][2]},
-              "ms_per_step": {f"{shapes[v][0]}x{shapes[v][1]}x{shapes[v][2]}": t for v, t in times.items()}}
+                         "columns_per_lane": shapes[best][2], "stage2_prefetch": shapes[best][3]},
+              "ms_per_step": {"x".join(str(v) for v in shapes[k]): t for k, t in times.items()}}
     return ms, n * n * K * ws / (ms * 1e-3), st, tuning
 
 

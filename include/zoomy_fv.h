@@ -253,12 +253,13 @@ int zfv_batch_status(zfv_batch* b, zfv_status* out, void* stream);
 int zfv_batch_units(const zfv_batch* b);
 /*
  * Strip shapes compiled into the library: (warps per block, cells per thread
- * in y, columns per lane: 1 = scalar sweep, 2 = packed-FP32 column pairs).
+ * in y, columns per lane: 1 = scalar sweep, 2 = packed-FP32 column pairs,
+ * prefetch: 1 = stage 2 loads its update inputs at the top of each row).
  * zfv_tile_variants writes up to max_n of them and returns how many exist;
  * zfv_batch_set_variant selects one (the autotuner in
  * zoomy_amrex_b200/autotune.py measures them and caches the fastest per n_dof_q).
  */
-int zfv_tile_variants(int* nw, int* cpt, int* cols, int max_n);
+int zfv_tile_variants(int* nw, int* cpt, int* cols, int* prefetch, int max_n);
 int zfv_batch_set_variant(zfv_batch* b, int variant, void* stream);
 
 /*

@@ -72,36 +72,35 @@ def test_batch_graph_replay_equals_eager(cuda):
 
 
 def test_batch_strip_variants_agree(cuda):
-    """Strip shapes of the same sweep (scalar, or packed column pairs) compute
-    bitwise the same cell values; only the order of the mass partial sums
-    differs. The packed sweep rounds differently (FP32 pair instructions) and
-    agrees with the scalar one to FP32 accuracy."""
+    """Every compiled strip shape advances the same instances to FP32
+    accuracy. Shapes move the boundary between interior and edge strips,
+    whose code paths the compiler contracts into FMAs differently, and the
+    packed sweep uses FP32 pair instructions, so values agree to rounding,
+    not bitwise."""
     from zoomy_amrex_b200.batch import Batch, tile_variants
     ens = _ens(4, seed=3, side_range=(40, 300))
     cfgs, Q0s, A0s = zip(*ens)
-    ref = {}
-    for v, (_, _, cols) in enumerate(tile_variants()):
+    shapes = tile_variants()
+    ref = None
+    for v, shape in enumerate(shapes):
         b = Batch(cfgs, Q0s, A0s, variant=v)
         b.begin(); b.evolve(30)
         Q = [q.cpu().numpy() for q in b.state64()]
         st = b.status()
         b.close()
-        if cols not in ref:
-            ref[cols] = (Q, st)
+        if ref is None:
+            ref = (Q, st)
             continue
         for k in range(len(ens)):
-            assert st[k]["time"] == ref[cols][1][k]["time"]
-            assert np.array_equal(Q[k], ref[cols][0][k]), (v, k)
-            assert abs(st[k]["mass"] - ref[cols][1][k]["mass"]) <= 1e-13 * abs(ref[cols][1][k]["mass"])
-    if 2 in ref and 1 in ref:
-        for k in range(len(ens)):
-            dh = np.abs(ref[2][0][k][1] - ref[1][0][k][1])
-            print(f"[packed vs scalar sweep] instance {k}: L1 {dh.mean():.2e} Linf {dh.max():.2e}")
+            dh = np.abs(Q[k][1] - ref[0][k][1])
+            print(f"[strip shape {shape} vs {shapes[0]}] instance {k}: "
+                  f"L1 {dh.mean():.2e} Linf {dh.max():.2e} bitwise {np.array_equal(Q[k], ref[0][k])}")
             assert dh.mean() <= 1e-6 and dh.max() <= 1e-4
-            assert abs(ref[2][1][k]["time"] - ref[1][1][k]["time"]) <= 1e-6 * ref[1][1][k]["time"]
+            assert abs(st[k]["time"] - ref[1][k]["time"]) <= 1e-6 * ref[1][k]["time"]
+            assert abs(st[k]["mass"] - ref[1][k]["mass"]) <= 1e-9 * abs(ref[1][k]["mass"])
 
 
-@pytest.mark.parametrize("variant", [0, 4])
+@pytest.mark.parametrize("variant", [0, 3, 7])
 def test_batch_depth_error_vs_fp64(cuda, oracle, variant):
     """Batch members against the FP64 oracle (L1 depth, 60 steps), scalar and
     packed sweeps."""
@@ -138,7 +137,7 @@ def test_packed_sweep_keeps_lake_at_rest(cuda):
     Q0s[1] = Q0s[1][:, :, :cfgs[1].nx].copy()
     A0s[1] = A0s[1][:, :, :cfgs[1].nx].copy()
     cfgs[1].prob_hi[0] = cfgs[1].nx * 0.1
-    b = Batch(cfgs, Q0s, A0s, variant=4)
+    b = Batch(cfgs, Q0s, A0s, variant=3)
     b.begin(); b.evolve(100)
     Q = [q.cpu().numpy() for q in b.state64()]
     b.close()

@@ -71,7 +71,7 @@ def lib():
     L.zfv_batch_evolve.argtypes = [vp, i, vp]
     L.zfv_batch_status.argtypes = [vp, C.POINTER(zfv_status), vp]
     L.zfv_batch_units.argtypes = [vp]
-    L.zfv_tile_variants.argtypes = [C.POINTER(i), C.POINTER(i), C.POINTER(i), i]
+    L.zfv_tile_variants.argtypes = [C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i), i]
     L.zfv_batch_set_variant.argtypes = [vp, i, vp]
     L.zfv_evolve_static.argtypes = [vp, vp, vp, i, i, C.POINTER(zfv_status), vp]
     L.zfv_run_state_bytes.restype = C.c_size_t

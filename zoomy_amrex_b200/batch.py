@@ -20,14 +20,16 @@ from . import _lib
 from ._abi import MODELS, ZFV_MODEL_SWE2D, ZFV_PREC_FP32, zfv_config, zfv_status
 
 
-def tile_variants() -> list[tuple[int, int, int]]:
-    """The compiled strip shapes as (warps per block, rows per warp, columns per lane)."""
+def tile_variants() -> list[tuple[int, int, int, int]]:
+    """The compiled strip shapes as (warps per block, rows per warp, columns
+    per lane, stage-2 prefetch)."""
     L = _lib.lib()
-    nw = (C.c_int * 16)()
-    cpt = (C.c_int * 16)()
-    cols = (C.c_int * 16)()
-    n = int(L.zfv_tile_variants(nw, cpt, cols, 16))
-    return [(nw[k], cpt[k], cols[k]) for k in range(n)]
+    nw = (C.c_int * 32)()
+    cpt = (C.c_int * 32)()
+    cols = (C.c_int * 32)()
+    pf = (C.c_int * 32)()
+    n = int(L.zfv_tile_variants(nw, cpt, cols, pf, 32))
+    return [(nw[k], cpt[k], cols[k], pf[k]) for k in range(n)]
 
 
 class Batch:

@@ -150,7 +150,7 @@ __device__ __forceinline__ C4 fetch(const float* __restrict__ bed, const float* 
 
 // One warp's sub-strip: columns x0-1 .. x0+30 (owned x0 .. x0+29), rows j0 .. j0+CPT-1.
 // Accumulates this lane's CFL max and mass into m_loc / s_loc (stage 2).
-template <int MODE, bool WB, bool IMPL, int CPT, bool INTERIOR>
+template <int MODE, bool WB, bool IMPL, int CPT, bool INTERIOR, bool PF>
 __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const float* __restrict__ X,
                                             const float* __restrict__ inc_in, float* __restrict__ inc_out,
                                             float* __restrict__ Y, float* __restrict__ lo, const Params& L,
@@ -185,6 +185,22 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
         // row j: w1; rows j-1, j+1, j+2: w0, w2, w3. Row j+3 is loaded one
         // iteration ahead so its latency overlaps this row's arithmetic.
         const C4 w4 = (r + 1 < CPT) ? fetch<MODE, INTERIOR>(bed, X, inc_in, L, i, j + 3) : w3;
+        // stage 2: this cell's FP32 state, stage-1 increment and remainder for
+        // the compensated update; PF loads them here so that they arrive during
+        // the face work, otherwise where they are used (fewer registers)
+        float cx[3] = {0.0f, 0.0f, 0.0f}, ci[3] = {0.0f, 0.0f, 0.0f}, cl[3] = {0.0f, 0.0f, 0.0f};
+        auto load_comp = [&]() {
+            if (owns) {
+                const long long c = (long long)j * nx + i;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    cx[q] = __ldg(X + q * pl + c);
+                    ci[q] = __ldg(inc_in + q * pl + c);
+                    cl[q] = lo[q * pl + c];
+                }
+            }
+        };
+        if constexpr (MODE == S2 && PF) load_comp();
         RS lo_1, hi_1;
         reconstruct(w1, w2, w3, lo_1, hi_1);  // row j+1 in y
         const FaceR ft = face_rs<1, WB>(top, lo_1, L);   // face above row j
@@ -253,11 +269,10 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
                 inc_out[c] = inc_e; inc_out[pl + c] = inc_u; inc_out[2 * pl + c] = inc_v;
             } else {
                 // compensated Heun update in FP64: Q^{n+1} = (hi + lo) + (inc1 + inc2) / 2
-                const float i1e = __ldg(inc_in + c), i1u = __ldg(inc_in + pl + c), i1v = __ldg(inc_in + 2 * pl + c);
-                const float xe_ = __ldg(X + c), xu = __ldg(X + pl + c), xv = __ldg(X + 2 * pl + c);
-                const double ne = (double(xe_) + double(lo[c])) + 0.5 * (double(i1e) + double(inc_e));
-                const double nu = (double(xu) + double(lo[pl + c])) + 0.5 * (double(i1u) + double(inc_u));
-                const double nv = (double(xv) + double(lo[2 * pl + c])) + 0.5 * (double(i1v) + double(inc_v));
+                if constexpr (!PF) load_comp();
+                const double ne = (double(cx[0]) + double(cl[0])) + 0.5 * (double(ci[0]) + double(inc_e));
+                const double nu = (double(cx[1]) + double(cl[1])) + 0.5 * (double(ci[1]) + double(inc_u));
+                const double nv = (double(cx[2]) + double(cl[2])) + 0.5 * (double(ci[2]) + double(inc_v));
                 const float he = float(ne), hu = float(nu), hv = float(nv);
                 Y[c] = he; Y[pl + c] = hu; Y[2 * pl + c] = hv;
                 lo[c] = float(ne - double(he));

@@ -180,7 +180,7 @@ __device__ __forceinline__ float2 shfl_up2(float2 v, int d) {
 }
 
 // One warp's sub-strip of the paired sweep: column pairs x0-2+2L, rows j0 .. j0+CPT-1.
-template <int MODE, bool WB, bool IMPL, int CPT, bool INTERIOR, bool VEC>
+template <int MODE, bool WB, bool IMPL, int CPT, bool INTERIOR, bool VEC, bool PF>
 __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, const float* __restrict__ X,
                                              const float* __restrict__ inc_in, float* __restrict__ inc_out,
                                              float* __restrict__ Y, float* __restrict__ lo, const Params& L,
@@ -212,6 +212,29 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
         if (j >= ny) break;                  // uniform across the warp
         // row j+3 is loaded one iteration ahead (latency hidden behind this row)
         const C42 w4 = (r + 1 < CPT) ? fetch2<MODE, INTERIOR, VEC>(bed, X, inc_in, L, cA, j + 3) : w3;
+        // stage 2: the pair's FP32 state, stage-1 increment and remainder for
+        // the compensated update; PF loads them here so that they arrive during
+        // the face work, otherwise where they are used (fewer registers)
+        float2 cx[3], ci[3], cl[3];
+        auto load_comp = [&]() {
+            const long long c = (long long)j * nx + cA;
+            if (vec_io && (ownA || ownB)) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    cx[q] = __ldg(reinterpret_cast<const float2*>(X + q * pl + c));
+                    ci[q] = __ldg(reinterpret_cast<const float2*>(inc_in + q * pl + c));
+                    cl[q] = *reinterpret_cast<const float2*>(lo + q * pl + c);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    cx[q] = f2(ownA ? __ldg(X + q * pl + c) : 0.0f, ownB ? __ldg(X + q * pl + c + 1) : 0.0f);
+                    ci[q] = f2(ownA ? __ldg(inc_in + q * pl + c) : 0.0f, ownB ? __ldg(inc_in + q * pl + c + 1) : 0.0f);
+                    cl[q] = f2(ownA ? lo[q * pl + c] : 0.0f, ownB ? lo[q * pl + c + 1] : 0.0f);
+                }
+            }
+        };
+        if constexpr (MODE == S2 && PF) load_comp();
         RS2 lo_1, hi_1;
         reconstruct2(w1, w2, w3, lo_1, hi_1);
         const Face2 ft = face2<1, WB>(top, lo_1, L);
@@ -307,26 +330,13 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                 }
             } else {
                 // compensated Heun update in FP64, per cell
+                if constexpr (!PF) load_comp();
                 float i1[2][3], xs[2][3], lw[2][3];
-                if (vec_io) {
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        const float2 a = __ldg(reinterpret_cast<const float2*>(inc_in + q * pl + c));
-                        const float2 b = __ldg(reinterpret_cast<const float2*>(X + q * pl + c));
-                        const float2 l = *reinterpret_cast<const float2*>(lo + q * pl + c);
-                        i1[0][q] = a.x; i1[1][q] = a.y; xs[0][q] = b.x; xs[1][q] = b.y; lw[0][q] = l.x; lw[1][q] = l.y;
-                    }
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 2; ++k) {
-                        const bool own = k == 0 ? ownA : ownB;
-#pragma unroll
-                        for (int q = 0; q < 3; ++q) {
-                            i1[k][q] = own ? __ldg(inc_in + q * pl + c + k) : 0.0f;
-                            xs[k][q] = own ? __ldg(X + q * pl + c + k) : 0.0f;
-                            lw[k][q] = own ? lo[q * pl + c + k] : 0.0f;
-                        }
-                    }
+                for (int q = 0; q < 3; ++q) {
+                    i1[0][q] = ci[q].x; i1[1][q] = ci[q].y;
+                    xs[0][q] = cx[q].x; xs[1][q] = cx[q].y;
+                    lw[0][q] = cl[q].x; lw[1][q] = cl[q].y;
                 }
                 const float i2[2][3] = {{inc_e.x, inc_u.x, inc_v.x}, {inc_e.y, inc_u.y, inc_v.y}};
                 const float bb[2] = {w1.b.x, w1.b.y};

@@ -109,24 +109,28 @@ enum Mode { S1 = 1, S2 = 2 };
 
 namespace zfv32 {
 
-// Compiled strip shapes: (warps per block, rows per warp = cells per thread,
-// columns per lane). A strip is 30 * PK columns x (NW * CPT) rows; PK = 2 is
-// the packed-FP32 paired-column sweep.
-constexpr int kNumVariants = 7;
-constexpr int kVarNW[kNumVariants] = {4, 4, 8, 2, 4, 4, 8};
-constexpr int kVarCPT[kNumVariants] = {16, 8, 8, 32, 16, 8, 8};
-constexpr int kVarPK[kNumVariants] = {1, 1, 1, 1, 2, 2, 2};
+// Compiled strip shapes: (warps per block NW, rows per warp CPT = cells per
+// thread, columns per lane PK, stage-2 prefetch PF). A strip is 30 * PK
+// columns x (NW * CPT) rows; PK = 2 is the packed-FP32 paired-column sweep;
+// PF loads the stage-2 update's own inputs at the top of each row (earlier
+// loads, more registers).
+constexpr int kNumVariants = 8;
+constexpr int kVarNW[kNumVariants] = {4, 4, 4, 4, 4, 4, 4, 4};
+constexpr int kVarCPT[kNumVariants] = {16, 8, 16, 8, 16, 8, 16, 8};
+constexpr int kVarPK[kNumVariants] = {1, 1, 2, 2, 1, 1, 2, 2};
+constexpr int kVarPF[kNumVariants] = {0, 0, 0, 0, 1, 1, 1, 1};
 
 template <class F>
 int with_variant(int v, F&& f) {
     switch (v) {
-    case 0: return f.template operator()<4, 16, 1>();
-    case 1: return f.template operator()<4, 8, 1>();
-    case 2: return f.template operator()<8, 8, 1>();
-    case 3: return f.template operator()<2, 32, 1>();
-    case 4: return f.template operator()<4, 16, 2>();
-    case 5: return f.template operator()<4, 8, 2>();
-    case 6: return f.template operator()<8, 8, 2>();
+    case 0: return f.template operator()<4, 16, 1, false>();
+    case 1: return f.template operator()<4, 8, 1, false>();
+    case 2: return f.template operator()<4, 16, 2, false>();
+    case 3: return f.template operator()<4, 8, 2, false>();
+    case 4: return f.template operator()<4, 16, 1, true>();
+    case 5: return f.template operator()<4, 8, 1, true>();
+    case 6: return f.template operator()<4, 16, 2, true>();
+    case 7: return f.template operator()<4, 8, 2, true>();
     default: return fail(-1, "unknown strip variant %d", v);
     }
 }
@@ -275,7 +279,7 @@ struct BatchCore {
 
     struct ImportF {
         BatchCore* b; cudaStream_t s; bool exp;
-        template <int NW, int CPT, int PK> int operator()() {
+        template <int NW, int CPT, int PK, bool PF> int operator()() {
             if (exp) k32b_export<NW, CPT, PK><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
             else k32b_import<NW, CPT, PK><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units());
             return cuda_check(cudaGetLastError(), "zfv_batch import/export launch");
@@ -292,7 +296,7 @@ struct BatchCore {
 
     struct BeginF {
         BatchCore* b; cudaStream_t s;
-        template <int NW, int CPT, int PK> int operator()() {
+        template <int NW, int CPT, int PK, bool PF> int operator()() {
             k32b_init<<<(b->n + 127) / 128, 128, 0, s>>>(b->d_desc(), b->n);
             k32b_reduce<NW, CPT, PK, 0><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
             return cuda_check(cudaGetLastError(), "zfv_batch begin launch");
@@ -302,7 +306,7 @@ struct BatchCore {
 
     struct MassF {
         BatchCore* b; cudaStream_t s;
-        template <int NW, int CPT, int PK> int operator()() {
+        template <int NW, int CPT, int PK, bool PF> int operator()() {
             k32b_reduce<NW, CPT, PK, 1><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
             return cuda_check(cudaGetLastError(), "zfv_batch mass launch");
         }
@@ -312,11 +316,11 @@ struct BatchCore {
     template <bool W, bool I>
     struct StepF {
         BatchCore* b; cudaStream_t s; int nsteps;
-        template <int NW, int CPT, int PK> int operator()() {
+        template <int NW, int CPT, int PK, bool PF> int operator()() {
             const int nu = b->nunits();
             for (int k = 0; k < nsteps; ++k) {
-                k32b_stage<S1, W, I, NW, CPT, PK><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
-                k32b_stage<S2, W, I, NW, CPT, PK><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+                k32b_stage<S1, W, I, NW, CPT, PK, PF><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+                k32b_stage<S2, W, I, NW, CPT, PK, PF><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
             }
             return cuda_check(cudaGetLastError(), "zfv_batch evolve launch");
         }
@@ -422,11 +426,12 @@ struct zfv_batch {
 
 extern "C" {
 
-int zfv_tile_variants(int* nw, int* cpt, int* cols, int max_n) {
+int zfv_tile_variants(int* nw, int* cpt, int* cols, int* prefetch, int max_n) {
     for (int v = 0; v < zfv32::kNumVariants && v < max_n; ++v) {
         if (nw) nw[v] = zfv32::kVarNW[v];
         if (cpt) cpt[v] = zfv32::kVarCPT[v];
         if (cols) cols[v] = zfv32::kVarPK[v];
+        if (prefetch) prefetch[v] = zfv32::kVarPF[v];
     }
     return zfv32::kNumVariants;
 }
