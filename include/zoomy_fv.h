@@ -295,6 +295,10 @@ size_t zfv_adj_work_bytes(const zfv_handle* h);
 int zfv_adj_record(zfv_handle* h, void* Q, void* aux, void* scratch, void* tape, int n_steps, void* stream);
 int zfv_adj_step(zfv_handle* h, const void* tape, int k, void* lam, double* grad, const void* aux0,
                  void* work, void* stream);
+/* Tile shapes compiled for the adjoint's face-reverse kernel (a process-wide
+ * tuning choice; every shape gives the same gradient up to rounding). */
+int zfv_adj_variants(void);
+int zfv_adj_set_variant(int variant);
 
 /*
  * zfv_evolve without caller-provided scratch. No counterpart in the reference

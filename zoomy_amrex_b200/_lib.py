@@ -22,7 +22,8 @@ SYMBOLS = ("zfv_last_error", "zfv_version", "zfv_sizeof_config", "zfv_sizeof_sta
            "zfv_batch_import", "zfv_batch_export", "zfv_batch_begin", "zfv_batch_evolve",
            "zfv_batch_status", "zfv_batch_units", "zfv_tile_variants", "zfv_batch_set_variant",
            "zfv_run_state_bytes", "zfv_save_run_state", "zfv_load_run_state", "zfv_adj_tape_bytes",
-           "zfv_adj_work_bytes", "zfv_adj_record", "zfv_adj_step")
+           "zfv_adj_work_bytes", "zfv_adj_record", "zfv_adj_step", "zfv_adj_variants",
+           "zfv_adj_set_variant")
 
 
 class ZfvError(RuntimeError):
@@ -83,6 +84,7 @@ def lib():
     L.zfv_adj_work_bytes.restype = C.c_size_t
     L.zfv_adj_record.argtypes = [vp, vp, vp, vp, vp, i, vp]
     L.zfv_adj_step.argtypes = [vp, vp, i, vp, vp, vp, vp, vp]
+    L.zfv_adj_set_variant.argtypes = [i]
     _lib = L
     return L
 

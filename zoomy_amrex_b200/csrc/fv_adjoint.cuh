@@ -116,8 +116,8 @@ struct AdjTile {
 // Pass B. X: stage input (bed from qbed, planes 1..3 from X). lamq, loc from
 // pass A; addend (NULL or 4 planes) * addscale is added (the Heun term
 // lam_{n+1}/2 of stage 1). lamX may alias addend.
-template <bool WB, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY)
+template <bool WB, int TX, int TY, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
 k_adj_face(const double* __restrict__ X, const double* __restrict__ qbed, const double* __restrict__ lamq,
            const double* __restrict__ loc, const double* addend, double addscale, P6 L,
            const double* __restrict__ meta, double* lamX) {
@@ -132,7 +132,9 @@ k_adj_face(const double* __restrict__ X, const double* __restrict__ qbed, const 
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int tid = threadIdx.x;
     const zadj::SweP<double> p = swe_params(L);
-    const bool wall[4] = {L.bc_tag[0] == 1, L.bc_tag[1] == 1, L.bc_tag[2] == 1, L.bc_tag[3] == 1};
+    // bit s set: side s (x_lo, x_hi, y_lo, y_hi) is a wall
+    const unsigned wall = (L.bc_tag[0] == 1 ? 1u : 0u) | (L.bc_tag[1] == 1 ? 2u : 0u) |
+                          (L.bc_tag[2] == 1 ? 4u : 0u) | (L.bc_tag[3] == 1 ? 8u : 0u);
 
     // 1. X tile with mirrored ghosts (walls flip the normal momentum)
     for (int k = tid; k < T::XH * T::XW; k += T::NT) {
@@ -142,8 +144,8 @@ k_adj_face(const double* __restrict__ X, const double* __restrict__ qbed, const 
         const int ii = mirror(gi, nx, ox), jj = mirror(gj, ny, oy);
         const long long c = (long long)jj * nx + ii;
         double v[4] = {qbed[c], X[pl + c], X[2 * pl + c], X[3 * pl + c]};
-        if (ox && wall[gi < 0 ? 0 : 1]) v[2] = -v[2];
-        else if (!ox && oy && wall[gj < 0 ? 2 : 3]) v[3] = -v[3];
+        if (ox && ((wall >> (gi < 0 ? 0 : 1)) & 1u)) v[2] = -v[2];
+        else if (!ox && oy && ((wall >> (gj < 0 ? 2 : 3)) & 1u)) v[3] = -v[3];
 #pragma unroll
         for (int n = 0; n < 4; ++n) sX[(n * T::XH + ly) * T::XW + lx] = v[n];
     }
@@ -234,7 +236,7 @@ k_adj_face(const double* __restrict__ X, const double* __restrict__ qbed, const 
                 for (int n = 0; n < 4; ++n) acc[n] += F[4 * k + n];
             }
             const int flip = 2 + D;
-            const bool wl = wall[2 * D], wh = wall[2 * D + 1];
+            const bool wl = (wall >> (2 * D)) & 1u, wh = (wall >> (2 * D + 1)) & 1u;
             if (ci <= 1) {             // ghost g = -1 - ci mirrors onto this cell
                 const int g = -1 - ci;
                 for (int a = g - 1; a <= g + 2; ++a) {

@@ -23,6 +23,14 @@
 #include "AMReX_Algorithm.H"
 #include "zb_portable_math.H"
 
+#ifdef __CUDACC__
+#  define ZADJ_UNROLL _Pragma("unroll")
+#  define ZADJ_INLINE __forceinline__
+#else
+#  define ZADJ_UNROLL
+#  define ZADJ_INLINE inline
+#endif
+
 #ifndef PORTABLE_FN
 #  ifdef __CUDACC__
 #    define PORTABLE_FN __host__ __device__
@@ -42,7 +50,7 @@ constexpr int kFaceOut = 11;
 
 // minmod with the index of the selected argument (0: none, 1: a, 2: b).
 template <class R>
-PORTABLE_FN inline R mm_sel(R a, R b, int& s) {
+PORTABLE_FN ZADJ_INLINE R mm_sel(R a, R b, int& s) {
     if (a * b <= R(0)) { s = 0; return R(0); }
     if (std::fabs(a) < std::fabs(b)) { s = 1; return a; }
     s = 2;
@@ -51,13 +59,13 @@ PORTABLE_FN inline R mm_sel(R a, R b, int& s) {
 
 // models/swe.H hinv_of and its derivative.
 template <class R>
-PORTABLE_FN inline R hinv(R h, R eps) {
+PORTABLE_FN ZADJ_INLINE R hinv(R h, R eps) {
     const R h2 = h * h;
     const R x0 = h2 * h2;
     return std::sqrt(R(2)) * h / std::sqrt(x0 + amrex::max(x0, eps));
 }
 template <class R>
-PORTABLE_FN inline R dhinv(R h, R eps) {
+PORTABLE_FN ZADJ_INLINE R dhinv(R h, R eps) {
     const R h2 = h * h;
     const R x0 = h2 * h2;
     const bool big = !(x0 < eps);          // amrex::max(x0, eps) takes x0
@@ -69,12 +77,13 @@ PORTABLE_FN inline R dhinv(R h, R eps) {
 }
 
 template <class R>
-PORTABLE_FN inline R sgn(R x) { return (x > R(0)) ? R(1) : ((x < R(0)) ? R(-1) : R(0)); }
+PORTABLE_FN ZADJ_INLINE R sgn(R x) { return (x > R(0)) ? R(1) : ((x < R(0)) ? R(-1) : R(0)); }
 
 // Forward face map (the values eval_face produces for SWE2D).
 template <int D, bool WB, class R>
-PORTABLE_FN inline void face_fwd(const R c[4][4], SweP<R> const& p, R o[kFaceOut]) {
+PORTABLE_FN ZADJ_INLINE void face_fwd(const R c[4][4], SweP<R> const& p, R o[kFaceOut]) {
     R qL[4], qR[4];
+    ZADJ_UNROLL
     for (int n = 0; n < 4; ++n) {
         int s;
         const R gL = mm_sel(c[1][n] - c[0][n], c[2][n] - c[1][n], s);
@@ -98,6 +107,7 @@ PORTABLE_FN inline void face_fwd(const R c[4][4], SweP<R> const& p, R o[kFaceOut
     const R hiL = hinv(hL, p.eps), hiR = hinv(hR, p.eps);
     R FL[3], FR[3];
     FL[0] = mL[D]; FR[0] = mR[D];
+    ZADJ_UNROLL
     for (int k = 0; k < 2; ++k) {
         FL[1 + k] = mL[k] * mL[D] * hiL + ((k == D) ? R(0.5) * g * hL * hL : R(0));
         FR[1 + k] = mR[k] * mR[D] * hiR + ((k == D) ? R(0.5) * g * hR * hR : R(0));
@@ -108,6 +118,7 @@ PORTABLE_FN inline void face_fwd(const R c[4][4], SweP<R> const& p, R o[kFaceOut
     const R db = bR - bL;
     const R Bn = g * (R(0.5) * (hL + hR));
     const R dq[3] = {hR - hL, mR[0] - mL[0], mR[1] - mL[1]};
+    ZADJ_UNROLL
     for (int n = 0; n < 3; ++n) {
         o[n] = R(0.5) * (FL[n] + FR[n]);
         const R bdq = (n == 1 + D) ? Bn * db : R(0);
@@ -123,11 +134,12 @@ PORTABLE_FN inline void face_fwd(const R c[4][4], SweP<R> const& p, R o[kFaceOut
 // wA, wB (lo[9] += wA h*_L, lo[10] += wB h*_R, the derivative of 0.5 g h^2
 // being g h), since h*_L, h*_R are only known inside.
 template <int D, bool WB, class R>
-PORTABLE_FN inline void face_rev(const R c[4][4], SweP<R> const& p, const R lo[kFaceOut],
+PORTABLE_FN ZADJ_INLINE void face_rev(const R c[4][4], SweP<R> const& p, const R lo[kFaceOut],
                                  R wA, R wB, R lc[4][4]) {
     // -- forward, keeping what the reverse needs
     R qL[4], qR[4];
     int sLsel[4], sRsel[4];
+    ZADJ_UNROLL
     for (int n = 0; n < 4; ++n) {
         const R gL = mm_sel(c[1][n] - c[0][n], c[2][n] - c[1][n], sLsel[n]);
         const R gR = mm_sel(c[2][n] - c[1][n], c[3][n] - c[2][n], sRsel[n]);
@@ -164,6 +176,7 @@ PORTABLE_FN inline void face_rev(const R c[4][4], SweP<R> const& p, const R lo[k
     R lhL = lo[9] + wA * hL, lhR = lo[10] + wB * hR;
     R lmL[2] = {0, 0}, lmR[2] = {0, 0};
     R lbL = 0, lbR = 0, ls = 0, lhiL = 0, lhiR = 0;
+    ZADJ_UNROLL
     for (int n = 0; n < 3; ++n) {
         const R lp = lo[3 + n], lm = lo[6 + n];
         ls += R(0.5) * dq[n] * (lp - lm);
@@ -230,6 +243,7 @@ PORTABLE_FN inline void face_rev(const R c[4][4], SweP<R> const& p, const R lo[k
         lqR[2] = lmR[0]; lqR[3] = lmR[1];
     }
     // MUSCL / minmod
+    ZADJ_UNROLL
     for (int n = 0; n < 4; ++n) {
         lc[1][n] += lqL[n];
         const R lgL = R(0.5) * lqL[n];
@@ -248,7 +262,7 @@ struct Manning {
     R k, dk_dh, ic, S[2], J[2][2];
 };
 template <class R>
-PORTABLE_FN inline Manning<R> manning(R h, R mx, R my, R hv, SweP<R> const& p) {
+PORTABLE_FN ZADJ_INLINE Manning<R> manning(R h, R mx, R my, R hv, SweP<R> const& p) {
     Manning<R> M;
     const R m = amrex::max(h, p.hfloor);
     M.ic = zb::inv_cbrt_pos(m);
@@ -272,7 +286,7 @@ PORTABLE_FN inline Manning<R> manning(R h, R mx, R my, R hv, SweP<R> const& p) {
 // elimination reduces to: the bed and depth rows of J and S are zero).
 // Returns false when the explicit fallback of make_rhs.H:501-508 is taken.
 template <class R>
-PORTABLE_FN inline bool implicit_fwd(R h, R mx, R my, R hv, R dt, SweP<R> const& p, R dq[2]) {
+PORTABLE_FN ZADJ_INLINE bool implicit_fwd(R h, R mx, R my, R hv, R dt, SweP<R> const& p, R dq[2]) {
     const Manning<R> M = manning(h, mx, my, hv, p);
     const R a = R(1) - dt * M.J[0][0], b = -dt * M.J[0][1];
     const R c = -dt * M.J[1][0], d = R(1) - dt * M.J[1][1];
@@ -292,7 +306,7 @@ PORTABLE_FN inline bool implicit_fwd(R h, R mx, R my, R hv, R dt, SweP<R> const&
 // q_out's momenta (the h and b rows pass through unchanged). Adds to
 // lq[1..3] (h, hu, hv of q*), lhv, lnm, ldt.
 template <class R>
-PORTABLE_FN inline void implicit_rev(R h, R mx, R my, R hv, R dt, SweP<R> const& p, const R lam[2],
+PORTABLE_FN ZADJ_INLINE void implicit_rev(R h, R mx, R my, R hv, R dt, SweP<R> const& p, const R lam[2],
                                      R lq[4], R& lhv, R& lnm, R& ldt) {
     const Manning<R> M = manning(h, mx, my, hv, p);
     const R a = R(1) - dt * M.J[0][0], b = -dt * M.J[0][1];

@@ -45,6 +45,9 @@ AdjLayout adj_layout(long long plane);
 int adj_step_swe2d(const void* Lp, bool wb, bool impl, const AdjLayout& A, const char* tape_step,
                    double* lam, double* grad, const double* aux0, int n_aux, char* work,
                    cudaStream_t s);
+// Process-wide tile shape of the face-reverse kernel (tuning).
+int adj_set_variant(int v);
+int adj_variants();
 
 // One compiled model/precision: owns its kernel instantiations.
 struct Runner {

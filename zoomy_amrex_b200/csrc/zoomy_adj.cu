@@ -2,6 +2,7 @@
 // sequence of the reverse of one recorded step (kernels in fv_adjoint.cuh).
 // Compiled with FMA contraction on: the reverse is checked against finite
 // differences and FP64 autograd, not bit for bit.
+#include <atomic>
 #include <cuda_runtime.h>
 #include "zfv_internal.H"
 #include "fv_adjoint.cuh"
@@ -10,8 +11,24 @@ namespace zfvi {
 
 namespace {
 constexpr int kCellNT = 256;
-constexpr int kTX = 32, kTY = 8;
 constexpr int kDtBlocks = 592;   // 4 x 148 SMs
+
+// Tile shapes of the face-reverse kernel: (TX, TY, minimum resident blocks
+// per SM). The kernel is register-heavy (FP64 reverse of a whole face), so
+// the shapes trade tile halo overhead against occupancy.
+constexpr int kAdjVariants = 4;
+std::atomic<int> g_adj_variant{1};
+
+template <class F>
+int with_adj_variant(int v, F&& f) {
+    switch (v) {
+    case 0: return f.template operator()<32, 8, 1>();
+    case 1: return f.template operator()<32, 4, 3>();
+    case 2: return f.template operator()<32, 8, 2>();
+    case 3: return f.template operator()<16, 8, 3>();
+    default: return fail(-1, "unknown adjoint tile variant %d", v);
+    }
+}
 }
 
 AdjLayout adj_layout(long long plane) {
@@ -39,13 +56,13 @@ AdjLayout adj_layout(long long plane) {
 
 namespace {
 
-template <bool WB, bool IMPL>
+template <bool WB, bool IMPL, int TX, int TY, int MINB>
 int step_impl(const zfv::adj::P6& L, const AdjLayout& A, const char* tape, double* lam, double* grad,
               const double* aux0, int n_aux, char* work, cudaStream_t s) {
     using namespace zfv::adj;
-    using Tile = AdjTile<kTX, kTY>;
+    using Tile = AdjTile<TX, TY>;
     // per device: cheap, so set on every call
-    int rc = cuda_check(cudaFuncSetAttribute(k_adj_face<WB, kTX, kTY>,
+    int rc = cuda_check(cudaFuncSetAttribute(k_adj_face<WB, TX, TY, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              int(Tile::smem_bytes)), "k_adj_face attribute");
     if (rc) return rc;
@@ -60,20 +77,29 @@ int step_impl(const zfv::adj::P6& L, const AdjLayout& A, const char* tape, doubl
     double* part = reinterpret_cast<double*>(work + A.w_part);
     double* amax = reinterpret_cast<double*>(work + A.w_amax);
     unsigned* counter = reinterpret_cast<unsigned*>(work + A.w_counter);
-    const dim3 fgrid((L.nx + kTX - 1) / kTX, (L.ny + kTY - 1) / kTY);
+    const dim3 fgrid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY);
     // stage 2: Y2 = stage(Y1), Q^{n+1} = (Q^n + Y2)/2 -> lam_Y2 = lam/2
     k_adj_cell<IMPL, kCellNT><<<A.nbA, kCellNT, 0, s>>>(lam, 0.5, Y1, qs2, L, meta, lamq, loc, part);
-    k_adj_face<WB, kTX, kTY><<<fgrid, kTX * kTY, Tile::smem_bytes, s>>>(
+    k_adj_face<WB, TX, TY, MINB><<<fgrid, TX * TY, Tile::smem_bytes, s>>>(
         Y1, X, lamq, loc, nullptr, 0.0, L, meta, lamY1);
     // stage 1: Y1 = stage(Q^n); lam_n = (dY1/dQ^n)^T lam_Y1 + lam/2
     k_adj_cell<IMPL, kCellNT><<<A.nbA, kCellNT, 0, s>>>(lamY1, 1.0, X, qs1, L, meta, lamq, loc,
                                                         part + 2 * A.nbA);
-    k_adj_face<WB, kTX, kTY><<<fgrid, kTX * kTY, Tile::smem_bytes, s>>>(
+    k_adj_face<WB, TX, TY, MINB><<<fgrid, TX * TY, Tile::smem_bytes, s>>>(
         X, X, lamq, loc, lam, 0.5, L, meta, lam);
     // dt_n = dt(Q^n)
     k_adj_dt<256><<<A.nbD, 256, 0, s>>>(X, aux0, n_aux, L, meta, part, 2 * A.nbA, amax, counter, lam, grad);
     return cuda_check(cudaGetLastError(), "zfv_adj_step launch");
 }
+
+template <bool WB, bool IMPL>
+struct StepF {
+    const zfv::adj::P6& L; const AdjLayout& A; const char* tape; double* lam; double* grad;
+    const double* aux0; int n_aux; char* work; cudaStream_t s;
+    template <int TX, int TY, int MINB> int operator()() {
+        return step_impl<WB, IMPL, TX, TY, MINB>(L, A, tape, lam, grad, aux0, n_aux, work, s);
+    }
+};
 
 }  // namespace
 
@@ -81,10 +107,19 @@ int adj_step_swe2d(const void* Lp, bool wb, bool impl, const AdjLayout& A, const
                    double* lam, double* grad, const double* aux0, int n_aux, char* work,
                    cudaStream_t s) {
     const auto& L = *static_cast<const zfv::adj::P6*>(Lp);
-    if (wb) return impl ? step_impl<true, true>(L, A, tape_step, lam, grad, aux0, n_aux, work, s)
-                        : step_impl<true, false>(L, A, tape_step, lam, grad, aux0, n_aux, work, s);
-    return impl ? step_impl<false, true>(L, A, tape_step, lam, grad, aux0, n_aux, work, s)
-                : step_impl<false, false>(L, A, tape_step, lam, grad, aux0, n_aux, work, s);
+    const int v = g_adj_variant.load();
+    if (wb) return impl ? with_adj_variant(v, StepF<true, true>{L, A, tape_step, lam, grad, aux0, n_aux, work, s})
+                        : with_adj_variant(v, StepF<true, false>{L, A, tape_step, lam, grad, aux0, n_aux, work, s});
+    return impl ? with_adj_variant(v, StepF<false, true>{L, A, tape_step, lam, grad, aux0, n_aux, work, s})
+                : with_adj_variant(v, StepF<false, false>{L, A, tape_step, lam, grad, aux0, n_aux, work, s});
 }
+
+int adj_set_variant(int v) {
+    if (v < 0 || v >= kAdjVariants) return fail(-1, "zfv_adj_set_variant: unknown variant %d", v);
+    g_adj_variant.store(v);
+    return 0;
+}
+
+int adj_variants() { return kAdjVariants; }
 
 }  // namespace zfvi

@@ -532,6 +532,10 @@ int zfv_adj_step(zfv_handle* h, const void* tape, int k, void* lam, double* grad
                             static_cast<const double*>(aux0), static_cast<char*>(work), (cudaStream_t)stream);
 }
 
+int zfv_adj_set_variant(int variant) { return adj_set_variant(variant); }
+
+int zfv_adj_variants(void) { return adj_variants(); }
+
 int zfv_log_capacity(const zfv_handle* h) { return h ? kLogCap : 0; }
 
 int zfv_read_log(zfv_handle* h, const void* scratch, double* out3, int max_entries,
