@@ -395,6 +395,10 @@ def adjoint_bench(local, n=1024, steps=200, every=20, n_dirs=32, eps=1e-6, seed=
         return 0.5 * (e * e).sum()
 
     base = torch.from_numpy(Q0).to(dev)
+    # warm-up: one short differentiable run (first launches load the kernels)
+    qw = base.clone().requires_grad_(True)
+    nmw = torch.tensor(0.03, dtype=torch.float64, device=dev, requires_grad=True)
+    loss_of(evolve_differentiable(qw, nmw, A, cfg, 4, checkpoint_every=2)).backward()
     # forward alone (zfv_evolve, no checkpoints)
     forward_only(base, A, cfg, 3)
     torch.cuda.synchronize()

@@ -106,10 +106,10 @@ struct AdjTile {
     static constexpr int LW = TX + 4, LH = TY + 4;      // lam_q* with 2 halo cells
     static constexpr int NFX = (TX + 3) * TY;           // x-faces x0-1 .. x0+TX+1 (right cell index)
     static constexpr int NFY = TX * (TY + 3);
-    static constexpr int NF = NFX > NFY ? NFX : NFY;
+    static constexpr int NF = NFX + NFY;                // both directions in one pass
     static constexpr size_t x_elems = size_t(4) * XH * XW;
     static constexpr size_t l_elems = size_t(3) * LH * LW;
-    static constexpr size_t f_elems = size_t(NF) * 16;
+    static constexpr size_t f_elems = size_t(NF) * 16;  // [16][NF]: face f's output q at q * NF + f
     static constexpr size_t smem_bytes = (x_elems + l_elems + f_elems) * sizeof(double);
 };
 
@@ -126,7 +126,7 @@ k_adj_face(const double* __restrict__ X, const double* __restrict__ qbed, const 
     extern __shared__ __align__(16) double smem[];
     double* sX = smem;                       // [4][XH][XW]
     double* sL = sX + T::x_elems;            // [3][LH][LW]
-    double* sF = sL + T::l_elems;            // [NF][16]
+    double* sF = sL + T::l_elems;            // [16][NF]
     const int nx = L.nx, ny = L.ny;
     const long long pl = L.plane;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -166,74 +166,75 @@ k_adj_face(const double* __restrict__ X, const double* __restrict__ qbed, const 
     auto sx = [&](int n, int gi, int gj) { return sX[(n * T::XH + (gj - y0 + 3)) * T::XW + (gi - x0 + 3)]; };
     auto sl = [&](int n, int gi, int gj) { return sL[(n * T::LH + (gj - y0 + 2)) * T::LW + (gi - x0 + 2)]; };
 
-#pragma unroll 1
-    for (int D = 0; D < 2; ++D) {
-        // 3. face reverses of this tile's faces in direction D
-        const int nf = D == 0 ? T::NFX : T::NFY;
+    // 3. face reverses of all this tile's faces, x then y in one pass. The
+    // outputs are stored component-major ([16][NF]) so that neighbouring
+    // threads write and read neighbouring words.
+    for (int f = tid; f < T::NF; f += T::NT) {
+        const int D = f < T::NFX ? 0 : 1;
+        const int ff = D == 0 ? f : f - T::NFX;
         const int fw = D == 0 ? TX + 3 : TX;
-        const double sc = dt / (D == 0 ? L.dx : L.dy);
-        for (int f = tid; f < nf; f += T::NT) {
-            // face a between cells A = a-1 and B = a along D (stencil a-2 .. a+1);
-            // a = 0 and a = n are the domain's boundary faces
-            const int fa = f % fw, fb = f / fw;
-            const int gi = D == 0 ? x0 - 1 + fa : x0 + fa;   // cell B
-            const int gj = D == 0 ? y0 + fb : y0 - 1 + fb;
-            const int a = D == 0 ? gi : gj, na = D == 0 ? nx : ny;
-            double* out = sF + 16 * f;
-            const bool real = a >= 0 && a <= na && (D == 0 ? gj < ny : gi < nx);
-            if (!real) {
+        // face a between cells A = a-1 and B = a along D (stencil a-2 .. a+1);
+        // a = 0 and a = n are the domain's boundary faces
+        const int fa = ff % fw, fb = ff / fw;
+        const int gi = D == 0 ? x0 - 1 + fa : x0 + fa;   // cell B
+        const int gj = D == 0 ? y0 + fb : y0 - 1 + fb;
+        const int a = D == 0 ? gi : gj, na = D == 0 ? nx : ny;
+        const bool real = a >= 0 && a <= na && (D == 0 ? gj < ny : gi < nx);
+        if (!real) {
 #pragma unroll
-                for (int k = 0; k < 16; ++k) out[k] = 0.0;
-                continue;
-            }
-            double c[4][4], lo[11], lA[3], lB[3];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int ci = D == 0 ? gi - 2 + k : gi, cj = D == 0 ? gj : gj - 2 + k;
-#pragma unroll
-                for (int n = 0; n < 4; ++n) c[k][n] = sx(n, ci, cj);
-            }
-#pragma unroll
-            for (int n = 0; n < 3; ++n) {
-                lA[n] = sl(n, D == 0 ? gi - 1 : gi, D == 0 ? gj : gj - 1);
-                lB[n] = sl(n, gi, gj);
-                lo[n] = sc * (lB[n] - lA[n]);
-                lo[3 + n] = -sc * lB[n];
-                lo[6 + n] = -sc * lA[n];
-            }
-            lo[9] = 0.0; lo[10] = 0.0;
-            const double wA = WB ? sc * p.g * lA[1 + D] : 0.0;
-            const double wB = WB ? -sc * p.g * lB[1 + D] : 0.0;
-            double lc[4][4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-#pragma unroll
-                for (int n = 0; n < 4; ++n) lc[k][n] = 0.0;
-            if (D == 0) zadj::face_rev<0, WB>(c, p, lo, wA, wB, lc);
-            else zadj::face_rev<1, WB>(c, p, lo, wA, wB, lc);
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-#pragma unroll
-                for (int n = 0; n < 4; ++n) out[4 * k + n] = lc[k][n];
+            for (int k = 0; k < 16; ++k) sF[k * T::NF + f] = 0.0;
+            continue;
         }
-        __syncthreads();
-        // 4. gather per owned cell, fixed order: direct stencil entries, then
-        // entries of ghost cells that mirror onto this cell
-        if (i < nx && j < ny) {
+        const double sc = dt / (D == 0 ? L.dx : L.dy);
+        double c[4][4], lo[11], lA[3], lB[3];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int ci = D == 0 ? gi - 2 + k : gi, cj = D == 0 ? gj : gj - 2 + k;
+#pragma unroll
+            for (int n = 0; n < 4; ++n) c[k][n] = sx(n, ci, cj);
+        }
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            lA[n] = sl(n, D == 0 ? gi - 1 : gi, D == 0 ? gj : gj - 1);
+            lB[n] = sl(n, gi, gj);
+            lo[n] = sc * (lB[n] - lA[n]);
+            lo[3 + n] = -sc * lB[n];
+            lo[6 + n] = -sc * lA[n];
+        }
+        lo[9] = 0.0; lo[10] = 0.0;
+        const double wA = WB ? sc * p.g * (D == 0 ? lA[1] : lA[2]) : 0.0;
+        const double wB = WB ? -sc * p.g * (D == 0 ? lB[1] : lB[2]) : 0.0;
+        double lc[4][4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int n = 0; n < 4; ++n) lc[k][n] = 0.0;
+        if (D == 0) zadj::face_rev<0, WB>(c, p, lo, wA, wB, lc);
+        else zadj::face_rev<1, WB>(c, p, lo, wA, wB, lc);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int n = 0; n < 4; ++n) sF[(4 * k + n) * T::NF + f] = lc[k][n];
+    }
+    __syncthreads();
+    // 4. gather per owned cell, fixed order: direct stencil entries, then
+    // entries of ghost cells that mirror onto this cell
+    if (i < nx && j < ny) {
+#pragma unroll 1
+        for (int D = 0; D < 2; ++D) {
             const int ci = D == 0 ? i : j, n_d = D == 0 ? nx : ny;
             const int lo_f = D == 0 ? x0 - 1 : y0 - 1;        // first face index of the tile
-            auto face_at = [&](int a) -> const double* {
-                const int fa = D == 0 ? a - lo_f : (i - x0);
-                const int fb = D == 0 ? (j - y0) : a - lo_f;
-                return sF + 16 * (fb * fw + fa);
+            auto face_at = [&](int a) -> int {
+                return D == 0 ? (j - y0) * (TX + 3) + (a - lo_f)
+                              : T::NFX + (a - lo_f) * TX + (i - x0);
             };
             // face a touches cells a-2 .. a+1 (stencil position k = cell - a + 2)
             for (int a = ci - 1; a <= ci + 2; ++a) {
                 if (a < 0 || a > n_d) continue;
-                const double* F = face_at(a);
+                const int fidx = face_at(a);
                 const int k = ci - a + 2;
 #pragma unroll
-                for (int n = 0; n < 4; ++n) acc[n] += F[4 * k + n];
+                for (int n = 0; n < 4; ++n) acc[n] += sF[(4 * k + n) * T::NF + fidx];
             }
             const int flip = 2 + D;
             const bool wl = (wall >> (2 * D)) & 1u, wh = (wall >> (2 * D + 1)) & 1u;
@@ -241,24 +242,29 @@ k_adj_face(const double* __restrict__ X, const double* __restrict__ qbed, const 
                 const int g = -1 - ci;
                 for (int a = g - 1; a <= g + 2; ++a) {
                     if (a < 0 || a > n_d) continue;
-                    const double* F = face_at(a);
+                    const int fidx = face_at(a);
                     const int k = g - a + 2;
 #pragma unroll
-                    for (int n = 0; n < 4; ++n) acc[n] += (n == flip && wl) ? -F[4 * k + n] : F[4 * k + n];
+                    for (int n = 0; n < 4; ++n) {
+                        const double v = sF[(4 * k + n) * T::NF + fidx];
+                        acc[n] += (n == flip && wl) ? -v : v;
+                    }
                 }
             }
             if (ci >= n_d - 2) {       // ghost g = 2 n - 1 - ci
                 const int g = 2 * n_d - 1 - ci;
                 for (int a = g - 1; a <= g + 2; ++a) {
                     if (a < 0 || a > n_d) continue;
-                    const double* F = face_at(a);
+                    const int fidx = face_at(a);
                     const int k = g - a + 2;
 #pragma unroll
-                    for (int n = 0; n < 4; ++n) acc[n] += (n == flip && wh) ? -F[4 * k + n] : F[4 * k + n];
+                    for (int n = 0; n < 4; ++n) {
+                        const double v = sF[(4 * k + n) * T::NF + fidx];
+                        acc[n] += (n == flip && wh) ? -v : v;
+                    }
                 }
             }
         }
-        __syncthreads();
     }
     // 5. lam_X = lam_q* + loc + faces (+ addend)
     if (i < nx && j < ny) {
