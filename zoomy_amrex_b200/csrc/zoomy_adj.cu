@@ -15,9 +15,11 @@ constexpr int kDtBlocks = 592;   // 4 x 148 SMs
 
 // Tile shapes of the face-reverse kernel: (TX, TY, minimum resident blocks
 // per SM). The kernel is register-heavy (FP64 reverse of a whole face), so
-// the shapes trade tile halo overhead against occupancy.
+// the shapes trade tile halo overhead against occupancy. Default: 32 x 8 with
+// two blocks per SM, the fastest measured at 1024^2 (206 ms for the backward
+// of 200 steps, against 265 / 219 / 216 ms for the others).
 constexpr int kAdjVariants = 4;
-std::atomic<int> g_adj_variant{1};
+std::atomic<int> g_adj_variant{2};
 
 template <class F>
 int with_adj_variant(int v, F&& f) {
