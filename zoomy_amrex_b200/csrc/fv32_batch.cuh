@@ -63,10 +63,13 @@ k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
     constexpr int NT = 32 * NW;
     __shared__ double red[2 * NW];
     __shared__ BInst sD;
+    // stage-2 staging of the update's own inputs (PF): 9 values per lane per warp
+    __shared__ __align__(16) float cstage[PF ? NW * 9 * 32 * PK : 1];
     const int2 u = units[blockIdx.x];
     stage_desc(insts, u.x, sD);
     const Params& L = sD.P;
     const int w = threadIdx.x >> 5;
+    float* wstage = cstage + (PF ? w * 9 * 32 * PK : 0);
     const int bx = u.y % sD.nbx, by = u.y / sD.nbx;
     const int x0 = bx * SW, y0 = by * (NW * CPT), j0 = y0 + w * CPT;
     zfv::DevState* st = sD.st;
@@ -82,22 +85,25 @@ k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
     if constexpr (PK == 1) {
         if (strip_interior<NW, CPT>(L, x0, y0))
             sweep_strip<MODE, WB, IMPL, CPT, true, PF>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
-                                                   float(dtd), dtd, m_loc, s_loc);
+                                                   float(dtd), dtd, m_loc, s_loc, wstage);
         else
             sweep_strip<MODE, WB, IMPL, CPT, false, PF>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
-                                                    float(dtd), dtd, m_loc, s_loc);
+                                                    float(dtd), dtd, m_loc, s_loc, wstage);
     } else {
         // 8-byte accesses need an even row length (x0 is even)
         if (pk::strip_interior2<NW, CPT>(L, x0, y0)) {
             if ((L.nx & 1) == 0)
                 pk::sweep_strip2<MODE, WB, IMPL, CPT, true, true, PF>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
-                                                                  j0, float(dtd), dtd, m_loc, s_loc);
+                                                                  j0, float(dtd), dtd, m_loc, s_loc,
+                                                                reinterpret_cast<float2*>(wstage));
             else
                 pk::sweep_strip2<MODE, WB, IMPL, CPT, true, false, PF>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
-                                                                   j0, float(dtd), dtd, m_loc, s_loc);
+                                                                   j0, float(dtd), dtd, m_loc, s_loc,
+                                                                reinterpret_cast<float2*>(wstage));
         } else {
             pk::sweep_strip2<MODE, WB, IMPL, CPT, false, false, PF>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
-                                                                j0, float(dtd), dtd, m_loc, s_loc);
+                                                                j0, float(dtd), dtd, m_loc, s_loc,
+                                                                reinterpret_cast<float2*>(wstage));
         }
     }
     if constexpr (MODE == S2) {

@@ -21,6 +21,7 @@
 // condition (extrapolation copies; a wall reverses the normal momentum), x side
 // first; strips whose stencil lies inside the domain skip that logic.
 #pragma once
+#include <cuda_pipeline.h>
 
 namespace zfv32 {
 
@@ -155,7 +156,7 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
                                             const float* __restrict__ inc_in, float* __restrict__ inc_out,
                                             float* __restrict__ Y, float* __restrict__ lo, const Params& L,
                                             int x0, int j0, float dt, double dtd, double& m_loc,
-                                            double& s_loc) {
+                                            double& s_loc, float* __restrict__ cstage) {
     const int lane = threadIdx.x & 31;
     const int nx = L.nx, ny = L.ny;
     const long long pl = L.plane;
@@ -186,8 +187,10 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
         // iteration ahead so its latency overlaps this row's arithmetic.
         const C4 w4 = (r + 1 < CPT) ? fetch<MODE, INTERIOR>(bed, X, inc_in, L, i, j + 3) : w3;
         // stage 2: this cell's FP32 state, stage-1 increment and remainder for
-        // the compensated update; PF loads them here so that they arrive during
-        // the face work, otherwise where they are used (fewer registers)
+        // the compensated update. PF: copied asynchronously into this warp's
+        // shared staging area (cp.async, no registers held) at the top of the
+        // row so that they arrive during the face work; otherwise loaded where
+        // they are used.
         float cx[3] = {0.0f, 0.0f, 0.0f}, ci[3] = {0.0f, 0.0f, 0.0f}, cl[3] = {0.0f, 0.0f, 0.0f};
         auto load_comp = [&]() {
             if (owns) {
@@ -200,7 +203,18 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
                 }
             }
         };
-        if constexpr (MODE == S2 && PF) load_comp();
+        if constexpr (MODE == S2 && PF) {
+            if (owns) {
+                const long long c = (long long)j * nx + i;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    __pipeline_memcpy_async(cstage + q * 32 + lane, X + q * pl + c, 4);
+                    __pipeline_memcpy_async(cstage + (3 + q) * 32 + lane, inc_in + q * pl + c, 4);
+                    __pipeline_memcpy_async(cstage + (6 + q) * 32 + lane, lo + q * pl + c, 4);
+                }
+                __pipeline_commit();
+            }
+        }
         RS lo_1, hi_1;
         reconstruct(w1, w2, w3, lo_1, hi_1);  // row j+1 in y
         const FaceR ft = face_rs<1, WB>(top, lo_1, L);   // face above row j
@@ -269,7 +283,17 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
                 inc_out[c] = inc_e; inc_out[pl + c] = inc_u; inc_out[2 * pl + c] = inc_v;
             } else {
                 // compensated Heun update in FP64: Q^{n+1} = (hi + lo) + (inc1 + inc2) / 2
-                if constexpr (!PF) load_comp();
+                if constexpr (PF) {
+                    __pipeline_wait_prior(0);
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        cx[q] = cstage[q * 32 + lane];
+                        ci[q] = cstage[(3 + q) * 32 + lane];
+                        cl[q] = cstage[(6 + q) * 32 + lane];
+                    }
+                } else {
+                    load_comp();
+                }
                 const double ne = (double(cx[0]) + double(cl[0])) + 0.5 * (double(ci[0]) + double(inc_e));
                 const double nu = (double(cx[1]) + double(cl[1])) + 0.5 * (double(ci[1]) + double(inc_u));
                 const double nv = (double(cx[2]) + double(cl[2])) + 0.5 * (double(ci[2]) + double(inc_v));

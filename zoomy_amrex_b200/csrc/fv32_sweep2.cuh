@@ -185,7 +185,7 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                                              const float* __restrict__ inc_in, float* __restrict__ inc_out,
                                              float* __restrict__ Y, float* __restrict__ lo, const Params& L,
                                              int x0, int j0, float dt, double dtd, double& m_loc,
-                                             double& s_loc) {
+                                             double& s_loc, float2* __restrict__ cstage) {
     const int lane = threadIdx.x & 31;
     const int nx = L.nx, ny = L.ny;
     const long long pl = L.plane;
@@ -213,8 +213,10 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
         // row j+3 is loaded one iteration ahead (latency hidden behind this row)
         const C42 w4 = (r + 1 < CPT) ? fetch2<MODE, INTERIOR, VEC>(bed, X, inc_in, L, cA, j + 3) : w3;
         // stage 2: the pair's FP32 state, stage-1 increment and remainder for
-        // the compensated update; PF loads them here so that they arrive during
-        // the face work, otherwise where they are used (fewer registers)
+        // the compensated update. PF: copied asynchronously into this warp's
+        // shared staging area (cp.async, no registers held) at the top of the
+        // row so that they arrive during the face work; otherwise loaded where
+        // they are used.
         float2 cx[3], ci[3], cl[3];
         auto load_comp = [&]() {
             const long long c = (long long)j * nx + cA;
@@ -234,7 +236,18 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                 }
             }
         };
-        if constexpr (MODE == S2 && PF) load_comp();
+        if constexpr (MODE == S2 && PF) {
+            if (vec_io && (ownA || ownB)) {
+                const long long c = (long long)j * nx + cA;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    __pipeline_memcpy_async(cstage + q * 32 + lane, X + q * pl + c, 8);
+                    __pipeline_memcpy_async(cstage + (3 + q) * 32 + lane, inc_in + q * pl + c, 8);
+                    __pipeline_memcpy_async(cstage + (6 + q) * 32 + lane, lo + q * pl + c, 8);
+                }
+                __pipeline_commit();
+            }
+        }
         RS2 lo_1, hi_1;
         reconstruct2(w1, w2, w3, lo_1, hi_1);
         const Face2 ft = face2<1, WB>(top, lo_1, L);
@@ -330,7 +343,21 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                 }
             } else {
                 // compensated Heun update in FP64, per cell
-                if constexpr (!PF) load_comp();
+                if constexpr (PF) {
+                    if (vec_io) {
+                        __pipeline_wait_prior(0);
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) {
+                            cx[q] = cstage[q * 32 + lane];
+                            ci[q] = cstage[(3 + q) * 32 + lane];
+                            cl[q] = cstage[(6 + q) * 32 + lane];
+                        }
+                    } else {
+                        load_comp();   // edge strips: plain loads
+                    }
+                } else {
+                    load_comp();
+                }
                 float i1[2][3], xs[2][3], lw[2][3];
 #pragma unroll
                 for (int q = 0; q < 3; ++q) {
