@@ -64,39 +64,8 @@ def parse():
     return ap.parse_args()
 
 
-def workload_fields(n: int, seed: int = SEED, rows: slice | None = None):
-    """Config-2 initial state (n x n over [0,100]^2): returns Q0 (4, ny, n), aux0 (7, ny, n)."""
-    rng = np.random.default_rng(seed)
-    cx, cy = rng.uniform(0, DOMAIN, 16), rng.uniform(0, DOMAIN, 16)
-    amp, wid = rng.uniform(0.2, 1.5, 16), rng.uniform(2.0, 10.0, 16)
-    hx, hy, hw = rng.uniform(0, DOMAIN), rng.uniform(0, DOMAIN), rng.uniform(2.0, 10.0)
-    dx = DOMAIN / n
-    x = (np.arange(n) + 0.5) * dx
-    ys = x if rows is None else x[rows]
-    ny = len(ys)
-    b = np.zeros((ny, n))
-    for k in range(16):
-        gx = np.exp(-((x - cx[k]) ** 2) / (2 * wid[k] ** 2))
-        gy = np.exp(-((ys - cy[k]) ** 2) / (2 * wid[k] ** 2))
-        b += amp[k] * np.outer(gy, gx)
-    eta = 1.0 + 0.3 * np.outer(np.exp(-((ys - hy) ** 2) / (2 * hw ** 2)),
-                               np.exp(-((x - hx) ** 2) / (2 * hw ** 2)))
-    h = np.maximum(eta - b, 0.0)
-    Q0 = np.zeros((4, ny, n))
-    Q0[0], Q0[1] = b, h
-    aux0 = np.zeros((7, ny, n))
-    aux0[1] = np.where(x < 0.5 * DOMAIN, 2.0, 1.0)[None, :]   # init_solution on aux
-    return Q0, aux0
-
-
-def workload_config(n: int, ny: int | None = None, y_extent: float | None = None):
-    from zoomy_amrex_b200._abi import ZFV_MODEL_SWE2D, make_config
-    ny = n if ny is None else ny
-    ye = DOMAIN if y_extent is None else y_extent
-    return make_config(ZFV_MODEL_SWE2D, n, ny, (0.0, 0.0), (DOMAIN, ye), spatial_order=2,
-                       well_balanced=True, implicit_source=True, clamp_positivity=False,
-                       cfl=0.45, dtmin=1e-7, dtmax=1.0, time_end=1e30, max_step=-1,
-                       bc=("wall",) * 4, params={"n_m": 0.03, "h_floor": 1e-6, "eps": 1e-24})
+from zoomy_amrex_b200.workloads import bump_workload_config as workload_config  # noqa: E402
+from zoomy_amrex_b200.workloads import bump_workload_fields as workload_fields  # noqa: E402
 
 
 def config_desc(n, K):

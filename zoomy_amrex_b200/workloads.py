@@ -3,6 +3,9 @@
 The reference quotes no public dataset for this path; these generators give
 the shapes and value distributions of its scenarios:
 
+* ``bump_workload_fields`` / ``bump_workload_config``: the 2-D wet/dry hump
+  over 16 Gaussian bumps (the benchmark's headline level);
+
 * ``bump_field``: Gaussian-bump bathymetry (centres uniform in the box,
   amplitudes U(0.2, 1.5) m, widths U(2, 10) m) under still water at eta0 plus
   an optional Gaussian hump;
@@ -15,6 +18,9 @@ from __future__ import annotations
 import numpy as np
 
 from ._abi import ZFV_MODEL_SWE2D, ZFV_PREC_FP32, ZFV_PREC_FP64, make_config
+
+BUMP_SEED = 2026
+BUMP_DOMAIN = 100.0
 
 
 def _bumps(rng, n_bumps, x_extent, y_extent, width=(2.0, 10.0)):
@@ -67,6 +73,46 @@ def dam_break_ensemble(n_inst: int = 256, seed: int = 4, side_range=(32, 512), d
                           params={"n_m": n_m}, precision=precision)
         out.append((cfg, Q0, aux0))
     return out
+
+
+def bump_workload_fields(n: int, seed: int = BUMP_SEED, rows: slice | None = None):
+    """Wet/dry hump over 16 seeded Gaussian bumps on n x n cells over
+    [0,100]^2 m: bumps with centres U(domain), amplitudes U(0.2,1.5) m,
+    widths U(2,10) m; eta = 1 m plus a 0.3 m Gaussian hump; h = max(eta - b, 0).
+    ``rows`` selects a strip of rows of the same grid. Returns Q0 (4, ny, n),
+    aux0 (7, ny, n) (aux row 1 carries the init_solution dam pattern)."""
+    rng = np.random.default_rng(seed)
+    cx, cy = rng.uniform(0, BUMP_DOMAIN, 16), rng.uniform(0, BUMP_DOMAIN, 16)
+    amp, wid = rng.uniform(0.2, 1.5, 16), rng.uniform(2.0, 10.0, 16)
+    hx, hy, hw = rng.uniform(0, BUMP_DOMAIN), rng.uniform(0, BUMP_DOMAIN), rng.uniform(2.0, 10.0)
+    dx = BUMP_DOMAIN / n
+    x = (np.arange(n) + 0.5) * dx
+    ys = x if rows is None else x[rows]
+    ny = len(ys)
+    b = np.zeros((ny, n))
+    for k in range(16):
+        gx = np.exp(-((x - cx[k]) ** 2) / (2 * wid[k] ** 2))
+        gy = np.exp(-((ys - cy[k]) ** 2) / (2 * wid[k] ** 2))
+        b += amp[k] * np.outer(gy, gx)
+    eta = 1.0 + 0.3 * np.outer(np.exp(-((ys - hy) ** 2) / (2 * hw ** 2)),
+                               np.exp(-((x - hx) ** 2) / (2 * hw ** 2)))
+    h = np.maximum(eta - b, 0.0)
+    Q0 = np.zeros((4, ny, n))
+    Q0[0], Q0[1] = b, h
+    aux0 = np.zeros((7, ny, n))
+    aux0[1] = np.where(x < 0.5 * BUMP_DOMAIN, 2.0, 1.0)[None, :]   # init_solution on aux
+    return Q0, aux0
+
+
+def bump_workload_config(n: int, ny: int | None = None, y_extent: float | None = None):
+    """The matching configuration: SWE2D, order 2, WB, point-implicit Manning n = 0.03, walls,
+    cfl 0.45, no stop time (callers set max_step / time_end)."""
+    ny = n if ny is None else ny
+    ye = BUMP_DOMAIN if y_extent is None else y_extent
+    return make_config(ZFV_MODEL_SWE2D, n, ny, (0.0, 0.0), (BUMP_DOMAIN, ye), spatial_order=2,
+                       well_balanced=True, implicit_source=True, clamp_positivity=False,
+                       cfl=0.45, dtmin=1e-7, dtmax=1.0, time_end=1e30, max_step=-1,
+                       bc=("wall",) * 4, params={"n_m": 0.03, "h_floor": 1e-6, "eps": 1e-24})
 
 
 def fp64_twin(cfg):
