@@ -43,7 +43,7 @@ BYTES_PER_CELL_STEP_FP32 = 92
 
 # DRAM bytes per cell per step (both k32b_stage launches), from
 # `ncu --set full` of `python -m zoomy_amrex_b200.profile_case fp32 --n 3072
-# --variant 7 --steps 3` (profiles/k32b_stage_fp32_3072.md): stage 1 read
+# --variant 7 --steps 3`: stage 1 read
 # 151.2 MB + wrote 78.2 MB, stage 2 read 378.0 MB + wrote 189.7 MB over
 # 3072^2 cells. The traffic scales with the cells, so it is scaled to the
 # benchmark grid per launch.
