@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=100,
                     help="steps of the 256-box batched-vs-per-box comparison (0 = skip)")
+    ap.add_argument("--amr-steps", type=int, default=10,
+                    help="coarse steps of the 3-level AMR hierarchy at base 1024^2 (0 = skip)")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the adjoint timing / gradient checks (1024^2, 200 steps)")
     ap.add_argument("--err-steps", type=int, default=1000,
@@ -330,6 +332,44 @@ def ensemble_bench(K, W, local, n_inst=256, seed=2027):
             "strip_shape_ms_per_step": {str(v): t for v, t in times.items()}, "picked_variant": best}
 
 
+def amr_bench(local, n=1024, steps=10, warm=2, max_level=2, B=64):
+    """A 3-level AMR hierarchy (ratio 2, base n^2, boxes of B^2, tagged where
+    |grad eta| > 0.01, regrid every 2 coarse steps, subcycling) of a dam
+    break over bumps: coarse steps per second and cell updates per second
+    over all levels (level l counts its cells 2^l times per coarse step)."""
+    import torch
+    from zoomy_amrex_b200.amr import AmrHierarchy
+    from zoomy_amrex_b200.workloads import dam_break_level
+    cfg, Q0 = dam_break_level(n)
+    hier = AmrHierarchy(cfg, Q0, max_level=max_level, B=B, threshold=0.01, regrid_int=2,
+                        device=f"cuda:{local}")
+    hier.run(warm)
+    torch.cuda.synchronize()
+    cells = 0
+    boxes = []
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(hier.stream)
+    for _ in range(steps):
+        cells += hier.cells_per_coarse_step()
+        hier.step()
+        boxes.append([lv.n for lv in hier.levels])
+    e1.record(hier.stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    wall = time.perf_counter() - t0
+    finest_uniform = (n << max_level) ** 2 * (1 << max_level) * steps
+    mass_ok = np.isfinite(hier.level_state(0)).all()
+    hier.close()
+    return {"workload": f"dam break over bumps, base {n}^2, {max_level + 1} levels, boxes {B}^2, "
+                        "tag |grad eta| > 0.01, regrid every 2 coarse steps, FP32 form",
+            "coarse_steps": steps, "ms_per_coarse_step": ms / steps, "wall_s": wall,
+            "cell_updates_per_s": cells / (ms * 1e-3),
+            "boxes_per_level_each_step": boxes,
+            "cell_updates_vs_uniform_finest": cells / finest_uniform,
+            "finite": bool(mass_ok)}
+
+
 def box5(a):
     """5 x 5 box filter with mirrored edges."""
     p = np.pad(a, 2, mode="symmetric")
@@ -533,6 +573,9 @@ def main():
     adj = None
     if args.adjoint and rank == 0:
         adj = adjoint_bench(local)
+    amr = None
+    if args.amr_steps > 0:
+        amr = amr_bench(local, steps=args.amr_steps)
 
     err = None
     if args.err_steps > 0 and rank == 0:
@@ -594,7 +637,7 @@ def main():
                 "forms": {"fp32_chosen": v32, "fp64_plain": v64, "fp32_over_fp64": v32 / v64,
                           "ms_per_step_fp32": ms32 / K, "ms_per_step_fp64": ms64 / K},
                 "depth_error_fp32_vs_fp64": err,
-                "autotune": tuning, "ensemble": ens, "adjoint": adj,
+                "autotune": tuning, "ensemble": ens, "adjoint": adj, "amr": amr,
                 "hbm_gbs": achieved32,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 2 * K, "clocks": clk.summary()}

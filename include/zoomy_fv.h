@@ -260,6 +260,61 @@ int zfv_batch_units(const zfv_batch* b);
  * zoomy_amrex_b200/autotune.py measures them and caches the fastest per n_dof_q).
  */
 int zfv_tile_variants(int* nw, int* cpt, int* cols, int* prefetch, int max_n);
+
+/*
+ * Batches whose instances are grouped: instances with the same group id
+ * (0 .. n_inst-1) share one run record — one dt, one CFL / mass reduction over
+ * all their cells, one step counter — as the boxes of one AMR level do
+ * (ZoomyAmr::ComputeDt reduces over the level's boxes, ZoomyAmr.cpp:448-515).
+ * Grouped instances must share the CFL constants.
+ */
+int zfv_batch_create_grouped(const zfv_config* cfgs, int n_inst, const int* groups, zfv_batch** out);
+/* Per instance, a ghost frame ((nx+4) x (ny+4) x 4 floats, [b, eta, hu, hv]
+ * planes) whose ring the kernels read instead of mirroring the box's own cells
+ * (NULL entries / NULL array: physical mirror). Re-uploads the descriptors. */
+int zfv_batch_set_frames(zfv_batch* b, const float* const* frames, void* stream);
+/* Set each instance's next dt from dts (device, one per instance; enqueued,
+ * no synchronization). AMR levels step with dt_0 / 2^l. */
+int zfv_batch_set_dt(zfv_batch* b, const double* dts, void* stream);
+/* One stage (1 or 2) of one SSP-RK2 step of every instance, so that ghost
+ * frames can be refilled between the stages (Advance's per-stage FillPatch,
+ * ZoomyAmr.cpp:561-572). */
+int zfv_batch_stage(zfv_batch* b, int stage, void* stream);
+/* Device address of the bound instance descriptors (for the AMR kernels). */
+const void* zfv_batch_descriptors(const zfv_batch* b);
+
+/*
+ * Block-structured AMR over grouped batches (ZoomyAmr.cpp:161-288, 733-762:
+ * FillPatch / FillPatchTwoLevels, average_down, ErrorEst, RemakeLevel). A
+ * level is a batch of B x B boxes on a block grid; map[by * nbx + bx] is the
+ * instance holding block (bx, by), -1 if absent; pos lists (bx, by) of the
+ * boxes to work on (device int pairs); frames is a device array of the boxes'
+ * ghost-frame pointers in the same order. Refinement ratio 2.
+ */
+typedef struct zfv_amr_level {
+    const void* insts;   /* zfv_batch_descriptors() of the level's batch */
+    const int* map;      /* device, nby * nbx */
+    int nbx, nby;        /* block grid */
+    int B;               /* cells per box side (even) */
+    int nx, ny;          /* the level's grid in cells */
+    int wall;            /* bit s set: side s (x_lo, x_hi, y_lo, y_hi) is a reflective wall */
+    int pad;
+} zfv_amr_level;
+/* Ghost frames before stage `stage` (1: the stage input; 2: neighbours'
+ * stage-2 input): same-level boxes, else conservative linear interpolation of
+ * `coarse` (NULL on level 0), physical boundaries by mirroring. */
+int zfv_amr_fill(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* pos, float* const* frames,
+                 int n_boxes, int stage, void* stream);
+/* Replace the coarse cells under the listed fine boxes by 2 x 2 averages. */
+int zfv_amr_average_down(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* pos, int n_boxes,
+                         void* stream);
+/* flags[k] = 1 (others untouched) for boxes with a cell where |grad eta| > threshold. */
+int zfv_amr_tag(const zfv_amr_level* level, const int* pos, int n_boxes, double dx, double dy, double threshold,
+                int* flags, void* stream);
+/* Fill freshly created boxes from the old boxes of the level (where present)
+ * or from the coarser level. */
+int zfv_amr_regrid_fill(const zfv_amr_level* level, const zfv_amr_level* old_level, const zfv_amr_level* coarse,
+                        const int* pos, int n_boxes, void* stream);
 int zfv_batch_set_variant(zfv_batch* b, int variant, void* stream);
 
 /*

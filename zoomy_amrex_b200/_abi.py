@@ -73,6 +73,11 @@ class zfv_status(C.Structure):
     ]
 
 
+class zfv_amr_level(C.Structure):
+    _fields_ = [("insts", C.c_void_p), ("map", C.c_void_p), ("nbx", C.c_int), ("nby", C.c_int),
+                ("B", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("wall", C.c_int), ("pad", C.c_int)]
+
+
 def make_config(model: int, nx: int, ny: int, prob_lo, prob_hi, *, spatial_order: int = 1,
                 well_balanced: bool = False, implicit_source: bool = False,
                 clamp_positivity: bool = False, positivity: str = "none", cfl: float = 0.9,

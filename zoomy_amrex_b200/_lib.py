@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes as C
 import pathlib
 
-from ._abi import zfv_config, zfv_status
+from ._abi import zfv_amr_level, zfv_config, zfv_status
 
 LIB_PATH = pathlib.Path(__file__).resolve().parent / "lib" / "libzoomyfv.so"
 
@@ -23,7 +23,9 @@ SYMBOLS = ("zfv_last_error", "zfv_version", "zfv_sizeof_config", "zfv_sizeof_sta
            "zfv_batch_status", "zfv_batch_units", "zfv_tile_variants", "zfv_batch_set_variant",
            "zfv_run_state_bytes", "zfv_save_run_state", "zfv_load_run_state", "zfv_adj_tape_bytes",
            "zfv_adj_work_bytes", "zfv_adj_record", "zfv_adj_step", "zfv_adj_variants",
-           "zfv_adj_set_variant")
+           "zfv_adj_set_variant", "zfv_batch_create_grouped", "zfv_batch_set_frames", "zfv_batch_set_dt",
+           "zfv_batch_stage", "zfv_batch_descriptors", "zfv_amr_fill", "zfv_amr_average_down", "zfv_amr_tag",
+           "zfv_amr_regrid_fill")
 
 
 class ZfvError(RuntimeError):
@@ -85,6 +87,17 @@ def lib():
     L.zfv_adj_record.argtypes = [vp, vp, vp, vp, vp, i, vp]
     L.zfv_adj_step.argtypes = [vp, vp, i, vp, vp, vp, vp, vp]
     L.zfv_adj_set_variant.argtypes = [i]
+    L.zfv_batch_create_grouped.argtypes = [C.POINTER(zfv_config), i, C.POINTER(i), C.POINTER(vp)]
+    L.zfv_batch_set_frames.argtypes = [vp, pp, vp]
+    L.zfv_batch_set_dt.argtypes = [vp, vp, vp]
+    L.zfv_batch_stage.argtypes = [vp, i, vp]
+    L.zfv_batch_descriptors.argtypes = [vp]
+    L.zfv_batch_descriptors.restype = vp
+    lv = C.POINTER(zfv_amr_level)
+    L.zfv_amr_fill.argtypes = [lv, lv, vp, vp, i, i, vp]
+    L.zfv_amr_average_down.argtypes = [lv, lv, vp, i, vp]
+    L.zfv_amr_tag.argtypes = [lv, vp, i, d, d, d, vp, vp]
+    L.zfv_amr_regrid_fill.argtypes = [lv, lv, lv, vp, i, vp]
     _lib = L
     return L
 

@@ -1,0 +1,301 @@
+"""Block-structured AMR hierarchy of the FP32 shallow-water form.
+
+The reference's AmrCore driver (ZoomyAmr.cpp:161-288, 733-762): a base level
+plus up to ``max_level`` refined levels (ratio 2), tagging by an eta-gradient
+threshold (ErrorEst), regridding, per-stage ghost filling from the same level
+or the coarser one (FillPatch / FillPatchTwoLevels with conservative linear
+interpolation), subcycling (a level-l step is followed by two level-(l+1)
+steps), and averaging the fine solution down onto the coarse level after them.
+There is no flux register, as in the reference (ZoomyAmr.H:85).
+
+Here every level is a batch of equal B x B boxes on a regular block grid (the
+box layout of a quadtree rather than AMReX's Berger-Rigoutsos clustering):
+one launch per RK stage advances all boxes of a level, the boxes of a level
+share one run record, and a box's ghost ring is a small frame array the stage
+kernels read in place of the physical mirror.
+
+Two choices differ from the reference, which steps each level with its own
+CFL dt (so fine levels need not land on the coarse time) and regrids at every
+coarse step: here dt_l = dt_0 / 2^l with dt_0 the largest step every level's
+CFL law allows, and regridding happens every ``regrid_int`` coarse steps.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._abi import ZFV_PREC_FP32, zfv_amr_level, zfv_config
+from .batch import Batch
+
+
+def _cfg_copy(c: zfv_config) -> zfv_config:
+    d = zfv_config()
+    C.memmove(C.byref(d), C.byref(c), C.sizeof(c))
+    return d
+
+
+class AmrLevel:
+    """All boxes of one level: a grouped batch plus its block map and frames."""
+
+    def __init__(self, hier, lev: int, blocks: list[tuple[int, int]], Q0s=None, variant=None):
+        self.h, self.lev = hier, lev
+        B = hier.B
+        self.B = B
+        self.nbx, self.nby = hier.nbx0 << lev, hier.nby0 << lev
+        self.nx, self.ny = self.nbx * B, self.nby * B
+        self.dx = hier.dx0 / (1 << lev)
+        self.dy = hier.dy0 / (1 << lev)
+        self.blocks = list(blocks)
+        dev = hier.device
+        cfgs = []
+        for (bx, by) in self.blocks:
+            c = _cfg_copy(hier.cfg)
+            c.nx = c.ny = B
+            c.prob_lo[0] = hier.lo[0] + bx * B * self.dx
+            c.prob_lo[1] = hier.lo[1] + by * B * self.dy
+            c.prob_hi[0] = c.prob_lo[0] + B * self.dx
+            c.prob_hi[1] = c.prob_lo[1] + B * self.dy
+            c.precision = ZFV_PREC_FP32
+            c.time_end = 1.0e30
+            c.max_step = -1
+            cfgs.append(c)
+        self.batch = Batch(cfgs, Q0s, None, device=dev, stream=hier.stream, groups=[0] * len(cfgs),
+                           variant=hier.variant if variant is None else variant)
+        n = len(self.blocks)
+        self.frames = torch.zeros((n, 4, B + 4, B + 4), dtype=torch.float32, device=dev)
+        self.batch.set_frames([self.frames[k] for k in range(n)])
+        self.map = torch.full((self.nby, self.nbx), -1, dtype=torch.int32)
+        for k, (bx, by) in enumerate(self.blocks):
+            self.map[by, bx] = k
+        self.map = self.map.to(dev)
+        self.pos = torch.tensor(self.blocks, dtype=torch.int32, device=dev).reshape(n, 2).contiguous()
+        self.frame_ptrs = torch.tensor([self.frames[k].data_ptr() for k in range(n)], dtype=torch.int64,
+                                       device=dev)
+        self.dts = torch.zeros(n, dtype=torch.float64, device=dev)
+        self.view = zfv_amr_level(C.c_void_p(self.batch.descriptors), C.c_void_p(self.map.data_ptr()),
+                                  self.nbx, self.nby, B, self.nx, self.ny, hier.wall, 0)
+
+    @property
+    def n(self) -> int:
+        return len(self.blocks)
+
+    def close(self):
+        self.batch.close()
+
+
+class AmrHierarchy:
+    """A ``max_level``-deep hierarchy over a base grid of ``nx0 x ny0`` cells.
+
+    cfg: an SWE2D configuration of the base grid (scheme switches, CFL
+    constants, parameters, boundary tags; nx/ny multiples of ``B``). Q0: the
+    base level's FP64 state [b, h, hu, hv]. Finer levels start as
+    interpolations of the coarser one, refined where tagged (a negative
+    ``threshold`` refines everywhere the nesting allows).
+    """
+
+    def __init__(self, cfg: zfv_config, Q0, max_level: int = 2, B: int = 64, threshold: float = 0.01,
+                 regrid_int: int = 2, device="cuda:0", variant: int = 1):
+        if cfg.nx % B or cfg.ny % B or B % 2:
+            raise ValueError("the base grid must be a multiple of the (even) box side B in both directions")
+        self.cfg = _cfg_copy(cfg)
+        self.B, self.max_level, self.threshold, self.regrid_int = B, max_level, threshold, regrid_int
+        self.device = torch.device(device)
+        self.stream = torch.cuda.Stream(self.device)
+        self.variant = variant
+        self.nbx0, self.nby0 = cfg.nx // B, cfg.ny // B
+        self.lo = (cfg.prob_lo[0], cfg.prob_lo[1])
+        self.dx0 = (cfg.prob_hi[0] - cfg.prob_lo[0]) / cfg.nx
+        self.dy0 = (cfg.prob_hi[1] - cfg.prob_lo[1]) / cfg.ny
+        self.wall = sum(1 << s for s in range(4) if cfg.bc_tag[s] == 1)
+        self.div = float(cfg.cfl_dimension * cfg.cfl_degree_factor)
+        self.time, self.steps = 0.0, 0
+        Q0 = np.asarray(Q0, dtype=np.float64)
+        blocks = [(bx, by) for by in range(self.nby0) for bx in range(self.nbx0)]
+        Q0s = [np.ascontiguousarray(Q0[:, by * B:(by + 1) * B, bx * B:(bx + 1) * B]) for bx, by in blocks]
+        self.levels: list[AmrLevel] = [AmrLevel(self, 0, blocks, Q0s)]
+        self.levels[0].batch.begin()
+        for _ in range(max_level):          # initial hierarchy (InitData's repeated regrid)
+            if not self.regrid():
+                break
+        self.sync()
+
+    # -- small helpers -------------------------------------------------------------
+    def _s(self):
+        return C.c_void_p(self.stream.cuda_stream)
+
+    def sync(self):
+        self.stream.synchronize()
+
+    def _coarse_view(self, lev):
+        return C.byref(self.levels[lev - 1].view) if lev > 0 else None
+
+    def fill(self, lev: int, stage: int):
+        L = self.levels[lev]
+        _lib.check(_lib.lib().zfv_amr_fill(C.byref(L.view), self._coarse_view(lev), L.pos.data_ptr(),
+                                           L.frame_ptrs.data_ptr(), L.n, stage, self._s()), "zfv_amr_fill")
+
+    def average_down(self, lev: int):
+        F, Cl = self.levels[lev], self.levels[lev - 1]
+        _lib.check(_lib.lib().zfv_amr_average_down(C.byref(F.view), C.byref(Cl.view), F.pos.data_ptr(), F.n,
+                                                   self._s()), "zfv_amr_average_down")
+
+    # -- regridding ------------------------------------------------------------------
+    def tags(self, lev: int) -> np.ndarray:
+        L = self.levels[lev]
+        flags = torch.zeros(L.n, dtype=torch.int32, device=self.device)
+        with torch.cuda.stream(self.stream):
+            _lib.check(_lib.lib().zfv_amr_tag(C.byref(L.view), L.pos.data_ptr(), L.n, L.dx, L.dy, self.threshold,
+                                              flags.data_ptr(), self._s()), "zfv_amr_tag")
+        self.sync()
+        return flags.cpu().numpy()
+
+    def _refined_blocks(self, lev: int) -> list[tuple[int, int]]:
+        """Level-(lev+1) blocks: children of tagged level-lev blocks and their
+        neighbours, restricted to level-lev blocks whose 8 neighbours exist at
+        level lev (or lie outside the domain), so that every ghost cell and
+        every interpolation stencil of the new level has coarse data."""
+        L = self.levels[lev]
+        have = np.zeros((L.nby, L.nbx), dtype=bool)
+        for bx, by in L.blocks:
+            have[by, bx] = True
+        tagged = np.zeros_like(have)
+        if self.threshold < 0:            # refine everything the nesting allows
+            tagged = have.copy()
+        else:
+            for k, f in enumerate(self.tags(lev)):
+                if f:
+                    bx, by = L.blocks[k]
+                    tagged[by, bx] = True
+        want = tagged.copy()
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                want |= np.roll(np.roll(tagged, dy, 0), dx, 1) & self._in_domain_shift(tagged.shape, dy, dx)
+        ok = have.copy()
+        padded = np.pad(have, 1, constant_values=True)       # outside the domain counts as present
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                ok &= padded[1 + dy:1 + dy + L.nby, 1 + dx:1 + dx + L.nbx]
+        sel = want & ok
+        out = []
+        for by, bx in zip(*np.nonzero(sel)):
+            for cy in (0, 1):
+                for cx in (0, 1):
+                    out.append((2 * int(bx) + cx, 2 * int(by) + cy))
+        return sorted(out, key=lambda p: (p[1], p[0]))
+
+    @staticmethod
+    def _in_domain_shift(shape, dy, dx):
+        m = np.ones(shape, dtype=bool)
+        if dy > 0:
+            m[:dy, :] = False
+        elif dy < 0:
+            m[dy:, :] = False
+        if dx > 0:
+            m[:, :dx] = False
+        elif dx < 0:
+            m[:, dx:] = False
+        return m
+
+    def regrid(self) -> bool:
+        """Rebuild levels 1..max_level from the tags, top down. Returns whether
+        the finest level count or any box set changed."""
+        changed = False
+        for lev in range(self.max_level):
+            if lev >= len(self.levels):
+                break
+            blocks = self._refined_blocks(lev)
+            old = self.levels[lev + 1] if lev + 1 < len(self.levels) else None
+            if old is not None and blocks == old.blocks:
+                continue
+            changed = True
+            if not blocks:
+                for L in self.levels[lev + 1:]:
+                    L.close()
+                del self.levels[lev + 1:]
+                break
+            new = AmrLevel(self, lev + 1, blocks)
+            ov = C.byref(old.view) if old is not None else None
+            with torch.cuda.stream(self.stream):
+                _lib.check(_lib.lib().zfv_amr_regrid_fill(C.byref(new.view), ov, C.byref(self.levels[lev].view),
+                                                          new.pos.data_ptr(), new.n, self._s()), "zfv_amr_regrid_fill")
+            new.batch.begin()
+            self.sync()
+            if old is not None:
+                old.close()
+                self.levels[lev + 1] = new
+            else:
+                self.levels.append(new)
+        return changed
+
+    # -- time stepping -----------------------------------------------------------------
+    def _dt0(self) -> float:
+        """The largest dt_0 with dt_0 / 2^l inside every level's CFL bound
+        (dt = cfl / (d (2k+1) max |lambda|/dx), ZoomyAmr.cpp:448-515)."""
+        c = self.cfg
+        dt0 = c.dtmax
+        for L in self.levels:
+            m = max(s["max_inv"] for s in L.batch.status()[:1])
+            if m > 1e-14:
+                dt0 = min(dt0, (1 << L.lev) * (c.cfl / (self.div * m)))
+        return max(dt0, c.dtmin)
+
+    def _advance(self, lev: int):
+        L = self.levels[lev]
+        L.batch.set_dt(L.dts)
+        self.fill(lev, 1)
+        L.batch.stage(1)
+        self.fill(lev, 2)
+        L.batch.stage(2)
+
+    def _time_step(self, lev: int):
+        self._advance(lev)
+        if lev + 1 < len(self.levels):
+            for _ in range(2):
+                self._time_step(lev + 1)
+            self.average_down(lev + 1)
+
+    def step(self):
+        """One coarse step of the whole hierarchy (ZoomyAmr::TimeStep's recursion)."""
+        if self.steps > 0 and self.regrid_int > 0 and self.steps % self.regrid_int == 0 and self.max_level > 0:
+            self.regrid()
+        dt0 = self._dt0()
+        with torch.cuda.stream(self.stream):
+            for L in self.levels:
+                L.dts.fill_(dt0 / (1 << L.lev))
+        self._time_step(0)
+        self.time += dt0
+        self.steps += 1
+        return dt0
+
+    def run(self, n_steps: int):
+        for _ in range(n_steps):
+            self.step()
+        self.sync()
+
+    # -- output ----------------------------------------------------------------------------
+    def cells_per_coarse_step(self) -> int:
+        """Cell updates of one coarse step: level l's cells times its 2^l substeps."""
+        return sum(L.n * self.B * self.B * (1 << L.lev) for L in self.levels)
+
+    def level_state(self, lev: int) -> np.ndarray:
+        """Level ``lev`` as a dense (4, ny, nx) FP64 array [b, h, hu, hv]; NaN where no box."""
+        L = self.levels[lev]
+        B = self.B
+        out = np.full((4, L.ny, L.nx), np.nan)
+        for (bx, by), q in zip(L.blocks, L.batch.state64()):
+            out[:, by * B:(by + 1) * B, bx * B:(bx + 1) * B] = q.cpu().numpy()
+        return out
+
+    def mass(self) -> float:
+        """Sum of h dx dy over the base level (finer levels are averaged onto it)."""
+        q = self.level_state(0)
+        return float(q[1].sum() * self.dx0 * self.dy0)
+
+    def close(self):
+        for L in self.levels:
+            L.close()
+        self.levels = []

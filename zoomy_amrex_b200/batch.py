@@ -41,10 +41,11 @@ class Batch:
     """
 
     def __init__(self, cfgs: Sequence[zfv_config], Q0s, A0s, device="cuda:0",
-                 stream: torch.cuda.Stream | None = None, variant: int | None = None):
+                 stream: torch.cuda.Stream | None = None, variant: int | None = None,
+                 groups: Sequence[int] | None = None):
         if not torch.cuda.is_available():
             raise _lib.ZfvError("zoomy_amrex_b200 needs a CUDA device (no CPU fallback)")
-        if not (len(cfgs) == len(Q0s) == len(A0s)):
+        if (Q0s is not None and len(Q0s) != len(cfgs)) or (A0s is not None and len(A0s) != len(cfgs)):
             raise ValueError("cfgs, Q0s and A0s must have the same length")
         for c in cfgs:
             if c.model != ZFV_MODEL_SWE2D or c.precision != ZFV_PREC_FP32:
@@ -55,15 +56,21 @@ class Batch:
         arr = (zfv_config * self.n)(*cfgs)
         self.cfgs = list(arr)
         h = C.c_void_p()
-        _lib.check(L.zfv_batch_create(arr, self.n, C.byref(h)), "zfv_batch_create")
+        if groups is None:
+            _lib.check(L.zfv_batch_create(arr, self.n, C.byref(h)), "zfv_batch_create")
+        else:
+            g = (C.c_int * self.n)(*[int(x) for x in groups])
+            _lib.check(L.zfv_batch_create_grouped(arr, self.n, g, C.byref(h)), "zfv_batch_create_grouped")
         self._h = h
         self.stream = stream if stream is not None else torch.cuda.Stream(self.device)
         self.stream.wait_stream(torch.cuda.current_stream(self.device))
         info = MODELS[ZFV_MODEL_SWE2D]
         self.Q, self.aux = [], []
-        for c, a0 in zip(self.cfgs, A0s):
+        for c, a0 in zip(self.cfgs, A0s if A0s is not None else [None] * self.n):
             self.Q.append(torch.empty((info["n_q"], c.ny, c.nx), dtype=torch.float32, device=self.device))
-            self.aux.append(self._f64(a0, (info["n_aux"], c.ny, c.nx)))
+            shape = (info["n_aux"], c.ny, c.nx)
+            self.aux.append(self._f64(a0, shape) if a0 is not None
+                            else torch.zeros(shape, dtype=torch.float64, device=self.device))
         self.scratch = torch.zeros(int(L.zfv_batch_scratch_bytes(h)), dtype=torch.uint8, device=self.device)
         self._qp = (C.c_void_p * self.n)(*[q.data_ptr() for q in self.Q])
         self._ap = (C.c_void_p * self.n)(*[a.data_ptr() for a in self.aux])
@@ -76,7 +83,8 @@ class Batch:
         if variant is not None:
             self.set_variant(variant)
         self.variant = 0 if variant is None else int(variant)
-        self.load(Q0s)
+        if Q0s is not None:
+            self.load(Q0s)
         self._graph = None
         self._graph_steps = 0
 
@@ -116,6 +124,24 @@ class Batch:
         torch.cuda.synchronize(self.device)
         _lib.check(_lib.lib().zfv_batch_import(self._h, ptrs, self._s()), "zfv_batch_import")
         del q64
+
+    @property
+    def descriptors(self) -> int:
+        """Device address of the instance descriptors (for the AMR kernels)."""
+        return int(_lib.lib().zfv_batch_descriptors(self._h) or 0)
+
+    def set_frames(self, frames):
+        """Ghost frames (one float32 tensor (4, ny+4, nx+4) per instance, or None)."""
+        ptrs = (C.c_void_p * self.n)(*[(f.data_ptr() if f is not None else None) for f in frames])
+        _lib.check(_lib.lib().zfv_batch_set_frames(self._h, ptrs, self._s()), "zfv_batch_set_frames")
+
+    def set_dt(self, dts: torch.Tensor):
+        """Next dt of every instance from a device float64 tensor (enqueued)."""
+        _lib.check(_lib.lib().zfv_batch_set_dt(self._h, dts.data_ptr(), self._s()), "zfv_batch_set_dt")
+
+    def stage(self, k: int):
+        """Stage k (1 or 2) of one step of every instance (enqueued)."""
+        _lib.check(_lib.lib().zfv_batch_stage(self._h, int(k), self._s()), "zfv_batch_stage")
 
     def begin(self):
         _lib.check(_lib.lib().zfv_batch_begin(self._h, self._s()), "zfv_batch_begin")

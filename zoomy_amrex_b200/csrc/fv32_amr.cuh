@@ -1,0 +1,235 @@
+// Block-structured AMR on top of the FP32 batch engine.
+//
+// Each level is a batch of equal square boxes (B x B cells) on a regular
+// block grid; `map` gives, per block position, the batch instance holding it
+// (-1: not present at this level). All boxes of a level share one run record
+// (one dt, one CFL reduction). Refinement ratio 2: a level-(l+1) box covers a
+// quarter of a level-l box.
+//
+// Kernels (the reference's AmrCore pieces, ZoomyAmr.cpp:161-288, 733-762):
+//   k32a_fill          ghost frames of every box of a level before a stage:
+//                      same-level neighbour (FillBoundary), else conservative
+//                      linear interpolation of the next coarser level
+//                      (FillPatchTwoLevels with cell_cons_interp), and the
+//                      physical boundary by mirroring (FillPhysicalBC_mf);
+//   k32a_average_down  fine -> coarse averages under each fine box;
+//   k32a_tag           per box: any cell with |grad eta| > threshold (ErrorEst);
+//   k32a_regrid_fill   fill new boxes from the old boxes of the same level
+//                      where they overlap, else from the coarser level
+//                      (RemakeLevel / MakeNewLevelFromCoarse).
+// The coarse data used for a fine box's ghosts is the coarse level's current
+// state (the reference fills from Q[lev-1] at t_new only).
+#pragma once
+
+namespace zfv32 {
+namespace amr {
+
+struct LevelView {
+    const BInst* insts;   // the level's batch descriptors (device)
+    const int* map;       // [nby * nbx] block position -> instance, -1 absent
+    int nbx, nby;         // block grid
+    int B;                // cells per box side
+    int nx, ny;           // level grid (cells)
+    int wall;             // bit s: side s (x_lo, x_hi, y_lo, y_hi) is a reflective wall
+    int pad_;
+};
+
+// The stage input of level cell (I, J): mirrored into the domain with the
+// wall sign flips; false when no box of the level holds the cell.
+__device__ __forceinline__ bool lookup(const LevelView& V, int I, int J, bool with_inc, C4& out) {
+    bool fu = false, fv = false;
+    if (I < 0) { I = -1 - I; fu = (V.wall & 1) != 0; }
+    else if (I >= V.nx) { I = 2 * V.nx - 1 - I; fu = (V.wall & 2) != 0; }
+    if (J < 0) { J = -1 - J; fv = (V.wall & 4) != 0; }
+    else if (J >= V.ny) { J = 2 * V.ny - 1 - J; fv = (V.wall & 8) != 0; }
+    if (I < 0 || I >= V.nx || J < 0 || J >= V.ny) return false;
+    const int bx = I / V.B, by = J / V.B;
+    const int k = V.map[by * V.nbx + bx];
+    if (k < 0) return false;
+    const BInst& D = V.insts[k];
+    const unsigned parity = *(volatile const unsigned*)&D.st->parity;
+    const float* X = parity ? D.alt : D.Qs;
+    const long long pl = D.P.plane;
+    const long long c = (long long)(J - by * V.B) * D.P.nx + (I - bx * V.B);
+    out.b = D.bed[c];
+    out.e = X[c];
+    out.u = X[pl + c];
+    out.v = X[2 * pl + c];
+    if (with_inc) {
+        out.e += D.inc[c];
+        out.u += D.inc[pl + c];
+        out.v += D.inc[2 * pl + c];
+    }
+    if (fu) out.u = -out.u;
+    if (fv) out.v = -out.v;
+    return true;
+}
+
+// Conservative linear interpolation of level-(l-1) data at level-l cell
+// (I, J) (inside the domain): minmod-limited slopes, so a constant field (a
+// lake at rest's eta) interpolates exactly and the 2 x 2 average of the fine
+// values is the coarse value.
+__device__ __forceinline__ C4 coarse_interp(const LevelView& C, int I, int J) {
+    const int ic = I >> 1, jc = J >> 1;
+    C4 c0{0.0f, 0.0f, 0.0f, 0.0f};
+    if (!lookup(C, ic, jc, false, c0)) return c0;
+    C4 xm = c0, xp = c0, ym = c0, yp = c0;
+    lookup(C, ic - 1, jc, false, xm);
+    lookup(C, ic + 1, jc, false, xp);
+    lookup(C, ic, jc - 1, false, ym);
+    lookup(C, ic, jc + 1, false, yp);
+    const float ox = (I & 1) ? 0.25f : -0.25f, oy = (J & 1) ? 0.25f : -0.25f;
+    C4 r;
+    r.b = c0.b + ox * mm(c0.b - xm.b, xp.b - c0.b) + oy * mm(c0.b - ym.b, yp.b - c0.b);
+    r.e = c0.e + ox * mm(c0.e - xm.e, xp.e - c0.e) + oy * mm(c0.e - ym.e, yp.e - c0.e);
+    r.u = c0.u + ox * mm(c0.u - xm.u, xp.u - c0.u) + oy * mm(c0.u - ym.u, yp.u - c0.u);
+    r.v = c0.v + ox * mm(c0.v - xm.v, xp.v - c0.v) + oy * mm(c0.v - ym.v, yp.v - c0.v);
+    return r;
+}
+
+// Ring cells of a (B+4)^2 frame, enumerated: bottom two rows, top two rows,
+// then the two left and two right columns of the box rows.
+__device__ __forceinline__ void ring_cell(int k, int B, int& fi, int& fj) {
+    const int W = B + 4;
+    if (k < 2 * W) { fj = k / W; fi = k % W; return; }
+    k -= 2 * W;
+    if (k < 2 * W) { fj = B + 2 + k / W; fi = k % W; return; }
+    k -= 2 * W;
+    fj = 2 + k / 4;
+    const int col = k % 4;
+    fi = col < 2 ? col : B + col;
+}
+
+// Ghost frames of all boxes of level F (coarse level C; C.insts == nullptr
+// for level 0). stage 1 fills the stage input Q; stage 2 fills Q + inc1 for
+// same-level neighbours (their stage-2 input) and the coarse state otherwise.
+__global__ void k32a_fill(LevelView F, LevelView C, const int2* __restrict__ pos, float* const* __restrict__ frames,
+                          int n_boxes, int stage) {
+    const int box = blockIdx.y;
+    if (box >= n_boxes) return;
+    const int B = F.B, W = B + 4;
+    const int ring = W * W - B * B;
+    const long long fp = (long long)W * W;
+    float* fr = frames[box];
+    const int2 p = pos[box];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ring; k += gridDim.x * blockDim.x) {
+        int fi, fj;
+        ring_cell(k, B, fi, fj);
+        const int I = p.x * B + fi - 2, J = p.y * B + fj - 2;
+        C4 q{0.0f, 0.0f, 0.0f, 0.0f};
+        const bool inside = I >= 0 && I < F.nx && J >= 0 && J < F.ny;
+        bool ok = lookup(F, I, J, stage == 2, q);
+        if (!ok && inside && C.insts) q = coarse_interp(C, I, J);
+        const long long f = (long long)fj * W + fi;
+        fr[f] = q.b; fr[fp + f] = q.e; fr[2 * fp + f] = q.u; fr[3 * fp + f] = q.v;
+    }
+}
+
+// Fine -> coarse: each 2 x 2 group of fine cells of a fine box replaces the
+// coarse cell under it (eta, hu, hv as the FP64 mean of value + remainder; the
+// coarse bed is kept).
+__global__ void k32a_average_down(LevelView F, LevelView C, const int2* __restrict__ pos, int n_boxes) {
+    const int box = blockIdx.y;
+    if (box >= n_boxes) return;
+    const int B = F.B, h = B / 2;
+    const int2 p = pos[box];
+    const int kf = F.map[p.y * F.nbx + p.x];
+    if (kf < 0) return;
+    const BInst& D = F.insts[kf];
+    const float* X = (*(volatile const unsigned*)&D.st->parity) ? D.alt : D.Qs;
+    const long long pl = D.P.plane;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < h * h; k += gridDim.x * blockDim.x) {
+        const int a = k % h, c = k / h;
+        const int ic = p.x * h + a, jc = p.y * h + c;   // coarse cell
+        const int bxc = ic / C.B, byc = jc / C.B;
+        const int kc = C.map[byc * C.nbx + bxc];
+        if (kc < 0) continue;
+        double s[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const long long cf = (long long)(2 * c + (d >> 1)) * D.P.nx + (2 * a + (d & 1));
+#pragma unroll
+            for (int q = 0; q < 3; ++q) s[q] += double(X[q * pl + cf]) + double(D.lo[q * pl + cf]);
+        }
+        const BInst& E = C.insts[kc];
+        float* Y = (*(volatile const unsigned*)&E.st->parity) ? E.alt : E.Qs;
+        const long long plc = E.P.plane;
+        const long long cc = (long long)(jc - byc * C.B) * E.P.nx + (ic - bxc * C.B);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double m = 0.25 * s[q];
+            const float hi = float(m);
+            Y[q * plc + cc] = hi;
+            E.lo[q * plc + cc] = float(m - double(hi));
+        }
+    }
+}
+
+// flags[box] = 1 when some cell of the box has |grad eta| > threshold
+// (centred differences over the level's own cells; the reference's ErrorEst
+// flags |grad h| or h > 1e-2, ZoomyAmr.cpp:224-252).
+__global__ void k32a_tag(LevelView V, const int2* __restrict__ pos, int n_boxes, float dx, float dy,
+                         float threshold, int* __restrict__ flags) {
+    const int box = blockIdx.y;
+    if (box >= n_boxes) return;
+    const int B = V.B;
+    const int2 p = pos[box];
+    int hit = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B * B; k += gridDim.x * blockDim.x) {
+        const int I = p.x * B + k % B, J = p.y * B + k / B;
+        C4 xm, xp, ym, yp;
+        if (!lookup(V, I - 1, J, false, xm) || !lookup(V, I + 1, J, false, xp) ||
+            !lookup(V, I, J - 1, false, ym) || !lookup(V, I, J + 1, false, yp))
+            continue;
+        const float gx = (xp.e - xm.e) / (2.0f * dx), gy = (yp.e - ym.e) / (2.0f * dy);
+        if (gx * gx + gy * gy > threshold * threshold) hit = 1;
+    }
+    if (__syncthreads_or(hit) && threadIdx.x == 0) flags[box] = 1;
+}
+
+// New boxes of a level: copy the old boxes of the same level where present
+// (value + remainder), else interpolate the coarser level (remainder 0).
+// New boxes start with parity 0 (their run record is fresh).
+__global__ void k32a_regrid_fill(LevelView N, LevelView O, LevelView C, const int2* __restrict__ pos, int n_boxes) {
+    const int box = blockIdx.y;
+    if (box >= n_boxes) return;
+    const int B = N.B;
+    const int2 p = pos[box];
+    const int kn = N.map[p.y * N.nbx + p.x];
+    if (kn < 0) return;
+    const BInst& D = N.insts[kn];
+    const long long pl = D.P.plane;
+    float* bed = const_cast<float*>(D.bed);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B * B; k += gridDim.x * blockDim.x) {
+        const int i = k % B, j = k / B;
+        const int I = p.x * B + i, J = p.y * B + j;
+        const long long c = (long long)j * D.P.nx + i;
+        bool done = false;
+        if (O.insts) {
+            const int bx = I / O.B, by = J / O.B;
+            const int ko = (bx < O.nbx && by < O.nby) ? O.map[by * O.nbx + bx] : -1;
+            if (ko >= 0) {
+                const BInst& E = O.insts[ko];
+                const float* X = (*(volatile const unsigned*)&E.st->parity) ? E.alt : E.Qs;
+                const long long plo = E.P.plane;
+                const long long co = (long long)(J - by * O.B) * E.P.nx + (I - bx * O.B);
+                bed[c] = E.bed[co];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    D.Qs[q * pl + c] = X[q * plo + co];
+                    D.lo[q * pl + c] = E.lo[q * plo + co];
+                }
+                done = true;
+            }
+        }
+        if (!done) {
+            const C4 q = coarse_interp(C, I, J);
+            bed[c] = q.b;
+            D.Qs[c] = q.e; D.Qs[pl + c] = q.u; D.Qs[2 * pl + c] = q.v;
+            D.lo[c] = 0.0f; D.lo[pl + c] = 0.0f; D.lo[2 * pl + c] = 0.0f;
+        }
+    }
+}
+
+}  // namespace amr
+}  // namespace zfv32

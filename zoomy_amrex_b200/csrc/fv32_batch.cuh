@@ -37,6 +37,8 @@ struct BInst {
     double* log3;
     int log_cap;
     int nbx, nby;          // units in x / y for the current strip shape
+    int unit_base;         // index of this instance's first unit within its run-record group
+    int group_units;       // units of the whole group (the CFL / mass reduction runs over them)
     int pad_;
 };
 
@@ -108,8 +110,8 @@ k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
     }
     if constexpr (MODE == S2) {
         const bool last = zfv::finish_step_units<NT>(m_loc, s_loc, red, sD.partials, sD.log3, sD.log_cap,
-                                                      st, L, dtd, time, false, unsigned(sD.nbx * sD.nby),
-                                                      unsigned(u.y));
+                                                      st, L, dtd, time, false, unsigned(sD.group_units),
+                                                      unsigned(sD.unit_base + u.y));
         if (last && threadIdx.x == 0) {   // every unit of the step has read parity by now
             st->parity = parity ^ 1u;
             __threadfence();
@@ -138,7 +140,7 @@ __global__ void k32b_import(const BInst* __restrict__ insts, const int2* __restr
     __shared__ BInst sD;
     const int2 u = units[blockIdx.x];
     stage_desc(insts, u.x, sD);
-    if (u.y == 0 && threadIdx.x == 0) sD.st->parity = 0u;
+    if (sD.unit_base + u.y == 0 && threadIdx.x == 0) sD.st->parity = 0u;
     const long long pl = sD.P.plane;
     const double* Q64 = sD.q64;
     float* Qb = const_cast<float*>(sD.bed);
@@ -220,11 +222,12 @@ k32b_reduce(const BInst* __restrict__ insts, const int2* __restrict__ units, int
         }
     });
     zfv::block_reduce_max_sum<NT>(m, s, red);
-    const unsigned nblk = unsigned(sD.nbx * sD.nby);
+    const unsigned nblk = unsigned(sD.group_units);
+    const unsigned blk = unsigned(sD.unit_base + u.y);
     zfv::DevState* st = sD.st;
     if (threadIdx.x == 0) {
-        sD.partials[2 * u.y] = m;
-        sD.partials[2 * u.y + 1] = s;
+        sD.partials[2 * blk] = m;
+        sD.partials[2 * blk + 1] = s;
         __threadfence();
         s_last = (atomicAdd(&st->counter, 1u) == nblk - 1) ? 1u : 0u;
     }
@@ -250,6 +253,12 @@ k32b_reduce(const BInst* __restrict__ insts, const int2* __restrict__ units, int
         st->counter = 0u;
         __threadfence();
     }
+}
+
+// Host-chosen step size per instance (AMR levels step with dt_0 / 2^l).
+__global__ void k32b_set_dt(const BInst* __restrict__ insts, int n, const double* __restrict__ dt) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) insts[k].st->dt = dt[k];
 }
 
 // Gather every instance's 64-byte status record into one array.

@@ -122,6 +122,15 @@ __device__ __forceinline__ C4 fetch(const float* __restrict__ bed, const float* 
     int ii = i, jj = j, side = -1;
     if constexpr (!INTERIOR) {
         const int nx = L.nx, ny = L.ny;
+        if (L.frame && (i < 0 || i > nx - 1 || j < 0 || j > ny - 1)) {
+            // AMR box: the ghost frame holds the stage input (corner cells,
+            // which no face reads, are clamped into the frame)
+            const int fi = min(max(i, -2), nx + 1) + 2, fj = min(max(j, -2), ny + 1) + 2;
+            const long long fp = (long long)(nx + 4) * (ny + 4);
+            const long long f = (long long)fj * (nx + 4) + fi;
+            return C4{__ldg(L.frame + f), __ldg(L.frame + fp + f), __ldg(L.frame + 2 * fp + f),
+                      __ldg(L.frame + 3 * fp + f)};
+        }
         if (i < 0) { ii = -1 - i; side = 0; }
         else if (i > nx - 1) { ii = 2 * (nx - 1) + 1 - i; side = 1; }
         if (j < 0) { jj = -1 - j; if (side < 0) side = 2; }

@@ -43,6 +43,11 @@ struct Params {
     int bc_tag[4];
     double cfl, dtmin, dtmax, time_end;
     int max_step, cfl_dimension, cfl_degree_factor;
+    // Ghost frame (AMR boxes): when set, the cells just outside the box are
+    // read from this (nx+4) x (ny+4) x 4 array ([b, eta, hu, hv] planes, ring
+    // filled by the caller before each stage, stage input already summed)
+    // instead of mirrored from the box's own cells.
+    const float* frame;
 };
 
 struct C4 { float b, e, u, v; };   // bed, surface eta = h + b, hu, hv
@@ -106,6 +111,7 @@ enum Mode { S1 = 1, S2 = 2 };
 }  // namespace zfv32
 
 #include "fv32_batch.cuh"
+#include "fv32_amr.cuh"
 
 namespace zfv32 {
 
@@ -151,6 +157,7 @@ Params make_params(const zfv_config& c) {
     for (int s = 0; s < 4; ++s) L.bc_tag[s] = c.bc_tag[s];
     L.cfl = c.cfl; L.dtmin = c.dtmin; L.dtmax = c.dtmax; L.time_end = c.time_end;
     L.max_step = c.max_step; L.cfl_dimension = c.cfl_dimension; L.cfl_degree_factor = c.cfl_degree_factor;
+    L.frame = nullptr;
     return L;
 }
 
@@ -169,6 +176,8 @@ int max_units_of(const zfv_config& c) {
 struct BatchCore {
     static constexpr int n_aux = zb::SWE<double, 2>::n_dof_qaux;
     std::vector<zfv_config> cfg;
+    std::vector<int> group;      // run-record group of each instance (own record if none)
+    std::vector<const float*> frames;
     int n = 0;
     bool wb = false, impl = false;
     int variant = 0;
@@ -183,10 +192,16 @@ struct BatchCore {
     char* scratch = nullptr;
     bool bound = false;
 
-    int init(const zfv_config* cfgs, int count) {
+    int init(const zfv_config* cfgs, int count, const int* groups = nullptr) {
         if (count < 1) return fail(-1, "zfv_batch_create: empty batch");
         n = count;
         cfg.assign(cfgs, cfgs + count);
+        group.resize(n);
+        for (int k = 0; k < n; ++k) {
+            group[k] = groups ? groups[k] : k;
+            if (group[k] < 0 || group[k] >= n) return fail(-1, "zfv_batch: group id %d out of range", group[k]);
+        }
+        frames.assign(n, nullptr);
         wb = cfg[0].well_balanced != 0;
         impl = cfg[0].implicit_source != 0;
         for (auto& c : cfg) {
@@ -208,11 +223,23 @@ struct BatchCore {
         off_status = o; o += align_up(sizeof(zfv::DevState) * n);
         off_state.resize(n); off_part.resize(n); off_log.resize(n);
         off_alt.resize(n); off_inc.resize(n); off_lo.resize(n);
+        // one run record, partials array and log per group (its first member's)
+        std::vector<int> first(n, -1);
+        std::vector<long long> group_units(n, 0);
+        for (int k = 0; k < n; ++k) group_units[group[k]] += max_units_of(cfg[k]);
         for (int k = 0; k < n; ++k) {
             const size_t pb = size_t(cfg[k].nx) * cfg[k].ny * sizeof(float);
-            off_state[k] = o; o += align_up(sizeof(zfv::DevState));
-            off_part[k] = o; o += align_up(sizeof(double) * 2 * max_units_of(cfg[k]));
-            off_log[k] = o; o += align_up(sizeof(double) * 3 * kLogCap);
+            const int g = group[k];
+            if (first[g] < 0) {
+                first[g] = k;
+                off_state[k] = o; o += align_up(sizeof(zfv::DevState));
+                off_part[k] = o; o += align_up(sizeof(double) * 2 * size_t(group_units[g]));
+                off_log[k] = o; o += align_up(sizeof(double) * 3 * kLogCap);
+            } else {
+                off_state[k] = off_state[first[g]];
+                off_part[k] = off_part[first[g]];
+                off_log[k] = off_log[first[g]];
+            }
             off_inc[k] = o; o += align_up(pb * 3);
             off_alt[k] = o; o += align_up(pb * 3);
             off_lo[k] = o; o += align_up(pb * 3);
@@ -225,12 +252,16 @@ struct BatchCore {
     void build_units() {
         units.clear();
         const int rows = kVarNW[variant] * kVarCPT[variant], sw = 30 * kVarPK[variant];
+        std::vector<int> base(n, 0);
         for (int k = 0; k < n; ++k) {
             const int nbx = (cfg[k].nx + sw - 1) / sw, nby = (cfg[k].ny + rows - 1) / rows;
             desc[k].nbx = nbx;
             desc[k].nby = nby;
+            desc[k].unit_base = base[group[k]];     // this instance's first unit in its group
+            base[group[k]] += nbx * nby;
             for (int u = 0; u < nbx * nby; ++u) units.push_back(make_int2(k, u));
         }
+        for (int k = 0; k < n; ++k) desc[k].group_units = base[group[k]];
     }
 
     int upload(cudaStream_t s) {
@@ -262,6 +293,7 @@ struct BatchCore {
             D.partials = reinterpret_cast<double*>(scr + off_part[k]);
             D.log3 = reinterpret_cast<double*>(scr + off_log[k]);
             D.log_cap = kLogCap;
+            D.P.frame = frames[k];
         }
         bound = true;
         return upload(s);
@@ -270,6 +302,19 @@ struct BatchCore {
     const BInst* d_desc() const { return reinterpret_cast<const BInst*>(scratch + off_desc); }
     const int2* d_units() const { return reinterpret_cast<const int2*>(scratch + off_units); }
     int nunits() const { return int(units.size()); }
+
+    int set_frames(const float* const* f, cudaStream_t s) {
+        for (int k = 0; k < n; ++k) {
+            frames[k] = f ? f[k] : nullptr;
+            desc[k].P.frame = frames[k];
+        }
+        return bound ? upload(s) : 0;
+    }
+
+    int set_dt(const double* dts_dev, cudaStream_t s) {
+        k32b_set_dt<<<(n + 127) / 128, 128, 0, s>>>(d_desc(), n, dts_dev);
+        return cuda_check(cudaGetLastError(), "zfv_batch_set_dt launch");
+    }
 
     int set_variant(int v, cudaStream_t s) {
         if (v < 0 || v >= kNumVariants) return fail(-1, "zfv_batch_set_variant: unknown variant %d", v);
@@ -313,23 +358,31 @@ struct BatchCore {
     };
     int mass(cudaStream_t s) { return with_variant(variant, MassF{this, s}); }
 
+    // stages: 3 = both stages of `nsteps` steps; 1 or 2 = that stage alone,
+    // once (AMR boxes refill their ghost frames between the stages)
     template <bool W, bool I>
     struct StepF {
-        BatchCore* b; cudaStream_t s; int nsteps;
+        BatchCore* b; cudaStream_t s; int nsteps; int stages;
         template <int NW, int CPT, int PK, bool PF> int operator()() {
             const int nu = b->nunits();
-            for (int k = 0; k < nsteps; ++k) {
+            if (stages == 1) {
                 k32b_stage<S1, W, I, NW, CPT, PK, PF><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+            } else if (stages == 2) {
                 k32b_stage<S2, W, I, NW, CPT, PK, PF><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+            } else {
+                for (int k = 0; k < nsteps; ++k) {
+                    k32b_stage<S1, W, I, NW, CPT, PK, PF><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+                    k32b_stage<S2, W, I, NW, CPT, PK, PF><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+                }
             }
             return cuda_check(cudaGetLastError(), "zfv_batch evolve launch");
         }
     };
-    int evolve(int nsteps, cudaStream_t s) {
-        if (wb) return impl ? with_variant(variant, StepF<true, true>{this, s, nsteps})
-                            : with_variant(variant, StepF<true, false>{this, s, nsteps});
-        return impl ? with_variant(variant, StepF<false, true>{this, s, nsteps})
-                    : with_variant(variant, StepF<false, false>{this, s, nsteps});
+    int evolve(int nsteps, cudaStream_t s, int stages = 3) {
+        if (wb) return impl ? with_variant(variant, StepF<true, true>{this, s, nsteps, stages})
+                            : with_variant(variant, StepF<true, false>{this, s, nsteps, stages});
+        return impl ? with_variant(variant, StepF<false, true>{this, s, nsteps, stages})
+                    : with_variant(variant, StepF<false, false>{this, s, nsteps, stages});
     }
 
     int status(zfv_status* out, cudaStream_t s) {
@@ -447,7 +500,108 @@ int zfv_batch_create(const zfv_config* cfgs, int n_inst, zfv_batch** out) {
     return 0;
 }
 
+int zfv_batch_create_grouped(const zfv_config* cfgs, int n_inst, const int* groups, zfv_batch** out) {
+    if (!cfgs || !out || !groups) return fail(-1, "zfv_batch_create_grouped: null argument");
+    *out = nullptr;
+    zfv_batch* b = new (std::nothrow) zfv_batch();
+    if (!b) return fail(-4, "zfv_batch_create_grouped: out of host memory");
+    for (int k = 1; k < n_inst; ++k) {
+        const zfv_config &a = cfgs[k], &f = cfgs[0];
+        if (a.cfl != f.cfl || a.cfl_dimension != f.cfl_dimension || a.cfl_degree_factor != f.cfl_degree_factor) {
+            delete b;
+            return fail(-1, "zfv_batch_create_grouped: instances must share the CFL constants");
+        }
+    }
+    const int rc = b->core.init(cfgs, n_inst, groups);
+    if (rc) { delete b; return rc; }
+    *out = b;
+    return 0;
+}
+
+int zfv_batch_set_frames(zfv_batch* b, const float* const* frames, void* stream) {
+    if (!b) return fail(-1, "zfv_batch_set_frames: null batch");
+    return b->core.set_frames(frames, (cudaStream_t)stream);
+}
+
+int zfv_batch_set_dt(zfv_batch* b, const double* dts, void* stream) {
+    if (!b || !dts || !b->core.bound) return fail(-1, "zfv_batch_set_dt: bind the batch first");
+    return b->core.set_dt(dts, (cudaStream_t)stream);
+}
+
+int zfv_batch_stage(zfv_batch* b, int stage, void* stream) {
+    if (!b || !b->core.bound) return fail(-1, "zfv_batch_stage: bind the batch first");
+    if (stage != 1 && stage != 2) return fail(-1, "zfv_batch_stage: stage must be 1 or 2");
+    return b->core.evolve(1, (cudaStream_t)stream, stage);
+}
+
+const void* zfv_batch_descriptors(const zfv_batch* b) {
+    return (b && b->core.bound) ? static_cast<const void*>(b->core.d_desc()) : nullptr;
+}
+
 int zfv_batch_destroy(zfv_batch* b) { delete b; return 0; }
+
+// ---- AMR (include/zoomy_fv.h) ----------------------------------------------
+static_assert(sizeof(zfv_amr_level) == sizeof(zfv32::amr::LevelView), "zfv_amr_level layout");
+
+static zfv32::amr::LevelView view_of(const zfv_amr_level* l) {
+    zfv32::amr::LevelView v{};
+    if (l) std::memcpy(&v, l, sizeof v);
+    return v;
+}
+
+static int amr_grid(int n_boxes, int per_box, dim3& g) {
+    if (n_boxes < 1 || n_boxes > 65535) return fail(-1, "zfv_amr: %d boxes (1 .. 65535 per call)", n_boxes);
+    g = dim3(unsigned((per_box + 255) / 256), unsigned(n_boxes), 1);
+    return 0;
+}
+
+int zfv_amr_fill(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* pos, float* const* frames,
+                 int n_boxes, int stage, void* stream) {
+    if (!fine || !pos || !frames) return fail(-1, "zfv_amr_fill: null argument");
+    if (stage != 1 && stage != 2) return fail(-1, "zfv_amr_fill: stage must be 1 or 2");
+    const int B = fine->B;
+    dim3 g;
+    int rc = amr_grid(n_boxes, (B + 4) * (B + 4) - B * B, g);
+    if (rc) return rc;
+    zfv32::amr::k32a_fill<<<g, 256, 0, (cudaStream_t)stream>>>(view_of(fine), view_of(coarse),
+                                                             reinterpret_cast<const int2*>(pos), frames, n_boxes, stage);
+    return cuda_check(cudaGetLastError(), "zfv_amr_fill launch");
+}
+
+int zfv_amr_average_down(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* pos, int n_boxes,
+                         void* stream) {
+    if (!fine || !coarse || !pos) return fail(-1, "zfv_amr_average_down: null argument");
+    if (fine->B % 2) return fail(-1, "zfv_amr_average_down: the box side must be even");
+    dim3 g;
+    int rc = amr_grid(n_boxes, (fine->B / 2) * (fine->B / 2), g);
+    if (rc) return rc;
+    zfv32::amr::k32a_average_down<<<g, 256, 0, (cudaStream_t)stream>>>(view_of(fine), view_of(coarse),
+                                                                     reinterpret_cast<const int2*>(pos), n_boxes);
+    return cuda_check(cudaGetLastError(), "zfv_amr_average_down launch");
+}
+
+int zfv_amr_tag(const zfv_amr_level* level, const int* pos, int n_boxes, double dx, double dy, double threshold,
+                int* flags, void* stream) {
+    if (!level || !pos || !flags) return fail(-1, "zfv_amr_tag: null argument");
+    dim3 g;
+    int rc = amr_grid(n_boxes, level->B * level->B, g);
+    if (rc) return rc;
+    zfv32::amr::k32a_tag<<<g, 256, 0, (cudaStream_t)stream>>>(view_of(level), reinterpret_cast<const int2*>(pos),
+                                                            n_boxes, float(dx), float(dy), float(threshold), flags);
+    return cuda_check(cudaGetLastError(), "zfv_amr_tag launch");
+}
+
+int zfv_amr_regrid_fill(const zfv_amr_level* level, const zfv_amr_level* old_level, const zfv_amr_level* coarse,
+                        const int* pos, int n_boxes, void* stream) {
+    if (!level || !pos) return fail(-1, "zfv_amr_regrid_fill: null argument");
+    if (!old_level && !coarse) return fail(-1, "zfv_amr_regrid_fill: needs an old level or a coarser level");
+    dim3 g;
+    int rc = amr_grid(n_boxes, level->B * level->B, g);
+    if (rc) return rc;
+    zfv32::amr::k32a_regrid_fill<<<g, 256, 0, (cudaStream_t)stream>>>(
+        view_of(level), view_of(old_level), view_of(coarse), reinterpret_cast<const int2*>(pos), n_boxes);
+    return cuda_check(cudaGetLastError(), "zfv_amr_regrid_fill launch");
+}
 
 size_t zfv_batch_scratch_bytes(const zfv_batch* b) { return b ? b->core.total : 0; }
 

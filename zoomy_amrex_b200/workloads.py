@@ -115,6 +115,26 @@ def bump_workload_config(n: int, ny: int | None = None, y_extent: float | None =
                        bc=("wall",) * 4, params={"n_m": 0.03, "h_floor": 1e-6, "eps": 1e-24})
 
 
+def dam_break_level(n: int, seed: int = 2029, L: float = 100.0, n_bumps: int = 16):
+    """One n x n dam break over Gaussian bumps on [0, L]^2 (the AMR
+    benchmark's base level): eta = r ~ U(1.2, 3.0) left of x = 0.4 L and 1 m
+    to the right, bumps with amplitudes U(0.2, 1.5) m and widths U(2, 10) m
+    scaled to L = 100, walls, Manning n = 0.03. Returns (cfg, Q0)."""
+    rng = np.random.default_rng(seed)
+    ratio = rng.uniform(1.2, 3.0)
+    bumps = _bumps(rng, n_bumps, L, L, width=(0.02 * L, 0.1 * L))
+    xs = (np.arange(n) + 0.5) * (L / n)
+    b = _bed(xs, xs, bumps)
+    eta = np.where(xs < 0.4 * L, ratio, 1.0)[None, :]
+    Q0 = np.zeros((4, n, n))
+    Q0[0] = b
+    Q0[1] = np.maximum(eta - b, 0.0)
+    cfg = make_config(ZFV_MODEL_SWE2D, n, n, (0.0, 0.0), (L, L), spatial_order=2, well_balanced=True,
+                      implicit_source=True, cfl=0.45, dtmin=1e-7, dtmax=1.0, time_end=1.0e30, max_step=-1,
+                      bc=("wall",) * 4, params={"n_m": 0.03})
+    return cfg, Q0
+
+
 def fp64_twin(cfg):
     """The same configuration in the FP64 plain form."""
     import ctypes as C
