@@ -254,7 +254,9 @@ int zfv_batch_units(const zfv_batch* b);
 /*
  * Strip shapes compiled into the library: (warps per block, cells per thread
  * in y, columns per lane: 1 = scalar sweep, 2 = packed-FP32 column pairs,
- * prefetch: 1 = stage 2 loads its update inputs at the top of each row).
+ * prefetch: 1 = stage 2 stages its update inputs in shared memory with
+ * asynchronous copies at the top of each row, 2 = the same with the stage-2
+ * kernel capped at 128 registers).
  * zfv_tile_variants writes up to max_n of them and returns how many exist;
  * zfv_batch_set_variant selects one (the autotuner in
  * zoomy_amrex_b200/autotune.py measures them and caches the fastest per n_dof_q).
@@ -311,6 +313,13 @@ int zfv_amr_average_down(const zfv_amr_level* fine, const zfv_amr_level* coarse,
 /* flags[k] = 1 (others untouched) for boxes with a cell where |grad eta| > threshold. */
 int zfv_amr_tag(const zfv_amr_level* level, const int* pos, int n_boxes, double dx, double dy, double threshold,
                 int* flags, void* stream);
+/* dt_0 = the largest step whose dt_0 / 2^l every level's CFL law allows (from
+ * each level's last CFL maximum), clamped to [dtmin, dtmax]; writes dt_0 / 2^l
+ * into level l's per-instance dt array (device) and adds dt_0 to *time
+ * (device, may be NULL). level_descs: zfv_batch_descriptors() of each level.
+ * Enqueued; no synchronization (a coarse step can be captured in a graph). */
+int zfv_amr_set_dt(const void* const* level_descs, double* const* dts, const int* n_inst, int n_levels,
+                   double cfl, double cfl_divisor, double dtmin, double dtmax, double* time, void* stream);
 /* Fill freshly created boxes from the old boxes of the level (where present)
  * or from the coarser level. */
 int zfv_amr_regrid_fill(const zfv_amr_level* level, const zfv_amr_level* old_level, const zfv_amr_level* coarse,

@@ -100,7 +100,7 @@ def test_batch_strip_variants_agree(cuda):
             assert abs(st[k]["mass"] - ref[1][k]["mass"]) <= 1e-9 * abs(ref[1][k]["mass"])
 
 
-@pytest.mark.parametrize("variant", [0, 3, 7])
+@pytest.mark.parametrize("variant", [0, 3, 7, 9])
 def test_batch_depth_error_vs_fp64(cuda, oracle, variant):
     """Batch members against the FP64 oracle (L1 depth, 60 steps), scalar and
     packed sweeps."""

@@ -22,8 +22,6 @@ CFL law allows, and regridding happens every ``regrid_int`` coarse steps.
 from __future__ import annotations
 
 import ctypes as C
-import math
-
 import numpy as np
 import torch
 
@@ -112,7 +110,10 @@ class AmrHierarchy:
         self.dy0 = (cfg.prob_hi[1] - cfg.prob_lo[1]) / cfg.ny
         self.wall = sum(1 << s for s in range(4) if cfg.bc_tag[s] == 1)
         self.div = float(cfg.cfl_dimension * cfg.cfl_degree_factor)
-        self.time, self.steps = 0.0, 0
+        self.steps = 0
+        self.use_graph = True
+        self._graph = None
+        self._time = torch.zeros(1, dtype=torch.float64, device=self.device)
         Q0 = np.asarray(Q0, dtype=np.float64)
         blocks = [(bx, by) for by in range(self.nby0) for bx in range(self.nbx0)]
         Q0s = [np.ascontiguousarray(Q0[:, by * B:(by + 1) * B, bx * B:(bx + 1) * B]) for bx, by in blocks]
@@ -232,16 +233,15 @@ class AmrHierarchy:
         return changed
 
     # -- time stepping -----------------------------------------------------------------
-    def _dt0(self) -> float:
-        """The largest dt_0 with dt_0 / 2^l inside every level's CFL bound
-        (dt = cfl / (d (2k+1) max |lambda|/dx), ZoomyAmr.cpp:448-515)."""
+    def _set_dt(self):
+        """dt_0 from every level's last CFL maximum, on the device (zfv_amr_set_dt)."""
+        n = len(self.levels)
+        descs = (C.c_void_p * n)(*[L.batch.descriptors for L in self.levels])
+        dts = (C.c_void_p * n)(*[L.dts.data_ptr() for L in self.levels])
+        cnt = (C.c_int * n)(*[L.n for L in self.levels])
         c = self.cfg
-        dt0 = c.dtmax
-        for L in self.levels:
-            m = max(s["max_inv"] for s in L.batch.status()[:1])
-            if m > 1e-14:
-                dt0 = min(dt0, (1 << L.lev) * (c.cfl / (self.div * m)))
-        return max(dt0, c.dtmin)
+        _lib.check(_lib.lib().zfv_amr_set_dt(descs, dts, cnt, n, c.cfl, self.div, c.dtmin, c.dtmax,
+                                             self._time.data_ptr(), self._s()), "zfv_amr_set_dt")
 
     def _advance(self, lev: int):
         L = self.levels[lev]
@@ -258,18 +258,34 @@ class AmrHierarchy:
                 self._time_step(lev + 1)
             self.average_down(lev + 1)
 
-    def step(self):
-        """One coarse step of the whole hierarchy (ZoomyAmr::TimeStep's recursion)."""
-        if self.steps > 0 and self.regrid_int > 0 and self.steps % self.regrid_int == 0 and self.max_level > 0:
-            self.regrid()
-        dt0 = self._dt0()
-        with torch.cuda.stream(self.stream):
-            for L in self.levels:
-                L.dts.fill_(dt0 / (1 << L.lev))
+    def _coarse_step(self):
+        self._set_dt()
         self._time_step(0)
-        self.time += dt0
+
+    def step(self):
+        """One coarse step of the whole hierarchy (ZoomyAmr::TimeStep's
+        recursion), replayed from a CUDA graph captured after each regrid."""
+        if self.steps > 0 and self.regrid_int > 0 and self.steps % self.regrid_int == 0 and self.max_level > 0:
+            if self.regrid():
+                self._graph = None
+        if self.use_graph:
+            if self._graph is None:
+                self.sync()
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.stream(self.stream):
+                    with torch.cuda.graph(g, stream=self.stream):
+                        self._coarse_step()
+                self._graph = g
+            with torch.cuda.stream(self.stream):
+                self._graph.replay()
+        else:
+            self._coarse_step()
         self.steps += 1
-        return dt0
+
+    @property
+    def time(self) -> float:
+        self.sync()
+        return float(self._time.item())
 
     def run(self, n_steps: int):
         for _ in range(n_steps):
@@ -296,6 +312,7 @@ class AmrHierarchy:
         return float(q[1].sum() * self.dx0 * self.dy0)
 
     def close(self):
+        self._graph = None
         for L in self.levels:
             L.close()
         self.levels = []

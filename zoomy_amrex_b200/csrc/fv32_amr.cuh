@@ -231,5 +231,39 @@ __global__ void k32a_regrid_fill(LevelView N, LevelView O, LevelView C, const in
     }
 }
 
+// dt_0 of the hierarchy from every level's last CFL maximum (the largest
+// step whose dt_0 / 2^l every level's CFL law allows, ZoomyAmr.cpp:448-515),
+// written as dt_0 / 2^l into each level's per-instance dt array, and the
+// hierarchy time advanced by dt_0. One block; no host round trip, so a coarse
+// step can be replayed from a CUDA graph.
+constexpr int kMaxLevels = 8;
+struct DtArgs {
+    const BInst* lev[kMaxLevels];
+    double* dts[kMaxLevels];
+    int n_inst[kMaxLevels];
+    int n_levels;
+    double cfl, div, dtmin, dtmax;
+    double* time;
+};
+
+__global__ void k32a_set_dt(DtArgs a) {
+    __shared__ double s_dt0;
+    if (threadIdx.x == 0) {
+        double dt0 = a.dtmax;
+        for (int l = 0; l < a.n_levels; ++l) {
+            const double m = *(volatile const double*)&a.lev[l][0].st->max_inv;
+            if (m > 1e-14) dt0 = fmin(dt0, double(1 << l) * (a.cfl / (a.div * m)));
+        }
+        dt0 = fmax(dt0, a.dtmin);
+        s_dt0 = dt0;
+        if (a.time) *a.time += dt0;
+    }
+    __syncthreads();
+    for (int l = 0; l < a.n_levels; ++l) {
+        const double dl = s_dt0 / double(1 << l);
+        for (int k = threadIdx.x; k < a.n_inst[l]; k += blockDim.x) a.dts[l][k] = dl;
+    }
+}
+
 }  // namespace amr
 }  // namespace zfv32

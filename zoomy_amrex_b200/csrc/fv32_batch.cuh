@@ -57,8 +57,8 @@ __device__ __forceinline__ const float* state_in(const BInst& D, unsigned parity
     return parity ? D.alt : D.Qs;
 }
 
-template <int MODE, bool WB, bool IMPL, int NW, int CPT, int PK, bool PF>
-__global__ void __launch_bounds__(32 * NW)
+template <int MODE, bool WB, bool IMPL, int NW, int CPT, int PK, int PF>
+__global__ void __launch_bounds__(32 * NW, (MODE == 2 && PF == 2) ? 4 : 1)
 k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
 {
     constexpr int SW = 30 * PK;                  // owned columns per strip
@@ -86,24 +86,24 @@ k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
     float* inc_out = (MODE == S1) ? sD.inc : nullptr;        // stage 1 writes it
     if constexpr (PK == 1) {
         if (strip_interior<NW, CPT>(L, x0, y0))
-            sweep_strip<MODE, WB, IMPL, CPT, true, PF>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
+            sweep_strip<MODE, WB, IMPL, CPT, true, (PF != 0)>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
                                                    float(dtd), dtd, m_loc, s_loc, wstage);
         else
-            sweep_strip<MODE, WB, IMPL, CPT, false, PF>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
+            sweep_strip<MODE, WB, IMPL, CPT, false, (PF != 0)>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
                                                     float(dtd), dtd, m_loc, s_loc, wstage);
     } else {
         // 8-byte accesses need an even row length (x0 is even)
         if (pk::strip_interior2<NW, CPT>(L, x0, y0)) {
             if ((L.nx & 1) == 0)
-                pk::sweep_strip2<MODE, WB, IMPL, CPT, true, true, PF>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
+                pk::sweep_strip2<MODE, WB, IMPL, CPT, true, true, (PF != 0)>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
                                                                   j0, float(dtd), dtd, m_loc, s_loc,
                                                                 reinterpret_cast<float2*>(wstage));
             else
-                pk::sweep_strip2<MODE, WB, IMPL, CPT, true, false, PF>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
+                pk::sweep_strip2<MODE, WB, IMPL, CPT, true, false, (PF != 0)>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
                                                                    j0, float(dtd), dtd, m_loc, s_loc,
                                                                 reinterpret_cast<float2*>(wstage));
         } else {
-            pk::sweep_strip2<MODE, WB, IMPL, CPT, false, false, PF>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
+            pk::sweep_strip2<MODE, WB, IMPL, CPT, false, false, (PF != 0)>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
                                                                 j0, float(dtd), dtd, m_loc, s_loc,
                                                                 reinterpret_cast<float2*>(wstage));
         }

@@ -116,27 +116,31 @@ enum Mode { S1 = 1, S2 = 2 };
 namespace zfv32 {
 
 // Compiled strip shapes: (warps per block NW, rows per warp CPT = cells per
-// thread, columns per lane PK, stage-2 prefetch PF). A strip is 30 * PK
+// thread, columns per lane PK, stage-2 staging PF). A strip is 30 * PK
 // columns x (NW * CPT) rows; PK = 2 is the packed-FP32 paired-column sweep;
-// PF loads the stage-2 update's own inputs at the top of each row (earlier
-// loads, more registers).
-constexpr int kNumVariants = 8;
-constexpr int kVarNW[kNumVariants] = {4, 4, 4, 4, 4, 4, 4, 4};
-constexpr int kVarCPT[kNumVariants] = {16, 8, 16, 8, 16, 8, 16, 8};
-constexpr int kVarPK[kNumVariants] = {1, 1, 2, 2, 1, 1, 2, 2};
-constexpr int kVarPF[kNumVariants] = {0, 0, 0, 0, 1, 1, 1, 1};
+// PF >= 1 stages the stage-2 update's own inputs in shared memory with
+// asynchronous copies issued at the top of each row; PF = 2 also caps the
+// stage-2 kernel at 128 registers (4 blocks of 128 threads per SM instead of
+// 3, at the cost of some spilling).
+constexpr int kNumVariants = 10;
+constexpr int kVarNW[kNumVariants] = {4, 4, 4, 4, 4, 4, 4, 4, 4, 4};
+constexpr int kVarCPT[kNumVariants] = {16, 8, 16, 8, 16, 8, 16, 8, 16, 8};
+constexpr int kVarPK[kNumVariants] = {1, 1, 2, 2, 1, 1, 2, 2, 2, 2};
+constexpr int kVarPF[kNumVariants] = {0, 0, 0, 0, 1, 1, 1, 1, 2, 2};
 
 template <class F>
 int with_variant(int v, F&& f) {
     switch (v) {
-    case 0: return f.template operator()<4, 16, 1, false>();
-    case 1: return f.template operator()<4, 8, 1, false>();
-    case 2: return f.template operator()<4, 16, 2, false>();
-    case 3: return f.template operator()<4, 8, 2, false>();
-    case 4: return f.template operator()<4, 16, 1, true>();
-    case 5: return f.template operator()<4, 8, 1, true>();
-    case 6: return f.template operator()<4, 16, 2, true>();
-    case 7: return f.template operator()<4, 8, 2, true>();
+    case 0: return f.template operator()<4, 16, 1, 0>();
+    case 1: return f.template operator()<4, 8, 1, 0>();
+    case 2: return f.template operator()<4, 16, 2, 0>();
+    case 3: return f.template operator()<4, 8, 2, 0>();
+    case 4: return f.template operator()<4, 16, 1, 1>();
+    case 5: return f.template operator()<4, 8, 1, 1>();
+    case 6: return f.template operator()<4, 16, 2, 1>();
+    case 7: return f.template operator()<4, 8, 2, 1>();
+    case 8: return f.template operator()<4, 16, 2, 2>();
+    case 9: return f.template operator()<4, 8, 2, 2>();
     default: return fail(-1, "unknown strip variant %d", v);
     }
 }
@@ -324,7 +328,7 @@ struct BatchCore {
 
     struct ImportF {
         BatchCore* b; cudaStream_t s; bool exp;
-        template <int NW, int CPT, int PK, bool PF> int operator()() {
+        template <int NW, int CPT, int PK, int PF> int operator()() {
             if (exp) k32b_export<NW, CPT, PK><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
             else k32b_import<NW, CPT, PK><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units());
             return cuda_check(cudaGetLastError(), "zfv_batch import/export launch");
@@ -341,7 +345,7 @@ struct BatchCore {
 
     struct BeginF {
         BatchCore* b; cudaStream_t s;
-        template <int NW, int CPT, int PK, bool PF> int operator()() {
+        template <int NW, int CPT, int PK, int PF> int operator()() {
             k32b_init<<<(b->n + 127) / 128, 128, 0, s>>>(b->d_desc(), b->n);
             k32b_reduce<NW, CPT, PK, 0><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
             return cuda_check(cudaGetLastError(), "zfv_batch begin launch");
@@ -351,7 +355,7 @@ struct BatchCore {
 
     struct MassF {
         BatchCore* b; cudaStream_t s;
-        template <int NW, int CPT, int PK, bool PF> int operator()() {
+        template <int NW, int CPT, int PK, int PF> int operator()() {
             k32b_reduce<NW, CPT, PK, 1><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
             return cuda_check(cudaGetLastError(), "zfv_batch mass launch");
         }
@@ -363,7 +367,7 @@ struct BatchCore {
     template <bool W, bool I>
     struct StepF {
         BatchCore* b; cudaStream_t s; int nsteps; int stages;
-        template <int NW, int CPT, int PK, bool PF> int operator()() {
+        template <int NW, int CPT, int PK, int PF> int operator()() {
             const int nu = b->nunits();
             if (stages == 1) {
                 k32b_stage<S1, W, I, NW, CPT, PK, PF><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
@@ -589,6 +593,24 @@ int zfv_amr_tag(const zfv_amr_level* level, const int* pos, int n_boxes, double 
     zfv32::amr::k32a_tag<<<g, 256, 0, (cudaStream_t)stream>>>(view_of(level), reinterpret_cast<const int2*>(pos),
                                                             n_boxes, float(dx), float(dy), float(threshold), flags);
     return cuda_check(cudaGetLastError(), "zfv_amr_tag launch");
+}
+
+int zfv_amr_set_dt(const void* const* level_descs, double* const* dts, const int* n_inst, int n_levels,
+                   double cfl, double cfl_divisor, double dtmin, double dtmax, double* time, void* stream) {
+    if (!level_descs || !dts || !n_inst) return fail(-1, "zfv_amr_set_dt: null argument");
+    if (n_levels < 1 || n_levels > zfv32::amr::kMaxLevels)
+        return fail(-1, "zfv_amr_set_dt: %d levels (1 .. %d)", n_levels, zfv32::amr::kMaxLevels);
+    zfv32::amr::DtArgs a{};
+    for (int l = 0; l < n_levels; ++l) {
+        a.lev[l] = static_cast<const zfv32::BInst*>(level_descs[l]);
+        a.dts[l] = dts[l];
+        a.n_inst[l] = n_inst[l];
+    }
+    a.n_levels = n_levels;
+    a.cfl = cfl; a.div = cfl_divisor; a.dtmin = dtmin; a.dtmax = dtmax;
+    a.time = time;
+    zfv32::amr::k32a_set_dt<<<1, 256, 0, (cudaStream_t)stream>>>(a);
+    return cuda_check(cudaGetLastError(), "zfv_amr_set_dt launch");
 }
 
 int zfv_amr_regrid_fill(const zfv_amr_level* level, const zfv_amr_level* old_level, const zfv_amr_level* coarse,
