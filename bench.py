@@ -332,7 +332,7 @@ def ensemble_bench(K, W, local, n_inst=256, seed=2027):
             "strip_shape_ms_per_step": {str(v): t for v, t in times.items()}, "picked_variant": best}
 
 
-def amr_bench(local, n=1024, steps=10, warm=2, max_level=2, B=64):
+def amr_bench(local, n=1024, steps=10, warm=2, max_level=2, B=64, variant=1):
     """A 3-level AMR hierarchy (ratio 2, base n^2, boxes of B^2, tagged where
     |grad eta| > 0.01, regrid every 2 coarse steps, subcycling) of a dam
     break over bumps: coarse steps per second and cell updates per second
@@ -342,7 +342,7 @@ def amr_bench(local, n=1024, steps=10, warm=2, max_level=2, B=64):
     from zoomy_amrex_b200.workloads import dam_break_level
     cfg, Q0 = dam_break_level(n)
     hier = AmrHierarchy(cfg, Q0, max_level=max_level, B=B, threshold=0.01, regrid_int=2,
-                        device=f"cuda:{local}")
+                        device=f"cuda:{local}", variant=variant)
     hier.run(warm)
     torch.cuda.synchronize()
     cells = 0

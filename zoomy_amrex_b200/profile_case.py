@@ -3,11 +3,14 @@
     python -m zoomy_amrex_b200.profile_case fp32    [--n 3072] [--variant V] [--steps 3]
     python -m zoomy_amrex_b200.profile_case fp64    [--n 3072] [--steps 3]
     python -m zoomy_amrex_b200.profile_case adjoint [--n 512]  [--steps 20] [--variant V]
+    python -m zoomy_amrex_b200.profile_case amr     [--n 1024] [--steps 4]  [--variant V]
 
 Each runs the benchmark's wet/dry bump level (``workloads.bump_workload_*``)
 on an n x n grid: the FP32 form as a batch of one with the given strip shape,
 the FP64 form through a Level, or the forward + backward of the FP64 adjoint
-with checkpoints every 20 steps. The launches are the product's own; a
+with checkpoints every 20 steps, or (amr) the 3-level AMR hierarchy of a dam
+break over bumps on an n x n base grid (boxes 64^2, one CUDA graph per coarse
+step). The launches are the product's own; a
 profiler selects them by kernel name (k32b_stage, k_stage, k_adj_face, ...).
 """
 from __future__ import annotations
@@ -17,7 +20,7 @@ import argparse
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("form", choices=["fp32", "fp64", "adjoint"])
+    ap.add_argument("form", choices=["fp32", "fp64", "adjoint", "amr"])
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--variant", type=int, default=None)
@@ -48,6 +51,16 @@ def main(argv=None):
         lev.evolve(steps)
         st = lev.status()
         lev.close()
+    elif a.form == "amr":
+        from .amr import AmrHierarchy
+        from .workloads import dam_break_level
+        n, steps = a.n or 1024, a.steps or 4
+        cfg, Q0 = dam_break_level(n)
+        hier = AmrHierarchy(cfg, Q0, max_level=2, B=64, threshold=0.01, regrid_int=2,
+                            variant=a.variant if a.variant is not None else 1)
+        hier.run(steps)
+        st = {"step": hier.steps, "boxes": [lv.n for lv in hier.levels], "time": hier.time}
+        hier.close()
     else:
         from . import _lib
         from .adjoint import evolve_differentiable
