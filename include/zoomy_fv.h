@@ -254,14 +254,14 @@ int zfv_batch_units(const zfv_batch* b);
 /*
  * Strip shapes compiled into the library: (warps per block, cells per thread
  * in y, columns per lane: 1 = scalar sweep, 2 = packed-FP32 column pairs,
- * prefetch: 1 = stage 2 stages its update inputs in shared memory with
- * asynchronous copies at the top of each row, 2 = the same with the stage-2
- * kernel capped at 128 registers).
+ * flags: bit 0 = stage 2 stages its update inputs in shared memory with
+ * asynchronous copies at the top of each row, bit 1 = the stage-2 kernel is
+ * capped at 128 registers).
  * zfv_tile_variants writes up to max_n of them and returns how many exist;
  * zfv_batch_set_variant selects one (the autotuner in
  * zoomy_amrex_b200/autotune.py measures them and caches the fastest per n_dof_q).
  */
-int zfv_tile_variants(int* nw, int* cpt, int* cols, int* prefetch, int max_n);
+int zfv_tile_variants(int* nw, int* cpt, int* cols, int* flags, int max_n);
 
 /*
  * Batches whose instances are grouped: instances with the same group id
@@ -295,24 +295,33 @@ const void* zfv_batch_descriptors(const zfv_batch* b);
  */
 typedef struct zfv_amr_level {
     const void* insts;   /* zfv_batch_descriptors() of the level's batch */
-    const int* map;      /* device, nby * nbx */
+    const int* map;      /* device, nby * nbx: (instance << 8) | block offset in the patch, -1 absent */
     int nbx, nby;        /* block grid */
-    int B;               /* cells per box side (even) */
+    int B;               /* cells per block side (even) */
     int nx, ny;          /* the level's grid in cells */
     int wall;            /* bit s set: side s (x_lo, x_hi, y_lo, y_hi) is a reflective wall */
     int pad;
 } zfv_amr_level;
-/* Ghost frames before stage `stage` (1: the stage input; 2: neighbours'
- * stage-2 input): same-level boxes, else conservative linear interpolation of
- * `coarse` (NULL on level 0), physical boundaries by mirroring. */
-int zfv_amr_fill(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* pos, float* const* frames,
-                 int n_boxes, int stage, void* stream);
-/* Replace the coarse cells under the listed fine boxes by 2 x 2 averages. */
-int zfv_amr_average_down(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* pos, int n_boxes,
-                         void* stream);
-/* flags[k] = 1 (others untouched) for boxes with a cell where |grad eta| > threshold. */
-int zfv_amr_tag(const zfv_amr_level* level, const int* pos, int n_boxes, double dx, double dy, double threshold,
-                int* flags, void* stream);
+/*
+ * Patches: a level's blocks grouped into horizontal runs of consecutive
+ * blocks of one block row, one batch instance of (nb * B) x B cells each.
+ * `patches` (device) holds 4 ints per patch: first block x, block row y,
+ * nb (1 .. 256), unused; max_blocks bounds nb over the list (it sizes the
+ * launch). Instance k of the level's batch is patch k.
+ */
+/* Ghost frames ((nb*B + 4) x (B + 4) x 4 floats per patch) before stage
+ * `stage` (1: the stage input; 2: neighbours' stage-2 input): same-level
+ * patches, else conservative linear interpolation of `coarse` (NULL on level
+ * 0), physical boundaries by mirroring. */
+int zfv_amr_fill(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* patches, float* const* frames,
+                 int n_patches, int max_blocks, int stage, void* stream);
+/* Replace the coarse cells under the listed fine patches by 2 x 2 averages. */
+int zfv_amr_average_down(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* patches, int n_patches,
+                         int max_blocks, void* stream);
+/* flags[by * nbx + bx] = 1 (others untouched) for the blocks of the listed
+ * patches with a cell where |grad eta| > threshold. */
+int zfv_amr_tag(const zfv_amr_level* level, const int* patches, int n_patches, int max_blocks, double dx, double dy,
+                double threshold, int* flags, void* stream);
 /* dt_0 = the largest step whose dt_0 / 2^l every level's CFL law allows (from
  * each level's last CFL maximum), clamped to [dtmin, dtmax]; writes dt_0 / 2^l
  * into level l's per-instance dt array (device) and adds dt_0 to *time
@@ -320,10 +329,10 @@ int zfv_amr_tag(const zfv_amr_level* level, const int* pos, int n_boxes, double 
  * Enqueued; no synchronization (a coarse step can be captured in a graph). */
 int zfv_amr_set_dt(const void* const* level_descs, double* const* dts, const int* n_inst, int n_levels,
                    double cfl, double cfl_divisor, double dtmin, double dtmax, double* time, void* stream);
-/* Fill freshly created boxes from the old boxes of the level (where present)
- * or from the coarser level. */
+/* Fill freshly created patches from the old patches of the level (where
+ * present) or from the coarser level. */
 int zfv_amr_regrid_fill(const zfv_amr_level* level, const zfv_amr_level* old_level, const zfv_amr_level* coarse,
-                        const int* pos, int n_boxes, void* stream);
+                        const int* patches, int n_patches, int max_blocks, void* stream);
 int zfv_batch_set_variant(zfv_batch* b, int variant, void* stream);
 
 /*

@@ -134,3 +134,31 @@ def test_adjoint_directional_derivatives_vs_fd(cuda):
     fd = float(lp - lm) / 2e-7
     print(f"[adjoint vs FD] n_m: fd {fd:.10e} adjoint {float(nm.grad):.10e}")
     assert abs(fd - float(nm.grad)) <= 1e-5 * (abs(fd) + abs(float(nm.grad)))
+
+
+def test_adjoint_tile_shapes_agree(cuda):
+    """Every compiled face-reverse tile shape gives the same gradients (the
+    per-cell gather order is fixed, so only FMA contraction differs)."""
+    import torch
+    from zoomy_amrex_b200 import _lib
+    from zoomy_amrex_b200.adjoint import evolve_differentiable
+    L = _lib.lib()
+    nx, ny, steps = 83, 45, 7
+    cfg, Q0, A0 = case(nx, ny, 5, dry=True)
+    eta_obs = torch.from_numpy(Q0[0] + Q0[1]).cuda() + 0.01
+    grads = []
+    try:
+        for v in range(int(L.zfv_adj_variants())):
+            _lib.check(L.zfv_adj_set_variant(v), "zfv_adj_set_variant")
+            q = torch.from_numpy(Q0).cuda().requires_grad_(True)
+            nm = torch.tensor(0.03, dtype=torch.float64, device="cuda", requires_grad=True)
+            QT = evolve_differentiable(q, nm, torch.from_numpy(A0).cuda(), cfg, steps, checkpoint_every=3)
+            _loss(QT, eta_obs).backward()
+            grads.append((q.grad.detach().clone(), float(nm.grad)))
+    finally:
+        _lib.check(L.zfv_adj_set_variant(2), "zfv_adj_set_variant")
+    g0, n0 = grads[0]
+    scale = float(g0.abs().max())
+    for v, (g, n) in enumerate(grads):
+        assert float((g - g0).abs().max()) <= 1e-12 * scale, v
+        assert abs(n - n0) <= 1e-12 * abs(n0), v

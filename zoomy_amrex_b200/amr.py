@@ -8,11 +8,13 @@ interpolation), subcycling (a level-l step is followed by two level-(l+1)
 steps), and averaging the fine solution down onto the coarse level after them.
 There is no flux register, as in the reference (ZoomyAmr.H:85).
 
-Here every level is a batch of equal B x B boxes on a regular block grid (the
-box layout of a quadtree rather than AMReX's Berger-Rigoutsos clustering):
-one launch per RK stage advances all boxes of a level, the boxes of a level
-share one run record, and a box's ghost ring is a small frame array the stage
-kernels read in place of the physical mirror.
+Here every level is refined in B x B blocks on a regular block grid (the
+layout of a quadtree rather than AMReX's Berger-Rigoutsos clustering); the
+blocks of a level are grouped into patches, horizontal runs of up to
+``patch_blocks`` consecutive blocks, each one instance of a grouped batch:
+one launch per RK stage advances all patches of a level, the patches of a
+level share one run record, and a patch's ghost ring is a small frame array
+the stage kernels read in place of the physical mirror.
 
 Two choices differ from the reference, which steps each level with its own
 CFL dt (so fine levels need not land on the coarse time) and regrids at every
@@ -36,10 +38,23 @@ def _cfg_copy(c: zfv_config) -> zfv_config:
     return d
 
 
-class AmrLevel:
-    """All boxes of one level: a grouped batch plus its block map and frames."""
+def group_patches(blocks, max_blocks: int) -> list[tuple[int, int, int]]:
+    """Blocks (bx, by) -> patches (bx0, by, nb): runs of consecutive blocks of
+    one block row, at most ``max_blocks`` long."""
+    out = []
+    for bx, by in sorted(blocks, key=lambda p: (p[1], p[0])):
+        if out and out[-1][1] == by and out[-1][0] + out[-1][2] == bx and out[-1][2] < max_blocks:
+            out[-1] = (out[-1][0], by, out[-1][2] + 1)
+        else:
+            out.append((bx, by, 1))
+    return out
 
-    def __init__(self, hier, lev: int, blocks: list[tuple[int, int]], Q0s=None, variant=None):
+
+class AmrLevel:
+    """All blocks of one level: a grouped batch of patches (horizontal runs
+    of blocks), their block map and ghost frames."""
+
+    def __init__(self, hier, lev: int, blocks: list[tuple[int, int]], Q0=None, variant=None):
         self.h, self.lev = hier, lev
         B = hier.B
         self.B = B
@@ -47,39 +62,50 @@ class AmrLevel:
         self.nx, self.ny = self.nbx * B, self.nby * B
         self.dx = hier.dx0 / (1 << lev)
         self.dy = hier.dy0 / (1 << lev)
-        self.blocks = list(blocks)
+        self.blocks = sorted(blocks, key=lambda p: (p[1], p[0]))
+        self.patches = group_patches(self.blocks, hier.patch_blocks)
+        self.max_blocks = max(nb for _, _, nb in self.patches)
         dev = hier.device
-        cfgs = []
-        for (bx, by) in self.blocks:
+        cfgs, Q0s = [], None if Q0 is None else []
+        for (bx, by, nb) in self.patches:
             c = _cfg_copy(hier.cfg)
-            c.nx = c.ny = B
+            c.nx, c.ny = nb * B, B
             c.prob_lo[0] = hier.lo[0] + bx * B * self.dx
             c.prob_lo[1] = hier.lo[1] + by * B * self.dy
-            c.prob_hi[0] = c.prob_lo[0] + B * self.dx
+            c.prob_hi[0] = c.prob_lo[0] + nb * B * self.dx
             c.prob_hi[1] = c.prob_lo[1] + B * self.dy
             c.precision = ZFV_PREC_FP32
             c.time_end = 1.0e30
             c.max_step = -1
             cfgs.append(c)
+            if Q0 is not None:
+                Q0s.append(np.ascontiguousarray(Q0[:, by * B:(by + 1) * B, bx * B:(bx + nb) * B]))
         self.batch = Batch(cfgs, Q0s, None, device=dev, stream=hier.stream, groups=[0] * len(cfgs),
                            variant=hier.variant if variant is None else variant)
-        n = len(self.blocks)
-        self.frames = torch.zeros((n, 4, B + 4, B + 4), dtype=torch.float32, device=dev)
-        self.batch.set_frames([self.frames[k] for k in range(n)])
-        self.map = torch.full((self.nby, self.nbx), -1, dtype=torch.int32)
-        for k, (bx, by) in enumerate(self.blocks):
-            self.map[by, bx] = k
-        self.map = self.map.to(dev)
-        self.pos = torch.tensor(self.blocks, dtype=torch.int32, device=dev).reshape(n, 2).contiguous()
-        self.frame_ptrs = torch.tensor([self.frames[k].data_ptr() for k in range(n)], dtype=torch.int64,
-                                       device=dev)
+        n = len(self.patches)
+        self.frames = [torch.zeros((4, B + 4, nb * B + 4), dtype=torch.float32, device=dev)
+                       for (_, _, nb) in self.patches]
+        self.batch.set_frames(self.frames)
+        m = torch.full((self.nby, self.nbx), -1, dtype=torch.int32)
+        for k, (bx, by, nb) in enumerate(self.patches):
+            for o in range(nb):
+                m[by, bx + o] = (k << 8) | o
+        self.map = m.to(dev)
+        self.pdesc = torch.tensor([[bx, by, nb, 0] for (bx, by, nb) in self.patches], dtype=torch.int32,
+                                  device=dev).reshape(n, 4).contiguous()
+        self.frame_ptrs = torch.tensor([f.data_ptr() for f in self.frames], dtype=torch.int64, device=dev)
         self.dts = torch.zeros(n, dtype=torch.float64, device=dev)
         self.view = zfv_amr_level(C.c_void_p(self.batch.descriptors), C.c_void_p(self.map.data_ptr()),
                                   self.nbx, self.nby, B, self.nx, self.ny, hier.wall, 0)
 
     @property
     def n(self) -> int:
+        """Blocks of the level."""
         return len(self.blocks)
+
+    @property
+    def n_patches(self) -> int:
+        return len(self.patches)
 
     def close(self):
         self.batch.close()
@@ -96,7 +122,7 @@ class AmrHierarchy:
     """
 
     def __init__(self, cfg: zfv_config, Q0, max_level: int = 2, B: int = 64, threshold: float = 0.01,
-                 regrid_int: int = 2, device="cuda:0", variant: int = 1):
+                 regrid_int: int = 2, device="cuda:0", variant: int = 5, patch_blocks: int = 16):
         if cfg.nx % B or cfg.ny % B or B % 2:
             raise ValueError("the base grid must be a multiple of the (even) box side B in both directions")
         self.cfg = _cfg_copy(cfg)
@@ -104,6 +130,9 @@ class AmrHierarchy:
         self.device = torch.device(device)
         self.stream = torch.cuda.Stream(self.device)
         self.variant = variant
+        if not 1 <= patch_blocks <= 256:
+            raise ValueError("patch_blocks must be in 1 .. 256")
+        self.patch_blocks = patch_blocks
         self.nbx0, self.nby0 = cfg.nx // B, cfg.ny // B
         self.lo = (cfg.prob_lo[0], cfg.prob_lo[1])
         self.dx0 = (cfg.prob_hi[0] - cfg.prob_lo[0]) / cfg.nx
@@ -116,8 +145,7 @@ class AmrHierarchy:
         self._time = torch.zeros(1, dtype=torch.float64, device=self.device)
         Q0 = np.asarray(Q0, dtype=np.float64)
         blocks = [(bx, by) for by in range(self.nby0) for bx in range(self.nbx0)]
-        Q0s = [np.ascontiguousarray(Q0[:, by * B:(by + 1) * B, bx * B:(bx + 1) * B]) for bx, by in blocks]
-        self.levels: list[AmrLevel] = [AmrLevel(self, 0, blocks, Q0s)]
+        self.levels: list[AmrLevel] = [AmrLevel(self, 0, blocks, Q0)]
         self.levels[0].batch.begin()
         for _ in range(max_level):          # initial hierarchy (InitData's repeated regrid)
             if not self.regrid():
@@ -136,23 +164,26 @@ class AmrHierarchy:
 
     def fill(self, lev: int, stage: int):
         L = self.levels[lev]
-        _lib.check(_lib.lib().zfv_amr_fill(C.byref(L.view), self._coarse_view(lev), L.pos.data_ptr(),
-                                           L.frame_ptrs.data_ptr(), L.n, stage, self._s()), "zfv_amr_fill")
+        _lib.check(_lib.lib().zfv_amr_fill(C.byref(L.view), self._coarse_view(lev), L.pdesc.data_ptr(),
+                                           L.frame_ptrs.data_ptr(), L.n_patches, L.max_blocks, stage, self._s()),
+                   "zfv_amr_fill")
 
     def average_down(self, lev: int):
         F, Cl = self.levels[lev], self.levels[lev - 1]
-        _lib.check(_lib.lib().zfv_amr_average_down(C.byref(F.view), C.byref(Cl.view), F.pos.data_ptr(), F.n,
-                                                   self._s()), "zfv_amr_average_down")
+        _lib.check(_lib.lib().zfv_amr_average_down(C.byref(F.view), C.byref(Cl.view), F.pdesc.data_ptr(),
+                                                   F.n_patches, F.max_blocks, self._s()), "zfv_amr_average_down")
 
     # -- regridding ------------------------------------------------------------------
     def tags(self, lev: int) -> np.ndarray:
+        """Tagged blocks of level ``lev`` as a boolean (nby, nbx) array."""
         L = self.levels[lev]
-        flags = torch.zeros(L.n, dtype=torch.int32, device=self.device)
         with torch.cuda.stream(self.stream):
-            _lib.check(_lib.lib().zfv_amr_tag(C.byref(L.view), L.pos.data_ptr(), L.n, L.dx, L.dy, self.threshold,
-                                              flags.data_ptr(), self._s()), "zfv_amr_tag")
+            flags = torch.zeros((L.nby, L.nbx), dtype=torch.int32, device=self.device)
+            _lib.check(_lib.lib().zfv_amr_tag(C.byref(L.view), L.pdesc.data_ptr(), L.n_patches, L.max_blocks,
+                                              L.dx, L.dy, self.threshold, flags.data_ptr(), self._s()),
+                       "zfv_amr_tag")
         self.sync()
-        return flags.cpu().numpy()
+        return flags.cpu().numpy() != 0
 
     def _refined_blocks(self, lev: int) -> list[tuple[int, int]]:
         """Level-(lev+1) blocks: children of tagged level-lev blocks and their
@@ -163,14 +194,10 @@ class AmrHierarchy:
         have = np.zeros((L.nby, L.nbx), dtype=bool)
         for bx, by in L.blocks:
             have[by, bx] = True
-        tagged = np.zeros_like(have)
         if self.threshold < 0:            # refine everything the nesting allows
             tagged = have.copy()
         else:
-            for k, f in enumerate(self.tags(lev)):
-                if f:
-                    bx, by = L.blocks[k]
-                    tagged[by, bx] = True
+            tagged = self.tags(lev) & have
         want = tagged.copy()
         for dy in (-1, 0, 1):
             for dx in (-1, 0, 1):
@@ -222,7 +249,8 @@ class AmrHierarchy:
             ov = C.byref(old.view) if old is not None else None
             with torch.cuda.stream(self.stream):
                 _lib.check(_lib.lib().zfv_amr_regrid_fill(C.byref(new.view), ov, C.byref(self.levels[lev].view),
-                                                          new.pos.data_ptr(), new.n, self._s()), "zfv_amr_regrid_fill")
+                                                          new.pdesc.data_ptr(), new.n_patches, new.max_blocks,
+                                                          self._s()), "zfv_amr_regrid_fill")
             new.batch.begin()
             self.sync()
             if old is not None:
@@ -238,7 +266,7 @@ class AmrHierarchy:
         n = len(self.levels)
         descs = (C.c_void_p * n)(*[L.batch.descriptors for L in self.levels])
         dts = (C.c_void_p * n)(*[L.dts.data_ptr() for L in self.levels])
-        cnt = (C.c_int * n)(*[L.n for L in self.levels])
+        cnt = (C.c_int * n)(*[L.n_patches for L in self.levels])
         c = self.cfg
         _lib.check(_lib.lib().zfv_amr_set_dt(descs, dts, cnt, n, c.cfl, self.div, c.dtmin, c.dtmax,
                                              self._time.data_ptr(), self._s()), "zfv_amr_set_dt")
@@ -302,8 +330,8 @@ class AmrHierarchy:
         L = self.levels[lev]
         B = self.B
         out = np.full((4, L.ny, L.nx), np.nan)
-        for (bx, by), q in zip(L.blocks, L.batch.state64()):
-            out[:, by * B:(by + 1) * B, bx * B:(bx + 1) * B] = q.cpu().numpy()
+        for (bx, by, nb), q in zip(L.patches, L.batch.state64()):
+            out[:, by * B:(by + 1) * B, bx * B:(bx + nb) * B] = q.cpu().numpy()
         return out
 
     def mass(self) -> float:

@@ -22,8 +22,8 @@ from ._abi import MODELS, ZFV_MODEL_SWE2D, ZFV_PREC_FP32, zfv_config, zfv_status
 
 def tile_variants() -> list[tuple[int, int, int, int]]:
     """The compiled strip shapes as (warps per block, rows per warp, columns
-    per lane, stage-2 staging: 0 none, 1 staged, 2 staged with the stage-2
-    kernel capped at 128 registers)."""
+    per lane, flags: bit 0 stage-2 staging, bit 1 stage-2 kernel capped at
+    128 registers)."""
     L = _lib.lib()
     nw = (C.c_int * 32)()
     cpt = (C.c_int * 32)()

@@ -1,24 +1,28 @@
 // Block-structured AMR on top of the FP32 batch engine.
 //
-// Each level is a batch of equal square boxes (B x B cells) on a regular
-// block grid; `map` gives, per block position, the batch instance holding it
-// (-1: not present at this level). All boxes of a level share one run record
-// (one dt, one CFL reduction). Refinement ratio 2: a level-(l+1) box covers a
-// quarter of a level-l box.
+// Each level lives on a regular grid of B x B blocks. The blocks present at a
+// level are grouped into patches: horizontal runs of consecutive blocks of
+// one block row, each patch one batch instance of (nb * B) x B cells (wide
+// patches keep the 30- and 60-column strips of the stage kernels full).
+// `map` gives, per block position, (instance << 8) | (block offset inside
+// the patch), or -1 when the level has no such block. All patches of a level
+// share one run record (one dt, one CFL reduction). Refinement ratio 2: a
+// level-(l+1) block covers a quarter of a level-l block.
 //
 // Kernels (the reference's AmrCore pieces, ZoomyAmr.cpp:161-288, 733-762):
-//   k32a_fill          ghost frames of every box of a level before a stage:
+//   k32a_fill          ghost frames of every patch of a level before a stage:
 //                      same-level neighbour (FillBoundary), else conservative
 //                      linear interpolation of the next coarser level
 //                      (FillPatchTwoLevels with cell_cons_interp), and the
 //                      physical boundary by mirroring (FillPhysicalBC_mf);
-//   k32a_average_down  fine -> coarse averages under each fine box;
-//   k32a_tag           per box: any cell with |grad eta| > threshold (ErrorEst);
-//   k32a_regrid_fill   fill new boxes from the old boxes of the same level
-//                      where they overlap, else from the coarser level
+//   k32a_average_down  fine -> coarse averages under each fine patch;
+//   k32a_tag           per block: any cell with |grad eta| > threshold (ErrorEst);
+//   k32a_regrid_fill   fill new patches from the old patches of the same
+//                      level where they overlap, else from the coarser level
 //                      (RemakeLevel / MakeNewLevelFromCoarse).
-// The coarse data used for a fine box's ghosts is the coarse level's current
-// state (the reference fills from Q[lev-1] at t_new only).
+// The coarse data used for a fine patch's ghosts is the coarse level's
+// current state (the reference fills from Q[lev-1] at t_new only).
+// Patch descriptors: int4 {first block x, block row y, blocks nb, unused}.
 #pragma once
 
 namespace zfv32 {
@@ -26,16 +30,30 @@ namespace amr {
 
 struct LevelView {
     const BInst* insts;   // the level's batch descriptors (device)
-    const int* map;       // [nby * nbx] block position -> instance, -1 absent
+    const int* map;       // [nby * nbx] block position -> (instance << 8) | offset, -1 absent
     int nbx, nby;         // block grid
-    int B;                // cells per box side
+    int B;                // cells per block side
     int nx, ny;           // level grid (cells)
     int wall;             // bit s: side s (x_lo, x_hi, y_lo, y_hi) is a reflective wall
     int pad_;
 };
 
+constexpr int kMaxPatchBlocks = 256;   // the offset field of a map entry
+
+// Instance and in-instance cell index of level cell (I, J) inside the
+// domain; false when no patch of the level holds it.
+__device__ __forceinline__ bool locate(const LevelView& V, int I, int J, int& k, long long& c) {
+    const int bx = I / V.B, by = J / V.B;
+    const int code = V.map[by * V.nbx + bx];
+    if (code < 0) return false;
+    k = code >> 8;
+    const int ob = code & (kMaxPatchBlocks - 1);
+    c = (long long)(J - by * V.B) * V.insts[k].P.nx + (I - (bx - ob) * V.B);
+    return true;
+}
+
 // The stage input of level cell (I, J): mirrored into the domain with the
-// wall sign flips; false when no box of the level holds the cell.
+// wall sign flips; false when no patch of the level holds the cell.
 __device__ __forceinline__ bool lookup(const LevelView& V, int I, int J, bool with_inc, C4& out) {
     bool fu = false, fv = false;
     if (I < 0) { I = -1 - I; fu = (V.wall & 1) != 0; }
@@ -43,14 +61,13 @@ __device__ __forceinline__ bool lookup(const LevelView& V, int I, int J, bool wi
     if (J < 0) { J = -1 - J; fv = (V.wall & 4) != 0; }
     else if (J >= V.ny) { J = 2 * V.ny - 1 - J; fv = (V.wall & 8) != 0; }
     if (I < 0 || I >= V.nx || J < 0 || J >= V.ny) return false;
-    const int bx = I / V.B, by = J / V.B;
-    const int k = V.map[by * V.nbx + bx];
-    if (k < 0) return false;
+    int k;
+    long long c;
+    if (!locate(V, I, J, k, c)) return false;
     const BInst& D = V.insts[k];
     const unsigned parity = *(volatile const unsigned*)&D.st->parity;
     const float* X = parity ? D.alt : D.Qs;
     const long long pl = D.P.plane;
-    const long long c = (long long)(J - by * V.B) * D.P.nx + (I - bx * V.B);
     out.b = D.bed[c];
     out.e = X[c];
     out.u = X[pl + c];
@@ -87,63 +104,63 @@ __device__ __forceinline__ C4 coarse_interp(const LevelView& C, int I, int J) {
     return r;
 }
 
-// Ring cells of a (B+4)^2 frame, enumerated: bottom two rows, top two rows,
-// then the two left and two right columns of the box rows.
-__device__ __forceinline__ void ring_cell(int k, int B, int& fi, int& fj) {
-    const int W = B + 4;
-    if (k < 2 * W) { fj = k / W; fi = k % W; return; }
-    k -= 2 * W;
-    if (k < 2 * W) { fj = B + 2 + k / W; fi = k % W; return; }
-    k -= 2 * W;
+// Ring cells of a (W+4) x (H+4) frame, enumerated: bottom two rows, top two
+// rows, then the two left and two right columns of the patch rows.
+__device__ __forceinline__ void ring_cell(int k, int W, int H, int& fi, int& fj) {
+    const int FW = W + 4;
+    if (k < 2 * FW) { fj = k / FW; fi = k % FW; return; }
+    k -= 2 * FW;
+    if (k < 2 * FW) { fj = H + 2 + k / FW; fi = k % FW; return; }
+    k -= 2 * FW;
     fj = 2 + k / 4;
     const int col = k % 4;
-    fi = col < 2 ? col : B + col;
+    fi = col < 2 ? col : W + col;
 }
 
-// Ghost frames of all boxes of level F (coarse level C; C.insts == nullptr
+// Ghost frames of all patches of level F (coarse level C; C.insts == nullptr
 // for level 0). stage 1 fills the stage input Q; stage 2 fills Q + inc1 for
 // same-level neighbours (their stage-2 input) and the coarse state otherwise.
-__global__ void k32a_fill(LevelView F, LevelView C, const int2* __restrict__ pos, float* const* __restrict__ frames,
-                          int n_boxes, int stage) {
-    const int box = blockIdx.y;
-    if (box >= n_boxes) return;
-    const int B = F.B, W = B + 4;
-    const int ring = W * W - B * B;
-    const long long fp = (long long)W * W;
-    float* fr = frames[box];
-    const int2 p = pos[box];
+__global__ void k32a_fill(LevelView F, LevelView C, const int4* __restrict__ patches, float* const* __restrict__ frames,
+                          int n_patches, int stage) {
+    const int pi = blockIdx.y;
+    if (pi >= n_patches) return;
+    const int4 p = patches[pi];
+    const int H = F.B, W = p.z * F.B, FW = W + 4;
+    const int ring = FW * (H + 4) - W * H;
+    const long long fp = (long long)FW * (H + 4);
+    float* fr = frames[pi];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ring; k += gridDim.x * blockDim.x) {
         int fi, fj;
-        ring_cell(k, B, fi, fj);
-        const int I = p.x * B + fi - 2, J = p.y * B + fj - 2;
+        ring_cell(k, W, H, fi, fj);
+        const int I = p.x * F.B + fi - 2, J = p.y * F.B + fj - 2;
         C4 q{0.0f, 0.0f, 0.0f, 0.0f};
         const bool inside = I >= 0 && I < F.nx && J >= 0 && J < F.ny;
         bool ok = lookup(F, I, J, stage == 2, q);
         if (!ok && inside && C.insts) q = coarse_interp(C, I, J);
-        const long long f = (long long)fj * W + fi;
+        const long long f = (long long)fj * FW + fi;
         fr[f] = q.b; fr[fp + f] = q.e; fr[2 * fp + f] = q.u; fr[3 * fp + f] = q.v;
     }
 }
 
-// Fine -> coarse: each 2 x 2 group of fine cells of a fine box replaces the
-// coarse cell under it (eta, hu, hv as the FP64 mean of value + remainder; the
-// coarse bed is kept).
-__global__ void k32a_average_down(LevelView F, LevelView C, const int2* __restrict__ pos, int n_boxes) {
-    const int box = blockIdx.y;
-    if (box >= n_boxes) return;
-    const int B = F.B, h = B / 2;
-    const int2 p = pos[box];
-    const int kf = F.map[p.y * F.nbx + p.x];
-    if (kf < 0) return;
-    const BInst& D = F.insts[kf];
+// Fine -> coarse: each 2 x 2 group of fine cells of a fine patch replaces
+// the coarse cell under it (eta, hu, hv as the FP64 mean of value +
+// remainder; the coarse bed is kept).
+__global__ void k32a_average_down(LevelView F, LevelView C, const int4* __restrict__ patches, int n_patches) {
+    const int pi = blockIdx.y;
+    if (pi >= n_patches) return;
+    const int4 p = patches[pi];
+    const int hh = F.B / 2, hw = p.z * F.B / 2;
+    const int code = F.map[p.y * F.nbx + p.x];
+    if (code < 0) return;
+    const BInst& D = F.insts[code >> 8];
     const float* X = (*(volatile const unsigned*)&D.st->parity) ? D.alt : D.Qs;
     const long long pl = D.P.plane;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < h * h; k += gridDim.x * blockDim.x) {
-        const int a = k % h, c = k / h;
-        const int ic = p.x * h + a, jc = p.y * h + c;   // coarse cell
-        const int bxc = ic / C.B, byc = jc / C.B;
-        const int kc = C.map[byc * C.nbx + bxc];
-        if (kc < 0) continue;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < hw * hh; k += gridDim.x * blockDim.x) {
+        const int a = k % hw, c = k / hw;
+        const int ic = p.x * hh + a, jc = p.y * hh + c;   // coarse cell
+        int kc;
+        long long cc;
+        if (!locate(C, ic, jc, kc, cc)) continue;
         double s[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
@@ -154,7 +171,6 @@ __global__ void k32a_average_down(LevelView F, LevelView C, const int2* __restri
         const BInst& E = C.insts[kc];
         float* Y = (*(volatile const unsigned*)&E.st->parity) ? E.alt : E.Qs;
         const long long plc = E.P.plane;
-        const long long cc = (long long)(jc - byc * C.B) * E.P.nx + (ic - bxc * C.B);
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             const double m = 0.25 * s[q];
@@ -165,64 +181,60 @@ __global__ void k32a_average_down(LevelView F, LevelView C, const int2* __restri
     }
 }
 
-// flags[box] = 1 when some cell of the box has |grad eta| > threshold
-// (centred differences over the level's own cells; the reference's ErrorEst
-// flags |grad h| or h > 1e-2, ZoomyAmr.cpp:224-252).
-__global__ void k32a_tag(LevelView V, const int2* __restrict__ pos, int n_boxes, float dx, float dy,
+// flags[by * nbx + bx] = 1 (others untouched) for blocks with a cell where
+// |grad eta| > threshold (centred differences over the level's own cells;
+// the reference's ErrorEst flags |grad h| or h > 1e-2, ZoomyAmr.cpp:224-252).
+__global__ void k32a_tag(LevelView V, const int4* __restrict__ patches, int n_patches, float dx, float dy,
                          float threshold, int* __restrict__ flags) {
-    const int box = blockIdx.y;
-    if (box >= n_boxes) return;
+    const int pi = blockIdx.y;
+    if (pi >= n_patches) return;
     const int B = V.B;
-    const int2 p = pos[box];
-    int hit = 0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B * B; k += gridDim.x * blockDim.x) {
-        const int I = p.x * B + k % B, J = p.y * B + k / B;
+    const int4 p = patches[pi];
+    const int W = p.z * B;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < W * B; k += gridDim.x * blockDim.x) {
+        const int i = k % W;
+        const int I = p.x * B + i, J = p.y * B + k / W;
         C4 xm, xp, ym, yp;
         if (!lookup(V, I - 1, J, false, xm) || !lookup(V, I + 1, J, false, xp) ||
             !lookup(V, I, J - 1, false, ym) || !lookup(V, I, J + 1, false, yp))
             continue;
         const float gx = (xp.e - xm.e) / (2.0f * dx), gy = (yp.e - ym.e) / (2.0f * dy);
-        if (gx * gx + gy * gy > threshold * threshold) hit = 1;
+        if (gx * gx + gy * gy > threshold * threshold) flags[p.y * V.nbx + p.x + i / B] = 1;
     }
-    if (__syncthreads_or(hit) && threadIdx.x == 0) flags[box] = 1;
 }
 
-// New boxes of a level: copy the old boxes of the same level where present
-// (value + remainder), else interpolate the coarser level (remainder 0).
-// New boxes start with parity 0 (their run record is fresh).
-__global__ void k32a_regrid_fill(LevelView N, LevelView O, LevelView C, const int2* __restrict__ pos, int n_boxes) {
-    const int box = blockIdx.y;
-    if (box >= n_boxes) return;
+// New patches of a level: copy the old patches of the same level where
+// present (value + remainder), else interpolate the coarser level
+// (remainder 0). New patches start with parity 0 (their run record is fresh).
+__global__ void k32a_regrid_fill(LevelView N, LevelView O, LevelView C, const int4* __restrict__ patches,
+                                 int n_patches) {
+    const int pi = blockIdx.y;
+    if (pi >= n_patches) return;
     const int B = N.B;
-    const int2 p = pos[box];
-    const int kn = N.map[p.y * N.nbx + p.x];
-    if (kn < 0) return;
-    const BInst& D = N.insts[kn];
+    const int4 p = patches[pi];
+    const int W = p.z * B;
+    const int code = N.map[p.y * N.nbx + p.x];
+    if (code < 0) return;
+    const BInst& D = N.insts[code >> 8];
     const long long pl = D.P.plane;
     float* bed = const_cast<float*>(D.bed);
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B * B; k += gridDim.x * blockDim.x) {
-        const int i = k % B, j = k / B;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < W * B; k += gridDim.x * blockDim.x) {
+        const int i = k % W, j = k / W;
         const int I = p.x * B + i, J = p.y * B + j;
         const long long c = (long long)j * D.P.nx + i;
-        bool done = false;
-        if (O.insts) {
-            const int bx = I / O.B, by = J / O.B;
-            const int ko = (bx < O.nbx && by < O.nby) ? O.map[by * O.nbx + bx] : -1;
-            if (ko >= 0) {
-                const BInst& E = O.insts[ko];
-                const float* X = (*(volatile const unsigned*)&E.st->parity) ? E.alt : E.Qs;
-                const long long plo = E.P.plane;
-                const long long co = (long long)(J - by * O.B) * E.P.nx + (I - bx * O.B);
-                bed[c] = E.bed[co];
+        int ko;
+        long long co;
+        if (O.insts && locate(O, I, J, ko, co)) {
+            const BInst& E = O.insts[ko];
+            const float* X = (*(volatile const unsigned*)&E.st->parity) ? E.alt : E.Qs;
+            const long long plo = E.P.plane;
+            bed[c] = E.bed[co];
 #pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    D.Qs[q * pl + c] = X[q * plo + co];
-                    D.lo[q * pl + c] = E.lo[q * plo + co];
-                }
-                done = true;
+            for (int q = 0; q < 3; ++q) {
+                D.Qs[q * pl + c] = X[q * plo + co];
+                D.lo[q * pl + c] = E.lo[q * plo + co];
             }
-        }
-        if (!done) {
+        } else {
             const C4 q = coarse_interp(C, I, J);
             bed[c] = q.b;
             D.Qs[c] = q.e; D.Qs[pl + c] = q.u; D.Qs[2 * pl + c] = q.v;

@@ -58,20 +58,19 @@ __device__ __forceinline__ const float* state_in(const BInst& D, unsigned parity
 }
 
 template <int MODE, bool WB, bool IMPL, int NW, int CPT, int PK, int PF>
-__global__ void __launch_bounds__(32 * NW, (MODE == 2 && PF == 2) ? 4 : 1)
-k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
+__device__ __forceinline__ void stage_body(const BInst* __restrict__ insts, const int2* __restrict__ units)
 {
     constexpr int SW = 30 * PK;                  // owned columns per strip
     constexpr int NT = 32 * NW;
     __shared__ double red[2 * NW];
     __shared__ BInst sD;
-    // stage-2 staging of the update's own inputs (PF): 9 values per lane per warp
-    __shared__ __align__(16) float cstage[PF ? NW * 9 * 32 * PK : 1];
+    // stage-2 staging of the update's own inputs (PF bit 0): 9 values per lane per warp
+    __shared__ __align__(16) float cstage[(PF & 1) ? NW * 9 * 32 * PK : 1];
     const int2 u = units[blockIdx.x];
     stage_desc(insts, u.x, sD);
     const Params& L = sD.P;
     const int w = threadIdx.x >> 5;
-    float* wstage = cstage + (PF ? w * 9 * 32 * PK : 0);
+    float* wstage = cstage + ((PF & 1) ? w * 9 * 32 * PK : 0);
     const int bx = u.y % sD.nbx, by = u.y / sD.nbx;
     const int x0 = bx * SW, y0 = by * (NW * CPT), j0 = y0 + w * CPT;
     zfv::DevState* st = sD.st;
@@ -86,24 +85,24 @@ k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
     float* inc_out = (MODE == S1) ? sD.inc : nullptr;        // stage 1 writes it
     if constexpr (PK == 1) {
         if (strip_interior<NW, CPT>(L, x0, y0))
-            sweep_strip<MODE, WB, IMPL, CPT, true, (PF != 0)>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
+            sweep_strip<MODE, WB, IMPL, CPT, true, (PF & 1) != 0>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
                                                    float(dtd), dtd, m_loc, s_loc, wstage);
         else
-            sweep_strip<MODE, WB, IMPL, CPT, false, (PF != 0)>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
+            sweep_strip<MODE, WB, IMPL, CPT, false, (PF & 1) != 0>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0, j0,
                                                     float(dtd), dtd, m_loc, s_loc, wstage);
     } else {
         // 8-byte accesses need an even row length (x0 is even)
         if (pk::strip_interior2<NW, CPT>(L, x0, y0)) {
             if ((L.nx & 1) == 0)
-                pk::sweep_strip2<MODE, WB, IMPL, CPT, true, true, (PF != 0)>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
+                pk::sweep_strip2<MODE, WB, IMPL, CPT, true, true, (PF & 1) != 0>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
                                                                   j0, float(dtd), dtd, m_loc, s_loc,
                                                                 reinterpret_cast<float2*>(wstage));
             else
-                pk::sweep_strip2<MODE, WB, IMPL, CPT, true, false, (PF != 0)>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
+                pk::sweep_strip2<MODE, WB, IMPL, CPT, true, false, (PF & 1) != 0>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
                                                                    j0, float(dtd), dtd, m_loc, s_loc,
                                                                 reinterpret_cast<float2*>(wstage));
         } else {
-            pk::sweep_strip2<MODE, WB, IMPL, CPT, false, false, (PF != 0)>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
+            pk::sweep_strip2<MODE, WB, IMPL, CPT, false, false, (PF & 1) != 0>(sD.bed, X, inc_in, inc_out, Y, sD.lo, L, x0,
                                                                 j0, float(dtd), dtd, m_loc, s_loc,
                                                                 reinterpret_cast<float2*>(wstage));
         }
@@ -117,6 +116,29 @@ k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units)
             __threadfence();
         }
     }
+}
+
+// One RK stage of every unit of the batch.
+template <int MODE, bool WB, bool IMPL, int NW, int CPT, int PK, int PF>
+__global__ void __launch_bounds__(32 * NW)
+k32b_stage(const BInst* __restrict__ insts, const int2* __restrict__ units) {
+    stage_body<MODE, WB, IMPL, NW, CPT, PK, PF>(insts, units);
+}
+
+// The same, held to 128 registers so that 4 blocks of 128 threads fit an SM
+// (the stage-2 kernel of the shapes with PF bit 1).
+template <int MODE, bool WB, bool IMPL, int NW, int CPT, int PK, int PF>
+__global__ void __launch_bounds__(32 * NW, 4)
+k32b_stage_r128(const BInst* __restrict__ insts, const int2* __restrict__ units) {
+    stage_body<MODE, WB, IMPL, NW, CPT, PK, PF>(insts, units);
+}
+
+template <int MODE, bool WB, bool IMPL, int NW, int CPT, int PK, int PF>
+inline void launch_stage(int n_units, cudaStream_t s, const BInst* insts, const int2* units) {
+    if constexpr (MODE == S2 && (PF & 2) != 0)
+        k32b_stage_r128<MODE, WB, IMPL, NW, CPT, PK, PF><<<n_units, 32 * NW, 0, s>>>(insts, units);
+    else
+        k32b_stage<MODE, WB, IMPL, NW, CPT, PK, PF><<<n_units, 32 * NW, 0, s>>>(insts, units);
 }
 
 // Per-cell helpers over the same unit table: each block covers its strip's

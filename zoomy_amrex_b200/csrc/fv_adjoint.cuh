@@ -99,9 +99,13 @@ __device__ __forceinline__ int mirror(int i, int n, bool& out) {
     return i < 0 ? 0 : (i >= n ? n - 1 : i);
 }
 
-template <int TX, int TY>
+// A TX x TY tile reversed by NT >= TX * TY threads: the face pass spreads
+// the tile's NF faces (more than 2 per cell with the halo) over all NT
+// threads; the first TX * TY threads then own one cell each.
+template <int TX, int TY, int NT_ = TX * TY>
 struct AdjTile {
-    static constexpr int NT = TX * TY;
+    static constexpr int NT = NT_;
+    static_assert(NT_ >= TX * TY, "one thread per cell at least");
     static constexpr int XW = TX + 6, XH = TY + 6;      // X with 3 halo cells
     static constexpr int LW = TX + 4, LH = TY + 4;      // lam_q* with 2 halo cells
     static constexpr int NFX = (TX + 3) * TY;           // x-faces x0-1 .. x0+TX+1 (right cell index)
@@ -116,12 +120,12 @@ struct AdjTile {
 // Pass B. X: stage input (bed from qbed, planes 1..3 from X). lamq, loc from
 // pass A; addend (NULL or 4 planes) * addscale is added (the Heun term
 // lam_{n+1}/2 of stage 1). lamX may alias addend.
-template <bool WB, int TX, int TY, int MINB>
-__global__ void __launch_bounds__(TX * TY, MINB)
+template <bool WB, int TX, int TY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
 k_adj_face(const double* __restrict__ X, const double* __restrict__ qbed, const double* __restrict__ lamq,
            const double* __restrict__ loc, const double* addend, double addscale, P6 L,
            const double* __restrict__ meta, double* lamX) {
-    using T = AdjTile<TX, TY>;
+    using T = AdjTile<TX, TY, NT>;
     const double dt = meta[1];
     extern __shared__ __align__(16) double smem[];
     double* sX = smem;                       // [4][XH][XW]
@@ -160,6 +164,7 @@ k_adj_face(const double* __restrict__ X, const double* __restrict__ qbed, const 
     }
     __syncthreads();
 
+    const bool owner = tid < TX * TY;       // this thread owns cell (i, j) of the tile
     const int tx = tid % TX, ty = tid / TX;
     const int i = x0 + tx, j = y0 + ty;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -219,7 +224,7 @@ k_adj_face(const double* __restrict__ X, const double* __restrict__ qbed, const 
     __syncthreads();
     // 4. gather per owned cell, fixed order: direct stencil entries, then
     // entries of ghost cells that mirror onto this cell
-    if (i < nx && j < ny) {
+    if (owner && i < nx && j < ny) {
 #pragma unroll 1
         for (int D = 0; D < 2; ++D) {
             const int ci = D == 0 ? i : j, n_d = D == 0 ? nx : ny;
@@ -267,7 +272,7 @@ k_adj_face(const double* __restrict__ X, const double* __restrict__ qbed, const 
         }
     }
     // 5. lam_X = lam_q* + loc + faces (+ addend)
-    if (i < nx && j < ny) {
+    if (owner && i < nx && j < ny) {
         const long long c = (long long)j * nx + i;
         double add[4] = {0.0, 0.0, 0.0, 0.0};
         if (addend) {

@@ -13,21 +13,27 @@ namespace {
 constexpr int kCellNT = 256;
 constexpr int kDtBlocks = 592;   // 4 x 148 SMs
 
-// Tile shapes of the face-reverse kernel: (TX, TY, minimum resident blocks
-// per SM). The kernel is register-heavy (FP64 reverse of a whole face), so
-// the shapes trade tile halo overhead against occupancy. Default: 32 x 8 with
-// two blocks per SM, the fastest measured at 1024^2 (206 ms for the backward
-// of 200 steps, against 265 / 219 / 216 ms for the others).
-constexpr int kAdjVariants = 4;
+// Tile shapes of the face-reverse kernel: (TX, TY, threads NT, minimum
+// resident blocks per SM). The kernel is register-heavy (FP64 reverse of a
+// whole face), so the shapes trade tile halo overhead, the share of threads
+// busy in the face pass (a tile has NF = (TX+3) TY + TX (TY+3) faces, spread
+// over NT threads) and occupancy. 32 x 8 with 256 threads and two blocks per
+// SM runs 3 face rounds per cell (632 faces); 32 x 6 with 256 threads runs
+// 2.67 (498 faces in two rounds); 32 x 13 with 512 threads 2.46 (967 faces)
+// at one block per SM.
+constexpr int kAdjVariants = 7;
 std::atomic<int> g_adj_variant{2};
 
 template <class F>
 int with_adj_variant(int v, F&& f) {
     switch (v) {
-    case 0: return f.template operator()<32, 8, 1>();
-    case 1: return f.template operator()<32, 4, 3>();
-    case 2: return f.template operator()<32, 8, 2>();
-    case 3: return f.template operator()<16, 8, 3>();
+    case 0: return f.template operator()<32, 8, 256, 1>();
+    case 1: return f.template operator()<32, 4, 128, 3>();
+    case 2: return f.template operator()<32, 8, 256, 2>();
+    case 3: return f.template operator()<16, 8, 128, 3>();
+    case 4: return f.template operator()<32, 6, 256, 2>();
+    case 5: return f.template operator()<32, 10, 384, 1>();
+    case 6: return f.template operator()<32, 13, 512, 1>();
     default: return fail(-1, "unknown adjoint tile variant %d", v);
     }
 }
@@ -58,13 +64,13 @@ AdjLayout adj_layout(long long plane) {
 
 namespace {
 
-template <bool WB, bool IMPL, int TX, int TY, int MINB>
+template <bool WB, bool IMPL, int TX, int TY, int NT, int MINB>
 int step_impl(const zfv::adj::P6& L, const AdjLayout& A, const char* tape, double* lam, double* grad,
               const double* aux0, int n_aux, char* work, cudaStream_t s) {
     using namespace zfv::adj;
-    using Tile = AdjTile<TX, TY>;
+    using Tile = AdjTile<TX, TY, NT>;
     // per device: cheap, so set on every call
-    int rc = cuda_check(cudaFuncSetAttribute(k_adj_face<WB, TX, TY, MINB>,
+    int rc = cuda_check(cudaFuncSetAttribute(k_adj_face<WB, TX, TY, NT, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              int(Tile::smem_bytes)), "k_adj_face attribute");
     if (rc) return rc;
@@ -82,12 +88,12 @@ int step_impl(const zfv::adj::P6& L, const AdjLayout& A, const char* tape, doubl
     const dim3 fgrid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY);
     // stage 2: Y2 = stage(Y1), Q^{n+1} = (Q^n + Y2)/2 -> lam_Y2 = lam/2
     k_adj_cell<IMPL, kCellNT><<<A.nbA, kCellNT, 0, s>>>(lam, 0.5, Y1, qs2, L, meta, lamq, loc, part);
-    k_adj_face<WB, TX, TY, MINB><<<fgrid, TX * TY, Tile::smem_bytes, s>>>(
+    k_adj_face<WB, TX, TY, NT, MINB><<<fgrid, NT, Tile::smem_bytes, s>>>(
         Y1, X, lamq, loc, nullptr, 0.0, L, meta, lamY1);
     // stage 1: Y1 = stage(Q^n); lam_n = (dY1/dQ^n)^T lam_Y1 + lam/2
     k_adj_cell<IMPL, kCellNT><<<A.nbA, kCellNT, 0, s>>>(lamY1, 1.0, X, qs1, L, meta, lamq, loc,
                                                         part + 2 * A.nbA);
-    k_adj_face<WB, TX, TY, MINB><<<fgrid, TX * TY, Tile::smem_bytes, s>>>(
+    k_adj_face<WB, TX, TY, NT, MINB><<<fgrid, NT, Tile::smem_bytes, s>>>(
         X, X, lamq, loc, lam, 0.5, L, meta, lam);
     // dt_n = dt(Q^n)
     k_adj_dt<256><<<A.nbD, 256, 0, s>>>(X, aux0, n_aux, L, meta, part, 2 * A.nbA, amax, counter, lam, grad);
@@ -98,8 +104,8 @@ template <bool WB, bool IMPL>
 struct StepF {
     const zfv::adj::P6& L; const AdjLayout& A; const char* tape; double* lam; double* grad;
     const double* aux0; int n_aux; char* work; cudaStream_t s;
-    template <int TX, int TY, int MINB> int operator()() {
-        return step_impl<WB, IMPL, TX, TY, MINB>(L, A, tape, lam, grad, aux0, n_aux, work, s);
+    template <int TX, int TY, int NT, int MINB> int operator()() {
+        return step_impl<WB, IMPL, TX, TY, NT, MINB>(L, A, tape, lam, grad, aux0, n_aux, work, s);
     }
 };
 

@@ -116,17 +116,17 @@ enum Mode { S1 = 1, S2 = 2 };
 namespace zfv32 {
 
 // Compiled strip shapes: (warps per block NW, rows per warp CPT = cells per
-// thread, columns per lane PK, stage-2 staging PF). A strip is 30 * PK
-// columns x (NW * CPT) rows; PK = 2 is the packed-FP32 paired-column sweep;
-// PF >= 1 stages the stage-2 update's own inputs in shared memory with
-// asynchronous copies issued at the top of each row; PF = 2 also caps the
-// stage-2 kernel at 128 registers (4 blocks of 128 threads per SM instead of
-// 3, at the cost of some spilling).
+// thread, columns per lane PK, flags PF). A strip is 30 * PK columns x
+// (NW * CPT) rows; PK = 2 is the packed-FP32 paired-column sweep. PF bits:
+//   1  stage 2 stages its update's own inputs in shared memory with
+//      asynchronous copies issued at the top of each row;
+//   2  the stage-2 kernel is capped at 128 registers (4 blocks of 128
+//      threads per SM instead of 3, at the cost of some spilling).
 constexpr int kNumVariants = 10;
 constexpr int kVarNW[kNumVariants] = {4, 4, 4, 4, 4, 4, 4, 4, 4, 4};
 constexpr int kVarCPT[kNumVariants] = {16, 8, 16, 8, 16, 8, 16, 8, 16, 8};
 constexpr int kVarPK[kNumVariants] = {1, 1, 2, 2, 1, 1, 2, 2, 2, 2};
-constexpr int kVarPF[kNumVariants] = {0, 0, 0, 0, 1, 1, 1, 1, 2, 2};
+constexpr int kVarPF[kNumVariants] = {0, 0, 0, 0, 1, 1, 1, 1, 3, 3};
 
 template <class F>
 int with_variant(int v, F&& f) {
@@ -139,8 +139,8 @@ int with_variant(int v, F&& f) {
     case 5: return f.template operator()<4, 8, 1, 1>();
     case 6: return f.template operator()<4, 16, 2, 1>();
     case 7: return f.template operator()<4, 8, 2, 1>();
-    case 8: return f.template operator()<4, 16, 2, 2>();
-    case 9: return f.template operator()<4, 8, 2, 2>();
+    case 8: return f.template operator()<4, 16, 2, 3>();
+    case 9: return f.template operator()<4, 8, 2, 3>();
     default: return fail(-1, "unknown strip variant %d", v);
     }
 }
@@ -370,13 +370,13 @@ struct BatchCore {
         template <int NW, int CPT, int PK, int PF> int operator()() {
             const int nu = b->nunits();
             if (stages == 1) {
-                k32b_stage<S1, W, I, NW, CPT, PK, PF><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+                launch_stage<S1, W, I, NW, CPT, PK, PF>(nu, s, b->d_desc(), b->d_units());
             } else if (stages == 2) {
-                k32b_stage<S2, W, I, NW, CPT, PK, PF><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+                launch_stage<S2, W, I, NW, CPT, PK, PF>(nu, s, b->d_desc(), b->d_units());
             } else {
                 for (int k = 0; k < nsteps; ++k) {
-                    k32b_stage<S1, W, I, NW, CPT, PK, PF><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
-                    k32b_stage<S2, W, I, NW, CPT, PK, PF><<<nu, 32 * NW, 0, s>>>(b->d_desc(), b->d_units());
+                    launch_stage<S1, W, I, NW, CPT, PK, PF>(nu, s, b->d_desc(), b->d_units());
+                    launch_stage<S2, W, I, NW, CPT, PK, PF>(nu, s, b->d_desc(), b->d_units());
                 }
             }
             return cuda_check(cudaGetLastError(), "zfv_batch evolve launch");
@@ -483,12 +483,12 @@ struct zfv_batch {
 
 extern "C" {
 
-int zfv_tile_variants(int* nw, int* cpt, int* cols, int* prefetch, int max_n) {
+int zfv_tile_variants(int* nw, int* cpt, int* cols, int* flags, int max_n) {
     for (int v = 0; v < zfv32::kNumVariants && v < max_n; ++v) {
         if (nw) nw[v] = zfv32::kVarNW[v];
         if (cpt) cpt[v] = zfv32::kVarCPT[v];
         if (cols) cols[v] = zfv32::kVarPK[v];
-        if (prefetch) prefetch[v] = zfv32::kVarPF[v];
+        if (flags) flags[v] = zfv32::kVarPF[v];
     }
     return zfv32::kNumVariants;
 }
@@ -553,45 +553,50 @@ static zfv32::amr::LevelView view_of(const zfv_amr_level* l) {
     return v;
 }
 
-static int amr_grid(int n_boxes, int per_box, dim3& g) {
-    if (n_boxes < 1 || n_boxes > 65535) return fail(-1, "zfv_amr: %d boxes (1 .. 65535 per call)", n_boxes);
-    g = dim3(unsigned((per_box + 255) / 256), unsigned(n_boxes), 1);
+static int amr_grid(int n_patches, int max_blocks, long long per_patch, dim3& g) {
+    if (n_patches < 1 || n_patches > 65535)
+        return fail(-1, "zfv_amr: %d patches (1 .. 65535 per call)", n_patches);
+    if (max_blocks < 1 || max_blocks > zfv32::amr::kMaxPatchBlocks)
+        return fail(-1, "zfv_amr: %d blocks per patch (1 .. %d)", max_blocks, zfv32::amr::kMaxPatchBlocks);
+    g = dim3(unsigned((per_patch + 255) / 256), unsigned(n_patches), 1);
     return 0;
 }
 
-int zfv_amr_fill(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* pos, float* const* frames,
-                 int n_boxes, int stage, void* stream) {
-    if (!fine || !pos || !frames) return fail(-1, "zfv_amr_fill: null argument");
+int zfv_amr_fill(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* patches, float* const* frames,
+                 int n_patches, int max_blocks, int stage, void* stream) {
+    if (!fine || !patches || !frames) return fail(-1, "zfv_amr_fill: null argument");
     if (stage != 1 && stage != 2) return fail(-1, "zfv_amr_fill: stage must be 1 or 2");
-    const int B = fine->B;
+    const long long B = fine->B, W = (long long)max_blocks * B;
     dim3 g;
-    int rc = amr_grid(n_boxes, (B + 4) * (B + 4) - B * B, g);
+    int rc = amr_grid(n_patches, max_blocks, (W + 4) * (B + 4) - W * B, g);
     if (rc) return rc;
-    zfv32::amr::k32a_fill<<<g, 256, 0, (cudaStream_t)stream>>>(view_of(fine), view_of(coarse),
-                                                             reinterpret_cast<const int2*>(pos), frames, n_boxes, stage);
+    zfv32::amr::k32a_fill<<<g, 256, 0, (cudaStream_t)stream>>>(
+        view_of(fine), view_of(coarse), reinterpret_cast<const int4*>(patches), frames, n_patches, stage);
     return cuda_check(cudaGetLastError(), "zfv_amr_fill launch");
 }
 
-int zfv_amr_average_down(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* pos, int n_boxes,
-                         void* stream) {
-    if (!fine || !coarse || !pos) return fail(-1, "zfv_amr_average_down: null argument");
-    if (fine->B % 2) return fail(-1, "zfv_amr_average_down: the box side must be even");
+int zfv_amr_average_down(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* patches, int n_patches,
+                         int max_blocks, void* stream) {
+    if (!fine || !coarse || !patches) return fail(-1, "zfv_amr_average_down: null argument");
+    if (fine->B % 2) return fail(-1, "zfv_amr_average_down: the block side must be even");
+    const long long h = fine->B / 2;
     dim3 g;
-    int rc = amr_grid(n_boxes, (fine->B / 2) * (fine->B / 2), g);
+    int rc = amr_grid(n_patches, max_blocks, (long long)max_blocks * h * h, g);
     if (rc) return rc;
-    zfv32::amr::k32a_average_down<<<g, 256, 0, (cudaStream_t)stream>>>(view_of(fine), view_of(coarse),
-                                                                     reinterpret_cast<const int2*>(pos), n_boxes);
+    zfv32::amr::k32a_average_down<<<g, 256, 0, (cudaStream_t)stream>>>(
+        view_of(fine), view_of(coarse), reinterpret_cast<const int4*>(patches), n_patches);
     return cuda_check(cudaGetLastError(), "zfv_amr_average_down launch");
 }
 
-int zfv_amr_tag(const zfv_amr_level* level, const int* pos, int n_boxes, double dx, double dy, double threshold,
-                int* flags, void* stream) {
-    if (!level || !pos || !flags) return fail(-1, "zfv_amr_tag: null argument");
+int zfv_amr_tag(const zfv_amr_level* level, const int* patches, int n_patches, int max_blocks, double dx, double dy,
+                double threshold, int* flags, void* stream) {
+    if (!level || !patches || !flags) return fail(-1, "zfv_amr_tag: null argument");
     dim3 g;
-    int rc = amr_grid(n_boxes, level->B * level->B, g);
+    const long long B = level->B;
+    int rc = amr_grid(n_patches, max_blocks, (long long)max_blocks * B * B, g);
     if (rc) return rc;
-    zfv32::amr::k32a_tag<<<g, 256, 0, (cudaStream_t)stream>>>(view_of(level), reinterpret_cast<const int2*>(pos),
-                                                            n_boxes, float(dx), float(dy), float(threshold), flags);
+    zfv32::amr::k32a_tag<<<g, 256, 0, (cudaStream_t)stream>>>(view_of(level), reinterpret_cast<const int4*>(patches),
+                                                            n_patches, float(dx), float(dy), float(threshold), flags);
     return cuda_check(cudaGetLastError(), "zfv_amr_tag launch");
 }
 
@@ -614,14 +619,15 @@ int zfv_amr_set_dt(const void* const* level_descs, double* const* dts, const int
 }
 
 int zfv_amr_regrid_fill(const zfv_amr_level* level, const zfv_amr_level* old_level, const zfv_amr_level* coarse,
-                        const int* pos, int n_boxes, void* stream) {
-    if (!level || !pos) return fail(-1, "zfv_amr_regrid_fill: null argument");
+                        const int* patches, int n_patches, int max_blocks, void* stream) {
+    if (!level || !patches) return fail(-1, "zfv_amr_regrid_fill: null argument");
     if (!old_level && !coarse) return fail(-1, "zfv_amr_regrid_fill: needs an old level or a coarser level");
     dim3 g;
-    int rc = amr_grid(n_boxes, level->B * level->B, g);
+    const long long B = level->B;
+    int rc = amr_grid(n_patches, max_blocks, (long long)max_blocks * B * B, g);
     if (rc) return rc;
     zfv32::amr::k32a_regrid_fill<<<g, 256, 0, (cudaStream_t)stream>>>(
-        view_of(level), view_of(old_level), view_of(coarse), reinterpret_cast<const int2*>(pos), n_boxes);
+        view_of(level), view_of(old_level), view_of(coarse), reinterpret_cast<const int4*>(patches), n_patches);
     return cuda_check(cudaGetLastError(), "zfv_amr_regrid_fill launch");
 }
 
