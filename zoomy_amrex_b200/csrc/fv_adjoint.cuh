@@ -69,9 +69,10 @@ k_adj_cell(const double* __restrict__ lam_in, double scale, const double* __rest
 #pragma unroll
         for (int n = 0; n < 4; ++n) lq[n] = scale * lam_in[n * pl + c];
         const double h = qs[c], mx = qs[pl + c], my = qs[2 * pl + c];
-        double lhv = 0.0;
+        double lhv = 0.0, dhv = 0.0;
         if constexpr (IMPL) {
             const double hv = zadj::hinv(X[pl + c], p.eps);
+            dhv = zadj::dhinv_r(X[pl + c], p.eps);
             double lqi[4] = {0.0, 0.0, 0.0, 0.0};
             const double lam[2] = {lq[2], lq[3]};
             zadj::implicit_rev(h, mx, my, hv, dt, p, lam, lqi, lhv, pnm, pdt);
@@ -81,7 +82,7 @@ k_adj_cell(const double* __restrict__ lam_in, double scale, const double* __rest
         pdt += (lq[1] * (h - X[pl + c]) + lq[2] * (mx - X[2 * pl + c]) + lq[3] * (my - X[3 * pl + c])) / dt;
 #pragma unroll
         for (int n = 0; n < 4; ++n) lamq[n * pl + c] = lq[n];
-        loc[c] = IMPL ? lhv * zadj::dhinv(X[pl + c], p.eps) : 0.0;
+        loc[c] = IMPL ? lhv * dhv : 0.0;
     }
     block_sum2<NT>(pnm, pdt, red);
     if (threadIdx.x == 0) {

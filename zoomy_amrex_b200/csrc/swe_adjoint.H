@@ -76,6 +76,32 @@ PORTABLE_FN ZADJ_INLINE R dhinv(R h, R eps) {
     return std::sqrt(R(2)) / den * (R(1) - h * dD / (R(2) * D));
 }
 
+// 1 / sqrt(x): the device's reciprocal square root (at most 1 ulp off in
+// FP64), 1 / sqrt on the host.
+template <class R>
+PORTABLE_FN ZADJ_INLINE R rsqrt_of(R x) {
+#ifdef __CUDA_ARCH__
+    return ::rsqrt(x);
+#else
+    return R(1) / std::sqrt(x);
+#endif
+}
+
+// dhinv from one reciprocal square root: with D = x0 + max(x0, eps),
+// dhinv = sqrt2 D^(-1/2) (1 - h D' / (2 D)). A derivative coefficient only:
+// values that decide a branch (hinv itself) are computed as the forward does.
+template <class R>
+PORTABLE_FN ZADJ_INLINE R dhinv_r(R h, R eps) {
+    const R h2 = h * h;
+    const R x0 = h2 * h2;
+    const bool big = !(x0 < eps);
+    const R D = x0 + (big ? x0 : eps);
+    if (!(D > R(0))) return R(0);
+    const R r = rsqrt_of(D);
+    const R dD = R(4) * h * h2 * (big ? R(2) : R(1));
+    return std::sqrt(R(2)) * r * (R(1) - R(0.5) * h * dD * (r * r));
+}
+
 template <class R>
 PORTABLE_FN ZADJ_INLINE R sgn(R x) { return (x > R(0)) ? R(1) : ((x < R(0)) ? R(-1) : R(0)); }
 
@@ -149,15 +175,19 @@ PORTABLE_FN ZADJ_INLINE void face_rev(const R c[4][4], SweP<R> const& p, const R
     R hL = qL[1], hR = qR[1];
     R mL[2] = {qL[2], qL[3]}, mR[2] = {qR[2], qR[3]};
     R bL = qL[0], bR = qR[0];
-    R bf = 0, tL = 0, tR = 0, hsL = 0, hsR = 0, sL = 1, sR = 1;
+    R bf = 0, tL = 0, tR = 0, hsL = 0, hsR = 0, sL = 1, sR = 1, iqL = 0, iqR = 0;
     if constexpr (WB) {
         bf = amrex::max(qL[0], qR[0]);
         tL = qL[1] + qL[0] - bf;
         tR = qR[1] + qR[0] - bf;
         hsL = amrex::max(R(0), tL);
         hsR = amrex::max(R(0), tR);
+        // the forward's values (they decide max / minmod branches below);
+        // iq = 1 / q_h serves the reverse only
         sL = (qL[1] > R(0)) ? hsL / qL[1] : R(0);
         sR = (qR[1] > R(0)) ? hsR / qR[1] : R(0);
+        iqL = (qL[1] > R(0)) ? R(1) / qL[1] : R(0);
+        iqR = (qR[1] > R(0)) ? R(1) / qR[1] : R(0);
         mL[0] *= sL; mL[1] *= sL; mR[0] *= sR; mR[1] *= sR;
         hL = hsL; hR = hsR; bL = bf; bR = bf;
     }
@@ -215,8 +245,8 @@ PORTABLE_FN ZADJ_INLINE void face_rev(const R c[4][4], SweP<R> const& p, const R
             if (hL > R(0)) lhL += lev * g / (R(2) * cL);
         }
     }
-    lhL += lhiL * dhinv(hL, p.eps);
-    lhR += lhiR * dhinv(hR, p.eps);
+    lhL += lhiL * dhinv_r(hL, p.eps);
+    lhR += lhiR * dhinv_r(hR, p.eps);
 
     // hydrostatic reconstruction
     R lqL[4], lqR[4];
@@ -228,8 +258,8 @@ PORTABLE_FN ZADJ_INLINE void face_rev(const R c[4][4], SweP<R> const& p, const R
         lqR[2] = lmR[0] * sR; lqR[3] = lmR[1] * sR;
         R lhsL = lhL, lhsR = lhR;
         lqL[1] = 0; lqR[1] = 0;
-        if (qL[1] > R(0)) { lhsL += lsL / qL[1]; lqL[1] -= lsL * hsL / (qL[1] * qL[1]); }
-        if (qR[1] > R(0)) { lhsR += lsR / qR[1]; lqR[1] -= lsR * hsR / (qR[1] * qR[1]); }
+        if (qL[1] > R(0)) { lhsL += lsL * iqL; lqL[1] -= lsL * sL * iqL; }
+        if (qR[1] > R(0)) { lhsR += lsR * iqR; lqR[1] -= lsR * sR * iqR; }
         const R ltL = (R(0) < tL) ? lhsL : R(0);
         const R ltR = (R(0) < tR) ? lhsR : R(0);
         R lbf = lbL + lbR - ltL - ltR;
@@ -270,10 +300,11 @@ PORTABLE_FN ZADJ_INLINE Manning<R> manning(R h, R mx, R my, R hv, SweP<R> const&
     const R heav = (h - p.hfloor > R(0)) ? R(1) : ((h - p.hfloor < R(0)) ? R(0) : R(0.5));
     M.dk_dh = -M.k * (M.ic * M.ic * M.ic) * R(1.0 / 3.0) * heav;
     const R ux = mx * hv, uy = my * hv;
-    const R sp = std::sqrt(ux * ux + uy * uy);
+    const R s2 = ux * ux + uy * uy;
+    const R rsp = (s2 > R(0)) ? rsqrt_of(s2) : R(0);   // 1 / |u|
+    const R sp = s2 * rsp;                              // |u|
     M.S[0] = p.g * p.ex * h - M.k * ux * sp;
     M.S[1] = p.g * p.ey * h - M.k * uy * sp;
-    const R rsp = (sp > R(0)) ? R(1) / sp : R(0);
     const R dsx = ux * hv * rsp, dsy = uy * hv * rsp;
     M.J[0][0] = -M.k * (hv * sp + ux * dsx);
     M.J[0][1] = -M.k * (ux * dsy);
@@ -314,16 +345,18 @@ PORTABLE_FN ZADJ_INLINE void implicit_rev(R h, R mx, R my, R hv, R dt, SweP<R> c
     const R det = a * d - b * c;
     R dq[2] = {0, 0}, mu[2];
     bool ok = false;
+    R rdet = R(0);
     if (std::fabs(det) > R(0) && std::isfinite(det)) {
         const R r0 = dt * M.S[0], r1 = dt * M.S[1];
-        dq[0] = (r0 * d - b * r1) / det;
-        dq[1] = (a * r1 - c * r0) / det;
+        rdet = R(1) / det;
+        dq[0] = (r0 * d - b * r1) * rdet;
+        dq[1] = (a * r1 - c * r0) * rdet;
         ok = std::isfinite(dq[0]) && std::isfinite(dq[1]);
     }
     if (ok) {
         // A^T mu = lam, A = [[a, b], [c, d]]
-        mu[0] = (lam[0] * d - c * lam[1]) / det;
-        mu[1] = (a * lam[1] - b * lam[0]) / det;
+        mu[0] = (lam[0] * d - c * lam[1]) * rdet;
+        mu[1] = (a * lam[1] - b * lam[0]) * rdet;
     } else {       // explicit fallback: q_out = q* + dt S (dq = 0 in the terms below)
         mu[0] = lam[0]; mu[1] = lam[1];
         dq[0] = dq[1] = R(0);
@@ -333,21 +366,22 @@ PORTABLE_FN ZADJ_INLINE void implicit_rev(R h, R mx, R my, R hv, R dt, SweP<R> c
     // Psi = |u| u + |u| w + u (u.w)/|u|
     const R ux = mx * hv, uy = my * hv;
     const R wx = hv * dq[0], wy = hv * dq[1];
-    const R sp = std::sqrt(ux * ux + uy * uy);
+    const R s2 = ux * ux + uy * uy;
     R Psi[2] = {0, 0}, lu[2] = {0, 0}, lw[2] = {0, 0};
     const R k = M.k;
-    if (sp > R(0)) {
-        const R ex = ux / sp, ey = uy / sp;
+    if (s2 > R(0)) {
+        const R rs = rsqrt_of(s2);          // 1 / |u|
+        const R sp = s2 * rs;
+        const R ex = ux * rs, ey = uy * rs;
         const R uw = ux * wx + uy * wy;
-        Psi[0] = sp * ux + sp * wx + ux * uw / sp;
-        Psi[1] = sp * uy + sp * wy + uy * uw / sp;
+        const R uwr = uw * rs, umr = (ux * mu[0] + uy * mu[1]) * rs;
+        Psi[0] = sp * ux + sp * wx + ux * uwr;
+        Psi[1] = sp * uy + sp * wy + uy * uwr;
         const R umu = ux * mu[0] + uy * mu[1];
         const R wmu = wx * mu[0] + wy * mu[1];
         // (dPsi/du)^T mu
-        const R gu0 = sp * mu[0] + ex * umu + ex * wmu + uw / sp * mu[0] + wx * umu / sp
-                      - ex * uw * umu / (sp * sp);
-        const R gu1 = sp * mu[1] + ey * umu + ey * wmu + uw / sp * mu[1] + wy * umu / sp
-                      - ey * uw * umu / (sp * sp);
+        const R gu0 = sp * mu[0] + ex * umu + ex * wmu + uwr * mu[0] + wx * umr - ex * uwr * umr;
+        const R gu1 = sp * mu[1] + ey * umu + ey * wmu + uwr * mu[1] + wy * umr - ey * uwr * umr;
         // (dPsi/dw)^T mu = (|u| I + u e^T)^T mu
         const R gw0 = sp * mu[0] + ex * umu;
         const R gw1 = sp * mu[1] + ey * umu;

@@ -20,9 +20,10 @@ constexpr int kDtBlocks = 592;   // 4 x 148 SMs
 // over NT threads) and occupancy. 32 x 8 with 256 threads and two blocks per
 // SM runs 3 face rounds per cell (632 faces); 32 x 6 with 256 threads runs
 // 2.67 (498 faces in two rounds); 32 x 13 with 512 threads 2.46 (967 faces)
-// at one block per SM.
+// at one block per SM. Default: 32 x 13 x 512, the fastest measured at 1024^2
+// (backward of 200 steps 179 ms against 187 for 32 x 8 x 256).
 constexpr int kAdjVariants = 7;
-std::atomic<int> g_adj_variant{2};
+std::atomic<int> g_adj_variant{6};
 
 template <class F>
 int with_adj_variant(int v, F&& f) {
