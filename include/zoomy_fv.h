@@ -319,16 +319,21 @@ int zfv_amr_fill(const zfv_amr_level* fine, const zfv_amr_level* coarse, const i
 int zfv_amr_average_down(const zfv_amr_level* fine, const zfv_amr_level* coarse, const int* patches, int n_patches,
                          int max_blocks, void* stream);
 /* flags[by * nbx + bx] = 1 (others untouched) for the blocks of the listed
- * patches with a cell where |grad eta| > threshold. */
+ * patches with a tagged cell. criterion 0: |grad eta| > threshold;
+ * criterion 1: the reference's ErrorEst (ZoomyAmr.cpp:224-252): b < b_max
+ * and (undivided |(h(i+1)-h(i-1), h(j+1)-h(j-1))| > threshold or h > 1e-2). */
 int zfv_amr_tag(const zfv_amr_level* level, const int* patches, int n_patches, int max_blocks, double dx, double dy,
-                double threshold, int* flags, void* stream);
+                double threshold, int criterion, double b_max, int* flags, void* stream);
 /* dt_0 = the largest step whose dt_0 / 2^l every level's CFL law allows (from
- * each level's last CFL maximum), clamped to [dtmin, dtmax]; writes dt_0 / 2^l
- * into level l's per-instance dt array (device) and adds dt_0 to *time
- * (device, may be NULL). level_descs: zfv_batch_descriptors() of each level.
- * Enqueued; no synchronization (a coarse step can be captured in a graph). */
+ * each level's last CFL maximum), clamped to [dtmin, dtmax] and then to land
+ * on time_end (0 once *time >= time_end, ZoomyAmr.cpp:746-749); writes
+ * dt_0 / 2^l into level l's per-instance dt array (device) and adds dt_0 to
+ * *time (device; NULL: no time, no time_end clamp). level_descs:
+ * zfv_batch_descriptors() of each level. Enqueued; no synchronization (a
+ * coarse step can be captured in a graph). */
 int zfv_amr_set_dt(const void* const* level_descs, double* const* dts, const int* n_inst, int n_levels,
-                   double cfl, double cfl_divisor, double dtmin, double dtmax, double* time, void* stream);
+                   double cfl, double cfl_divisor, double dtmin, double dtmax, double time_end, double* time,
+                   void* stream);
 /* Fill freshly created patches from the old patches of the level (where
  * present) or from the coarser level. */
 int zfv_amr_regrid_fill(const zfv_amr_level* level, const zfv_amr_level* old_level, const zfv_amr_level* coarse,

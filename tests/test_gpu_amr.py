@@ -122,3 +122,29 @@ def test_amr_graph_replay_equals_eager_launches(cuda):
     assert ta == tb and ba == bb
     for a, b in zip(qa, qb):
         assert np.array_equal(np.nan_to_num(a, nan=-7.0), np.nan_to_num(b, nan=-7.0))
+
+
+def test_amr_reference_tagging_and_time_end(cuda):
+    """The reference's ErrorEst criterion (undivided |grad h| or h > 1e-2, gated
+    by b < b_max) refines every wet block of the dam break, a b_max below every
+    bed value refines nothing; evolve() lands on time_end like
+    ZoomyAmr::TimeStep."""
+    from zoomy_amrex_b200.amr import AmrHierarchy
+    nx, ny, L = 128, 128, 50.0
+    Q0 = _fields(nx, ny, L)
+    cfg = _cfg(nx, ny, L)
+    cfg.time_end = 0.05
+    full = AmrHierarchy(cfg, Q0, max_level=1, B=32, threshold=0.01, tag="reference")
+    gated = AmrHierarchy(cfg, Q0, max_level=1, B=32, threshold=0.01, tag="reference",
+                         tag_b_max=float(Q0[0].min()))
+    n_full, n_gated = full.levels[1].n, len(gated.levels) - 1
+    steps = full.evolve()
+    t = full.time
+    q = full.level_state(1)
+    full.close()
+    gated.close()
+    print(f"[amr reference tags] level-1 blocks {n_full}, {steps} steps to t = {t!r}")
+    assert n_full == (2 * nx // 32) * (2 * ny // 32)     # every wet block, refined with full nesting
+    assert n_gated == 0
+    assert abs(t - 0.05) < 1e-12
+    assert np.isfinite(q[~np.isnan(q)]).all()

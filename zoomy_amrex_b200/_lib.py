@@ -96,9 +96,9 @@ def lib():
     lv = C.POINTER(zfv_amr_level)
     L.zfv_amr_fill.argtypes = [lv, lv, vp, vp, i, i, i, vp]
     L.zfv_amr_average_down.argtypes = [lv, lv, vp, i, i, vp]
-    L.zfv_amr_tag.argtypes = [lv, vp, i, i, d, d, d, vp, vp]
+    L.zfv_amr_tag.argtypes = [lv, vp, i, i, d, d, d, i, d, vp, vp]
     L.zfv_amr_regrid_fill.argtypes = [lv, lv, lv, vp, i, i, vp]
-    L.zfv_amr_set_dt.argtypes = [pp, pp, C.POINTER(i), i, d, d, d, d, vp, vp]
+    L.zfv_amr_set_dt.argtypes = [pp, pp, C.POINTER(i), i, d, d, d, d, d, vp, vp]
     _lib = L
     return L
 

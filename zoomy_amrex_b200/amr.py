@@ -2,7 +2,9 @@
 
 The reference's AmrCore driver (ZoomyAmr.cpp:161-288, 733-762): a base level
 plus up to ``max_level`` refined levels (ratio 2), tagging by an eta-gradient
-threshold (ErrorEst), regridding, per-stage ghost filling from the same level
+threshold or by the reference's ErrorEst criterion (``tag="reference"``:
+undivided |grad h| > threshold or h > 1e-2, below ``tag_b_max``), regridding,
+per-stage ghost filling from the same level
 or the coarser one (FillPatch / FillPatchTwoLevels with conservative linear
 interpolation), subcycling (a level-l step is followed by two level-(l+1)
 steps), and averaging the fine solution down onto the coarse level after them.
@@ -121,8 +123,11 @@ class AmrHierarchy:
     ``threshold`` refines everywhere the nesting allows).
     """
 
+    TAGS = {"eta_gradient": 0, "reference": 1}
+
     def __init__(self, cfg: zfv_config, Q0, max_level: int = 2, B: int = 64, threshold: float = 0.01,
-                 regrid_int: int = 2, device="cuda:0", variant: int = 5, patch_blocks: int = 16):
+                 regrid_int: int = 2, device="cuda:0", variant: int = 5, patch_blocks: int = 16,
+                 tag: str = "eta_gradient", tag_b_max: float = 1.0e30):
         if cfg.nx % B or cfg.ny % B or B % 2:
             raise ValueError("the base grid must be a multiple of the (even) box side B in both directions")
         self.cfg = _cfg_copy(cfg)
@@ -132,6 +137,9 @@ class AmrHierarchy:
         self.variant = variant
         if not 1 <= patch_blocks <= 256:
             raise ValueError("patch_blocks must be in 1 .. 256")
+        if tag not in self.TAGS:
+            raise ValueError(f"tag must be one of {sorted(self.TAGS)}")
+        self.criterion, self.tag_b_max = self.TAGS[tag], float(tag_b_max)
         self.patch_blocks = patch_blocks
         self.nbx0, self.nby0 = cfg.nx // B, cfg.ny // B
         self.lo = (cfg.prob_lo[0], cfg.prob_lo[1])
@@ -180,8 +188,8 @@ class AmrHierarchy:
         with torch.cuda.stream(self.stream):
             flags = torch.zeros((L.nby, L.nbx), dtype=torch.int32, device=self.device)
             _lib.check(_lib.lib().zfv_amr_tag(C.byref(L.view), L.pdesc.data_ptr(), L.n_patches, L.max_blocks,
-                                              L.dx, L.dy, self.threshold, flags.data_ptr(), self._s()),
-                       "zfv_amr_tag")
+                                              L.dx, L.dy, self.threshold, self.criterion, self.tag_b_max,
+                                              flags.data_ptr(), self._s()), "zfv_amr_tag")
         self.sync()
         return flags.cpu().numpy() != 0
 
@@ -268,7 +276,7 @@ class AmrHierarchy:
         dts = (C.c_void_p * n)(*[L.dts.data_ptr() for L in self.levels])
         cnt = (C.c_int * n)(*[L.n_patches for L in self.levels])
         c = self.cfg
-        _lib.check(_lib.lib().zfv_amr_set_dt(descs, dts, cnt, n, c.cfl, self.div, c.dtmin, c.dtmax,
+        _lib.check(_lib.lib().zfv_amr_set_dt(descs, dts, cnt, n, c.cfl, self.div, c.dtmin, c.dtmax, c.time_end,
                                              self._time.data_ptr(), self._s()), "zfv_amr_set_dt")
 
     def _advance(self, lev: int):
@@ -319,6 +327,17 @@ class AmrHierarchy:
         for _ in range(n_steps):
             self.step()
         self.sync()
+
+    def evolve(self, check_every: int = 16) -> int:
+        """Coarse steps until the configuration's time_end (the last dt_0 lands
+        on it) or max_step, like ZoomyAmr::Evolve; returns the steps taken.
+        The time is read every ``check_every`` steps; steps past time_end have
+        dt_0 = 0 and change nothing."""
+        c = self.cfg
+        while (c.max_step < 0 or self.steps < c.max_step) and self.time < c.time_end:
+            n = check_every if c.max_step < 0 else min(check_every, c.max_step - self.steps)
+            self.run(n)
+        return self.steps
 
     # -- output ----------------------------------------------------------------------------
     def cells_per_coarse_step(self) -> int:

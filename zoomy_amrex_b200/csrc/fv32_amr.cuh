@@ -181,11 +181,13 @@ __global__ void k32a_average_down(LevelView F, LevelView C, const int4* __restri
     }
 }
 
-// flags[by * nbx + bx] = 1 (others untouched) for blocks with a cell where
-// |grad eta| > threshold (centred differences over the level's own cells;
-// the reference's ErrorEst flags |grad h| or h > 1e-2, ZoomyAmr.cpp:224-252).
+// flags[by * nbx + bx] = 1 (others untouched) for blocks with a tagged cell.
+// criterion 0: |grad eta| > threshold (centred differences per unit length);
+// criterion 1: the reference's ErrorEst (ZoomyAmr.cpp:224-252): cells with
+// b < b_max whose undivided |(h(i+1) - h(i-1), h(j+1) - h(j-1))| exceeds the
+// threshold, or with h > 1e-2.
 __global__ void k32a_tag(LevelView V, const int4* __restrict__ patches, int n_patches, float dx, float dy,
-                         float threshold, int* __restrict__ flags) {
+                         float threshold, int criterion, float b_max, int* __restrict__ flags) {
     const int pi = blockIdx.y;
     if (pi >= n_patches) return;
     const int B = V.B;
@@ -198,8 +200,18 @@ __global__ void k32a_tag(LevelView V, const int4* __restrict__ patches, int n_pa
         if (!lookup(V, I - 1, J, false, xm) || !lookup(V, I + 1, J, false, xp) ||
             !lookup(V, I, J - 1, false, ym) || !lookup(V, I, J + 1, false, yp))
             continue;
-        const float gx = (xp.e - xm.e) / (2.0f * dx), gy = (yp.e - ym.e) / (2.0f * dy);
-        if (gx * gx + gy * gy > threshold * threshold) flags[p.y * V.nbx + p.x + i / B] = 1;
+        bool hit;
+        if (criterion == 0) {
+            const float gx = (xp.e - xm.e) / (2.0f * dx), gy = (yp.e - ym.e) / (2.0f * dy);
+            hit = gx * gx + gy * gy > threshold * threshold;
+        } else {
+            C4 c;
+            lookup(V, I, J, false, c);
+            if (c.b >= b_max) continue;
+            const float hx = (xp.e - xp.b) - (xm.e - xm.b), hy = (yp.e - yp.b) - (ym.e - ym.b);
+            hit = sqrtf(hx * hx + hy * hy) > threshold || (c.e - c.b) > 1.0e-2f;
+        }
+        if (hit) flags[p.y * V.nbx + p.x + i / B] = 1;
     }
 }
 
@@ -246,15 +258,16 @@ __global__ void k32a_regrid_fill(LevelView N, LevelView O, LevelView C, const in
 // dt_0 of the hierarchy from every level's last CFL maximum (the largest
 // step whose dt_0 / 2^l every level's CFL law allows, ZoomyAmr.cpp:448-515),
 // written as dt_0 / 2^l into each level's per-instance dt array, and the
-// hierarchy time advanced by dt_0. One block; no host round trip, so a coarse
-// step can be replayed from a CUDA graph.
+// hierarchy time advanced by dt_0 (dt_0 clamped to land on time_end; zero
+// once time_end is reached). One block; no host round trip, so a coarse step
+// can be replayed from a CUDA graph.
 constexpr int kMaxLevels = 8;
 struct DtArgs {
     const BInst* lev[kMaxLevels];
     double* dts[kMaxLevels];
     int n_inst[kMaxLevels];
     int n_levels;
-    double cfl, div, dtmin, dtmax;
+    double cfl, div, dtmin, dtmax, time_end;
     double* time;
 };
 
@@ -267,8 +280,13 @@ __global__ void k32a_set_dt(DtArgs a) {
             if (m > 1e-14) dt0 = fmin(dt0, double(1 << l) * (a.cfl / (a.div * m)));
         }
         dt0 = fmax(dt0, a.dtmin);
+        if (a.time) {
+            // land on time_end (ZoomyAmr.cpp:746-749); past it, steps are no-ops
+            const double remaining = a.time_end - *a.time;
+            dt0 = remaining > 0.0 ? fmin(dt0, remaining) : 0.0;
+            *a.time += dt0;
+        }
         s_dt0 = dt0;
-        if (a.time) *a.time += dt0;
     }
     __syncthreads();
     for (int l = 0; l < a.n_levels; ++l) {

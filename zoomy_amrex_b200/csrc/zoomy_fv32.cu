@@ -589,19 +589,22 @@ int zfv_amr_average_down(const zfv_amr_level* fine, const zfv_amr_level* coarse,
 }
 
 int zfv_amr_tag(const zfv_amr_level* level, const int* patches, int n_patches, int max_blocks, double dx, double dy,
-                double threshold, int* flags, void* stream) {
+                double threshold, int criterion, double b_max, int* flags, void* stream) {
     if (!level || !patches || !flags) return fail(-1, "zfv_amr_tag: null argument");
+    if (criterion != 0 && criterion != 1) return fail(-1, "zfv_amr_tag: criterion must be 0 or 1");
     dim3 g;
     const long long B = level->B;
     int rc = amr_grid(n_patches, max_blocks, (long long)max_blocks * B * B, g);
     if (rc) return rc;
     zfv32::amr::k32a_tag<<<g, 256, 0, (cudaStream_t)stream>>>(view_of(level), reinterpret_cast<const int4*>(patches),
-                                                            n_patches, float(dx), float(dy), float(threshold), flags);
+                                                            n_patches, float(dx), float(dy), float(threshold),
+                                                            criterion, float(fmin(b_max, 3.0e38)), flags);
     return cuda_check(cudaGetLastError(), "zfv_amr_tag launch");
 }
 
 int zfv_amr_set_dt(const void* const* level_descs, double* const* dts, const int* n_inst, int n_levels,
-                   double cfl, double cfl_divisor, double dtmin, double dtmax, double* time, void* stream) {
+                   double cfl, double cfl_divisor, double dtmin, double dtmax, double time_end, double* time,
+                   void* stream) {
     if (!level_descs || !dts || !n_inst) return fail(-1, "zfv_amr_set_dt: null argument");
     if (n_levels < 1 || n_levels > zfv32::amr::kMaxLevels)
         return fail(-1, "zfv_amr_set_dt: %d levels (1 .. %d)", n_levels, zfv32::amr::kMaxLevels);
@@ -612,7 +615,7 @@ int zfv_amr_set_dt(const void* const* level_descs, double* const* dts, const int
         a.n_inst[l] = n_inst[l];
     }
     a.n_levels = n_levels;
-    a.cfl = cfl; a.div = cfl_divisor; a.dtmin = dtmin; a.dtmax = dtmax;
+    a.cfl = cfl; a.div = cfl_divisor; a.dtmin = dtmin; a.dtmax = dtmax; a.time_end = time_end;
     a.time = time;
     zfv32::amr::k32a_set_dt<<<1, 256, 0, (cudaStream_t)stream>>>(a);
     return cuda_check(cudaGetLastError(), "zfv_amr_set_dt launch");
