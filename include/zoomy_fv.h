@@ -78,6 +78,9 @@ typedef struct zfv_config {
     int implicit_source;    /* solver.implicit_source: point-implicit source after each stage */
     int clamp_positivity;   /* solver.clamp_positivity: h<0 -> 0 in UpdateState    */
     int positivity_mood;    /* solver.positivity == "mood": whole-step order-1 redo */
+    int implicit_global;    /* solver.implicit_global: with implicit_source, the source
+                               is solved for the whole field by Jacobian-free
+                               Newton-Krylov (imex_solver.H) instead of per cell */
     double cfl;             /* solver.cfl (pure safety factor)                      */
     double dtmin, dtmax;    /* solver.dtmin / solver.dtmax                          */
     double time_end;        /* solver.time_end                                      */

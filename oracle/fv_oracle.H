@@ -264,6 +264,59 @@ struct OracleKernels {
 // ---------------------------------------------------------------------------
 // Restatement of the single-level driver in Source/ZoomyAmr.cpp.
 // ---------------------------------------------------------------------------
+// solver.implicit_global (imex_solver.H:102-160) solves
+// F(Q) = Q - Qexp - dt S(Q) = 0 for the whole field by Jacobian-free
+// Newton-Krylov, with S evaluated on aux refreshed from the state
+// (ComputeSourceField, :21-58). For a cell-local source that system is one
+// small system per cell; this solves each one exactly (Newton with the
+// model's analytic source Jacobian, to round-off): the answer the field solve
+// approaches within its stopping rule (|F| < 1e-9 |F_0|).
+template <class Model, class A4, class VP, class VX>
+void implicit_source_exact(int i, int j, A4 const& Q, Real dt, VP const& p, Real time, VX const& X) {
+    constexpr int nq = Model::n_dof_q;
+    using VQ = amrex::SmallMatrix<Real, nq, 1>;
+    using VA = amrex::SmallMatrix<Real, Model::n_dof_qaux, 1>;
+    VQ qe, q;
+    for (int n = 0; n < nq; ++n) qe(n, 0) = q(n, 0) = Q(i, j, 0, n);
+    for (int it = 0; it < 50; ++it) {
+        VA a;
+        for (int n = 0; n < Model::n_dof_qaux; ++n) a(n, 0) = 0.0;
+        a = Model::update_aux_variables(q, a, p, time, X);
+        const auto S = Model::source(q, a, p, time, X);
+        const auto JQ = Model::source_jacobian_wrt_variables(q, a, p);
+        Real M[nq][nq], b[nq], fmax = 0.0, qmax = 0.0;
+        for (int r = 0; r < nq; ++r) {
+            b[r] = -((q(r, 0) - qe(r, 0)) - dt * S(r, 0));
+            fmax = std::max(fmax, std::abs(b[r]));
+            qmax = std::max(qmax, std::abs(q(r, 0)));
+            for (int c = 0; c < nq; ++c) M[r][c] = (r == c ? 1.0 : 0.0) - dt * JQ(r * nq + c, 0);
+        }
+        if (!(fmax > 1e-16 * (1.0 + qmax))) break;
+        for (int k = 0; k < nq; ++k) {      // Gaussian elimination, partial pivoting
+            int piv = k;
+            for (int r = k + 1; r < nq; ++r)
+                if (std::abs(M[r][k]) > std::abs(M[piv][k])) piv = r;
+            if (!(std::abs(M[piv][k]) > 0.0)) return;
+            if (piv != k) {
+                for (int c = k; c < nq; ++c) std::swap(M[k][c], M[piv][c]);
+                std::swap(b[k], b[piv]);
+            }
+            for (int r = k + 1; r < nq; ++r) {
+                const Real f = M[r][k] / M[k][k];
+                for (int c = k; c < nq; ++c) M[r][c] -= f * M[k][c];
+                b[r] -= f * b[k];
+            }
+        }
+        for (int r = nq - 1; r >= 0; --r) {
+            Real t = b[r];
+            for (int c = r + 1; c < nq; ++c) t -= M[r][c] * b[c];
+            b[r] = t / M[r][r];
+        }
+        for (int n = 0; n < nq; ++n) q(n, 0) += b[n];
+    }
+    for (int n = 0; n < nq; ++n) Q(i, j, 0, n) = q(n, 0);
+}
+
 struct StepLog { Real dt, time, mass; };
 
 template <class Model, class Numerics, class K>
@@ -479,7 +532,11 @@ struct Level {
         for (int j = 0; j < ny; ++j)
             for (int i = 0; i < nx; ++i)
                 for (int n = 0; n < nq; ++n) q4(i, j, 0, n) += dt * r4(i, j, 0, n);
-        if (cfg.implicit_source) {
+        if (cfg.implicit_source && cfg.implicit_global) {
+#pragma omp parallel for schedule(static)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) implicit_source_exact<Model>(i, j, q4, dt, p, t, centre(i, j));
+        } else if (cfg.implicit_source) {
             amrex::Array4<const Real> ac(a4);
 #pragma omp parallel for schedule(static)
             for (int j = 0; j < ny; ++j)

@@ -78,3 +78,26 @@ def test_oracle_equals_reference_make_rhs(oracle, ref_oracle, name):
     a = oracle.run(cfg, Q0, A0)
     b = ref_oracle.run(cfg, Q0, A0)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+
+
+def test_oracle_implicit_global_solves_backward_euler(oracle):
+    """The oracle's implicit_global path solves q = q_exp + dt S(q) per cell:
+    without a source term it equals the point-implicit path bitwise; with
+    Manning friction it differs from the one linearised step by O(dt^2)."""
+    from zoomy_amrex_b200._abi import ZFV_MODEL_SWE2D, make_config
+    nx, ny = 24, 20
+    x = (np.arange(nx) + 0.5) / nx * 5.0
+    X, Y = np.meshgrid(x, (np.arange(ny) + 0.5) / ny * 5.0)
+    h = 1.0 + 0.2 * np.exp(-((X - 2.5) ** 2 + (Y - 2.0) ** 2))
+    Q0 = np.array([0 * h, h, 0.5 * h, -0.2 * h])
+    A0 = np.zeros((7, ny, nx))
+    out = {}
+    for n_m in (0.0, 0.05):
+        for glob in (False, True):
+            cfg = make_config(ZFV_MODEL_SWE2D, nx, ny, (0, 0), (5, 5), spatial_order=2, implicit_source=True,
+                              implicit_global=glob, cfl=0.45, time_end=1e30, max_step=6,
+                              params={"n_m": n_m})
+            out[(n_m, glob)] = oracle.run(cfg, Q0, A0)[0]
+    assert np.array_equal(out[(0.0, False)], out[(0.0, True)])
+    d = np.abs(out[(0.05, True)] - out[(0.05, False)]).max()
+    assert 0.0 < d < 1e-4

@@ -47,6 +47,7 @@ class zfv_config(C.Structure):
         ("implicit_source", C.c_int),
         ("clamp_positivity", C.c_int),
         ("positivity_mood", C.c_int),
+        ("implicit_global", C.c_int),
         ("cfl", C.c_double),
         ("dtmin", C.c_double),
         ("dtmax", C.c_double),
@@ -84,14 +85,17 @@ def make_config(model: int, nx: int, ny: int, prob_lo, prob_hi, *, spatial_order
                 dtmin: float = 1.0e-7, dtmax: float = 1.0, time_end: float = 1.0,
                 max_step: int = -1, cfl_dimension: int | None = None,
                 cfl_degree_factor: int | None = None, bc=("extrapolation",) * 4,
-                params: dict | None = None, precision: int = ZFV_PREC_FP64) -> zfv_config:
+                params: dict | None = None, precision: int = ZFV_PREC_FP64,
+                implicit_global: bool = False) -> zfv_config:
     """Build a zfv_config the way the reference's deck + MarchConstants.H define it.
 
     ``bc`` names the boundary tag per side (x_lo, x_hi, y_lo, y_hi); each name
     is resolved against the model's sorted tag list, and an unknown non-empty
     name is an error (ZoomyAmr.cpp:361-372). ``cfl_dimension`` defaults to the
     model dimension d and ``cfl_degree_factor`` to 2k+1 with k = order - 1
-    (zoomy_amrex/_constants.py:8-13, run_case.py:391-395).
+    (zoomy_amrex/_constants.py:8-13, run_case.py:391-395). ``implicit_global``
+    (solver.implicit_global, ZoomyAmr.cpp:48) solves the implicit source for
+    the whole field by Jacobian-free Newton-Krylov.
     """
     info = MODELS[model]
     if positivity not in ("none", "mood"):
@@ -109,6 +113,7 @@ def make_config(model: int, nx: int, ny: int, prob_lo, prob_hi, *, spatial_order
     c.implicit_source = int(bool(implicit_source))
     c.clamp_positivity = int(bool(clamp_positivity))
     c.positivity_mood = int(positivity == "mood")
+    c.implicit_global = int(bool(implicit_global))
     c.cfl, c.dtmin, c.dtmax, c.time_end = float(cfl), float(dtmin), float(dtmax), float(time_end)
     c.max_step = int(max_step)
     c.cfl_dimension = int(info["dimension"] if cfl_dimension is None else cfl_dimension)

@@ -32,7 +32,10 @@ enum StageMode : int {
     // positivity = "mood" (ZoomyAmr.cpp:685-720):
     MODE_S2M = 4,   // stage 2 writing the Heun candidate to a buffer and flagging troubled cells
     MODE_R1 = 5,    // order-1 redo, stage 1 (runs only when the step is troubled)
-    MODE_R2 = 6     // order-1 redo, stage 2 + final UpdateState + reduction (troubled only)
+    MODE_R2 = 6,    // order-1 redo, stage 2 + final UpdateState + reduction (troubled only)
+    // solver.implicit_global (imex_solver.H): the stage state after the flux
+    // update, before any source; the global Newton-Krylov solve follows
+    MODE_X = 7
 };
 
 // Face records in shared memory hold make_rhs.H:310-315's components
@@ -367,8 +370,8 @@ k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
 #pragma unroll
                 for (int n = n0; n < nq; ++n) qstar[(n - n0) * plane + c] = q(n, 0);
             }
-            if constexpr (IMPL) implicit_source_cell<Model, R>(q, ac, dt, p, time, X);
-            if constexpr (MODE == MODE_S1 || MODE == MODE_R1) {
+            if constexpr (IMPL && MODE != MODE_X) implicit_source_cell<Model, R>(q, ac, dt, p, time, X);
+            if constexpr (MODE == MODE_S1 || MODE == MODE_R1 || MODE == MODE_X) {
 #pragma unroll
                 for (int n = (sbed ? 1 : 0); n < nq; ++n) qout[n * plane + c] = q(n, 0);
             } else if constexpr (MODE == MODE_S2M) {

@@ -20,6 +20,7 @@
 #include "zfv_internal.H"
 #include "swe.H"
 #include "fv_kernels.cuh"
+#include "fv_jfnk.cuh"
 
 namespace zfvi {
 
@@ -86,12 +87,17 @@ struct RunnerT final : Runner {
         S.log = S.partials + align_up(sizeof(double) * 2 * nblk);
         S.stage = S.log + align_up(sizeof(double) * 3 * kLogCap);
         S.lo = 0;
-        if (mood()) {   // second stage buffer for the MOOD candidate
+        S.jfnk = 0;
+        if (mood() || jfnk()) {   // second stage buffer: the MOOD candidate / the stage-2 Newton state
             S.alt = S.stage + align_up(plane_bytes * nq);
             S.total = S.alt + align_up(plane_bytes * nq);
         } else {
             S.alt = 0;
             S.total = S.stage + align_up(plane_bytes * nq);
+        }
+        if (jfnk()) {
+            S.jfnk = S.total;
+            S.total += jfnk_bytes();
         }
     }
 
@@ -122,6 +128,7 @@ struct RunnerT final : Runner {
     template <int ORDER, bool WB, bool IMPL>
     int setup_combo() {
         int rc = 0;
+        if constexpr (IMPL) rc |= set_smem<ORDER, zfv::MODE_X, WB, IMPL>();
         rc |= set_smem<ORDER, zfv::MODE_RHS, WB, IMPL>();
         if constexpr (ORDER == 2) {
             rc |= set_smem<ORDER, zfv::MODE_S1, WB, IMPL>();
@@ -243,12 +250,250 @@ struct RunnerT final : Runner {
         double* Q = (double*)Qv;
         double* Q1 = stage(scratch);
         const bool sbed = zfv::static_bed<Model>::value;
-        int rc = with_combo(EvolveF{this, Q, Q1, scratch, n, s, sbed});
+        int rc = jfnk() ? with_combo(JfnkEvolveF{this, Q, scratch, n, s})
+                        : with_combo(EvolveF{this, Q, Q1, scratch, n, s, sbed});
         if (rc) return rc;
         const int nb = int((L.plane + 255) / 256);
         zfv::k_aux_from_state<Model><<<nb, 256, 0, s>>>(Q, (double*)Av, L, st(scratch));
         return cuda_check(cudaGetLastError(), "zfv_evolve aux launch");
     }
+
+    // -- global implicit source (solver.implicit_global, imex_solver.H) ---------
+    // Newton: at most 12 iterations, stop at |F| < 1e-12 or |F| < 1e-9 |F_0|,
+    // linear tolerance 1e-4 relative (imex_solver.H:124-140). GMRES: restarted
+    // every 30 iterations, at most 40 iterations per solve, classical
+    // Gram-Schmidt applied twice, Givens rotations on the host.
+    static constexpr int n0 = zfv::static_bed<Model>::value ? 1 : 0;
+    static constexpr int kNewtonMax = 12;
+    static constexpr int kRestart = 30;
+    static constexpr int kMaxIter = 40;
+    static_assert(kRestart + 1 <= zfv::jfnk::kMaxDots, "Krylov basis larger than one multi-dot launch");
+
+    bool jfnk() const { return h->cfg.implicit_source && h->cfg.implicit_global; }
+    long long jN() const { return (long long)(nq - n0) * L.plane; }
+    int jvec_blocks() const {
+        const long long b = (jN() + zfv::jfnk::kNT - 1) / zfv::jfnk::kNT;
+        return int(std::min<long long>(b, kReduceBlocksMax));
+    }
+    int jcell_blocks() const { return int((L.plane + zfv::jfnk::kNT - 1) / zfv::jfnk::kNT); }
+    size_t jpart_elems() const {
+        return std::max<size_t>(size_t(jcell_blocks()), size_t(zfv::jfnk::kMaxDots) * jvec_blocks());
+    }
+    size_t jvec_bytes() const { return align_up(size_t(jN()) * sizeof(double)); }
+    size_t jfnk_bytes() const {
+        return jvec_bytes() * (5 + kRestart + 1) + align_up(jpart_elems() * sizeof(double)) +
+               align_up(zfv::jfnk::kMaxDots * sizeof(double));
+    }
+    struct JW {
+        double *qexp, *S, *F, *x, *w, *V, *part, *out;
+    };
+    JW jwork(char* scratch) const {
+        const size_t vb = jvec_bytes();
+        char* b = scratch + h->lay.jfnk;
+        JW W;
+        W.qexp = (double*)(b);
+        W.S = (double*)(b + vb);
+        W.F = (double*)(b + 2 * vb);
+        W.x = (double*)(b + 3 * vb);
+        W.w = (double*)(b + 4 * vb);
+        W.V = (double*)(b + 5 * vb);
+        W.part = (double*)(b + (5 + kRestart + 1) * vb);
+        W.out = (double*)(b + (5 + kRestart + 1) * vb + align_up(jpart_elems() * sizeof(double)));
+        return W;
+    }
+    long long jstride() const { return (long long)(jvec_bytes() / sizeof(double)); }
+
+    // host[k] = w . V_k for k < nv (synchronizes the stream).
+    int jdots(const JW& W, const double* w, const double* V, long long vstride, int nv, long long n,
+              double* host, cudaStream_t s) {
+        const int nb = jvec_blocks();
+        zfv::jfnk::k_dots<<<dim3(nb, nv), zfv::jfnk::kNT, 0, s>>>(w, V, vstride, n, W.part);
+        zfv::jfnk::k_sum_partials<<<nv, zfv::jfnk::kNT, 0, s>>>(W.part, nb, W.out);
+        int rc = cuda_check(cudaMemcpyAsync(host, W.out, sizeof(double) * nv, cudaMemcpyDeviceToHost, s),
+                            "implicit_global dot read-back");
+        if (!rc) rc = cuda_check(cudaStreamSynchronize(s), "implicit_global dot");
+        return rc;
+    }
+    void jcombine(double* y, double a, const double* V, int nv, const double* c, cudaStream_t s) {
+        zfv::jfnk::Coefs cf{};
+        for (int k = 0; k < nv; ++k) cf.c[k] = c[k];
+        zfv::jfnk::k_combine<<<jvec_blocks(), zfv::jfnk::kNT, 0, s>>>(y, a, V, jstride(), nv, cf, jN());
+    }
+    void jscale(double* dst, const double* src, double f, cudaStream_t s) {
+        zfv::jfnk::k_scale<<<jvec_blocks(), zfv::jfnk::kNT, 0, s>>>(dst, src, f, jN());
+    }
+    // Ax = J x at Qv (ImpSrcOp::apply): eps = 1e-7 (1 + |Q|) / |x|
+    void jjvp(const double* Qv, const double* qbed, const JW& W, const zfv::DevState* state, const double* x,
+              double xnorm, double nrmQ, double* Ax, cudaStream_t s) {
+        if (xnorm == 0.0) {
+            cudaMemsetAsync(Ax, 0, sizeof(double) * jN(), s);
+            return;
+        }
+        const double eps = 1e-7 * (1.0 + nrmQ) / xnorm;
+        zfv::jfnk::k_jvp<Model><<<jcell_blocks(), zfv::jfnk::kNT, 0, s>>>(Qv, qbed, W.S, x, eps, Ax, L, state);
+    }
+
+    // GMRES on J x = b from x = 0 (x, b: vectors; J at the Newton iterate Qv
+    // with S(Qv) in W.S).
+    int jgmres(const double* Qv, const double* qbed, const JW& W, const zfv::DevState* state, const double* b,
+               double* x, double nrmQ, double rtol, cudaStream_t s) {
+        const long long N = jN(), vs = jstride();
+        double beta;
+        int rc = jdots(W, b, b, 0, 1, N, &beta, s);
+        if (rc) return rc;
+        beta = std::sqrt(beta);
+        if (!(beta > 0.0)) return 0;
+        const double target = rtol * beta;
+        double H[kRestart + 1][kRestart], cs[kRestart], sn[kRestart], g[kRestart + 1], hcol[kRestart + 1],
+            h2[kRestart + 1], y[kRestart];
+        int iters = 0;
+        jscale(W.V, b, 1.0 / beta, s);                      // V_0 = r / beta, r = b
+        for (;;) {
+            for (int k = 0; k <= kRestart; ++k) g[k] = 0.0;
+            g[0] = beta;
+            int kdim = 0;
+            double res = beta;
+            for (int j = 0; j < kRestart && iters < kMaxIter; ++j) {
+                double* Vj = W.V + j * vs;
+                jjvp(Qv, qbed, W, state, Vj, 1.0, nrmQ, W.w, s);   // |V_j| = 1
+                rc = jdots(W, W.w, W.V, vs, j + 1, N, hcol, s);
+                if (rc) return rc;
+                for (int k = 0; k <= j; ++k) hcol[k] = -hcol[k];
+                jcombine(W.w, 1.0, W.V, j + 1, hcol, s);
+                rc = jdots(W, W.w, W.V, vs, j + 1, N, h2, s);
+                if (rc) return rc;
+                for (int k = 0; k <= j; ++k) { hcol[k] = -hcol[k] + h2[k]; h2[k] = -h2[k]; }
+                jcombine(W.w, 1.0, W.V, j + 1, h2, s);
+                double hn;
+                rc = jdots(W, W.w, W.w, 0, 1, N, &hn, s);
+                if (rc) return rc;
+                hn = std::sqrt(hn);
+                for (int k = 0; k <= j; ++k) H[k][j] = hcol[k];
+                H[j + 1][j] = hn;
+                for (int k = 0; k < j; ++k) {              // previous rotations
+                    const double t = cs[k] * H[k][j] + sn[k] * H[k + 1][j];
+                    H[k + 1][j] = -sn[k] * H[k][j] + cs[k] * H[k + 1][j];
+                    H[k][j] = t;
+                }
+                const double den = std::hypot(H[j][j], H[j + 1][j]);
+                cs[j] = den > 0.0 ? H[j][j] / den : 1.0;
+                sn[j] = den > 0.0 ? H[j + 1][j] / den : 0.0;
+                H[j][j] = den;
+                H[j + 1][j] = 0.0;
+                g[j + 1] = -sn[j] * g[j];
+                g[j] = cs[j] * g[j];
+                res = std::fabs(g[j + 1]);
+                ++iters;
+                kdim = j + 1;
+                if (hn > 0.0) jscale(W.V + (j + 1) * vs, W.w, 1.0 / hn, s);
+                if (res <= target || !(hn > 0.0)) break;
+            }
+            for (int i = kdim - 1; i >= 0; --i) {         // H y = g
+                double t = g[i];
+                for (int k = i + 1; k < kdim; ++k) t -= H[i][k] * y[k];
+                y[i] = H[i][i] != 0.0 ? t / H[i][i] : 0.0;
+            }
+            jcombine(x, 1.0, W.V, kdim, y, s);
+            if (res <= target || iters >= kMaxIter || kdim == 0) break;
+            // restart: r = b - J x into V_0
+            double xn;
+            rc = jdots(W, x, x, 0, 1, N, &xn, s);
+            if (rc) return rc;
+            jjvp(Qv, qbed, W, state, x, std::sqrt(xn), nrmQ, W.w, s);
+            jscale(W.V, b, 1.0, s);
+            const double m1 = -1.0;
+            jcombine(W.V, 1.0, W.w, 1, &m1, s);
+            rc = jdots(W, W.V, W.V, 0, 1, N, &beta, s);
+            if (rc) return rc;
+            beta = std::sqrt(beta);
+            if (!(beta > target)) break;
+            jscale(W.V, W.V, 1.0 / beta, s);
+        }
+        return cuda_check(cudaGetLastError(), "implicit_global GMRES launch");
+    }
+
+    // SolveImplicitSourceGlobal (imex_solver.H:102-160) on the stage state Qv
+    // (a vector; it holds Qexp on entry and the Newton solution on exit).
+    int jsolve(double* Qv, const double* qbed, char* scratch, cudaStream_t s) {
+        const JW W = jwork(scratch);
+        const long long N = jN();
+        int rc = cuda_check(cudaMemcpyAsync(W.qexp, Qv, sizeof(double) * N, cudaMemcpyDeviceToDevice, s),
+                            "implicit_global copy");
+        if (rc) return rc;
+        double resid0 = -1.0;
+        for (int it = 0; it < kNewtonMax; ++it) {
+            zfv::jfnk::k_residual<Model><<<jcell_blocks(), zfv::jfnk::kNT, 0, s>>>(
+                Qv, qbed, W.qexp, W.S, W.F, L, st(scratch), W.part);
+            zfv::jfnk::k_sum_partials<<<1, zfv::jfnk::kNT, 0, s>>>(W.part, jcell_blocks(), W.out);
+            double r2;
+            rc = cuda_check(cudaMemcpyAsync(&r2, W.out, sizeof(double), cudaMemcpyDeviceToHost, s),
+                            "implicit_global residual read-back");
+            if (!rc) rc = cuda_check(cudaStreamSynchronize(s), "implicit_global residual");
+            if (rc) return rc;
+            const double resid = std::sqrt(r2);
+            if (it == 0) resid0 = resid;
+            if (resid < 1e-12 || (resid0 > 0.0 && resid < 1e-9 * resid0)) break;
+            jscale(W.F, W.F, -1.0, s);                      // rhs = -F
+            double qq, bb = 0.0;                            // |Q| over all components
+            rc = jdots(W, Qv, Qv, 0, 1, N, &qq, s);
+            if (!rc && n0 == 1) rc = jdots(W, qbed, qbed, 0, 1, L.plane, &bb, s);
+            if (rc) return rc;
+            const double nrmQ = std::sqrt(qq + bb);
+            rc = cuda_check(cudaMemsetAsync(W.x, 0, sizeof(double) * N, s), "implicit_global memset");
+            if (!rc) rc = jgmres(Qv, qbed, W, st(scratch), W.F, W.x, nrmQ, 1e-4, s);
+            if (rc) return rc;
+            const double one = 1.0;
+            jcombine(Qv, 1.0, W.x, 1, &one, s);             // Q += delta
+        }
+        return cuda_check(cudaGetLastError(), "implicit_global launch");
+    }
+
+    struct JfnkEvolveF {
+        RunnerT* r; double* Q; char* scratch; int n; cudaStream_t s;
+        template <int O, bool W, bool I> int operator()() {
+            if constexpr (!I) {
+                return fail(-2, "implicit_global needs implicit_source");
+            } else {
+                cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+                int rc = cuda_check(cudaStreamIsCapturing(s, &cap), "cudaStreamIsCapturing");
+                if (rc) return rc;
+                if (cap != cudaStreamCaptureStatusNone)
+                    return fail(-2, "zfv_evolve: implicit_global reads Newton-Krylov norms on the host and "
+                                    "cannot run inside a CUDA graph capture");
+                const long long pl = r->L.plane;
+                double* E1 = r->stage(scratch);
+                double* E2 = r->stage2(scratch);
+                for (int k = 0; k < n; ++k) {
+                    unsigned flags = 0;
+                    rc = cuda_check(cudaMemcpyAsync(&flags, &r->st(scratch)->flags, sizeof flags,
+                                                    cudaMemcpyDeviceToHost, s), "implicit_global flags");
+                    if (!rc) rc = cuda_check(cudaStreamSynchronize(s), "implicit_global flags");
+                    if (rc) return rc;
+                    if (flags & zfv::kFlagDone) break;
+                    const int nbc = r->jcell_blocks();
+                    if constexpr (O == 2) {
+                        r->template launch<2, zfv::MODE_X, W, I>(Q, Q, nullptr, E1, scratch, s);
+                        rc = r->jsolve(E1 + n0 * pl, Q, scratch, s);
+                        if (rc) return rc;
+                        r->template launch<2, zfv::MODE_X, W, I>(E1, Q, nullptr, E2, scratch, s);
+                        rc = r->jsolve(E2 + n0 * pl, Q, scratch, s);
+                        if (rc) return rc;
+                        zfv::jfnk::k_finish<Model, Numerics, true><<<nbc, zfv::jfnk::kNT, 0, s>>>(
+                            E2 + n0 * pl, Q, r->L, r->st(scratch), r->partials(scratch), r->log3(scratch), kLogCap);
+                    } else {
+                        r->template launch<1, zfv::MODE_X, W, I>(Q, Q, nullptr, E1, scratch, s);
+                        rc = r->jsolve(E1 + n0 * pl, Q, scratch, s);
+                        if (rc) return rc;
+                        zfv::jfnk::k_finish<Model, Numerics, false><<<nbc, zfv::jfnk::kNT, 0, s>>>(
+                            E1 + n0 * pl, Q, r->L, r->st(scratch), r->partials(scratch), r->log3(scratch), kLogCap);
+                    }
+                    rc = cuda_check(cudaGetLastError(), "implicit_global step launch");
+                    if (rc) return rc;
+                }
+                return 0;
+            }
+        }
+    };
 
     struct RhsF {
         RunnerT* r; const double* Q; double* out; double time; cudaStream_t s;
@@ -271,6 +516,8 @@ struct RunnerT final : Runner {
             return fail(-2, "%s: the adjoint is implemented for the FP64 SWE2D form, order 2", what);
         if (c.positivity_mood || c.clamp_positivity)
             return fail(-2, "%s: the adjoint does not differentiate clamp_positivity / MOOD", what);
+        if (c.implicit_source && c.implicit_global)
+            return fail(-2, "%s: the adjoint differentiates the point-implicit source, not implicit_global", what);
         return 0;
     }
 
@@ -381,6 +628,12 @@ int zfv_create(const zfv_config* cfg, zfv_handle** out) {
             return fail(-1, "zfv_create: the FP32 form is built for ZFV_MODEL_SWE2D only");
         if (cfg->clamp_positivity)
             return fail(-1, "zfv_create: the FP32 form does not implement clamp_positivity");
+    }
+    if (cfg->implicit_global && cfg->implicit_source) {
+        if (cfg->precision != ZFV_PREC_FP64)
+            return fail(-1, "zfv_create: implicit_global is built for the FP64 form");
+        if (cfg->positivity_mood)
+            return fail(-1, "zfv_create: implicit_global with positivity mood is not built");
     }
     if (cfg->nx < 1 || cfg->ny < 1) return fail(-1, "zfv_create: bad grid %d x %d", cfg->nx, cfg->ny);
     if (dim == 1 && cfg->ny != 1) return fail(-1, "zfv_create: 1-D model needs ny == 1 (got %d)", cfg->ny);

@@ -133,7 +133,11 @@ class Level:
                     flags=int(st.flags), done=bool(st.flags & 4), mood_redos=int(st.mood_redos))
 
     def run(self, max_steps: int | None = None, chunk: int = 64, use_graph: bool = False) -> dict:
-        """Evolve until time_end / max_step (or max_steps), syncing once per chunk."""
+        """Evolve until time_end / max_step (or max_steps), syncing once per chunk.
+        With implicit_global the steps always run uncaptured (the Newton-Krylov
+        iteration reads norms on the host)."""
+        if self.cfg.implicit_source and self.cfg.implicit_global:
+            use_graph = False
         self.begin()
         done_steps = 0
         last_step = -1

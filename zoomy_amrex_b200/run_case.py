@@ -58,6 +58,8 @@ def run_case(model: SWE, settings: dict, output_dir: str | None = None, on_progr
         plots.append(write_level_state(out, identifier, index, st["time"], Qp, lev.aux.cpu().numpy(),
                                        lo, hi))
 
+    if cfg.implicit_source and cfg.implicit_global:
+        use_graph = False            # the Newton-Krylov iteration reads norms on the host
     try:
         lev.begin()
         if out is not None:

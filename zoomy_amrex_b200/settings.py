@@ -37,7 +37,9 @@ def config_from_settings(model: SWE, settings: dict, *, precision: int = ZFV_PRE
     Keys (defaults as the reference's run_case/write_inputs apply them):
       time_end (0.1), cfl (0.45), spatial_order (1), well_balanced (False),
       positivity ("none"), dtmax (time_end), dtmin (1e-7), max_step (-1),
-      implicit_source (False), clamp_positivity (False), params ({}).
+      implicit_source (False), implicit_global (False: the deck's
+      solver.implicit_global, ZoomyAmr.cpp:48), clamp_positivity (False),
+      params ({}).
     """
     dim, nx, ny, lo, hi = grid(settings)
     if dim != model.dimension:
@@ -66,4 +68,5 @@ def config_from_settings(model: SWE, settings: dict, *, precision: int = ZFV_PRE
         bc=model.side_kinds(),
         params=params,
         precision=precision,
+        implicit_global=bool(settings.get("implicit_global", False)),
     )
