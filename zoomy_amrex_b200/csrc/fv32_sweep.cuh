@@ -291,7 +291,9 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
             if constexpr (MODE == S1) {
                 inc_out[c] = inc_e; inc_out[pl + c] = inc_u; inc_out[2 * pl + c] = inc_v;
             } else {
-                // compensated Heun update in FP64: Q^{n+1} = (hi + lo) + (inc1 + inc2) / 2
+                // compensated Heun update Q^{n+1} = (hi + lo) + (inc1 + inc2) / 2: the
+                // small part t = lo + (inc1 + inc2) / 2 in FP32, then an exact
+                // two-sum hi + t -> (hi', lo')
                 if constexpr (PF) {
                     __pipeline_wait_prior(0);
 #pragma unroll
@@ -303,14 +305,12 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
                 } else {
                     load_comp();
                 }
-                const double ne = (double(cx[0]) + double(cl[0])) + 0.5 * (double(ci[0]) + double(inc_e));
-                const double nu = (double(cx[1]) + double(cl[1])) + 0.5 * (double(ci[1]) + double(inc_u));
-                const double nv = (double(cx[2]) + double(cl[2])) + 0.5 * (double(ci[2]) + double(inc_v));
-                const float he = float(ne), hu = float(nu), hv = float(nv);
+                float he, hu, hv, le, lu, lv;
+                two_sum(cx[0], __fadd_rn(cl[0], 0.5f * __fadd_rn(ci[0], inc_e)), he, le);
+                two_sum(cx[1], __fadd_rn(cl[1], 0.5f * __fadd_rn(ci[1], inc_u)), hu, lu);
+                two_sum(cx[2], __fadd_rn(cl[2], 0.5f * __fadd_rn(ci[2], inc_v)), hv, lv);
                 Y[c] = he; Y[pl + c] = hu; Y[2 * pl + c] = hv;
-                lo[c] = float(ne - double(he));
-                lo[pl + c] = float(nu - double(hu));
-                lo[2 * pl + c] = float(nv - double(hv));
+                lo[c] = le; lo[pl + c] = lu; lo[2 * pl + c] = lv;
                 // CFL terms of the new state (ZoomyAmr.cpp:472-487) and its FP64 mass
                 const float hn = he - w1.b;
                 const float hin = kp_hinv(hn, L.eps);
@@ -321,7 +321,7 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
                 if (evx > mm_) mm_ = evx;
                 if (evy > mm_) mm_ = evy;
                 if (double(mm_) > m_loc) m_loc = double(mm_);
-                s_loc = s_loc + (ne - double(w1.b));
+                s_loc = s_loc + ((double(he) - double(w1.b)) + double(le));
             }
         }
         // advance: row j+1 becomes the current row

@@ -175,6 +175,14 @@ __device__ __forceinline__ void manning_implicit2(float2 h, float2 u, float2 v, 
     dv = f2(okx ? x1.x : (isfinite(r1.x) ? r1.x : 0.0f), oky ? x1.y : (isfinite(r1.y) ? r1.y : 0.0f));
 }
 
+// Two-sum on both columns: s + e == a + b exactly per lane pair.
+__device__ __forceinline__ void two_sum2(float2 a, float2 b, float2& s, float2& e) {
+    s = add(a, b);
+    const float2 bp = sub(s, a);
+    const float2 ap = sub(s, bp);
+    e = add(sub(a, ap), sub(b, bp));
+}
+
 __device__ __forceinline__ float2 shfl_up2(float2 v, int d) {
     return f2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
 }
@@ -342,7 +350,7 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                     if (ownB) { inc_out[c + 1] = inc_e.y; inc_out[pl + c + 1] = inc_u.y; inc_out[2 * pl + c + 1] = inc_v.y; }
                 }
             } else {
-                // compensated Heun update in FP64, per cell
+                // stage 2: the update's own inputs (hi, inc1, lo)
                 if constexpr (PF) {
                     if (vec_io) {
                         __pipeline_wait_prior(0);
@@ -358,25 +366,23 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                 } else {
                     load_comp();
                 }
-                float i1[2][3], xs[2][3], lw[2][3];
+                // compensated Heun update Q^{n+1} = (hi + lo) + (inc1 + inc2) / 2: the
+                // small part t = lo + (inc1 + inc2) / 2 in packed FP32, then an
+                // exact two-sum hi + t -> (hi', lo')
+                const float2 i2[3] = {inc_e, inc_u, inc_v};
+                float2 nf2[3], nl2[3];
 #pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    i1[0][q] = ci[q].x; i1[1][q] = ci[q].y;
-                    xs[0][q] = cx[q].x; xs[1][q] = cx[q].y;
-                    lw[0][q] = cl[q].x; lw[1][q] = cl[q].y;
-                }
-                const float i2[2][3] = {{inc_e.x, inc_u.x, inc_v.x}, {inc_e.y, inc_u.y, inc_v.y}};
-                const float bb[2] = {w1.b.x, w1.b.y};
+                for (int q = 0; q < 3; ++q)
+                    two_sum2(cx[q], add(cl[q], mul(s2(0.5f), add(ci[q], i2[q]))), nf2[q], nl2[q]);
                 float nf[2][3], nl[2][3];
 #pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    double nd[3];
+                for (int q = 0; q < 3; ++q) {
+                    nf[0][q] = nf2[q].x; nf[1][q] = nf2[q].y;
+                    nl[0][q] = nl2[q].x; nl[1][q] = nl2[q].y;
+                }
+                const float bb[2] = {w1.b.x, w1.b.y};
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        nd[q] = (double(xs[k][q]) + double(lw[k][q])) + 0.5 * (double(i1[k][q]) + double(i2[k][q]));
-                        nf[k][q] = float(nd[q]);
-                        nl[k][q] = float(nd[q] - double(nf[k][q]));
-                    }
+                for (int k = 0; k < 2; ++k) {
                     const bool own = k == 0 ? ownA : ownB;
                     if (own) {
                         // CFL terms of the new state (ZoomyAmr.cpp:472-487) and its FP64 mass
@@ -387,7 +393,7 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                         const float evy = (fabsf(nf[k][2] * hin) + c0) * L.rfdy;
                         const float mm_ = fmaxf(fmaxf(evx, evy), 0.0f);
                         if (double(mm_) > m_loc) m_loc = double(mm_);
-                        s_loc = s_loc + (nd[0] - double(bb[k]));
+                        s_loc = s_loc + ((double(nf[k][0]) - double(bb[k])) + double(nl[k][0]));
                     }
                 }
                 if (vec_io) {

@@ -11,10 +11,12 @@
 //    the flux and the well-balancing bed source as the same FP32 values, which
 //    cancel exactly;
 //  * the update is compensated: stage 1 stores only its FP32 increment inc1,
-//    stage 2 forms Q^{n+1} = (hi + lo) + (inc1 + inc2)/2 in FP64 per cell and
-//    splits it again into an FP32 value (hi, the state the fluxes read) and an
-//    FP32 remainder (lo, kept in scratch); so round-off of the stored state
-//    does not accumulate step after step;
+//    stage 2 forms the small part t = lo + (inc1 + inc2)/2 in FP32 and adds it
+//    to the stored value by an exact two-sum, giving Q^{n+1} = hi' + lo' as an
+//    FP32 value (hi', the state the fluxes read) and an FP32 remainder (lo',
+//    kept in scratch); so round-off of the stored state does not accumulate
+//    step after step (only the FP32 rounding of t, relative to the step's
+//    increment, enters);
 //  * FP64 is used only in the point-implicit source solve of near-dry cells
 //    (h < 1e-3) and in the mass sum.
 // Kernels are compiled with FMA contraction on (this file only).
@@ -57,6 +59,15 @@ constexpr float kNearDry = 1.0e-3f;   // FP64 implicit solve below this depth
 __device__ __forceinline__ float mm(float a, float b) {
     if (a * b <= 0.0f) return 0.0f;
     return (fabsf(a) < fabsf(b)) ? a : b;
+}
+
+// Knuth's two-sum: s + e == a + b exactly (round-to-nearest, no contraction:
+// the _rn intrinsics are never fused into FMAs).
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = __fadd_rn(a, b);
+    const float bp = __fsub_rn(s, a);
+    const float ap = __fsub_rn(s, bp);
+    e = __fadd_rn(__fsub_rn(a, ap), __fsub_rn(b, bp));
 }
 
 // Kurganov-Petrova desingularised 1/h (the model's update_aux_variables), FP32.
