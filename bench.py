@@ -44,10 +44,10 @@ BYTES_PER_CELL_STEP_FP32 = 92
 # DRAM bytes per cell per step (both stage launches), from `ncu --set full`
 # of `python -m zoomy_amrex_b200.profile_case fp32 --n 3072 --variant 9
 # --steps 3` (the shape the autotuner picks for the 4096^2 level): stage 1
-# read 151.2 MB + wrote 78.8 MB, stage 2 read 381.3 MB + wrote 196.4 MB over
+# read 151.2 MB + wrote 78.2 MB, stage 2 read 380.8 MB + wrote 195.4 MB over
 # 3072^2 cells. The traffic scales with the cells, so it is scaled to the
 # benchmark grid per launch.
-NCU_TRAFFIC_PER_CELL_STEP_FP32 = 85.58
+NCU_TRAFFIC_PER_CELL_STEP_FP32 = 85.36
 
 
 def parse():

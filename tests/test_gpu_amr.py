@@ -148,3 +148,32 @@ def test_amr_reference_tagging_and_time_end(cuda):
     assert n_gated == 0
     assert abs(t - 0.05) < 1e-12
     assert np.isfinite(q[~np.isnan(q)]).all()
+
+
+def test_amr_plotfile_holds_every_level(cuda, tmp_path):
+    """write_plotfile puts every level's patches into one AMReX plotfile (the
+    multi-level format the reference's reader accepts, pinned by
+    tests/test_plotfile.py); read back, each level equals level_state and the
+    aux hinv row is 1/h of the written depth on wet cells."""
+    from zoomy_amrex_b200.amr import AmrHierarchy
+    from zoomy_amrex_b200.plotfile import read_plotfile
+    nx, ny, L = 128, 128, 50.0
+    Q0 = _fields(nx, ny, L)
+    hier = AmrHierarchy(_cfg(nx, ny, L), Q0, max_level=2, B=32, threshold=0.01, regrid_int=2)
+    hier.run(6)
+    path = hier.write_plotfile(tmp_path, "amr")
+    head, levels = read_plotfile(path)
+    assert head["finest_level"] == len(hier.levels) - 1 and head["ref_ratios"] == [2] * head["finest_level"]
+    assert abs(head["time"] - hier.time) < 1e-15
+    for lev, Lr in enumerate(levels):
+        dense = hier.level_state(lev)
+        assert Lr.step == 6 << lev
+        assert sum(P.data.shape[1] * P.data.shape[2] for P in Lr.patches) == hier.levels[lev].n * 32 * 32
+        for P in Lr.patches:
+            i0, j0 = P.lo
+            ny_, nx_ = P.data.shape[1:]
+            assert np.array_equal(P.data[:4], dense[:, j0:j0 + ny_, i0:i0 + nx_])
+            h = P.data[1]
+            wet = h > 1e-3
+            assert np.allclose(P.data[-1][wet], 1.0 / h[wet], rtol=1e-6)
+    hier.close()

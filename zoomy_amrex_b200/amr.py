@@ -353,6 +353,29 @@ class AmrHierarchy:
             out[:, by * B:(by + 1) * B, bx * B:(bx + nb) * B] = q.cpu().numpy()
         return out
 
+    def write_plotfile(self, out_dir, identifier: str = "", step: int | None = None) -> str:
+        """All levels as one AMReX plotfile, as ZoomyAmr::WritePlotFile does
+        (ZoomyAmr.cpp:821-882): per level its patches (boxes) with components
+        var0..var3 (b, h, hu, hv) then aux0..aux6, ref ratio 2, level l's step
+        count = coarse steps x 2^l. Returns the plotfile's path."""
+        import os
+        from .plotfile import LevelData, PatchData, component_names, plotfile_name, write_plotfile
+        step = self.steps if step is None else int(step)
+        B = self.B
+        levels = []
+        for L in self.levels:
+            qs = L.batch.state64()                       # also refreshes the aux hinv row
+            patches = [PatchData(np.concatenate([q.cpu().numpy(), a.cpu().numpy()], axis=0), (bx * B, by * B))
+                       for (bx, by, nb), q, a in zip(L.patches, qs, L.batch.aux)]
+            levels.append(LevelData((0, 0), (L.nx - 1, L.ny - 1), (L.dx, L.dy), patches,
+                                    step=self.steps << L.lev))
+        c = self.cfg
+        n_aux = self.levels[0].batch.aux[0].shape[0]
+        path = os.path.join(str(out_dir), plotfile_name(identifier, step))
+        return write_plotfile(path, levels, component_names(4, n_aux), self.time,
+                              (c.prob_lo[0], c.prob_lo[1]), (c.prob_hi[0], c.prob_hi[1]),
+                              [2] * (len(levels) - 1))
+
     def mass(self) -> float:
         """Sum of h dx dy over the base level (finer levels are averaged onto it)."""
         q = self.level_state(0)
