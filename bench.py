@@ -332,7 +332,7 @@ def ensemble_bench(K, W, local, n_inst=256, seed=2027):
             "strip_shape_ms_per_step": {str(v): t for v, t in times.items()}, "picked_variant": best}
 
 
-def amr_bench(local, n=1024, steps=10, warm=2, max_level=2, B=64, variant=5):
+def amr_bench(local, n=1024, steps=10, warm=2, max_level=2, B=64, variant=9):
     """A 3-level AMR hierarchy (ratio 2, base n^2, boxes of B^2, tagged where
     |grad eta| > 0.01, regrid every 2 coarse steps, subcycling) of a dam
     break over bumps: coarse steps per second and cell updates per second

@@ -298,7 +298,8 @@ const void* zfv_batch_descriptors(const zfv_batch* b);
  */
 typedef struct zfv_amr_level {
     const void* insts;   /* zfv_batch_descriptors() of the level's batch */
-    const int* map;      /* device, nby * nbx: (instance << 8) | block offset in the patch, -1 absent */
+    const int* map;      /* device, nby * nbx: (instance << 10) | (block row offset << 5) |
+                            block column offset inside the patch, -1 absent */
     int nbx, nby;        /* block grid */
     int B;               /* cells per block side (even) */
     int nx, ny;          /* the level's grid in cells */
@@ -306,13 +307,13 @@ typedef struct zfv_amr_level {
     int pad;
 } zfv_amr_level;
 /*
- * Patches: a level's blocks grouped into horizontal runs of consecutive
- * blocks of one block row, one batch instance of (nb * B) x B cells each.
- * `patches` (device) holds 4 ints per patch: first block x, block row y,
- * nb (1 .. 256), unused; max_blocks bounds nb over the list (it sizes the
- * launch). Instance k of the level's batch is patch k.
+ * Patches: a level's blocks grouped into rectangles of nbx x nby blocks
+ * (each side 1 .. 32), one batch instance of (nbx * B) x (nby * B) cells
+ * each. `patches` (device) holds 4 ints per patch: first block x, first
+ * block row y, nbx, nby; max_blocks bounds nbx * nby over the list (it sizes
+ * the launch). Instance k of the level's batch is patch k.
  */
-/* Ghost frames ((nb*B + 4) x (B + 4) x 4 floats per patch) before stage
+/* Ghost frames ((nby*B + 4) x (nbx*B + 4) x 4 floats per patch) before stage
  * `stage` (1: the stage input; 2: neighbours' stage-2 input): same-level
  * patches, else conservative linear interpolation of `coarse` (NULL on level
  * 0), physical boundaries by mirroring. */

@@ -137,3 +137,21 @@ def test_hyperbolic_solver_validation():
     s = HyperbolicSolver(CFL=0.45, order=2)._legacy_settings(
         {"domain": [0, 1, 0, 1], "n_cells": [10, 10]}, {"time_end": 0.2})
     assert s["dimension"] == 2 and s["time_end"] == 0.2 and s["n_cells"] == [10, 10]
+
+
+def test_amr_patches_tile_the_blocks():
+    """group_patches covers every refined block exactly once with rectangles
+    no larger than the side limit (the AMR kernels' map offsets rely on it)."""
+    import numpy as np
+    from zoomy_amrex_b200.amr import group_patches
+    rng = np.random.default_rng(5)
+    for trial in range(20):
+        mask = rng.random((24, 40)) < rng.uniform(0.2, 0.9)
+        blocks = [(int(x), int(y)) for y, x in zip(*np.nonzero(mask))]
+        side = int(rng.integers(1, 9))
+        rects = group_patches(blocks, side)
+        cover = np.zeros_like(mask, dtype=int)
+        for bx, by, nbx, nby in rects:
+            assert 1 <= nbx <= side and 1 <= nby <= side
+            cover[by:by + nby, bx:bx + nbx] += 1
+        assert np.array_equal(cover, mask.astype(int))

@@ -12,8 +12,8 @@ There is no flux register, as in the reference (ZoomyAmr.H:85).
 
 Here every level is refined in B x B blocks on a regular block grid (the
 layout of a quadtree rather than AMReX's Berger-Rigoutsos clustering); the
-blocks of a level are grouped into patches, horizontal runs of up to
-``patch_blocks`` consecutive blocks, each one instance of a grouped batch:
+blocks of a level are grouped into patches, rectangles of up to
+``patch_blocks`` x ``patch_blocks`` blocks, each one instance of a grouped batch:
 one launch per RK stage advances all patches of a level, the patches of a
 level share one run record, and a patch's ghost ring is a small frame array
 the stage kernels read in place of the physical mirror.
@@ -40,16 +40,27 @@ def _cfg_copy(c: zfv_config) -> zfv_config:
     return d
 
 
-def group_patches(blocks, max_blocks: int) -> list[tuple[int, int, int]]:
-    """Blocks (bx, by) -> patches (bx0, by, nb): runs of consecutive blocks of
-    one block row, at most ``max_blocks`` long."""
-    out = []
+def group_patches(blocks, max_side: int) -> list[tuple[int, int, int, int]]:
+    """Blocks (bx, by) -> patches (bx0, by0, nbx, nby): rectangles made of
+    runs of consecutive blocks of a block row (at most ``max_side`` long),
+    stacked while the run below starts and ends in the same columns (at most
+    ``max_side`` runs high)."""
+    runs = []
     for bx, by in sorted(blocks, key=lambda p: (p[1], p[0])):
-        if out and out[-1][1] == by and out[-1][0] + out[-1][2] == bx and out[-1][2] < max_blocks:
-            out[-1] = (out[-1][0], by, out[-1][2] + 1)
+        if runs and runs[-1][1] == by and runs[-1][0] + runs[-1][2] == bx and runs[-1][2] < max_side:
+            runs[-1] = (runs[-1][0], by, runs[-1][2] + 1)
         else:
-            out.append((bx, by, 1))
-    return out
+            runs.append((bx, by, 1))
+    rects, open_ = [], {}
+    for bx0, by, nb in runs:
+        r = open_.get((bx0, nb))
+        if r is not None and rects[r][1] + rects[r][3] == by and rects[r][3] < max_side:
+            rects[r] = (bx0, rects[r][1], nb, rects[r][3] + 1)
+        else:
+            rects.append((bx0, by, nb, 1))
+            r = len(rects) - 1
+        open_[(bx0, nb)] = r
+    return sorted(rects, key=lambda p: (p[1], p[0]))
 
 
 class AmrLevel:
@@ -66,34 +77,35 @@ class AmrLevel:
         self.dy = hier.dy0 / (1 << lev)
         self.blocks = sorted(blocks, key=lambda p: (p[1], p[0]))
         self.patches = group_patches(self.blocks, hier.patch_blocks)
-        self.max_blocks = max(nb for _, _, nb in self.patches)
+        self.max_blocks = max(nbx * nby for _, _, nbx, nby in self.patches)
         dev = hier.device
         cfgs, Q0s = [], None if Q0 is None else []
-        for (bx, by, nb) in self.patches:
+        for (bx, by, nbx, nby) in self.patches:
             c = _cfg_copy(hier.cfg)
-            c.nx, c.ny = nb * B, B
+            c.nx, c.ny = nbx * B, nby * B
             c.prob_lo[0] = hier.lo[0] + bx * B * self.dx
             c.prob_lo[1] = hier.lo[1] + by * B * self.dy
-            c.prob_hi[0] = c.prob_lo[0] + nb * B * self.dx
-            c.prob_hi[1] = c.prob_lo[1] + B * self.dy
+            c.prob_hi[0] = c.prob_lo[0] + nbx * B * self.dx
+            c.prob_hi[1] = c.prob_lo[1] + nby * B * self.dy
             c.precision = ZFV_PREC_FP32
             c.time_end = 1.0e30
             c.max_step = -1
             cfgs.append(c)
             if Q0 is not None:
-                Q0s.append(np.ascontiguousarray(Q0[:, by * B:(by + 1) * B, bx * B:(bx + nb) * B]))
+                Q0s.append(np.ascontiguousarray(Q0[:, by * B:(by + nby) * B, bx * B:(bx + nbx) * B]))
         self.batch = Batch(cfgs, Q0s, None, device=dev, stream=hier.stream, groups=[0] * len(cfgs),
                            variant=hier.variant if variant is None else variant)
         n = len(self.patches)
-        self.frames = [torch.zeros((4, B + 4, nb * B + 4), dtype=torch.float32, device=dev)
-                       for (_, _, nb) in self.patches]
+        self.frames = [torch.zeros((4, nby * B + 4, nbx * B + 4), dtype=torch.float32, device=dev)
+                       for (_, _, nbx, nby) in self.patches]
         self.batch.set_frames(self.frames)
         m = torch.full((self.nby, self.nbx), -1, dtype=torch.int32)
-        for k, (bx, by, nb) in enumerate(self.patches):
-            for o in range(nb):
-                m[by, bx + o] = (k << 8) | o
+        for k, (bx, by, nbx, nby) in enumerate(self.patches):
+            for oy in range(nby):
+                for ox in range(nbx):
+                    m[by + oy, bx + ox] = (k << 10) | (oy << 5) | ox
         self.map = m.to(dev)
-        self.pdesc = torch.tensor([[bx, by, nb, 0] for (bx, by, nb) in self.patches], dtype=torch.int32,
+        self.pdesc = torch.tensor([list(p) for p in self.patches], dtype=torch.int32,
                                   device=dev).reshape(n, 4).contiguous()
         self.frame_ptrs = torch.tensor([f.data_ptr() for f in self.frames], dtype=torch.int64, device=dev)
         self.dts = torch.zeros(n, dtype=torch.float64, device=dev)
@@ -126,7 +138,7 @@ class AmrHierarchy:
     TAGS = {"eta_gradient": 0, "reference": 1}
 
     def __init__(self, cfg: zfv_config, Q0, max_level: int = 2, B: int = 64, threshold: float = 0.01,
-                 regrid_int: int = 2, device="cuda:0", variant: int = 5, patch_blocks: int = 16,
+                 regrid_int: int = 2, device="cuda:0", variant: int = 9, patch_blocks: int = 16,
                  tag: str = "eta_gradient", tag_b_max: float = 1.0e30):
         if cfg.nx % B or cfg.ny % B or B % 2:
             raise ValueError("the base grid must be a multiple of the (even) box side B in both directions")
@@ -135,8 +147,8 @@ class AmrHierarchy:
         self.device = torch.device(device)
         self.stream = torch.cuda.Stream(self.device)
         self.variant = variant
-        if not 1 <= patch_blocks <= 256:
-            raise ValueError("patch_blocks must be in 1 .. 256")
+        if not 1 <= patch_blocks <= 32:
+            raise ValueError("patch_blocks must be in 1 .. 32")
         if tag not in self.TAGS:
             raise ValueError(f"tag must be one of {sorted(self.TAGS)}")
         self.criterion, self.tag_b_max = self.TAGS[tag], float(tag_b_max)
@@ -349,8 +361,8 @@ class AmrHierarchy:
         L = self.levels[lev]
         B = self.B
         out = np.full((4, L.ny, L.nx), np.nan)
-        for (bx, by, nb), q in zip(L.patches, L.batch.state64()):
-            out[:, by * B:(by + 1) * B, bx * B:(bx + nb) * B] = q.cpu().numpy()
+        for (bx, by, nbx, nby), q in zip(L.patches, L.batch.state64()):
+            out[:, by * B:(by + nby) * B, bx * B:(bx + nbx) * B] = q.cpu().numpy()
         return out
 
     def write_plotfile(self, out_dir, identifier: str = "", step: int | None = None) -> str:
@@ -366,7 +378,7 @@ class AmrHierarchy:
         for L in self.levels:
             qs = L.batch.state64()                       # also refreshes the aux hinv row
             patches = [PatchData(np.concatenate([q.cpu().numpy(), a.cpu().numpy()], axis=0), (bx * B, by * B))
-                       for (bx, by, nb), q, a in zip(L.patches, qs, L.batch.aux)]
+                       for (bx, by, _, _), q, a in zip(L.patches, qs, L.batch.aux)]
             levels.append(LevelData((0, 0), (L.nx - 1, L.ny - 1), (L.dx, L.dy), patches,
                                     step=self.steps << L.lev))
         c = self.cfg

@@ -1,11 +1,12 @@
 // Block-structured AMR on top of the FP32 batch engine.
 //
 // Each level lives on a regular grid of B x B blocks. The blocks present at a
-// level are grouped into patches: horizontal runs of consecutive blocks of
-// one block row, each patch one batch instance of (nb * B) x B cells (wide
-// patches keep the 30- and 60-column strips of the stage kernels full).
-// `map` gives, per block position, (instance << 8) | (block offset inside
-// the patch), or -1 when the level has no such block. All patches of a level
+// level are grouped into patches: rectangles of nbx x nby blocks, each patch
+// one batch instance of (nbx * B) x (nby * B) cells (wide patches keep the
+// 30- and 60-column strips of the stage kernels full; tall ones let most
+// strips take the interior path). `map` gives, per block position,
+// (instance << 10) | (block row offset << 5) | (block column offset) inside
+// the patch, or -1 when the level has no such block. All patches of a level
 // share one run record (one dt, one CFL reduction). Refinement ratio 2: a
 // level-(l+1) block covers a quarter of a level-l block.
 //
@@ -22,7 +23,7 @@
 //                      (RemakeLevel / MakeNewLevelFromCoarse).
 // The coarse data used for a fine patch's ghosts is the coarse level's
 // current state (the reference fills from Q[lev-1] at t_new only).
-// Patch descriptors: int4 {first block x, block row y, blocks nb, unused}.
+// Patch descriptors: int4 {first block x, first block row y, nbx, nby}.
 #pragma once
 
 namespace zfv32 {
@@ -30,7 +31,7 @@ namespace amr {
 
 struct LevelView {
     const BInst* insts;   // the level's batch descriptors (device)
-    const int* map;       // [nby * nbx] block position -> (instance << 8) | offset, -1 absent
+    const int* map;       // [nby * nbx] block position -> (instance << 10) | (oy << 5) | ox, -1 absent
     int nbx, nby;         // block grid
     int B;                // cells per block side
     int nx, ny;           // level grid (cells)
@@ -38,7 +39,7 @@ struct LevelView {
     int pad_;
 };
 
-constexpr int kMaxPatchBlocks = 256;   // the offset field of a map entry
+constexpr int kMaxPatchSide = 32;      // blocks per patch side: the offset fields of a map entry
 
 // Instance and in-instance cell index of level cell (I, J) inside the
 // domain; false when no patch of the level holds it.
@@ -46,9 +47,9 @@ __device__ __forceinline__ bool locate(const LevelView& V, int I, int J, int& k,
     const int bx = I / V.B, by = J / V.B;
     const int code = V.map[by * V.nbx + bx];
     if (code < 0) return false;
-    k = code >> 8;
-    const int ob = code & (kMaxPatchBlocks - 1);
-    c = (long long)(J - by * V.B) * V.insts[k].P.nx + (I - (bx - ob) * V.B);
+    k = code >> 10;
+    const int ox = code & (kMaxPatchSide - 1), oy = (code >> 5) & (kMaxPatchSide - 1);
+    c = (long long)(J - (by - oy) * V.B) * V.insts[k].P.nx + (I - (bx - ox) * V.B);
     return true;
 }
 
@@ -125,7 +126,7 @@ __global__ void k32a_fill(LevelView F, LevelView C, const int4* __restrict__ pat
     const int pi = blockIdx.y;
     if (pi >= n_patches) return;
     const int4 p = patches[pi];
-    const int H = F.B, W = p.z * F.B, FW = W + 4;
+    const int H = p.w * F.B, W = p.z * F.B, FW = W + 4;
     const int ring = FW * (H + 4) - W * H;
     const long long fp = (long long)FW * (H + 4);
     float* fr = frames[pi];
@@ -149,15 +150,15 @@ __global__ void k32a_average_down(LevelView F, LevelView C, const int4* __restri
     const int pi = blockIdx.y;
     if (pi >= n_patches) return;
     const int4 p = patches[pi];
-    const int hh = F.B / 2, hw = p.z * F.B / 2;
+    const int hb = F.B / 2, hw = p.z * hb, hh = p.w * hb;
     const int code = F.map[p.y * F.nbx + p.x];
     if (code < 0) return;
-    const BInst& D = F.insts[code >> 8];
+    const BInst& D = F.insts[code >> 10];
     const float* X = (*(volatile const unsigned*)&D.st->parity) ? D.alt : D.Qs;
     const long long pl = D.P.plane;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < hw * hh; k += gridDim.x * blockDim.x) {
         const int a = k % hw, c = k / hw;
-        const int ic = p.x * hh + a, jc = p.y * hh + c;   // coarse cell
+        const int ic = p.x * hb + a, jc = p.y * hb + c;   // coarse cell
         int kc;
         long long cc;
         if (!locate(C, ic, jc, kc, cc)) continue;
@@ -192,10 +193,10 @@ __global__ void k32a_tag(LevelView V, const int4* __restrict__ patches, int n_pa
     if (pi >= n_patches) return;
     const int B = V.B;
     const int4 p = patches[pi];
-    const int W = p.z * B;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < W * B; k += gridDim.x * blockDim.x) {
-        const int i = k % W;
-        const int I = p.x * B + i, J = p.y * B + k / W;
+    const int W = p.z * B, H = p.w * B;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < W * H; k += gridDim.x * blockDim.x) {
+        const int i = k % W, j = k / W;
+        const int I = p.x * B + i, J = p.y * B + j;
         C4 xm, xp, ym, yp;
         if (!lookup(V, I - 1, J, false, xm) || !lookup(V, I + 1, J, false, xp) ||
             !lookup(V, I, J - 1, false, ym) || !lookup(V, I, J + 1, false, yp))
@@ -211,7 +212,7 @@ __global__ void k32a_tag(LevelView V, const int4* __restrict__ patches, int n_pa
             const float hx = (xp.e - xp.b) - (xm.e - xm.b), hy = (yp.e - yp.b) - (ym.e - ym.b);
             hit = sqrtf(hx * hx + hy * hy) > threshold || (c.e - c.b) > 1.0e-2f;
         }
-        if (hit) flags[p.y * V.nbx + p.x + i / B] = 1;
+        if (hit) flags[(p.y + j / B) * V.nbx + p.x + i / B] = 1;
     }
 }
 
@@ -224,13 +225,13 @@ __global__ void k32a_regrid_fill(LevelView N, LevelView O, LevelView C, const in
     if (pi >= n_patches) return;
     const int B = N.B;
     const int4 p = patches[pi];
-    const int W = p.z * B;
+    const int W = p.z * B, H = p.w * B;
     const int code = N.map[p.y * N.nbx + p.x];
     if (code < 0) return;
-    const BInst& D = N.insts[code >> 8];
+    const BInst& D = N.insts[code >> 10];
     const long long pl = D.P.plane;
     float* bed = const_cast<float*>(D.bed);
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < W * B; k += gridDim.x * blockDim.x) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < W * H; k += gridDim.x * blockDim.x) {
         const int i = k % W, j = k / W;
         const int I = p.x * B + i, J = p.y * B + j;
         const long long c = (long long)j * D.P.nx + i;

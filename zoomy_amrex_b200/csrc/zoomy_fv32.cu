@@ -567,8 +567,9 @@ static zfv32::amr::LevelView view_of(const zfv_amr_level* l) {
 static int amr_grid(int n_patches, int max_blocks, long long per_patch, dim3& g) {
     if (n_patches < 1 || n_patches > 65535)
         return fail(-1, "zfv_amr: %d patches (1 .. 65535 per call)", n_patches);
-    if (max_blocks < 1 || max_blocks > zfv32::amr::kMaxPatchBlocks)
-        return fail(-1, "zfv_amr: %d blocks per patch (1 .. %d)", max_blocks, zfv32::amr::kMaxPatchBlocks);
+    constexpr int kMax = zfv32::amr::kMaxPatchSide * zfv32::amr::kMaxPatchSide;
+    if (max_blocks < 1 || max_blocks > kMax)
+        return fail(-1, "zfv_amr: %d blocks per patch (1 .. %d)", max_blocks, kMax);
     g = dim3(unsigned((per_patch + 255) / 256), unsigned(n_patches), 1);
     return 0;
 }
@@ -577,9 +578,10 @@ int zfv_amr_fill(const zfv_amr_level* fine, const zfv_amr_level* coarse, const i
                  int n_patches, int max_blocks, int stage, void* stream) {
     if (!fine || !patches || !frames) return fail(-1, "zfv_amr_fill: null argument");
     if (stage != 1 && stage != 2) return fail(-1, "zfv_amr_fill: stage must be 1 or 2");
-    const long long B = fine->B, W = (long long)max_blocks * B;
+    // a patch of nbx x nby <= max_blocks blocks has a ring of 2 (W + H) + 16 <= 2 B (max_blocks + 1) + 16 cells per layer
+    const long long B = fine->B;
     dim3 g;
-    int rc = amr_grid(n_patches, max_blocks, (W + 4) * (B + 4) - W * B, g);
+    int rc = amr_grid(n_patches, max_blocks, 4 * B * (max_blocks + 1) + 16, g);
     if (rc) return rc;
     zfv32::amr::k32a_fill<<<g, 256, 0, (cudaStream_t)stream>>>(
         view_of(fine), view_of(coarse), reinterpret_cast<const int4*>(patches), frames, n_patches, stage);

@@ -57,7 +57,7 @@ def main(argv=None):
         n, steps = a.n or 1024, a.steps or 4
         cfg, Q0 = dam_break_level(n)
         hier = AmrHierarchy(cfg, Q0, max_level=2, B=64, threshold=0.01, regrid_int=2,
-                            variant=a.variant if a.variant is not None else 5)
+                            variant=a.variant if a.variant is not None else 9)
         hier.run(steps)
         st = {"step": hier.steps, "boxes": [lv.n for lv in hier.levels], "time": hier.time}
         hier.close()
