@@ -150,6 +150,11 @@ int zfv_begin(zfv_handle* h, const void* Q, const void* aux, void* scratch, void
  * Q and aux are updated in place.
  */
 int zfv_update_state(zfv_handle* h, void* Q, void* aux, double time, void* stream);
+/* Work of the global implicit source (implicit_global; SolveImplicitSourceGlobal,
+ * imex_solver.H:102-160) since the last zfv_begin: field solves (one per
+ * stage), Newton iterations that ran a linear solve, and GMRES iterations.
+ * Host counters; any pointer may be NULL. Zero for the point-implicit form. */
+int zfv_implicit_global_stats(const zfv_handle* h, long long* solves, long long* newton, long long* gmres);
 
 /*
  * ZoomyAmr::ComputeDt (Source/ZoomyAmr.cpp:448-515) on (Q, aux) as stored.

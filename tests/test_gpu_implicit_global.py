@@ -37,6 +37,12 @@ def test_implicit_global_matches_exact_cell_solves(cuda, oracle, order):
         lev = Level(cfg, Q0, A0)
         st = lev.run(chunk=5, use_graph=True)      # graphs are skipped for implicit_global
         res[glob] = (lev.state64().cpu().numpy(), st)
+        stats = lev.implicit_global_stats()
+        if glob:
+            print(f"[implicit_global order {order}] work {stats}")
+            assert stats["solves"] == steps * order and stats["newton"] >= stats["solves"]
+        else:
+            assert stats == dict(solves=0, newton=0, gmres=0)
         lev.close()
     cfg, Q0, A0 = _case(nx, ny, order, True)
     cfg.max_step = steps

@@ -25,7 +25,7 @@ SYMBOLS = ("zfv_last_error", "zfv_version", "zfv_sizeof_config", "zfv_sizeof_sta
            "zfv_adj_work_bytes", "zfv_adj_record", "zfv_adj_step", "zfv_adj_variants",
            "zfv_adj_set_variant", "zfv_batch_create_grouped", "zfv_batch_set_frames", "zfv_batch_set_dt",
            "zfv_batch_stage", "zfv_batch_descriptors", "zfv_amr_fill", "zfv_amr_average_down", "zfv_amr_tag",
-           "zfv_amr_regrid_fill", "zfv_amr_set_dt")
+           "zfv_amr_regrid_fill", "zfv_amr_set_dt", "zfv_implicit_global_stats")
 
 
 class ZfvError(RuntimeError):
@@ -99,6 +99,8 @@ def lib():
     L.zfv_amr_tag.argtypes = [lv, vp, i, i, d, d, d, i, d, vp, vp]
     L.zfv_amr_regrid_fill.argtypes = [lv, lv, lv, vp, i, i, vp]
     L.zfv_amr_set_dt.argtypes = [pp, pp, C.POINTER(i), i, d, d, d, d, d, vp, vp]
+    L.zfv_implicit_global_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                            C.POINTER(C.c_longlong)]
     _lib = L
     return L
 

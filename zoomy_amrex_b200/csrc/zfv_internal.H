@@ -73,6 +73,9 @@ struct Runner {
     virtual int adj_step(const char*, int, double*, double*, const double*, char*, cudaStream_t) {
         return fail(-2, "zfv_adj_step: the adjoint is implemented for the FP64 SWE2D form, order 2");
     }
+    // Global implicit source (implicit_global): iteration counts since the
+    // last begin (Newton iterations, GMRES iterations, source solves).
+    long long jfnk_newton = 0, jfnk_gmres = 0, jfnk_solves = 0;
 };
 
 }  // namespace zfvi

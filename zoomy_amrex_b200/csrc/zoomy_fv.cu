@@ -173,6 +173,7 @@ struct RunnerT final : Runner {
     }
 
     int begin(const void* Q, const void* A, char* scratch, cudaStream_t s) override {
+        jfnk_newton = jfnk_gmres = jfnk_solves = 0;
         zfv::k_begin<<<1, 1, 0, s>>>(st(scratch), L);
         zfv::k_reduce<Model, Numerics, kReduceNT, 0, true><<<reduce_blocks(), kReduceNT, 0, s>>>(
             (const double*)Q, (const double*)A, L, st(scratch), partials(scratch));
@@ -384,6 +385,7 @@ struct RunnerT final : Runner {
                 g[j] = cs[j] * g[j];
                 res = std::fabs(g[j + 1]);
                 ++iters;
+                ++jfnk_gmres;
                 kdim = j + 1;
                 if (hn > 0.0) jscale(W.V + (j + 1) * vs, W.w, 1.0 / hn, s);
                 if (res <= target || !(hn > 0.0)) break;
@@ -421,6 +423,7 @@ struct RunnerT final : Runner {
                             "implicit_global copy");
         if (rc) return rc;
         double resid0 = -1.0;
+        ++jfnk_solves;
         for (int it = 0; it < kNewtonMax; ++it) {
             zfv::jfnk::k_residual<Model><<<jcell_blocks(), zfv::jfnk::kNT, 0, s>>>(
                 Qv, qbed, W.qexp, W.S, W.F, L, st(scratch), W.part);
@@ -433,6 +436,7 @@ struct RunnerT final : Runner {
             const double resid = std::sqrt(r2);
             if (it == 0) resid0 = resid;
             if (resid < 1e-12 || (resid0 > 0.0 && resid < 1e-9 * resid0)) break;
+            ++jfnk_newton;
             jscale(W.F, W.F, -1.0, s);                      // rhs = -F
             double qq, bb = 0.0;                            // |Q| over all components
             rc = jdots(W, Qv, Qv, 0, 1, N, &qq, s);
@@ -690,6 +694,14 @@ size_t zfv_scratch_bytes(const zfv_handle* h) { return h ? h->lay.total : 0; }
 int zfv_begin(zfv_handle* h, const void* Q, const void* aux, void* scratch, void* stream) {
     if (!h || !Q || !aux || !scratch) return fail(-1, "zfv_begin: null argument");
     return h->run->begin(Q, aux, (char*)scratch, (cudaStream_t)stream);
+}
+
+int zfv_implicit_global_stats(const zfv_handle* h, long long* solves, long long* newton, long long* gmres) {
+    if (!h) return fail(-1, "zfv_implicit_global_stats: null handle");
+    if (solves) *solves = h->run->jfnk_solves;
+    if (newton) *newton = h->run->jfnk_newton;
+    if (gmres) *gmres = h->run->jfnk_gmres;
+    return 0;
 }
 
 int zfv_update_state(zfv_handle* h, void* Q, void* aux, double time, void* stream) {

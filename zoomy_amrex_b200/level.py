@@ -160,6 +160,14 @@ class Level:
             last_step = st["step"]
         return self.status()
 
+    def implicit_global_stats(self) -> dict:
+        """Field solves, Newton iterations and GMRES iterations of the global
+        implicit source since the last begin (zeros for the point-implicit form)."""
+        v = [C.c_longlong(0) for _ in range(3)]
+        _lib.check(_lib.lib().zfv_implicit_global_stats(self._h, *[C.byref(x) for x in v]),
+                   "zfv_implicit_global_stats")
+        return dict(solves=v[0].value, newton=v[1].value, gmres=v[2].value)
+
     def state64(self) -> torch.Tensor:
         """The state in the reference layout [b, h, hu, (hv)], float64 (synchronizes)."""
         if not self.fp32:
