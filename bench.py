@@ -576,6 +576,12 @@ def main():
     amr = None
     if args.amr_steps > 0:
         amr = amr_bench(local, steps=args.amr_steps)
+        if n == 4096:
+            # the hierarchy's finest level is 4096^2: one coarse step on a
+            # uniform 4096^2 grid is 4 steps of the single-level FP32 form
+            uni = 4 * ms32 / K
+            amr["uniform_finest_ms_per_coarse_step"] = uni
+            amr["speedup_vs_uniform_finest"] = uni / amr["ms_per_coarse_step"]
 
     err = None
     if args.err_steps > 0 and rank == 0:
