@@ -121,13 +121,14 @@ k_jvp(const double* __restrict__ Qbase, const double* __restrict__ qbed, const d
     }
 }
 
-// partials[k * nblk + block] = sum over the block of w . V_k, k < nv
-// (blockIdx.y = k; V_k = V + k * vstride).
+// partials[k * nblk + block] = sum over the block of w . V_k for k <
+// gridDim.y (blockIdx.y = k; V_k = V + k * vstride); with self_last the last
+// k is w . w instead.
 __global__ void __launch_bounds__(kNT)
 k_dots(const double* __restrict__ w, const double* __restrict__ V, long long vstride, long long N,
-       double* __restrict__ partials) {
+       double* __restrict__ partials, int self_last) {
     __shared__ double red[kNT / 32];
-    const double* v = V + blockIdx.y * vstride;
+    const double* v = (self_last && blockIdx.y == gridDim.y - 1) ? w : V + blockIdx.y * vstride;
     double s = 0.0;
     for (long long e = (long long)blockIdx.x * kNT + threadIdx.x; e < N; e += (long long)gridDim.x * kNT)
         s += w[e] * v[e];

@@ -263,12 +263,13 @@ struct RunnerT final : Runner {
     // Newton: at most 12 iterations, stop at |F| < 1e-12 or |F| < 1e-9 |F_0|,
     // linear tolerance 1e-4 relative (imex_solver.H:124-140). GMRES: restarted
     // every 30 iterations, at most 40 iterations per solve, classical
-    // Gram-Schmidt applied twice, Givens rotations on the host.
+    // Gram-Schmidt applied twice (two host round trips per iteration: the
+    // second pass also returns |w|^2), Givens rotations on the host.
     static constexpr int n0 = zfv::static_bed<Model>::value ? 1 : 0;
     static constexpr int kNewtonMax = 12;
     static constexpr int kRestart = 30;
     static constexpr int kMaxIter = 40;
-    static_assert(kRestart + 1 <= zfv::jfnk::kMaxDots, "Krylov basis larger than one multi-dot launch");
+    static_assert(kRestart + 2 <= zfv::jfnk::kMaxDots, "Krylov basis larger than one multi-dot launch");
 
     bool jfnk() const { return h->cfg.implicit_source && h->cfg.implicit_global; }
     long long jN() const { return (long long)(nq - n0) * L.plane; }
@@ -304,13 +305,15 @@ struct RunnerT final : Runner {
     }
     long long jstride() const { return (long long)(jvec_bytes() / sizeof(double)); }
 
-    // host[k] = w . V_k for k < nv (synchronizes the stream).
+    // host[k] = w . V_k for k < nv, and with self_last host[nv] = w . w
+    // (synchronizes the stream).
     int jdots(const JW& W, const double* w, const double* V, long long vstride, int nv, long long n,
-              double* host, cudaStream_t s) {
+              double* host, cudaStream_t s, bool self_last = false) {
         const int nb = jvec_blocks();
-        zfv::jfnk::k_dots<<<dim3(nb, nv), zfv::jfnk::kNT, 0, s>>>(w, V, vstride, n, W.part);
-        zfv::jfnk::k_sum_partials<<<nv, zfv::jfnk::kNT, 0, s>>>(W.part, nb, W.out);
-        int rc = cuda_check(cudaMemcpyAsync(host, W.out, sizeof(double) * nv, cudaMemcpyDeviceToHost, s),
+        const int nt = nv + (self_last ? 1 : 0);
+        zfv::jfnk::k_dots<<<dim3(nb, nt), zfv::jfnk::kNT, 0, s>>>(w, V, vstride, n, W.part, self_last ? 1 : 0);
+        zfv::jfnk::k_sum_partials<<<nt, zfv::jfnk::kNT, 0, s>>>(W.part, nb, W.out);
+        int rc = cuda_check(cudaMemcpyAsync(host, W.out, sizeof(double) * nt, cudaMemcpyDeviceToHost, s),
                             "implicit_global dot read-back");
         if (!rc) rc = cuda_check(cudaStreamSynchronize(s), "implicit_global dot");
         return rc;
@@ -361,14 +364,19 @@ struct RunnerT final : Runner {
                 if (rc) return rc;
                 for (int k = 0; k <= j; ++k) hcol[k] = -hcol[k];
                 jcombine(W.w, 1.0, W.V, j + 1, hcol, s);
-                rc = jdots(W, W.w, W.V, vs, j + 1, N, h2, s);
+                // second pass, with |w|^2 in the same reduction: after it
+                // |w'|^2 = |w|^2 - |h2|^2 (V orthonormal; h2 is round-off
+                // small after the first pass, so nothing cancels)
+                rc = jdots(W, W.w, W.V, vs, j + 1, N, h2, s, true);
                 if (rc) return rc;
-                for (int k = 0; k <= j; ++k) { hcol[k] = -hcol[k] + h2[k]; h2[k] = -h2[k]; }
+                double hn = h2[j + 1];
+                for (int k = 0; k <= j; ++k) {
+                    hn -= h2[k] * h2[k];
+                    hcol[k] = -hcol[k] + h2[k];
+                    h2[k] = -h2[k];
+                }
                 jcombine(W.w, 1.0, W.V, j + 1, h2, s);
-                double hn;
-                rc = jdots(W, W.w, W.w, 0, 1, N, &hn, s);
-                if (rc) return rc;
-                hn = std::sqrt(hn);
+                hn = std::sqrt(std::max(hn, 0.0));
                 for (int k = 0; k <= j; ++k) H[k][j] = hcol[k];
                 H[j + 1][j] = hn;
                 for (int k = 0; k < j; ++k) {              // previous rotations
