@@ -133,11 +133,15 @@ namespace zfv32 {
 //      asynchronous copies issued at the top of each row;
 //   2  the stage-2 kernel is capped at 128 registers (4 blocks of 128
 //      threads per SM instead of 3, at the cost of some spilling).
-constexpr int kNumVariants = 10;
-constexpr int kVarNW[kNumVariants] = {4, 4, 4, 4, 4, 4, 4, 4, 4, 4};
-constexpr int kVarCPT[kNumVariants] = {16, 8, 16, 8, 16, 8, 16, 8, 16, 8};
-constexpr int kVarPK[kNumVariants] = {1, 1, 2, 2, 1, 1, 2, 2, 2, 2};
-constexpr int kVarPF[kNumVariants] = {0, 0, 0, 0, 1, 1, 1, 1, 3, 3};
+// Short strips (4 or 2 rows per warp) spend more on the y halo but finish a
+// unit sooner: levels of a few million cells (AMR levels, ensemble boxes)
+// fill the GPU for about one wave, so a launch there lasts about as long as
+// one unit takes.
+constexpr int kNumVariants = 13;
+constexpr int kVarNW[kNumVariants] = {4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4};
+constexpr int kVarCPT[kNumVariants] = {16, 8, 16, 8, 16, 8, 16, 8, 16, 8, 4, 4, 2};
+constexpr int kVarPK[kNumVariants] = {1, 1, 2, 2, 1, 1, 2, 2, 2, 2, 1, 2, 2};
+constexpr int kVarPF[kNumVariants] = {0, 0, 0, 0, 1, 1, 1, 1, 3, 3, 1, 3, 3};
 
 template <class F>
 int with_variant(int v, F&& f) {
@@ -152,6 +156,9 @@ int with_variant(int v, F&& f) {
     case 7: return f.template operator()<4, 8, 2, 1>();
     case 8: return f.template operator()<4, 16, 2, 3>();
     case 9: return f.template operator()<4, 8, 2, 3>();
+    case 10: return f.template operator()<4, 4, 1, 1>();
+    case 11: return f.template operator()<4, 4, 2, 3>();
+    case 12: return f.template operator()<4, 2, 2, 3>();
     default: return fail(-1, "unknown strip variant %d", v);
     }
 }
