@@ -15,6 +15,7 @@ updates over all ranks divided by it.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import pathlib
@@ -408,12 +409,19 @@ def adjoint_bench(local, n=1024, steps=200, every=20, n_dirs=32, eps=1e-6, seed=
         return 0.5 * (e * e).sum()
 
     base = torch.from_numpy(Q0).to(dev)
-    # warm-up: one short differentiable run (first launches load the kernels)
+    # warm-up: one short differentiable run with the timed run's checkpoint
+    # interval (first launches load the kernels; the tape of one segment is
+    # then in torch's caching allocator, as in any repeated gradient loop)
     qw = base.clone().requires_grad_(True)
     nmw = torch.tensor(0.03, dtype=torch.float64, device=dev, requires_grad=True)
-    loss_of(evolve_differentiable(qw, nmw, A, cfg, 4, checkpoint_every=2)).backward()
-    # forward alone (zfv_evolve, no checkpoints)
+    loss_of(evolve_differentiable(qw, nmw, A, cfg, 2 * every, checkpoint_every=every)).backward()
+    del qw, nmw
+    # forward alone (zfv_evolve, no checkpoints); Python's cyclic collector
+    # is run before, and kept out of, the timed regions (host stalls there
+    # would show up as device idle time between the events)
     forward_only(base, A, cfg, 3)
+    gc.collect()
+    gc.disable()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -436,6 +444,7 @@ def adjoint_bench(local, n=1024, steps=200, every=20, n_dirs=32, eps=1e-6, seed=
     b1.record()
     torch.cuda.synchronize()
     ms_bwd = b0.elapsed_time(b1)
+    gc.enable()
     gq, gnm = q.grad.detach(), float(nm.grad)
     # central differences on seeded directions (wet cells only for h, hu, hv:
     # a dry cell's depth cannot be perturbed both ways)
