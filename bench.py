@@ -49,6 +49,12 @@ BYTES_PER_CELL_STEP_FP32 = 92
 # 3072^2 cells. The traffic scales with the cells, so it is scaled to the
 # benchmark grid per launch.
 NCU_TRAFFIC_PER_CELL_STEP_FP32 = 85.36
+# Warp instructions per cell per step of the same capture (stage 1 13.51 +
+# stage 2 17.80): the FP32 stages are bound by instruction issue, so the
+# line also reports the issue rate they reach against the SMs' peak (148 SMs
+# x 4 schedulers x 1 warp instruction per cycle at the sampled SM clock).
+NCU_WARP_INSTR_PER_CELL_STEP_FP32 = 31.31
+N_SM, SCHEDULERS_PER_SM = 148, 4
 
 
 def parse():
@@ -575,6 +581,14 @@ def main():
                 "fp64_plain": {"achieved": achieved64, "frac": achieved64 / peak,
                                "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_FP64,
                                "bound": "fp64 alu"}}
+    sm_mhz = (clk.summary() or {}).get("sm_mhz") or 1965.0
+    issue_peak = N_SM * SCHEDULERS_PER_SM * sm_mhz * 1e6
+    issue = cells * NCU_WARP_INSTR_PER_CELL_STEP_FP32 / step32
+    roofline["issue"] = {"achieved": issue, "peak": issue_peak, "unit": "warp instructions/s",
+                         "frac": issue / issue_peak,
+                         "warp_instructions_per_cell_step": NCU_WARP_INSTR_PER_CELL_STEP_FP32,
+                         "note": "the bound the FP32 stages meet (ncu: issue active 57-68 %); "
+                                 "instructions per cell from the ncu capture of the same kernels"}
 
     ens = None
     if args.ensemble_steps > 0:
