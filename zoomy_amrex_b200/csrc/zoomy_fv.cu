@@ -327,14 +327,13 @@ struct RunnerT final : Runner {
         zfv::jfnk::k_scale<<<jvec_blocks(), zfv::jfnk::kNT, 0, s>>>(dst, src, f, jN());
     }
     // Ax = J x at Qv (ImpSrcOp::apply): eps = 1e-7 (1 + |Q|) / |x|
-    void jjvp(const double* Qv, const double* qbed, const JW& W, const zfv::DevState* state, const double* x,
-              double xnorm, double nrmQ, double* Ax, cudaStream_t s) {
-        if (xnorm == 0.0) {
-            cudaMemsetAsync(Ax, 0, sizeof(double) * jN(), s);
-            return;
-        }
+    int jjvp(const double* Qv, const double* qbed, const JW& W, const zfv::DevState* state, const double* x,
+             double xnorm, double nrmQ, double* Ax, cudaStream_t s) {
+        if (xnorm == 0.0)
+            return cuda_check(cudaMemsetAsync(Ax, 0, sizeof(double) * jN(), s), "implicit_global memset");
         const double eps = 1e-7 * (1.0 + nrmQ) / xnorm;
         zfv::jfnk::k_jvp<Model><<<jcell_blocks(), zfv::jfnk::kNT, 0, s>>>(Qv, qbed, W.S, x, eps, Ax, L, state);
+        return cuda_check(cudaGetLastError(), "implicit_global J x launch");
     }
 
     // GMRES on J x = b from x = 0 (x, b: vectors; J at the Newton iterate Qv
@@ -359,8 +358,8 @@ struct RunnerT final : Runner {
             double res = beta;
             for (int j = 0; j < kRestart && iters < kMaxIter; ++j) {
                 double* Vj = W.V + j * vs;
-                jjvp(Qv, qbed, W, state, Vj, 1.0, nrmQ, W.w, s);   // |V_j| = 1
-                rc = jdots(W, W.w, W.V, vs, j + 1, N, hcol, s);
+                rc = jjvp(Qv, qbed, W, state, Vj, 1.0, nrmQ, W.w, s);   // |V_j| = 1
+                if (!rc) rc = jdots(W, W.w, W.V, vs, j + 1, N, hcol, s);
                 if (rc) return rc;
                 for (int k = 0; k <= j; ++k) hcol[k] = -hcol[k];
                 jcombine(W.w, 1.0, W.V, j + 1, hcol, s);
@@ -409,7 +408,8 @@ struct RunnerT final : Runner {
             double xn;
             rc = jdots(W, x, x, 0, 1, N, &xn, s);
             if (rc) return rc;
-            jjvp(Qv, qbed, W, state, x, std::sqrt(xn), nrmQ, W.w, s);
+            rc = jjvp(Qv, qbed, W, state, x, std::sqrt(xn), nrmQ, W.w, s);
+            if (rc) return rc;
             jscale(W.V, b, 1.0, s);
             const double m1 = -1.0;
             jcombine(W.V, 1.0, W.w, 1, &m1, s);
