@@ -257,6 +257,7 @@ k32b_reduce(const BInst* __restrict__ insts, const int2* __restrict__ units, int
     if (!s_last) return;
     __threadfence();
     double gm = 0.0, gs = 0.0;
+#pragma unroll 8
     for (unsigned b = threadIdx.x; b < nblk; b += NT) {
         const double pm = __ldcg(&sD.partials[2 * b]), ps = __ldcg(&sD.partials[2 * b + 1]);
         if (pm > gm) gm = pm;

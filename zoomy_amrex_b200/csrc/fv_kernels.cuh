@@ -124,6 +124,9 @@ __device__ __forceinline__ bool finish_step_units(double m, double s, double* re
     if (!s_last) return false;
     __threadfence();
     double gm = 0.0, gs = 0.0;
+    // unrolled so that many loads are in flight: this loop is the serial tail
+    // of every step (same order of additions as a plain loop)
+#pragma unroll 8
     for (unsigned b = threadIdx.x; b < nblk; b += NT) {
         const double pm = __ldcg(&partials[2 * b]);
         const double ps = __ldcg(&partials[2 * b + 1]);
@@ -547,6 +550,7 @@ k_reduce(const double* Q, const double* A, LevelParams<double, Model::n_paramete
     if (!s_last) return;
     __threadfence();
     double gm = 0.0, gs = 0.0;
+#pragma unroll 8
     for (unsigned b = threadIdx.x; b < gridDim.x; b += NT) {
         const double pm = __ldcg(&partials[2 * b]), ps = __ldcg(&partials[2 * b + 1]);
         if (pm > gm) gm = pm;
