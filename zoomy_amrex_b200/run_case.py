@@ -1,4 +1,5 @@
-"""``run_case`` — run a model on a structured single-level grid on the GPU.
+"""``run_case`` — run a model on a structured grid on the GPU (one level, or an
+AMR hierarchy when ``max_level > 0``).
 
 Same entry shape as zoomy_amrex.run_case.run_case (zoomy_amrex/run_case.py:346-426):
 ``run_case(model, settings, output_dir)``. The reference generates C++,
@@ -23,6 +24,16 @@ from .models import SWE, initial_state
 from .settings import config_from_settings, grid
 
 
+def _precision(settings: dict) -> int:
+    """settings['precision']: "fp64" (default; the reference's arithmetic) or
+    "fp32" (the FP32 chosen form: SWE2D, order 2)."""
+    from ._abi import ZFV_PREC_FP32, ZFV_PREC_FP64
+    p = str(settings.get("precision", "fp64")).lower()
+    if p not in ("fp64", "fp32"):
+        raise ValueError(f"precision must be 'fp64' or 'fp32', got {p!r}")
+    return ZFV_PREC_FP32 if p == "fp32" else ZFV_PREC_FP64
+
+
 @dataclass
 class CaseResult:
     Q: np.ndarray          # (n_q, ny, nx) final state
@@ -39,11 +50,12 @@ def run_case(model: SWE, settings: dict, output_dir: str | None = None, on_progr
     """March ``model`` to settings['time_end'] (or settings['max_step'] steps)."""
     from .level import Level   # needs torch + the CUDA library
 
-    if settings.get("max_level", 0):
-        raise NotImplementedError("adaptive refinement (max_level > 0) is not part of this build")
     if settings.get("mpi_ranks", 1) not in (None, 1):
         raise NotImplementedError("one level runs on one GPU; mpi_ranks must be 1")
-    cfg = config_from_settings(model, settings)
+    if int(settings.get("max_level", 0) or 0) > 0:
+        return _run_case_amr(model, settings, output_dir, on_progress, device)
+    precision = _precision(settings)
+    cfg = config_from_settings(model, settings, precision=precision)
     _, nx, ny, lo, hi = grid(settings)
     Q0, A0 = initial_state(model, nx, ny, lo, hi)
     lev = Level(cfg, Q0, A0, device=device)
@@ -102,5 +114,72 @@ def run_case(model: SWE, settings: dict, output_dir: str | None = None, on_progr
     if out is not None:
         p = out / "final.npz"
         np.savez(p, Q=Q, Qaux=A, time=res.time, steps=res.steps, log=log)
+        res.path = str(p)
+    return res
+
+
+def _run_case_amr(model: SWE, settings: dict, output_dir, on_progress, device) -> CaseResult:
+    """max_level > 0: the AMR hierarchy (amr.AmrHierarchy, FP32 form) with the
+    deck the reference's run_case writes for it (build.py:96-119: ref ratio 2,
+    regrid every 2 coarse steps, tagging.threshold 0.02 with its ErrorEst
+    criterion, optional tagging.b_max, boxes up to max_grid_size 64). Blocks
+    are the largest power of two <= max_grid_size (>= 8) dividing both grid
+    sides. Plotfiles of all levels are written at the reference's output
+    times; the result holds the base level."""
+    from ._abi import ZFV_PREC_FP32
+    from .amr import AmrHierarchy
+    if model.dimension != 2 or int(settings.get("spatial_order", 1)) != 2:
+        raise NotImplementedError("AMR runs the FP32 form: 2-D SWE at spatial_order 2")
+    if str(settings.get("positivity", "none")) == "mood" or settings.get("clamp_positivity"):
+        raise NotImplementedError("AMR runs the FP32 form, which has no MOOD / clamp_positivity")
+    cfg = config_from_settings(model, settings, precision=ZFV_PREC_FP32)
+    _, nx, ny, lo, hi = grid(settings)
+    Q0, _ = initial_state(model, nx, ny, lo, hi)
+    mgs = int(settings.get("max_grid_size", 64))
+    B = next((b for b in (64, 32, 16, 8) if b <= mgs and nx % b == 0 and ny % b == 0), None)
+    if B is None:
+        raise ValueError(f"AMR needs both grid sides ({nx} x {ny}) divisible by a block side of 8 .. "
+                         f"{min(64, mgs)}")
+    hier = AmrHierarchy(cfg, Q0, max_level=int(settings["max_level"]), B=B,
+                        threshold=float(settings.get("tag_threshold", 0.02)), regrid_int=2, device=device,
+                        tag="reference", tag_b_max=float(settings.get("tag_b_max", 1.0e30)))
+    out = pathlib.Path(output_dir) if output_dir is not None else None
+    tend = float(settings.get("time_end", 1.0))
+    plot_dt = tend / max(1, int(settings.get("output_snapshots", 10)))
+    identifier = str(settings.get("identifier", "0"))
+    max_step = cfg.max_step
+    plots = []
+    try:
+        if out is not None:
+            out.mkdir(parents=True, exist_ok=True)
+        next_plot, index = 0.0, 0
+        t = hier.time
+        while t < tend and (max_step < 0 or hier.steps < max_step):
+            if out is not None and t >= next_plot:
+                plots.append(hier.write_plotfile(out, identifier, index))
+                next_plot += plot_dt
+                index += 1
+            hier.step()
+            t_new = hier.time
+            if on_progress is not None:
+                on_progress(hier.steps, t_new, t_new - t)
+            if not t_new > t:
+                raise RuntimeError(f"run_case (AMR): no progress at coarse step {hier.steps}, time {t_new}")
+            t = t_new
+        if out is not None:
+            plots.append(hier.write_plotfile(out, identifier, index))
+        Q = hier.level_state(0)
+        L0 = hier.levels[0]
+        A = np.zeros((L0.batch.aux[0].shape[0], L0.ny, L0.nx))
+        for (bx, by, nbx, nby), a in zip(L0.patches, L0.batch.aux):
+            A[:, by * B:(by + nby) * B, bx * B:(bx + nbx) * B] = a.cpu().numpy()
+        steps = hier.steps
+    finally:
+        hier.close()
+    res = CaseResult(Q=Q, Qaux=A, time=t, steps=steps, log=np.zeros((0, 3)))
+    res.plotfiles = plots
+    if out is not None:
+        p = out / "final.npz"
+        np.savez(p, Q=Q, Qaux=A, time=t, steps=steps)
         res.path = str(p)
     return res

@@ -56,7 +56,8 @@ class HyperbolicSolver:
              "time_end": _get(settings, "time_end", 1.0),
              "output_snapshots": _get(settings, "output.snapshots", 10),
              "max_level": _get(settings, "max_level", 0)}
-        for k in ("dtmax", "dtmin", "max_step", "params", "implicit_source"):
+        for k in ("dtmax", "dtmin", "max_step", "params", "implicit_source", "implicit_global", "precision",
+                  "max_grid_size"):
             v = _get(settings, k)
             if v is not None:
                 s[k] = v
