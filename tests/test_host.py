@@ -155,3 +155,13 @@ def test_amr_patches_tile_the_blocks():
             assert 1 <= nbx <= side and 1 <= nby <= side
             cover[by:by + nby, bx:bx + nbx] += 1
         assert np.array_equal(cover, mask.astype(int))
+
+
+def test_run_case_rejects_fluxes_not_built():
+    """A non-default Riemann solver is refused before any device work."""
+    import pytest
+    from zoomy_amrex_b200.models import SWE
+    from zoomy_amrex_b200.run_case import run_case
+    with pytest.raises(NotImplementedError, match="NonconservativeRusanov"):
+        run_case(SWE(2, "wall", None), dict(dimension=2, domain=[0, 1, 0, 1], n_cells=[8, 8],
+                                            riemann="PositiveNonconservativeHLL"))

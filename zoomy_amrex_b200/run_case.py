@@ -52,6 +52,10 @@ def run_case(model: SWE, settings: dict, output_dir: str | None = None, on_progr
 
     if settings.get("mpi_ranks", 1) not in (None, 1):
         raise NotImplementedError("one level runs on one GPU; mpi_ranks must be 1")
+    riemann = settings.get("riemann")
+    if riemann is not None and getattr(riemann, "__name__", riemann) != "NonconservativeRusanov":
+        raise NotImplementedError(f"riemann={riemann!r}: the flux built here is the printer's default "
+                                  "NonconservativeRusanov (zoomy_core's other solvers are not part of the reference)")
     if int(settings.get("max_level", 0) or 0) > 0:
         return _run_case_amr(model, settings, output_dir, on_progress, device)
     precision = _precision(settings)
