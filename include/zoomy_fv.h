@@ -150,6 +150,14 @@ int zfv_begin(zfv_handle* h, const void* Q, const void* aux, void* scratch, void
  * Q and aux are updated in place.
  */
 int zfv_update_state(zfv_handle* h, void* Q, void* aux, double time, void* stream);
+/*
+ * init_solution (Source/init_solution.cpp:78-116) on the device into a
+ * (n_comp, ny, nx) float64 field of the handle's grid: zeros, and for
+ * n_comp >= 2 the flat-bed dam break b = 0, h = 2 (x < x mid-point) | 1.
+ * InitData applies it to Q and Qaux (ZoomyAmr.cpp:174-175); a caller uses
+ * it to create aux0 on the device instead of copying it from the host.
+ */
+int zfv_init_solution(const zfv_handle* h, double* field, int n_comp, void* stream);
 /* Work of the global implicit source (implicit_global; SolveImplicitSourceGlobal,
  * imex_solver.H:102-160) since the last zfv_begin: field solves (one per
  * stage), Newton iterations that ran a linear solve, and GMRES iterations.
@@ -266,10 +274,16 @@ int zfv_batch_units(const zfv_batch* b);
  * asynchronous copies at the top of each row, bit 1 = the stage-2 kernel is
  * capped at 128 registers).
  * zfv_tile_variants writes up to max_n of them and returns how many exist;
- * zfv_batch_set_variant selects one (the autotuner in
- * zoomy_amrex_b200/autotune.py measures them and caches the fastest per n_dof_q).
+ * zfv_batch_set_variant selects one for a batch, zfv_set_variant for a
+ * single FP32 level (the autotuner in zoomy_amrex_b200/autotune.py measures
+ * them and caches the fastest per n_dof_q). Until one is selected, batches and
+ * FP32 levels use variant 9 (4 warps x 8 rows, column pairs, flags 3).
+ * The FP64 form has one tile shape: zfv_set_variant fails with -2 there and
+ * zfv_get_variant returns -1.
  */
 int zfv_tile_variants(int* nw, int* cpt, int* cols, int* flags, int max_n);
+int zfv_set_variant(zfv_handle* h, int variant, void* stream);
+int zfv_get_variant(const zfv_handle* h);
 
 /*
  * Batches whose instances are grouped: instances with the same group id

@@ -13,9 +13,9 @@ from zoomy_amrex_b200.workloads import dam_break_ensemble, fp64_twin
 pytestmark = pytest.mark.gpu
 
 
-def _single(cfg, Q0, A0, steps_chunk=16):
+def _single(cfg, Q0, A0, steps_chunk=16, variant=None):
     from zoomy_amrex_b200.level import Level
-    lev = Level(cfg, Q0, A0)
+    lev = Level(cfg, Q0, A0, variant=variant)
     try:
         st = lev.run(chunk=steps_chunk)
         return lev.state64().cpu().numpy(), lev.aux.cpu().numpy(), st, lev.log()
@@ -35,13 +35,13 @@ def test_batch_equals_single_levels(cuda):
         cfg.max_step = 20 + 7 * k           # instances stop at different steps
         cfg.params[3] = 0.01 * (k + 1)      # own Manning n
     cfgs, Q0s, A0s = zip(*ens)
-    b = Batch(cfgs, Q0s, A0s, variant=0)   # the strip shape of a single FP32 level
+    b = Batch(cfgs, Q0s, A0s, variant=0)
     st = b.run(chunk=16)
     Qb = [q.cpu().numpy() for q in b.state64()]
     Ab = [a.cpu().numpy() for a in b.aux]
     b.close()
     for k, (cfg, Q0, A0) in enumerate(ens):
-        Qs, As, ss, _ = _single(cfg, Q0, A0)
+        Qs, As, ss, _ = _single(cfg, Q0, A0, variant=0)   # the same strip shape
         assert st[k]["step"] == ss["step"] == cfg.max_step
         assert st[k]["time"] == ss["time"]
         assert np.array_equal(Qb[k], Qs), k
@@ -154,3 +154,42 @@ def test_batch_rejects_mixed_schemes(cuda):
     cfgs, Q0s, A0s = zip(*ens)
     with pytest.raises(_lib.ZfvError, match="share well_balanced"):
         Batch(cfgs, Q0s, A0s)
+
+
+def test_single_level_strip_shape_selection(cuda):
+    """An FP32 level starts on the library's default strip shape, switches
+    shape on request (a batch of one on the same shape gives the same bits),
+    and the FP64 form refuses a shape."""
+    from zoomy_amrex_b200 import _lib
+    from zoomy_amrex_b200.batch import DEFAULT_VARIANT, Batch, tile_variants
+    from zoomy_amrex_b200.level import Level
+    cfg, Q0, A0 = _ens(1, seed=9, side_range=(150, 151))[0]
+    cfg.max_step = 12
+    lev = Level(cfg, Q0, A0, variant=None)
+    try:
+        from zoomy_amrex_b200.autotune import cached_variant
+        want = cached_variant(4, "fp32", cfg.nx * cfg.ny)
+        assert lev.variant == (DEFAULT_VARIANT if want is None else want)
+        for v in (0, 3, len(tile_variants()) - 1):
+            lev.set_variant(v)
+            assert lev.variant == v
+        with pytest.raises(_lib.ZfvError):
+            lev.set_variant(len(tile_variants()))
+    finally:
+        lev.close()
+    for v in (1, 11):
+        Qs, _, ss, _ = _single(cfg, Q0, A0, variant=v)
+        b = Batch([cfg], [Q0], [A0], variant=v)
+        st = b.run(chunk=16)
+        Qb = b.state64()[0].cpu().numpy()
+        b.close()
+        assert st[0]["step"] == ss["step"] == 12
+        assert np.array_equal(Qb, Qs), v
+    from zoomy_amrex_b200.workloads import fp64_twin
+    lev64 = Level(fp64_twin(cfg), Q0, A0)
+    try:
+        assert lev64.variant == -1
+        with pytest.raises(_lib.ZfvError):
+            lev64.set_variant(0)
+    finally:
+        lev64.close()

@@ -271,3 +271,57 @@ def test_mood_whole_step_redo_bitwise(cuda, oracle):
         assert st["mood_redos"] == redos and st["flags"] & 2
         assert np.array_equal(Qg, Qo) and np.array_equal(Ag, Ao)
         assert np.array_equal(logg[:, :2], logo[:, :2])
+
+
+@pytest.mark.parametrize("name", ["dambreak_o2", "wetdry_o1_impl", "wetdry_moving_o2_mixed_bc"])
+def test_init_solution_on_device_bitwise(cuda, oracle, name):
+    """zfv_init_solution writes init_solution's fields (init_solution.cpp:78-116)
+    bit for bit as the oracle does, for the state's and the aux's component
+    counts; a level created with aux0 = None (aux made on the device) runs
+    bitwise like one given the host aux."""
+    import torch
+    from zoomy_amrex_b200 import _lib
+    from zoomy_amrex_b200.level import Level
+    cfg, Q0, A0 = setup(*CASES_2D[name])
+    Qi, Ai = oracle.init_solution(cfg)
+    lev = Level(cfg, Q0, None)
+    try:
+        for ref in (Qi, Ai):
+            f = torch.full(ref.shape, float("nan"), dtype=torch.float64, device=lev.device)
+            _lib.check(_lib.lib().zfv_init_solution(lev.handle, f.data_ptr(), ref.shape[0], lev._s()),
+                       "zfv_init_solution")
+            lev.sync()
+            assert np.array_equal(f.cpu().numpy(), ref)
+        assert np.array_equal(lev.aux.cpu().numpy(), A0)
+        st = lev.run(chunk=16)
+        Qg, Ag = lev.Q.cpu().numpy(), lev.aux.cpu().numpy()
+    finally:
+        lev.close()
+    Qo, Ao, n, t, _, _ = oracle.run(cfg, Q0, A0)
+    assert st["step"] == n and st["time"] == t
+    assert np.array_equal(Qg, Qo) and np.array_equal(Ag, Ao)
+
+
+@pytest.mark.parametrize("shape", [(1, 37, 1), (2, 33, 17)])
+def test_init_solution_odd_grids_and_offsets(cuda, oracle, shape):
+    """Grids with an odd cell count and a shifted x range (the split point is
+    then a cell boundary or a cell centre), 1-D and 2-D."""
+    import torch
+    from zoomy_amrex_b200 import _lib
+    from zoomy_amrex_b200.level import Level
+    from zoomy_amrex_b200._abi import ZFV_MODEL_SWE1D, ZFV_MODEL_SWE2D, make_config
+    dim, nx, ny = shape
+    model = ZFV_MODEL_SWE1D if dim == 1 else ZFV_MODEL_SWE2D
+    cfg = make_config(model, nx, ny, (-3.25, 0.0), (7.0, 1.0), spatial_order=2, bc=("extrapolation",) * 4)
+    Qi, Ai = oracle.init_solution(cfg)
+    lev = Level(cfg, Qi, None)
+    try:
+        assert np.array_equal(lev.aux.cpu().numpy(), Ai)
+        for ref in (Qi, Ai):
+            f = torch.empty(ref.shape, dtype=torch.float64, device=lev.device)
+            _lib.check(_lib.lib().zfv_init_solution(lev.handle, f.data_ptr(), ref.shape[0], lev._s()),
+                       "zfv_init_solution")
+            lev.sync()
+            assert np.array_equal(f.cpu().numpy(), ref)
+    finally:
+        lev.close()

@@ -25,7 +25,8 @@ SYMBOLS = ("zfv_last_error", "zfv_version", "zfv_sizeof_config", "zfv_sizeof_sta
            "zfv_adj_work_bytes", "zfv_adj_record", "zfv_adj_step", "zfv_adj_variants",
            "zfv_adj_set_variant", "zfv_batch_create_grouped", "zfv_batch_set_frames", "zfv_batch_set_dt",
            "zfv_batch_stage", "zfv_batch_descriptors", "zfv_amr_fill", "zfv_amr_average_down", "zfv_amr_tag",
-           "zfv_amr_regrid_fill", "zfv_amr_set_dt", "zfv_implicit_global_stats")
+           "zfv_amr_regrid_fill", "zfv_amr_set_dt", "zfv_implicit_global_stats",
+           "zfv_init_solution", "zfv_set_variant", "zfv_get_variant")
 
 
 class ZfvError(RuntimeError):
@@ -52,6 +53,9 @@ def lib():
     L.zfv_scratch_bytes.restype = C.c_size_t
     L.zfv_begin.argtypes = [vp, vp, vp, vp, vp]
     L.zfv_update_state.argtypes = [vp, vp, vp, d, vp]
+    L.zfv_init_solution.argtypes = [vp, vp, i, vp]
+    L.zfv_set_variant.argtypes = [vp, i, vp]
+    L.zfv_get_variant.argtypes = [vp]
     L.zfv_compute_dt.argtypes = [vp, vp, vp, vp, vp]
     L.zfv_evolve.argtypes = [vp, vp, vp, vp, i, vp]
     L.zfv_rhs.argtypes = [vp, vp, vp, vp, d, vp]

@@ -20,6 +20,11 @@ from . import _lib
 from ._abi import MODELS, ZFV_MODEL_SWE2D, ZFV_PREC_FP32, zfv_config, zfv_status
 
 
+# The strip shape batches and FP32 levels use until one is selected (the
+# library's default: 4 warps x 8 rows, column pairs, flags 3).
+DEFAULT_VARIANT = 9
+
+
 def tile_variants() -> list[tuple[int, int, int, int]]:
     """The compiled strip shapes as (warps per block, rows per warp, columns
     per lane, flags: bit 0 stage-2 staging, bit 1 stage-2 kernel capped at
@@ -83,7 +88,7 @@ class Batch:
             variant = cached_variant(info["n_q"], "fp32", np.mean([c.nx * c.ny for c in self.cfgs]))
         if variant is not None:
             self.set_variant(variant)
-        self.variant = 0 if variant is None else int(variant)
+        self.variant = DEFAULT_VARIANT if variant is None else int(variant)
         if Q0s is not None:
             self.load(Q0s)
         self._graph = None

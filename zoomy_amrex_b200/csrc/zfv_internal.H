@@ -73,6 +73,12 @@ struct Runner {
     virtual int adj_step(const char*, int, double*, double*, const double*, char*, cudaStream_t) {
         return fail(-2, "zfv_adj_step: the adjoint is implemented for the FP64 SWE2D form, order 2");
     }
+    // Strip shape of the FP32 stage kernels (zfv_set_variant); the FP64 form
+    // has one tile shape.
+    virtual int set_variant(int, cudaStream_t) {
+        return fail(-2, "zfv_set_variant: strip shapes are a property of the FP32 form");
+    }
+    virtual int variant() const { return -1; }
     // Global implicit source (implicit_global): iteration counts since the
     // last begin (Newton iterations, GMRES iterations, source solves).
     long long jfnk_newton = 0, jfnk_gmres = 0, jfnk_solves = 0;

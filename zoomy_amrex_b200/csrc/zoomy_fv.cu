@@ -605,11 +605,44 @@ int model_shape(int model, int* nq, int* na, int* np, int* dim) {
     }
 }
 
+// init_solution (Source/init_solution.cpp:78-116) on the device, as the
+// reference's InitData applies it to Q and Qaux (ZoomyAmr.cpp:174-175): every
+// component zero, and for a field of >= 2 components the flat-bed dam break
+// b = 0, h = 2 | 1 split at the x mid-point. Component-major (n_comp, ny, nx).
+__global__ void k_init_solution(double* __restrict__ f, int n_comp, long long plane, int nx, double lo,
+                                double hi) {
+    const double dx = (hi - lo) / nx;
+    const double x_mid = 0.5 * (lo + hi);
+    const long long total = plane * n_comp;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        double v = 0.0;
+        if (n_comp >= 2 && e >= plane && e < 2 * plane) {
+            const int i = int((e - plane) % nx);
+            const double x = lo + (i + 0.5) * dx;
+            v = (x < x_mid) ? 2.0 : 1.0;
+        }
+        f[e] = v;
+    }
+}
+
 }  // namespace
 
 extern "C" {
 
 const char* zfv_last_error(void) { return g_err.c_str(); }
+
+int zfv_init_solution(const zfv_handle* h, double* field, int n_comp, void* stream) {
+    if (!h || !field) return fail(-1, "zfv_init_solution: null argument");
+    if (n_comp < 1) return fail(-1, "zfv_init_solution: n_comp must be >= 1");
+    const long long plane = (long long)h->cfg.nx * h->cfg.ny;
+    const long long total = plane * n_comp;
+    const long long want = (total + 255) / 256;
+    const int blocks = int(want < 148LL * 16 ? (want > 0 ? want : 1) : 148LL * 16);
+    k_init_solution<<<blocks, 256, 0, (cudaStream_t)stream>>>(field, n_comp, plane, h->cfg.nx, h->cfg.prob_lo[0],
+                                                              h->cfg.prob_hi[0]);
+    return cuda_check(cudaGetLastError(), "zfv_init_solution launch");
+}
 
 const char* zfv_version(void) { return "zoomyfv 0.1 sm_100a fp64"; }
 
@@ -703,6 +736,13 @@ int zfv_begin(zfv_handle* h, const void* Q, const void* aux, void* scratch, void
     if (!h || !Q || !aux || !scratch) return fail(-1, "zfv_begin: null argument");
     return h->run->begin(Q, aux, (char*)scratch, (cudaStream_t)stream);
 }
+
+int zfv_set_variant(zfv_handle* h, int variant, void* stream) {
+    if (!h) return fail(-1, "zfv_set_variant: null handle");
+    return h->run->set_variant(variant, (cudaStream_t)stream);
+}
+
+int zfv_get_variant(const zfv_handle* h) { return h ? h->run->variant() : -1; }
 
 int zfv_implicit_global_stats(const zfv_handle* h, long long* solves, long long* newton, long long* gmres) {
     if (!h) return fail(-1, "zfv_implicit_global_stats: null handle");

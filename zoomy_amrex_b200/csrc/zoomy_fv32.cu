@@ -142,6 +142,10 @@ constexpr int kVarNW[kNumVariants] = {4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4};
 constexpr int kVarCPT[kNumVariants] = {16, 8, 16, 8, 16, 8, 16, 8, 16, 8, 4, 4, 2};
 constexpr int kVarPK[kNumVariants] = {1, 1, 2, 2, 1, 1, 2, 2, 2, 2, 1, 2, 2};
 constexpr int kVarPF[kNumVariants] = {0, 0, 0, 0, 1, 1, 1, 1, 3, 3, 1, 3, 3};
+// Strip shape used until a caller picks one (zfv_set_variant /
+// zfv_batch_set_variant): 4 warps x 8 rows, column pairs, stage-2 staging with
+// the 128-register stage 2 -- the shape measured fastest on large levels.
+constexpr int kDefaultVariant = 9;
 
 template <class F>
 int with_variant(int v, F&& f) {
@@ -202,7 +206,7 @@ struct BatchCore {
     std::vector<const float*> frames;
     int n = 0;
     bool wb = false, impl = false;
-    int variant = 0;
+    int variant = kDefaultVariant;
     // scratch layout
     size_t off_desc = 0, off_units = 0, off_status = 0;
     std::vector<size_t> off_state, off_part, off_log, off_alt, off_inc, off_lo;
@@ -485,6 +489,8 @@ struct Runner32 final : Runner {
     int fill_ghosts(const void*, const void*, void*, void*, double, cudaStream_t) override {
         return fail(-2, "zfv_fill_ghosts: validation entry of the FP64 form only");
     }
+    int set_variant(int v, cudaStream_t s) override { return core.set_variant(v, s); }
+    int variant() const override { return core.variant; }
 };
 
 }  // namespace zfv32

@@ -35,11 +35,12 @@ class Level:
            low-order remainders of eta, hu, hv in scratch, so the state is
            read through state64() (the reference layout, FP64), which also
            refreshes aux's hinv row.
-    aux: (n_aux, ny, nx) float64, last row hinv (both forms)
+    aux: (n_aux, ny, nx) float64, last row hinv (both forms); aux0 = None
+         creates it on the device as init_solution does (zfv_init_solution)
     """
 
-    def __init__(self, cfg: zfv_config, Q0, aux0, device: str | torch.device = "cuda:0",
-                 stream: torch.cuda.Stream | None = None):
+    def __init__(self, cfg: zfv_config, Q0, aux0=None, device: str | torch.device = "cuda:0",
+                 stream: torch.cuda.Stream | None = None, variant: int | None = None):
         if not torch.cuda.is_available():
             raise _lib.ZfvError("zoomy_amrex_b200 needs a CUDA device (no CPU fallback)")
         self.cfg = cfg
@@ -52,11 +53,17 @@ class Level:
         nq, na = self.info["n_q"], self.info["n_aux"]
         shape_q, shape_a = (nq, cfg.ny, cfg.nx), (na, cfg.ny, cfg.nx)
         self.fp32 = cfg.precision == ZFV_PREC_FP32
-        self.aux = self._as_tensor(aux0, shape_a)
         nbytes = int(L.zfv_scratch_bytes(h))
         self.scratch = torch.zeros(nbytes, dtype=torch.uint8, device=self.device)
         # A dedicated stream: CUDA graphs cannot be captured on the default stream.
         self.stream = stream if stream is not None else torch.cuda.Stream(self.device)
+        if aux0 is None:
+            # init_solution on the device, as InitData fills Qaux (ZoomyAmr.cpp:174-175)
+            self.aux = torch.empty(shape_a, dtype=_DTYPE, device=self.device)
+            self.stream.wait_stream(torch.cuda.current_stream(self.device))
+            _lib.check(L.zfv_init_solution(h, _ptr(self.aux), na, self._s()), "zfv_init_solution")
+        else:
+            self.aux = self._as_tensor(aux0, shape_a)
         if self.fp32:
             q64 = self._as_tensor(Q0, shape_q)
             self.Q = torch.empty(shape_q, dtype=torch.float32, device=self.device)
@@ -70,6 +77,14 @@ class Level:
         self.stream.wait_stream(torch.cuda.current_stream(self.device))
         self._graph = None
         self._graph_steps = 0
+        if self.fp32:
+            if variant is None:   # the autotuner's pick for this size, if one was measured
+                from .autotune import cached_variant
+                variant = cached_variant(nq, "fp32", cfg.nx * cfg.ny)
+            if variant is not None:
+                self.set_variant(variant)
+        elif variant is not None:
+            raise ValueError("strip shapes (variant) are a property of the FP32 form")
 
     def _as_tensor(self, a, shape):
         t = torch.as_tensor(np.asarray(a) if not torch.is_tensor(a) else a)
@@ -79,6 +94,16 @@ class Level:
     @property
     def handle(self):
         return self._h
+
+    @property
+    def variant(self) -> int:
+        """Strip shape of the FP32 stage kernels (index into batch.tile_variants()); -1 for FP64."""
+        return int(_lib.lib().zfv_get_variant(self._h))
+
+    def set_variant(self, variant: int):
+        """Select the FP32 strip shape (drops a captured graph)."""
+        self._graph = None
+        _lib.check(_lib.lib().zfv_set_variant(self._h, int(variant), self._s()), "zfv_set_variant")
 
     def _s(self):
         return C.c_void_p(self.stream.cuda_stream)
