@@ -209,7 +209,18 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
     RS2 lo_m, hi_m, lo_0, hi_0;
     reconstruct2(wm, w0, w1, lo_m, hi_m);
     reconstruct2(w0, w1, w2, lo_0, hi_0);
-    Face2 fb = face2<1, WB>(hi_m, lo_0, L);
+    // The face below the current row enters the y balance only through
+    // f - D+ (and - P(h*_R) with WB): carry those three values from row to row
+    // instead of the whole face (6 registers instead of 14).
+    float2 gb0, gb1, gb2;
+    {
+        const Face2 fb = face2<1, WB>(hi_m, lo_0, L);
+        gb0 = sub(fb.f0, fb.dp0);
+        gb1 = sub(fb.f1, fb.dp1);
+        gb2 = sub(fb.f2, fb.dp2);
+        if constexpr (WB) gb2 = sub(gb2, fb.pr);
+    }
+    float m_f = 0.0f;    // CFL max of this sweep (>= 0, never NaN), merged into m_loc at the end
     RS2 top = hi_0;
     const float2 rdx = s2(L.rdx), rdy = s2(L.rdy), vdt = s2(dt);
     C42 w3 = fetch2<MODE, INTERIOR, VEC>(bed, X, inc_in, L, cA, j0 + 2);
@@ -291,12 +302,12 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
             float2 Ax0 = sub(sub(neg(sub(fr.f0, fl.f0)), fr.dm0), fl.dp0);
             float2 Ax1 = sub(sub(neg(sub(fr.f1, fl.f1)), fr.dm1), fl.dp1);
             float2 Ax2 = sub(sub(neg(sub(fr.f2, fl.f2)), fr.dm2), fl.dp2);
-            float2 Ay0 = sub(sub(neg(sub(ft.f0, fb.f0)), ft.dm0), fb.dp0);
-            float2 Ay1 = sub(sub(neg(sub(ft.f1, fb.f1)), ft.dm1), fb.dp1);
-            float2 Ay2 = sub(sub(neg(sub(ft.f2, fb.f2)), ft.dm2), fb.dp2);
+            float2 Ay0 = sub(sub(gb0, ft.f0), ft.dm0);
+            float2 Ay1 = sub(sub(gb1, ft.f1), ft.dm1);
+            float2 Ay2 = sub(sub(gb2, ft.f2), ft.dm2);
             if constexpr (WB) {
                 Ax1 = add(Ax1, sub(fr.pl, fl.pr));
-                Ay2 = add(Ay2, sub(ft.pl, fb.pr));
+                Ay2 = add(Ay2, ft.pl);
             }
             const float2 r0 = fma(Ax0, rdx, mul(Ay0, rdy));
             const float2 r1 = fma(Ax1, rdx, mul(Ay1, rdy));
@@ -392,7 +403,7 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                         const float evx = (fabsf(nf[k][1] * hin) + c0) * L.rfdx;
                         const float evy = (fabsf(nf[k][2] * hin) + c0) * L.rfdy;
                         const float mm_ = fmaxf(fmaxf(evx, evy), 0.0f);
-                        if (double(mm_) > m_loc) m_loc = double(mm_);
+                        m_f = fmaxf(m_f, mm_);
                         s_loc = s_loc + ((double(nf[k][0]) - double(bb[k])) + double(nl[k][0]));
                     }
                 }
@@ -415,11 +426,15 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                 }
             }
         }
-        fb = ft;
+        gb0 = sub(ft.f0, ft.dp0);
+        gb1 = sub(ft.f1, ft.dp1);
+        gb2 = sub(ft.f2, ft.dp2);
+        if constexpr (WB) gb2 = sub(gb2, ft.pr);
         top = hi_1;
         w0 = w1; w1 = w2; w2 = w3; w3 = w4;
     }
     (void)w0;
+    if (double(m_f) > m_loc) m_loc = double(m_f);
 }
 
 // Whether a paired strip's stencil lies inside the domain (columns x0-2 ..
