@@ -62,16 +62,20 @@ __device__ __forceinline__ void reconstruct2(const C42& m, const C42& c, const C
     lo = RS2{sub(c.b, hb), sub(h, hh), sub(c.e, he), sub(c.u, hu), sub(c.v, hv)};
 }
 
-struct Face2 {
-    float2 f0, f1, f2;       // central flux (h, hu, hv)
-    float2 dp0, dp1, dp2;    // D+
-    float2 dm0, dm1, dm2;    // D-
-    float2 pl, pr;           // P(h*_L), P(h*_R)
+// What a face contributes to the balance of its two cells (make_rhs.H:346-399):
+// the cell on its high side gets  l = f - D+ (- P(h*_R) in the momentum
+// normal to the face, the WB bed source), the cell on its low side loses
+// r = f + D- (- P(h*_L)); a cell's balance is l(low face) - r(high face).
+// D+ and D- differ only in the sign of the Rusanov term for h (so l0 = r0)
+// and in the bed term of the normal momentum, so 5 values describe a face.
+struct FaceLR {
+    float2 l0, l1, l2;
+    float2 r1, r2;
 };
 
 // Two faces at once from their reconstructed left (a) / right (c) states.
 template <int DIR, bool WB>
-__device__ __forceinline__ Face2 face2(RS2 a, RS2 c, const Params& L) {
+__device__ __forceinline__ FaceLR face2(RS2 a, RS2 c, const Params& L) {
     float2 db = s2(0.0f);
     if constexpr (WB) {
         const float2 bf = fmax2(a.b, c.b);
@@ -98,24 +102,24 @@ __device__ __forceinline__ Face2 face2(RS2 a, RS2 c, const Params& L) {
         fuL = mul(a.u, qL);  fvL = fma(a.v, qL, pL);
         fuR = mul(c.u, qR);  fvR = fma(c.v, qR, pR);
     }
-    Face2 F;
-    F.f0 = mul(half, add(unL, unR));
-    F.f1 = mul(half, add(fuL, fuR));
-    F.f2 = mul(half, add(fvL, fvR));
+    const float2 f0 = mul(half, add(unL, unR));
+    const float2 f1 = mul(half, add(fuL, fuR));
+    const float2 f2_ = mul(half, add(fvL, fvR));
     const float2 evL = add(fabs2(qL), sqrt2(mul(g, fmax2(a.h, s2(0.0f)))));
     const float2 evR = add(fabs2(qR), sqrt2(mul(g, fmax2(c.h, s2(0.0f)))));
-    const float2 hs = mul(half, fmax2(evL, evR));
+    const float2 nhs = neg(mul(half, fmax2(evL, evR)));    // -(Rusanov speed) / 2
     const float2 dh = sub(c.h, a.h), du = sub(c.u, a.u), dv = sub(c.v, a.v);
-    float2 bu = s2(0.0f), bv = s2(0.0f);
-    if constexpr (!WB) {
-        const float2 Bn = mul(mul(hg, mul(half, add(a.h, c.h))), db);
-        if (DIR == 0) bu = Bn; else bv = Bn;
-    }
-    F.dp0 = mul(hs, dh);      F.dm0 = neg(F.dp0);
-    F.dp1 = fma(hs, du, bu);  F.dm1 = fma(neg(hs), du, bu);
-    F.dp2 = fma(hs, dv, bv);  F.dm2 = fma(neg(hs), dv, bv);
-    F.pl = pL;
-    F.pr = pR;
+    FaceLR F;
+    F.l0 = fma(nhs, dh, f0);
+    const float2 b1 = fma(nhs, du, f1), b2 = fma(nhs, dv, f2_);
+    F.l1 = F.r1 = b1;
+    F.l2 = F.r2 = b2;
+    // the normal momentum: WB pressure terms P(h*_R) / P(h*_L), else the
+    // path-conservative bed product g (hL + hR)/2 (bR - bL) in D+ and D-
+    const float2 kl = WB ? pR : mul(mul(hg, mul(half, add(a.h, c.h))), db);
+    const float2 kr = WB ? pL : neg(kl);
+    if constexpr (DIR == 0) { F.l1 = sub(b1, kl); F.r1 = sub(b1, kr); }
+    else                    { F.l2 = sub(b2, kl); F.r2 = sub(b2, kr); }
     return F;
 }
 
@@ -214,11 +218,8 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
     // instead of the whole face (6 registers instead of 14).
     float2 gb0, gb1, gb2;
     {
-        const Face2 fb = face2<1, WB>(hi_m, lo_0, L);
-        gb0 = sub(fb.f0, fb.dp0);
-        gb1 = sub(fb.f1, fb.dp1);
-        gb2 = sub(fb.f2, fb.dp2);
-        if constexpr (WB) gb2 = sub(gb2, fb.pr);
+        const FaceLR fb = face2<1, WB>(hi_m, lo_0, L);
+        gb0 = fb.l0; gb1 = fb.l1; gb2 = fb.l2;
     }
     float m_f = 0.0f;    // CFL max of this sweep (>= 0, never NaN), merged into m_loc at the end
     RS2 top = hi_0;
@@ -269,7 +270,7 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
         }
         RS2 lo_1, hi_1;
         reconstruct2(w1, w2, w3, lo_1, hi_1);
-        const Face2 ft = face2<1, WB>(top, lo_1, L);
+        const FaceLR ft = face2<1, WB>(top, lo_1, L);
 
         // x: A's left neighbour is lane-1's B, B's right neighbour is lane+1's A
         const float pb = __shfl_up_sync(0xffffffffu, w1.b.y, 1), pe = __shfl_up_sync(0xffffffffu, w1.e.y, 1);
@@ -286,29 +287,16 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                      f2(__shfl_up_sync(0xffffffffu, xhi.e.y, 1), xhi.e.x),
                      f2(__shfl_up_sync(0xffffffffu, xhi.u.y, 1), xhi.u.x),
                      f2(__shfl_up_sync(0xffffffffu, xhi.v.y, 1), xhi.v.x)};
-        const Face2 fl = face2<0, WB>(xl, xlo, L);   // faces left of A and between A and B
-        // faces right of A and B: (A|B, lane+1's left-of-A)
-        Face2 fr;
-        fr.f0 = f2(fl.f0.y, __shfl_down_sync(0xffffffffu, fl.f0.x, 1));
-        fr.f1 = f2(fl.f1.y, __shfl_down_sync(0xffffffffu, fl.f1.x, 1));
-        fr.f2 = f2(fl.f2.y, __shfl_down_sync(0xffffffffu, fl.f2.x, 1));
-        fr.dm0 = f2(fl.dm0.y, __shfl_down_sync(0xffffffffu, fl.dm0.x, 1));
-        fr.dm1 = f2(fl.dm1.y, __shfl_down_sync(0xffffffffu, fl.dm1.x, 1));
-        fr.dm2 = f2(fl.dm2.y, __shfl_down_sync(0xffffffffu, fl.dm2.x, 1));
-        fr.pl = f2(fl.pl.y, __shfl_down_sync(0xffffffffu, fl.pl.x, 1));
+        const FaceLR fl = face2<0, WB>(xl, xlo, L);   // faces left of A and between A and B
+        // r of the faces right of A and B: (A|B, lane+1's left-of-A)
+        const float2 fr0 = f2(fl.l0.y, __shfl_down_sync(0xffffffffu, fl.l0.x, 1));
+        const float2 fr1 = f2(fl.r1.y, __shfl_down_sync(0xffffffffu, fl.r1.x, 1));
+        const float2 fr2 = f2(fl.r2.y, __shfl_down_sync(0xffffffffu, fl.r2.x, 1));
 
         if (ownA || ownB) {
-            // make_rhs.H:346-399, WB bed source folded in before the 1/dx scaling
-            float2 Ax0 = sub(sub(neg(sub(fr.f0, fl.f0)), fr.dm0), fl.dp0);
-            float2 Ax1 = sub(sub(neg(sub(fr.f1, fl.f1)), fr.dm1), fl.dp1);
-            float2 Ax2 = sub(sub(neg(sub(fr.f2, fl.f2)), fr.dm2), fl.dp2);
-            float2 Ay0 = sub(sub(gb0, ft.f0), ft.dm0);
-            float2 Ay1 = sub(sub(gb1, ft.f1), ft.dm1);
-            float2 Ay2 = sub(sub(gb2, ft.f2), ft.dm2);
-            if constexpr (WB) {
-                Ax1 = add(Ax1, sub(fr.pl, fl.pr));
-                Ay2 = add(Ay2, ft.pl);
-            }
+            // make_rhs.H:346-399 (WB bed source folded into l / r before the 1/dx scaling)
+            const float2 Ax0 = sub(fl.l0, fr0), Ax1 = sub(fl.l1, fr1), Ax2 = sub(fl.l2, fr2);
+            const float2 Ay0 = sub(gb0, ft.l0), Ay1 = sub(gb1, ft.r1), Ay2 = sub(gb2, ft.r2);
             const float2 r0 = fma(Ax0, rdx, mul(Ay0, rdy));
             const float2 r1 = fma(Ax1, rdx, mul(Ay1, rdy));
             const float2 r2 = fma(Ax2, rdx, mul(Ay2, rdy));
@@ -426,10 +414,7 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                 }
             }
         }
-        gb0 = sub(ft.f0, ft.dp0);
-        gb1 = sub(ft.f1, ft.dp1);
-        gb2 = sub(ft.f2, ft.dp2);
-        if constexpr (WB) gb2 = sub(gb2, ft.pr);
+        gb0 = ft.l0; gb1 = ft.l1; gb2 = ft.l2;
         top = hi_1;
         w0 = w1; w1 = w2; w2 = w3; w3 = w4;
     }
