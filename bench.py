@@ -587,7 +587,7 @@ def main():
     roofline["issue"] = {"achieved": issue, "peak": issue_peak, "unit": "warp instructions/s",
                          "frac": issue / issue_peak,
                          "warp_instructions_per_cell_step": NCU_WARP_INSTR_PER_CELL_STEP_FP32,
-                         "note": "the bound the FP32 stages meet (ncu: issue active 57-68 %); "
+                         "note": "the bound the FP32 stages meet (ncu: issue active 59-67 %); "
                                  "instructions per cell from the ncu capture of the same kernels"}
 
     ens = None
