@@ -58,11 +58,15 @@ __device__ __forceinline__ void reconstruct(const C4& m, const C4& c, const C4& 
     lo = RS{c.b - hb, h - hh, c.e - he, c.u - hu, c.v - hv};
 }
 
+// What a face contributes to the balance of its two cells (make_rhs.H:346-399):
+// the cell on its high side gets  l = f - D+ (- P(h*_R) in the momentum
+// normal to the face, the WB bed source), the cell on its low side loses
+// r = f + D- (- P(h*_L)); a cell's balance is l(low face) - r(high face).
+// D+ and D- differ only in the sign of the Rusanov term for h (so l0 = r0)
+// and in the bed term of the normal momentum, so 5 values describe a face.
 struct FaceR {
-    float f0, f1, f2;      // central flux (h, hu, hv)
-    float dp0, dp1, dp2;   // D+
-    float dm0, dm1, dm2;   // D-
-    float pl, pr;          // P(h*_L), P(h*_R)
+    float l0, l1, l2;
+    float r1, r2;
 };
 
 // One face from its reconstructed left/right states (make_rhs.H:77-131 from
@@ -93,24 +97,24 @@ __device__ __forceinline__ FaceR face_rs(RS a, RS c, const Params& L) {
         fuL = a.u * qL;  fvL = a.v * qL + pL;
         fuR = c.u * qR;  fvR = c.v * qR + pR;
     }
-    FaceR F;
-    F.f0 = 0.5f * (unL + unR);
-    F.f1 = 0.5f * (fuL + fuR);
-    F.f2 = 0.5f * (fvL + fvR);
+    const float f0 = 0.5f * (unL + unR);
+    const float f1 = 0.5f * (fuL + fuR);
+    const float f2 = 0.5f * (fvL + fvR);
     const float evL = fabsf(qL) + sqrtf(g * fmaxf(a.h, 0.0f));
     const float evR = fabsf(qR) + sqrtf(g * fmaxf(c.h, 0.0f));
     const float hs = 0.5f * fmaxf(evL, evR);
     const float dh = c.h - a.h, du = c.u - a.u, dv = c.v - a.v;
-    float bu = 0.0f, bv = 0.0f;
-    if constexpr (!WB) {
-        const float Bn = 0.5f * g * (0.5f * (a.h + c.h)) * db;
-        if (DIR == 0) bu = Bn; else bv = Bn;
-    }
-    F.dp0 = hs * dh;       F.dm0 = -hs * dh;
-    F.dp1 = bu + hs * du;  F.dm1 = bu - hs * du;
-    F.dp2 = bv + hs * dv;  F.dm2 = bv - hs * dv;
-    F.pl = pL;
-    F.pr = pR;
+    FaceR F;
+    F.l0 = f0 - hs * dh;
+    const float b1 = f1 - hs * du, b2 = f2 - hs * dv;
+    F.l1 = F.r1 = b1;
+    F.l2 = F.r2 = b2;
+    // the normal momentum: WB pressure terms P(h*_R) / P(h*_L), else the
+    // path-conservative bed product g (hL + hR)/2 (bR - bL) in D+ and D-
+    const float kl = WB ? pR : 0.5f * g * (0.5f * (a.h + c.h)) * db;
+    const float kr = WB ? pL : -kl;
+    if constexpr (DIR == 0) { F.l1 = b1 - kl; F.r1 = b1 - kr; }
+    else                    { F.l2 = b2 - kl; F.r2 = b2 - kr; }
     return F;
 }
 
@@ -184,7 +188,13 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
     RS lo_m, hi_m, lo_0, hi_0;
     reconstruct(wm, w0, w1, lo_m, hi_m);     // row j0-1
     reconstruct(w0, w1, w2, lo_0, hi_0);     // row j0
-    FaceR fb = face_rs<1, WB>(hi_m, lo_0, L);   // face below row j0
+    // l of the face below the current row, carried from row to row
+    float gb0, gb1, gb2;
+    {
+        const FaceR fb = face_rs<1, WB>(hi_m, lo_0, L);   // face below row j0
+        gb0 = fb.l0; gb1 = fb.l1; gb2 = fb.l2;
+    }
+    float m_f = 0.0f;    // CFL max of this sweep (>= 0, never NaN), merged into m_loc at the end
     RS top = hi_0;                           // row j0's state at its upper face
     C4 w3 = fetch<MODE, INTERIOR>(bed, X, inc_in, L, i, j0 + 2);
 
@@ -240,27 +250,15 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
         reconstruct(left, w1, right, xlo, xhi);
         const RS lhi = shfl_up_rs(xhi, 1);              // left neighbour's state at our left face
         const FaceR fl = face_rs<0, WB>(lhi, xlo, L);   // face on the left of column i (lanes >= 1)
-        FaceR fr;                                       // face on the right: lane+1's left face
-        fr.f0 = __shfl_down_sync(0xffffffffu, fl.f0, 1);
-        fr.f1 = __shfl_down_sync(0xffffffffu, fl.f1, 1);
-        fr.f2 = __shfl_down_sync(0xffffffffu, fl.f2, 1);
-        fr.dm0 = __shfl_down_sync(0xffffffffu, fl.dm0, 1);
-        fr.dm1 = __shfl_down_sync(0xffffffffu, fl.dm1, 1);
-        fr.dm2 = __shfl_down_sync(0xffffffffu, fl.dm2, 1);
-        fr.pl = __shfl_down_sync(0xffffffffu, fl.pl, 1);
+        // r of the face on the right: lane+1's left face
+        const float fr0 = __shfl_down_sync(0xffffffffu, fl.l0, 1);
+        const float fr1 = __shfl_down_sync(0xffffffffu, fl.r1, 1);
+        const float fr2 = __shfl_down_sync(0xffffffffu, fl.r2, 1);
 
         if (owns) {
-            // make_rhs.H:346-399, the WB bed source folded in before the 1/dx scaling
-            float Ax0 = -(fr.f0 - fl.f0) - fr.dm0 - fl.dp0;
-            float Ax1 = -(fr.f1 - fl.f1) - fr.dm1 - fl.dp1;
-            float Ax2 = -(fr.f2 - fl.f2) - fr.dm2 - fl.dp2;
-            float Ay0 = -(ft.f0 - fb.f0) - ft.dm0 - fb.dp0;
-            float Ay1 = -(ft.f1 - fb.f1) - ft.dm1 - fb.dp1;
-            float Ay2 = -(ft.f2 - fb.f2) - ft.dm2 - fb.dp2;
-            if constexpr (WB) {
-                Ax1 += fr.pl - fl.pr;
-                Ay2 += ft.pl - fb.pr;
-            }
+            // make_rhs.H:346-399 (WB bed source folded into l / r before the 1/dx scaling)
+            const float Ax0 = fl.l0 - fr0, Ax1 = fl.l1 - fr1, Ax2 = fl.l2 - fr2;
+            const float Ay0 = gb0 - ft.l0, Ay1 = gb1 - ft.r1, Ay2 = gb2 - ft.r2;
             const float r0 = Ax0 * L.rdx + Ay0 * L.rdy;
             const float r1 = Ax1 * L.rdx + Ay1 * L.rdy;
             const float r2 = Ax2 * L.rdx + Ay2 * L.rdy;
@@ -320,15 +318,16 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
                 float mm_ = 0.0f;
                 if (evx > mm_) mm_ = evx;
                 if (evy > mm_) mm_ = evy;
-                if (double(mm_) > m_loc) m_loc = double(mm_);
+                m_f = fmaxf(m_f, mm_);
                 s_loc = s_loc + ((double(he) - double(w1.b)) + double(le));
             }
         }
         // advance: row j+1 becomes the current row
-        fb = ft;
+        gb0 = ft.l0; gb1 = ft.l1; gb2 = ft.l2;
         top = hi_1;
         w0 = w1; w1 = w2; w2 = w3; w3 = w4;
     }
+    if (double(m_f) > m_loc) m_loc = double(m_f);
 }
 
 // Whether a strip's stencil (two ghost layers around its cells and its two
