@@ -165,3 +165,27 @@ def test_run_case_rejects_fluxes_not_built():
     with pytest.raises(NotImplementedError, match="NonconservativeRusanov"):
         run_case(SWE(2, "wall", None), dict(dimension=2, domain=[0, 1, 0, 1], n_cells=[8, 8],
                                             riemann="PositiveNonconservativeHLL"))
+
+
+def _record_many(args):
+    from zoomy_amrex_b200.autotune import record
+    path, k = args
+    shapes = [(4, 8, 2, 3)] * 13
+    for i in range(40):
+        record(4, "fp32", 4096.0 * 4096.0, (k + i) % 13, {0: 1.0 + k, 1: 2.0}, shapes, path=path)
+    return k
+
+
+def test_autotune_cache_survives_concurrent_writers(tmp_path):
+    """One process per GPU tunes and records at the same time: every write
+    succeeds and the cache stays a complete JSON document."""
+    import json
+    import multiprocessing as mp
+    from zoomy_amrex_b200.autotune import cached_variant
+    path = tmp_path / "autotune.json"
+    with mp.get_context("spawn").Pool(4) as pool:
+        assert sorted(pool.map(_record_many, [(path, k) for k in range(4)])) == [0, 1, 2, 3]
+    data = json.loads(path.read_text())
+    assert list(data) == ["n_q=4/fp32/large"]
+    assert cached_variant(4, "fp32", 4096.0 * 4096.0, path=path) in range(13)
+    assert not list(tmp_path.glob("*.tmp"))

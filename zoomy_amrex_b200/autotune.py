@@ -11,6 +11,7 @@ to the library; ``cached_variant`` looks it up.
 from __future__ import annotations
 
 import json
+import os
 import pathlib
 
 import numpy as np
@@ -52,9 +53,15 @@ def record(n_q: int, precision: str, cells_per_instance: float, variant: int, ti
     data[_key(n_q, precision, size_class(cells_per_instance))] = dict(
         variant=int(variant), shape=list(shapes[variant]),
         ms_per_step={str(k): float(v) for k, v in times_ms.items()})
-    tmp = path.with_suffix(".json.tmp")
-    tmp.write_text(json.dumps(data, indent=1, sort_keys=True))
-    tmp.replace(path)
+    # one temporary file per process, then an atomic rename: processes that
+    # tune at the same time (one per GPU) never write the same file, and the
+    # cache is whichever complete version was renamed last
+    tmp = path.with_suffix(f".json.{os.getpid()}.tmp")
+    try:
+        tmp.write_text(json.dumps(data, indent=1, sort_keys=True))
+        tmp.replace(path)
+    except OSError:   # the cache is an optimisation: a read-only install just re-tunes
+        tmp.unlink(missing_ok=True)
 
 
 def time_variant(batch, variant: int, steps: int = 10, warmup: int = 3, repeats: int = 3) -> float:
