@@ -171,3 +171,26 @@ def test_fp32_tiny_and_ragged_grids_every_strip_shape(cuda, oracle, shape):
         b32 = Q0[0].astype(np.float32).astype(np.float64)   # depth measured from the FP32 bed
         m0, m1 = ((Q0[1] + Q0[0]) - b32).sum(), Q[1].sum()
         assert abs(m1 - m0) <= 1e-10 * m0, (v, abs(m1 - m0) / m0)
+
+
+def test_fp32_level_with_device_made_aux(cuda):
+    """An FP32 level created without a host aux (init_solution on the device)
+    runs and exports bit for bit like one given the host aux: the FP32 stages
+    never read aux, and the export refreshes its hinv row."""
+    from zoomy_amrex_b200.level import Level
+    model = SWE(2, "wall", bumps(19, moving=True), parameters={"n_m": 0.03})
+    s = _settings(56, 30)
+    cfg64, Q0, A0 = setup(model, s)
+    cfg = config_from_settings(model, s, precision=ZFV_PREC_FP32)
+    out = []
+    for aux0 in (A0, None):
+        lev = Level(cfg, Q0, aux0)
+        try:
+            assert np.array_equal(lev.aux.cpu().numpy(), A0)
+            st = lev.run(chunk=8)
+            out.append((lev.state64().cpu().numpy(), lev.aux.cpu().numpy(), st["step"], st["time"]))
+        finally:
+            lev.close()
+    (Qa, Aa, na, ta), (Qb, Ab, nb, tb) = out
+    assert na == nb == 30 and ta == tb
+    assert np.array_equal(Qa, Qb) and np.array_equal(Aa, Ab)
