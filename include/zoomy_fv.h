@@ -411,14 +411,21 @@ int zfv_adj_set_variant(int variant);
  * Scratch is a 64 MiB array compiled into the library (every GPU that loads
  * the library holds it until exit); levels whose zfv_scratch_bytes() exceeds
  * it (about 2 million cells for ZFV_MODEL_SWE2D) are rejected with an error.
+ * Only FP64 handles are accepted: the FP32 form keeps a part of its state
+ * (the compensation remainder) in scratch, where only zfv_state_import and
+ * zfv_state_export reach it, so it needs caller-provided scratch.
  * restart != 0 starts a run like zfv_begin (clearing the device run record);
  * restart == 0 continues the run that the previous call on this device left
- * in the array. Every call on a device shares the one array: calls that
- * overlap on the GPU (other streams, other handles) race, and interleaving
- * runs of different handles needs restart != 0. The first call on each device
- * looks up the array's device address (cudaGetSymbolAddress); make that first
- * call before any stream capture. If status_out is not NULL the run status is
- * copied into it and the stream is synchronized. Allocates no device memory.
+ * in the array, and is refused with an error unless the last restart on this
+ * device was made with the same handle. Every call on a device shares the one
+ * array: calls that overlap on the GPU (other streams, other handles) race,
+ * and interleaving runs of different handles needs restart != 0. The first
+ * call on each device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * If status_out is not NULL the run status is copied into it and the stream
+ * is synchronized before the call returns; with status_out == NULL the call
+ * only enqueues the work and returns before the stream has finished it.
+ * Allocates no device memory.
  */
 int zfv_evolve_static(zfv_handle* h, void* Q, void* aux, int n_steps, int restart,
                       zfv_status* status_out, void* stream);

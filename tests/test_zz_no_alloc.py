@@ -116,3 +116,28 @@ def test_static_scratch_rejects_levels_that_do_not_fit(cuda):
     msg = lib.zfv_last_error().decode()
     lib.zfv_destroy(h)
     assert rc != 0 and "static" in msg and "too large" in msg
+
+
+def test_static_scratch_refuses_fp32_and_foreign_continuations(cuda):
+    import torch
+    from zoomy_amrex_b200._abi import ZFV_PREC_FP32
+    lib = _lib.lib()
+    Q = torch.empty(16, dtype=torch.float64, device="cuda")
+    st = zfv_status()
+    # the FP32 form keeps its state remainder in scratch that only the
+    # import/export entry points reach, so it is refused before any device work
+    cfg32 = make_config(ZFV_MODEL_SWE2D, 64, 64, (0.0, 0.0), (1.0, 1.0), spatial_order=2,
+                        precision=ZFV_PREC_FP32)
+    h32 = _create(lib, cfg32)
+    rc = lib.zfv_evolve_static(h32, _vp(Q), _vp(Q), 1, 1, C.byref(st), None)
+    msg = lib.zfv_last_error().decode()
+    lib.zfv_destroy(h32)
+    assert rc != 0 and "FP64" in msg
+    # continuing (restart == 0) with a handle that did not make the last restart
+    # on this device is refused before any kernel runs
+    cfg = make_config(ZFV_MODEL_SWE2D, 64, 64, (0.0, 0.0), (1.0, 1.0), spatial_order=2)
+    h = _create(lib, cfg)
+    rc = lib.zfv_evolve_static(h, _vp(Q), _vp(Q), 1, 0, C.byref(st), None)
+    msg = lib.zfv_last_error().decode()
+    lib.zfv_destroy(h)
+    assert rc != 0 and "restart" in msg

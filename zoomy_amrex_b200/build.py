@@ -27,9 +27,15 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # arithmetic is bitwise the CPU build's; the FP32 chosen form uses FMA and the
 # hardware's approximate FP32 division / square root (its FP64 parts are
 # unaffected by these flags); the adjoint (FP64, checked to tolerances) uses FMA.
-SOURCES = [("zoomy_fv.cu", ["--fmad=false"]),
-           ("zoomy_fv32.cu", ["--fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
-           ("zoomy_adj.cu", ["--fmad=true"])]
+FP32_FLAGS = ["--fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]
+N_FP32_SHAPES = 13   # kNumVariants in csrc/fv32_shapes.H
+# (source, extra flags, object stem). The FP32 strip shapes are one source
+# compiled once per shape (-DZFV32_SHAPE=k) so that they build in parallel.
+SOURCES = ([("zoomy_fv.cu", ["--fmad=false"], "zoomy_fv"),
+            ("zoomy_fv32.cu", FP32_FLAGS, "zoomy_fv32"),
+            ("zoomy_adj.cu", ["--fmad=true"], "zoomy_adj")]
+           + [("zoomy_fv32_shape.cu", FP32_FLAGS + [f"-DZFV32_SHAPE={k}"], f"zoomy_fv32_shape{k}")
+              for k in range(N_FP32_SHAPES)])
 
 
 def nvcc() -> str:
@@ -52,13 +58,29 @@ def up_to_date() -> bool:
     return all(p.stat().st_mtime <= t for p in _deps())
 
 
+def _reap(running) -> None:
+    """Wait for the first of the running compilers to finish; raise if it failed."""
+    import time
+    while True:
+        for k, (p, cmd) in enumerate(running):
+            rc = p.poll()
+            if rc is not None:
+                running.pop(k)
+                if rc != 0:
+                    for q, _ in running:
+                        q.wait()
+                    raise subprocess.CalledProcessError(rc, cmd)
+                return
+        time.sleep(0.2)
+
+
 def build(verbose: bool = False, force: bool = False) -> pathlib.Path:
     if not force and up_to_date():
         return LIB
     LIB_DIR.mkdir(exist_ok=True)
     objs, jobs = [], []
-    for src, flags in SOURCES:
-        obj = LIB_DIR / (pathlib.Path(src).stem + ".o")
+    for src, flags, stem in SOURCES:
+        obj = LIB_DIR / (stem + ".o")
         cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", *flags, "-std=c++17",
                "-Xcompiler", "-fPIC", "-I", str(CSRC), "-I", str(CSRC / "amrex_compat"),
                "-I", str(CSRC / "models"), "-I", str(INCLUDE), "-c", str(CSRC / src), "-o", str(obj)]
@@ -66,11 +88,16 @@ def build(verbose: bool = False, force: bool = False) -> pathlib.Path:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd))
         jobs.append((cmd, obj))
-    procs = [subprocess.Popen(cmd) for cmd, _ in jobs]
-    for p, (cmd, obj) in zip(procs, jobs):
-        if p.wait() != 0:
-            raise subprocess.CalledProcessError(p.returncode, cmd)
+    # at most one compiler per core; the longest units first
+    width = max(1, os.cpu_count() or 1)
+    running = []
+    for cmd, obj in jobs:
+        while len(running) >= width:
+            _reap(running)
+        running.append((subprocess.Popen(cmd), cmd))
         objs.append(str(obj))
+    while running:
+        _reap(running)
     tmp = LIB.with_suffix(".so.tmp")
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)

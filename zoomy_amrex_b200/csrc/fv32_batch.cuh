@@ -203,7 +203,7 @@ __global__ void k32b_export(const BInst* __restrict__ insts, const int2* __restr
 }
 
 // Start of a run for every instance: time 0, step 0, stop flag.
-__global__ void k32b_init(const BInst* __restrict__ insts, int n) {
+static __global__ void k32b_init(const BInst* __restrict__ insts, int n) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     zfv::DevState* st = insts[k].st;
@@ -279,13 +279,13 @@ k32b_reduce(const BInst* __restrict__ insts, const int2* __restrict__ units, int
 }
 
 // Host-chosen step size per instance (AMR levels step with dt_0 / 2^l).
-__global__ void k32b_set_dt(const BInst* __restrict__ insts, int n, const double* __restrict__ dt) {
+static __global__ void k32b_set_dt(const BInst* __restrict__ insts, int n, const double* __restrict__ dt) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) insts[k].st->dt = dt[k];
 }
 
 // Gather every instance's 64-byte status record into one array.
-__global__ void k32b_status(const BInst* __restrict__ insts, int n, zfv::DevState* out) {
+static __global__ void k32b_status(const BInst* __restrict__ insts, int n, zfv::DevState* out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) out[k] = *insts[k].st;
 }

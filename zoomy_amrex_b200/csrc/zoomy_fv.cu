@@ -626,6 +626,10 @@ __global__ void k_init_solution(double* __restrict__ f, int n_comp, long long pl
     }
 }
 
+// Drops a destroyed handle from the static-scratch ownership record, so a
+// later handle allocated at the same address cannot continue its run.
+void static_scratch_forget(const zfv_handle* h);
+
 }  // namespace
 
 extern "C" {
@@ -726,6 +730,7 @@ int zfv_create(const zfv_config* cfg, zfv_handle** out) {
 }
 
 int zfv_destroy(zfv_handle* h) {
+    static_scratch_forget(h);
     delete h;
     return 0;
 }
@@ -901,6 +906,17 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBy
 // symbol's name is only a host-side stand-in, never a device address.
 constexpr int kMaxDevices = 64;
 std::atomic<void*> g_static_scratch_addr[kMaxDevices];
+// The handle whose run the array holds, per device: set by a restart, checked
+// by a continuation (restart == 0), so a call never continues a run record
+// laid out for another handle or one that no restart ever initialised.
+std::atomic<const zfv_handle*> g_static_scratch_owner[kMaxDevices];
+
+void static_scratch_forget(const zfv_handle* h) {
+    for (int d = 0; d < kMaxDevices; ++d) {
+        const zfv_handle* expect = h;
+        g_static_scratch_owner[d].compare_exchange_strong(expect, nullptr, std::memory_order_acq_rel);
+    }
+}
 
 }  // namespace
 
@@ -908,6 +924,10 @@ extern "C" int zfv_evolve_static(zfv_handle* h, void* Q, void* aux, int n_steps,
                                  zfv_status* status_out, void* stream) {
     if (!h || !Q || !aux) return fail(-1, "zfv_evolve_static: null argument");
     if (n_steps < 0) return fail(-1, "zfv_evolve_static: negative step count");
+    if (h->cfg.precision != ZFV_PREC_FP64)
+        return fail(-1, "zfv_evolve_static: only FP64 handles are accepted (the FP32 form keeps its "
+                        "state remainder in scratch, which only zfv_state_import/export reach; use "
+                        "zfv_evolve with caller-provided scratch)");
     if (h->lay.total > kStaticScratchBytes)
         return fail(-5, "zfv_evolve_static: this level needs %zu bytes of scratch; the static "
                         "scratch holds %zu bytes (grid %d x %d is too large for this entry point, "
@@ -930,8 +950,14 @@ extern "C" int zfv_evolve_static(zfv_handle* h, void* Q, void* aux, int n_steps,
     cudaStream_t s = (cudaStream_t)stream;
     if (restart) {
         // the run record (time, step, flags, reduction counter) must start at zero
+        g_static_scratch_owner[dev].store(nullptr, std::memory_order_release);
         rc = h->run->begin(Q, aux, scratch, s);
         if (rc) return rc;
+        g_static_scratch_owner[dev].store(h, std::memory_order_release);
+    } else if (g_static_scratch_owner[dev].load(std::memory_order_acquire) != h) {
+        return fail(-1, "zfv_evolve_static: restart == 0 continues the run this handle started on "
+                        "device %d, but the array holds no run of this handle (no restart yet, or "
+                        "another handle restarted since)", dev);
     }
     rc = h->run->evolve(Q, aux, scratch, n_steps, s);
     if (rc) return rc;

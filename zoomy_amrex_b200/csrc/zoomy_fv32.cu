@@ -33,139 +33,16 @@
 
 using namespace zfvi;
 
-namespace zfv32 {
-
-struct Params {
-    int nx, ny;
-    long long plane;
-    double dx, dy, plox, ploy;       // FP64 (reductions, dt)
-    float fdx, fdy, rdx, rdy, rfdx, rfdy;
-    float g, ex, ey, nm, hfloor, eps;
-    double gd, exd, eyd, nmd, hfloord, epsd;
-    int bc_tag[4];
-    double cfl, dtmin, dtmax, time_end;
-    int max_step, cfl_dimension, cfl_degree_factor;
-    // Ghost frame (AMR boxes): when set, the cells just outside the box are
-    // read from this (nx+4) x (ny+4) x 4 array ([b, eta, hu, hv] planes, ring
-    // filled by the caller before each stage, stage input already summed)
-    // instead of mirrored from the box's own cells.
-    const float* frame;
-};
-
-struct C4 { float b, e, u, v; };   // bed, surface eta = h + b, hu, hv
-
-constexpr float kNearDry = 1.0e-3f;   // FP64 implicit solve below this depth
-
-__device__ __forceinline__ float mm(float a, float b) {
-    if (a * b <= 0.0f) return 0.0f;
-    return (fabsf(a) < fabsf(b)) ? a : b;
-}
-
-// Knuth's two-sum: s + e == a + b exactly (round-to-nearest, no contraction:
-// the _rn intrinsics are never fused into FMAs).
-__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
-    s = __fadd_rn(a, b);
-    const float bp = __fsub_rn(s, a);
-    const float ap = __fsub_rn(s, bp);
-    e = __fadd_rn(__fsub_rn(a, ap), __fsub_rn(b, bp));
-}
-
-// Kurganov-Petrova desingularised 1/h (the model's update_aux_variables), FP32.
-__device__ __forceinline__ float kp_hinv(float h, float eps) {
-    const float h2 = h * h;
-    const float x0 = h2 * h2;
-    return 1.41421356237f * h * rsqrtf(x0 + fmaxf(x0, eps));
-}
-__device__ __forceinline__ double kp_hinv_d(double h, double eps) {
-    const double h2 = h * h;
-    const double x0 = h2 * h2;
-    return 1.4142135623730951 * h / sqrt(x0 + fmax(x0, eps));
-}
-
-// Manning friction S_m = g e_m h - k u_m |u|, k = g n^2 max(h, h_floor)^(-1/3),
-// and its Jacobian w.r.t. (hu, hv) with hinv held fixed; the point-implicit
-// update solves (I - dt J) dq = dt S on the momentum block (the bed and depth
-// rows of J are zero, so the reference's 4x4 elimination reduces to it).
-template <class T>
-__device__ __forceinline__ void manning_implicit(T h, T u, T v, T hinv, T dt, T g, T ex, T ey, T nm,
-                                                 T hfloor, T& du, T& dv) {
-    const T m = (h > hfloor) ? h : hfloor;
-    const T k = g * nm * nm * zb::inv_cbrt_pos(m);
-    const T ux = u * hinv, uy = v * hinv;
-    const T sp = sqrt(ux * ux + uy * uy);
-    const T Su = g * ex * h - k * ux * sp;
-    const T Sv = g * ey * h - k * uy * sp;
-    const T rsp = (sp > T(0)) ? T(1) / sp : T(0);
-    const T dsx = ux * hinv * rsp, dsy = uy * hinv * rsp;
-    const T J22 = -k * (hinv * sp + ux * dsx), J23 = -k * (ux * dsy);
-    const T J32 = -k * (uy * dsx), J33 = -k * (hinv * sp + uy * dsy);
-    const T a = T(1) - dt * J22, b = -dt * J23, c = -dt * J32, d = T(1) - dt * J33;
-    const T det = a * d - b * c;
-    const T r0 = dt * Su, r1 = dt * Sv;
-    bool ok = (fabs(det) > T(0)) && isfinite(det);
-    T x0 = T(0), x1 = T(0);
-    if (ok) {
-        x0 = (r0 * d - b * r1) / det;
-        x1 = (a * r1 - c * r0) / det;
-        ok = isfinite(x0) && isfinite(x1);
-    }
-    if (!ok) {   // explicit fallback, as make_rhs.H:501-508
-        x0 = isfinite(r0) ? r0 : T(0);
-        x1 = isfinite(r1) ? r1 : T(0);
-    }
-    du = x0;
-    dv = x1;
-}
-
-enum Mode { S1 = 1, S2 = 2 };
-
-}  // namespace zfv32
-
+#include "fv32_common.cuh"
 #include "fv32_batch.cuh"
+#include "fv32_shapes.H"
 #include "fv32_amr.cuh"
 
 namespace zfv32 {
 
-// Compiled strip shapes: (warps per block NW, rows per warp CPT = cells per
-// thread, columns per lane PK, flags PF). A strip is 30 * PK columns x
-// (NW * CPT) rows; PK = 2 is the packed-FP32 paired-column sweep. PF bits:
-//   1  stage 2 stages its update's own inputs in shared memory with
-//      asynchronous copies issued at the top of each row;
-//   2  the stage-2 kernel is capped at 128 registers (4 blocks of 128
-//      threads per SM instead of 3, at the cost of some spilling).
-// Short strips (4 or 2 rows per warp) spend more on the y halo but finish a
-// unit sooner: levels of a few million cells (AMR levels, ensemble boxes)
-// fill the GPU for about one wave, so a launch there lasts about as long as
-// one unit takes.
-constexpr int kNumVariants = 13;
-constexpr int kVarNW[kNumVariants] = {4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4};
-constexpr int kVarCPT[kNumVariants] = {16, 8, 16, 8, 16, 8, 16, 8, 16, 8, 4, 4, 2};
-constexpr int kVarPK[kNumVariants] = {1, 1, 2, 2, 1, 1, 2, 2, 2, 2, 1, 2, 2};
-constexpr int kVarPF[kNumVariants] = {0, 0, 0, 0, 1, 1, 1, 1, 3, 3, 1, 3, 3};
-// Strip shape used until a caller picks one (zfv_set_variant /
-// zfv_batch_set_variant): 4 warps x 8 rows, column pairs, stage-2 staging with
-// the 128-register stage 2 -- the shape measured fastest on large levels.
-constexpr int kDefaultVariant = 9;
-
-template <class F>
-int with_variant(int v, F&& f) {
-    switch (v) {
-    case 0: return f.template operator()<4, 16, 1, 0>();
-    case 1: return f.template operator()<4, 8, 1, 0>();
-    case 2: return f.template operator()<4, 16, 2, 0>();
-    case 3: return f.template operator()<4, 8, 2, 0>();
-    case 4: return f.template operator()<4, 16, 1, 1>();
-    case 5: return f.template operator()<4, 8, 1, 1>();
-    case 6: return f.template operator()<4, 16, 2, 1>();
-    case 7: return f.template operator()<4, 8, 2, 1>();
-    case 8: return f.template operator()<4, 16, 2, 3>();
-    case 9: return f.template operator()<4, 8, 2, 3>();
-    case 10: return f.template operator()<4, 4, 1, 1>();
-    case 11: return f.template operator()<4, 4, 2, 3>();
-    case 12: return f.template operator()<4, 2, 2, 3>();
-    default: return fail(-1, "unknown strip variant %d", v);
-    }
-}
+#define ZFV32_SHAPE_PTR(k) &kShapeOps##k,
+const ShapeOps* const kShapeTable[kNumVariants] = {ZFV32_SHAPE_LIST(ZFV32_SHAPE_PTR)};
+#undef ZFV32_SHAPE_PTR
 
 Params make_params(const zfv_config& c) {
     Params L;
@@ -348,67 +225,34 @@ struct BatchCore {
         return bound ? upload(s) : 0;
     }
 
-    struct ImportF {
-        BatchCore* b; cudaStream_t s; bool exp;
-        template <int NW, int CPT, int PK, int PF> int operator()() {
-            if (exp) k32b_export<NW, CPT, PK><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
-            else k32b_import<NW, CPT, PK><<<b->nunits(), 256, 0, s>>>(b->d_desc(), b->d_units());
-            return cuda_check(cudaGetLastError(), "zfv_batch import/export launch");
-        }
-    };
+    const ShapeOps& ops() const { return *kShapeTable[variant]; }
+
     int convert(const double* const* q64, bool exp, cudaStream_t s) {
         for (int k = 0; k < n; ++k) desc[k].q64 = q64[k];
         int rc = upload(s);
         if (rc) return rc;
-        rc = with_variant(variant, ImportF{this, s, exp});
+        ops().convert(nunits(), s, d_desc(), d_units(), n_aux, exp);
+        rc = cuda_check(cudaGetLastError(), "zfv_batch import/export launch");
         if (rc) return rc;
         return cuda_check(cudaStreamSynchronize(s), "zfv_batch import/export sync");
     }
 
-    struct BeginF {
-        BatchCore* b; cudaStream_t s;
-        template <int NW, int CPT, int PK, int PF> int operator()() {
-            k32b_init<<<(b->n + 127) / 128, 128, 0, s>>>(b->d_desc(), b->n);
-            k32b_reduce<NW, CPT, PK, 0><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
-            return cuda_check(cudaGetLastError(), "zfv_batch begin launch");
-        }
-    };
-    int begin(cudaStream_t s) { return with_variant(variant, BeginF{this, s}); }
+    int begin(cudaStream_t s) {
+        k32b_init<<<(n + 127) / 128, 128, 0, s>>>(d_desc(), n);
+        ops().reduce(nunits(), s, d_desc(), d_units(), n_aux, 0);
+        return cuda_check(cudaGetLastError(), "zfv_batch begin launch");
+    }
 
-    struct MassF {
-        BatchCore* b; cudaStream_t s;
-        template <int NW, int CPT, int PK, int PF> int operator()() {
-            k32b_reduce<NW, CPT, PK, 1><<<b->nunits(), 32 * NW, 0, s>>>(b->d_desc(), b->d_units(), n_aux);
-            return cuda_check(cudaGetLastError(), "zfv_batch mass launch");
-        }
-    };
-    int mass(cudaStream_t s) { return with_variant(variant, MassF{this, s}); }
+    int mass(cudaStream_t s) {
+        ops().reduce(nunits(), s, d_desc(), d_units(), n_aux, 1);
+        return cuda_check(cudaGetLastError(), "zfv_batch mass launch");
+    }
 
     // stages: 3 = both stages of `nsteps` steps; 1 or 2 = that stage alone,
     // once (AMR boxes refill their ghost frames between the stages)
-    template <bool W, bool I>
-    struct StepF {
-        BatchCore* b; cudaStream_t s; int nsteps; int stages;
-        template <int NW, int CPT, int PK, int PF> int operator()() {
-            const int nu = b->nunits();
-            if (stages == 1) {
-                launch_stage<S1, W, I, NW, CPT, PK, PF>(nu, s, b->d_desc(), b->d_units());
-            } else if (stages == 2) {
-                launch_stage<S2, W, I, NW, CPT, PK, PF>(nu, s, b->d_desc(), b->d_units());
-            } else {
-                for (int k = 0; k < nsteps; ++k) {
-                    launch_stage<S1, W, I, NW, CPT, PK, PF>(nu, s, b->d_desc(), b->d_units());
-                    launch_stage<S2, W, I, NW, CPT, PK, PF>(nu, s, b->d_desc(), b->d_units());
-                }
-            }
-            return cuda_check(cudaGetLastError(), "zfv_batch evolve launch");
-        }
-    };
     int evolve(int nsteps, cudaStream_t s, int stages = 3) {
-        if (wb) return impl ? with_variant(variant, StepF<true, true>{this, s, nsteps, stages})
-                            : with_variant(variant, StepF<true, false>{this, s, nsteps, stages});
-        return impl ? with_variant(variant, StepF<false, true>{this, s, nsteps, stages})
-                    : with_variant(variant, StepF<false, false>{this, s, nsteps, stages});
+        ops().step(nunits(), s, d_desc(), d_units(), wb, impl, nsteps, stages);
+        return cuda_check(cudaGetLastError(), "zfv_batch evolve launch");
     }
 
     int status(zfv_status* out, cudaStream_t s) {
