@@ -20,6 +20,7 @@ import json
 import os
 import pathlib
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -92,13 +93,15 @@ class Clocks:
     """nvidia-smi sampling during the timed region."""
 
     def __init__(self, index: int):
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+        # a private temporary file; the samples end up summarised in the JSON line
+        fd, name = tempfile.mkstemp(prefix=f"zfv_clocks_rank{index}_", suffix=".csv")
+        os.close(fd)
+        self.path = pathlib.Path(name)
         self.index = index
         self.proc = None
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
             q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")

@@ -5,7 +5,7 @@ Two builds share one API:
                              single-level ZoomyAmr driver (oracle/fv_oracle.H);
   * ``_ref/libzoomyref.so`` — the same driver with the per-cell work done by the
                              reference's own Source/make_rhs.H (built by
-                             ``make -C oracle ref`` where the reference tree exists).
+                             ``make -C oracle ref REF_SRC=<reference tree>/Source``).
 
 Only tests, the smoke check and the benchmark's CPU baseline use this module.
 """
@@ -28,12 +28,15 @@ _libs: dict = {}
 
 
 def build(ref: bool | None = None) -> None:
-    """Compile the oracle (and the reference build when the tree is present)."""
+    """Compile the oracle, and the reference build when the environment variable
+    REF_SRC names the reference's Source directory (holding make_rhs.H)."""
     import subprocess
     targets = ["all"]
     if ref is None:
-        ref = pathlib.Path(os.environ.get("REF_SRC", "/root/reference/Source"), "make_rhs.H").exists()
+        ref = bool(os.environ.get("REF_SRC")) and pathlib.Path(os.environ["REF_SRC"], "make_rhs.H").exists()
     if ref:
+        if not os.environ.get("REF_SRC"):
+            raise RuntimeError("building the reference kernels needs REF_SRC=<reference tree>/Source")
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", str(HERE)] + targets, check=True)
 

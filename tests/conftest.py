@@ -30,6 +30,19 @@ def ref_oracle():
 
 
 @pytest.fixture(scope="session")
+def parity_oracle():
+    """The parity authority for GPU comparisons: the reference's own
+    make_rhs.H under the oracle's driver (oracle/_ref) where it was built,
+    else the restatement (liboracle)."""
+    from oracle.oracle import LIB_ORACLE, LIB_REF, Oracle, build
+    if LIB_REF.exists():
+        return Oracle("ref")
+    if not LIB_ORACLE.exists():
+        build(ref=False)
+    return Oracle("oracle")
+
+
+@pytest.fixture(scope="session")
 def cuda():
     import torch
     if not torch.cuda.is_available():

@@ -13,6 +13,13 @@ from zoomy_amrex_b200.workloads import dam_break_ensemble, fp64_twin
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(scope="module")
+def oracle(parity_oracle):
+    """The FP64 authority: the reference's own make_rhs.H under the oracle's
+    driver (oracle/_ref) where it was built, else the restatement."""
+    return parity_oracle
+
+
 def _single(cfg, Q0, A0, steps_chunk=16, variant=None):
     from zoomy_amrex_b200.level import Level
     lev = Level(cfg, Q0, A0, variant=variant)

@@ -8,12 +8,19 @@ is built for — an exactly well-balanced lake at rest, FP64-accurate mass.
 import numpy as np
 import pytest
 
-from cases import setup
+from cases import config2_strip_setup, setup
 from zoomy_amrex_b200._abi import ZFV_PREC_FP32
 from zoomy_amrex_b200.models import SWE
 from zoomy_amrex_b200.settings import config_from_settings
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def oracle(parity_oracle):
+    """The FP64 authority: the reference's own make_rhs.H under the oracle's
+    driver (oracle/_ref) where it was built, else the restatement."""
+    return parity_oracle
 
 
 def bumps(seed, n_b=8, hump=0.3, eta0=1.0, wet_everywhere=False, moving=False):
@@ -101,6 +108,32 @@ def test_fp32_depth_error_vs_fp64_oracle(cuda, oracle, moving):
     assert linf <= 1e-4, linf
     assert np.abs(Q32[2:] - Qo[2:]).max() <= 1e-4
     # dry cells agree on being dry
+    assert ((Q32[1] <= 1e-6) == (Qo[1] <= 1e-6)).mean() > 0.999
+
+
+def test_fp32_config2_strip_error_vs_fp64_oracle(cuda, oracle):
+    """The benchmark's own fields (a 4096 x 64 strip of the 4096^2 level: 16
+    seeded bumps, hump, Manning n = 0.03, walls, WB, order 2), 200 steps:
+    L1 / Linf depth error of the chosen form against the FP64 oracle."""
+    from zoomy_amrex_b200.level import Level
+    from zoomy_amrex_b200.workloads import fp64_twin
+    cfg64, Q0, A0 = config2_strip_setup(steps=200)
+    cfg = fp64_twin(cfg64)
+    cfg.precision = ZFV_PREC_FP32
+    lev = Level(cfg, Q0, A0)
+    try:
+        st = lev.run(chunk=50)
+        Q32 = lev.state64().cpu().numpy()
+    finally:
+        lev.close()
+    Qo, Ao, n, t, logo, _ = oracle.run(cfg64, Q0, A0)
+    assert st["step"] == n == 200
+    dh = np.abs(Q32[1] - Qo[1])
+    l1, linf = dh.mean(), dh.max()
+    print(f"[fp32 vs fp64 oracle, config-2 strip] L1 {l1:.3e} Linf {linf:.3e} "
+          f"mom {np.abs(Q32[2:] - Qo[2:]).max():.3e}")
+    assert l1 <= 1e-6, l1
+    assert linf <= 1e-4, linf
     assert ((Q32[1] <= 1e-6) == (Qo[1] <= 1e-6)).mean() > 0.999
 
 

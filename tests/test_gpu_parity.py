@@ -8,10 +8,19 @@ order differs) to 1e-13 relative.
 import numpy as np
 import pytest
 
-from cases import GOLDEN_CASES, golden_setup, setup
+from cases import CASES_1D, CASES_2D, GOLDEN_CASES, config2_strip_setup, golden_setup, setup, wetdry_ic
 from zoomy_amrex_b200.models import SWE
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def oracle(parity_oracle):
+    """Every comparison in this module is against the reference's own
+    make_rhs.H under the oracle's driver (oracle/_ref) where it was built,
+    else against the restatement (which equals it bitwise on every case here,
+    tests/test_oracle_golden.py)."""
+    return parity_oracle
 
 
 def run_gpu(cfg, Q0, A0, use_graph=False, chunk=16):
@@ -43,91 +52,6 @@ def test_golden_cases_bitwise_vs_oracle(cuda, oracle, name):
     assert_same_run(*golden_setup(name), oracle)
 
 
-def _bumps(x, seed, n=6, lo=0.0, hi=10.0, amp=(0.2, 1.2), width=(0.5, 2.0)):
-    rng = np.random.default_rng(seed)
-    b = np.zeros(x.shape[1])
-    for _ in range(n):
-        cx, cy = rng.uniform(lo, hi, 2)
-        a, w = rng.uniform(*amp), rng.uniform(*width)
-        b += a * np.exp(-((x[0] - cx) ** 2 + (x[1] - cy) ** 2) / (2 * w * w))
-    return b
-
-
-def wetdry_ic(seed, eta0=1.0, hump=0.3, moving=False):
-    def ic(x):
-        b = _bumps(x, seed)
-        rng = np.random.default_rng(seed + 1)
-        cx, cy = rng.uniform(2, 8, 2)
-        eta = eta0 + hump * np.exp(-((x[0] - cx) ** 2 + (x[1] - cy) ** 2) / 2.0)
-        h = np.maximum(eta - b, 0.0)
-        hu = h * rng.uniform(-0.1, 0.1, h.shape) if moving else np.zeros_like(h)
-        hv = h * rng.uniform(-0.1, 0.1, h.shape) if moving else np.zeros_like(h)
-        return np.array([b, h, hu, hv])
-    return ic
-
-
-def dambreak_2d(x):
-    h = np.where(x[0] < 0.5, 2.0, 1.0)
-    z = np.zeros_like(h)
-    return np.array([z, h, z, z])
-
-
-CASES_2D = {
-    # config 1: 100x100 dam break, order 2, cfl 0.45 (Exec/inputs), extrapolation, t=0.1
-    "dambreak_o2": (SWE(2, "extrapolation", None),
-                    dict(dimension=2, domain=[0, 1, 0, 1], n_cells=[100, 100], spatial_order=2,
-                         cfl=0.45, time_end=0.1, dtmax=0.1)),
-    "dambreak_o2_clamp": (SWE(2, "extrapolation", None),
-                          dict(dimension=2, domain=[0, 1, 0, 1], n_cells=[100, 100], spatial_order=2,
-                               cfl=0.45, time_end=0.1, dtmax=0.1, clamp_positivity=True)),
-    "wetdry_wb_manning_o2": (SWE(2, "wall", wetdry_ic(3), parameters={"n_m": 0.03}),
-                             dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[48, 40],
-                                  spatial_order=2, cfl=0.9, time_end=1e30, max_step=40,
-                                  well_balanced=True, implicit_source=True)),
-    "wetdry_moving_o2_mixed_bc": (SWE(2, {"West": "wall", "East": "extrapolation", "South": "extrapolation",
-                                          "North": "wall"}, wetdry_ic(5, moving=True),
-                                      parameters={"n_m": 0.05}),
-                                  dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[33, 17],
-                                       spatial_order=2, cfl=0.9, time_end=1e30, max_step=30,
-                                       well_balanced=True, implicit_source=True)),
-    "wetdry_o1_impl": (SWE(2, "wall", wetdry_ic(7, moving=True), parameters={"n_m": 0.03}),
-                       dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[37, 29], spatial_order=1,
-                            cfl=0.9, time_end=1e30, max_step=25, well_balanced=True,
-                            implicit_source=True)),
-    "tiny_7x5_o2": (SWE(2, "wall", wetdry_ic(11, moving=True)),
-                    dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[7, 5], spatial_order=2,
-                         cfl=0.9, time_end=1e30, max_step=20, well_balanced=True)),
-    "strip_65x2_o2": (SWE(2, "extrapolation", wetdry_ic(13, moving=True)),
-                      dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[65, 2], spatial_order=2,
-                           cfl=0.9, time_end=1e30, max_step=10)),
-}
-
-
-def ritter_o2(x):
-    h = np.where(x[0] < 5.0, 0.005, 0.0)
-    z = np.zeros_like(h)
-    return np.array([z, h, z])
-
-
-def bump_1d(x):
-    b = 0.3 * np.exp(-((x[0] - 4.0) ** 2)) + 0.8 * np.exp(-((x[0] - 7.0) ** 2) * 4)
-    h = np.maximum(0.9 - b, 0.0)
-    return np.array([b, h, 0.02 * h])
-
-
-CASES_1D = {
-    "ritter_o2": (SWE(1, "swashes", ritter_o2),
-                  dict(dimension=1, domain=[0, 10], n_cells=129, spatial_order=2, cfl=0.9, time_end=2.0)),
-    "bump_wall_wb_impl_o2": (SWE(1, "wall", bump_1d, parameters={"n_m": 0.04}),
-                             dict(dimension=1, domain=[0, 10], n_cells=200, spatial_order=2, cfl=0.9,
-                                  time_end=1e30, max_step=60, well_balanced=True, implicit_source=True)),
-    "bump_o1_explicit_manning": (SWE(1, {"West": "wall", "East": "extrapolation"}, bump_1d,
-                                     parameters={"n_m": 0.04}),
-                                 dict(dimension=1, domain=[0, 10], n_cells=301, spatial_order=1,
-                                      cfl=0.9, time_end=1e30, max_step=40, well_balanced=True)),
-}
-
-
 @pytest.mark.parametrize("name", sorted(CASES_2D))
 def test_2d_cases_bitwise_vs_oracle(cuda, oracle, name):
     assert_same_run(*setup(*CASES_2D[name]), oracle)
@@ -136,6 +60,13 @@ def test_2d_cases_bitwise_vs_oracle(cuda, oracle, name):
 @pytest.mark.parametrize("name", sorted(CASES_1D))
 def test_1d_cases_bitwise_vs_oracle(cuda, oracle, name):
     assert_same_run(*setup(*CASES_1D[name]), oracle)
+
+
+def test_config2_strip_bitwise_vs_oracle(cuda, oracle):
+    """The benchmark's own fields (16 seeded bumps over [0,100]^2 m at 4096
+    cells across, hump, Manning n = 0.03, walls, WB, order 2): a 4096 x 64
+    strip of rows for 20 steps, bitwise."""
+    assert_same_run(*config2_strip_setup(steps=20), oracle)
 
 
 def test_explicit_friction_blow_up_is_reproduced(cuda, oracle):

@@ -24,7 +24,7 @@ def check(name, Q, Qaux):   # tests/refs.py:check
 
 
 def march(model, settings, t_end, cfl):
-    r = run_case(model, dict(settings, time_end=t_end, cfl=cfl))
+    r = run_case(model, dict(settings, time_end=t_end, cfl=cfl), return_result=True)
     return r.Q, r.Qaux
 
 
@@ -59,15 +59,28 @@ def test_lake_at_rest_over_bump(cuda):
     check("wb_lake", Q, Qaux)
 
 
-def test_swe_2d_pulse(cuda):
+def test_swe_2d_pulse(cuda, tmp_path):
+    """HyperbolicSolver.solve returns the run's .pvd path, as the reference's
+    does (solvers.py:120-124 -> run_case.py:426); the last data set's cell
+    data holds the golden state and aux."""
+    from zoomy_amrex_b200.vtk import read_pvd, read_vtu
     solver = HyperbolicSolver(CFL=CFL_2D, order=1, well_balanced=False)
-    r = solver.solve(SME(level=0, dimension=3, bc="extrapolation", initial_conditions=gaussian_pulse_2d),
-                     {"domain": [-1.0, 1.0, -1.0, 1.0], "n_cells": [32, 32]},
-                     {"time_end": 0.1, "output": {"snapshots": 1}})
-    Q = r.Q
+    path = solver.solve(SME(level=0, dimension=3, bc="extrapolation", initial_conditions=gaussian_pulse_2d),
+                        {"domain": [-1.0, 1.0, -1.0, 1.0], "n_cells": [32, 32]},
+                        {"time_end": 0.1, "output": {"snapshots": 1, "directory": str(tmp_path)}})
+    assert isinstance(path, str) and path.endswith(".pvd") and pathlib.Path(path).is_file()
+    sets = read_pvd(path)
+    assert sets and abs(sets[-1][0] - 0.1) < 1e-12
+    d = read_vtu(sets[-1][2])
+    assert d["Points"].shape == (33 * 33, 3)
+    Q = np.stack([d[n].reshape(32, 32) for n in ("b", "h", "hu", "hv")])
+    Qaux = np.stack([d[f"var{c}"].reshape(32, 32) for c in range(4, 11)])
     assert np.isfinite(Q).all() and Q[1].min() > 0.0
     assert np.abs(Q[2]).max() > 0.0 and np.abs(Q[3]).max() > 0.0
-    check("swe_2d", Q, r.Qaux)
+    check("swe_2d", Q, Qaux)
+    with pytest.raises(ValueError, match="directory"):
+        solver.solve(SME(level=0, dimension=3), {"domain": [-1.0, 1.0, -1.0, 1.0], "n_cells": [8, 8]},
+                     {"time_end": 0.1})
 
 
 @pytest.mark.parametrize("n_cells", [100, 200])
@@ -97,7 +110,7 @@ def test_plotfiles_like_evolve(cuda, oracle, tmp_path):
     from zoomy_amrex_b200.plotfile import read_plotfile
     model = SME(level=0, dimension=2, bc="swashes", initial_conditions=stoker_ic)
     settings = dict(ONE_D, time_end=1.0, cfl=CFL_1D, output_snapshots=7)
-    r = run_case(model, settings, str(tmp_path))
+    r = run_case(model, settings, str(tmp_path), return_result=True)
     plts = sorted(tmp_path.glob("plt_*"))
     assert [p.name for p in plts] == [f"plt_0{k:05d}" for k in range(len(plts))]
     H, levels = read_plotfile(plts[-1])
@@ -129,8 +142,8 @@ def test_run_case_fp32_precision_follows_fp64(cuda):
     model = SWE(2, "wall", ic, parameters={"n_m": 0.03})
     s = dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[64, 48], spatial_order=2, cfl=0.45, time_end=0.3,
              well_balanced=True, implicit_source=True, output_snapshots=1)
-    r64 = run_case(model, dict(s))
-    r32 = run_case(model, dict(s, precision="fp32"))
+    r64 = run_case(model, dict(s), return_result=True)
+    r32 = run_case(model, dict(s, precision="fp32"), return_result=True)
     assert abs(r32.time - r64.time) < 1e-9 and abs(r32.steps - r64.steps) <= 1
     assert np.abs(r32.Q[1] - r64.Q[1]).max() < 1e-4
 
@@ -148,9 +161,12 @@ def test_run_case_max_level_runs_the_amr_hierarchy(cuda, tmp_path):
     model = SWE(2, "wall", ic, parameters={"n_m": 0.03})
     s = dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[128, 128], spatial_order=2, cfl=0.45, time_end=0.2,
              well_balanced=True, implicit_source=True, output_snapshots=4, max_level=2, tag_b_max=0.2)
-    r = run_case(model, s, str(tmp_path))
+    r = run_case(model, s, str(tmp_path), return_result=True)
     plts = sorted(tmp_path.glob("plt_*"))
     assert len(plts) >= 5 and r.plotfiles[-1] == str(plts[-1])
+    from zoomy_amrex_b200.vtk import read_pvd
+    parts = read_pvd(r.path)
+    assert {p for _, p, _ in parts} >= {0, 1} and all(pathlib.Path(f).is_file() for _, _, f in parts)
     head, levels = read_plotfile(plts[-1])
     print(f"[run_case amr] {r.steps} coarse steps to t = {r.time}, levels {len(levels)}, "
           f"patches {[len(L.patches) for L in levels]}")

@@ -164,7 +164,7 @@ def test_run_case_rejects_fluxes_not_built():
     from zoomy_amrex_b200.run_case import run_case
     with pytest.raises(NotImplementedError, match="NonconservativeRusanov"):
         run_case(SWE(2, "wall", None), dict(dimension=2, domain=[0, 1, 0, 1], n_cells=[8, 8],
-                                            riemann="PositiveNonconservativeHLL"))
+                                            riemann="PositiveNonconservativeHLL"), return_result=True)
 
 
 def _record_many(args):
@@ -174,6 +174,27 @@ def _record_many(args):
     for i in range(40):
         record(4, "fp32", 4096.0 * 4096.0, (k + i) % 13, {0: 1.0 + k, 1: 2.0}, shapes, path=path)
     return k
+
+
+def _record_own_key(args):
+    from zoomy_amrex_b200.autotune import record
+    path, k = args
+    shapes = [(4, 8, 2, 3)] * 13
+    for i in range(20):
+        record(4 + k, "fp32", 4096.0 * 4096.0, i % 13, {0: 1.0}, shapes, path=path)
+    return k
+
+
+def test_autotune_concurrent_writers_keep_every_key(tmp_path):
+    """Processes tuning different keys at the same time all keep their entry
+    (the read-modify-write runs under a lock)."""
+    import json
+    import multiprocessing as mp
+    path = tmp_path / "autotune.json"
+    with mp.get_context("spawn").Pool(4) as pool:
+        pool.map(_record_own_key, [(path, k) for k in range(4)])
+    data = json.loads(path.read_text())
+    assert sorted(data) == sorted(f"n_q={4 + k}/fp32/large" for k in range(4))
 
 
 def test_autotune_cache_survives_concurrent_writers(tmp_path):

@@ -49,3 +49,24 @@ def test_level_state_plotfile_round_trip(tmp_path):
     assert H["time"] == 0.5 and H["finest_level"] == 0
     d = levels[0].patches[0].data
     assert np.array_equal(d[:4], Q) and np.array_equal(d[4:], A)
+
+
+def test_plotfiles_convert_to_pvd_and_vtu(tmp_path):
+    """The run's ParaView output (run_case.py:128-178 of the reference): one
+    .vtu per plotfile and level, cell data by state name then var<c>, listed
+    in simulation.pvd with the plotfile times."""
+    from zoomy_amrex_b200.plotfile import write_level_state
+    from zoomy_amrex_b200.vtk import plotfiles_to_vtk, read_pvd, read_vtu
+    rng = np.random.default_rng(3)
+    Q, A = rng.random((4, 5, 7)), rng.random((7, 5, 7))
+    p1 = write_level_state(tmp_path, "0", 0, 0.0, Q, A, (0.0, 0.0), (7.0, 5.0))
+    p2 = write_level_state(tmp_path, "0", 1, 0.5, 2 * Q, A, (0.0, 0.0), (7.0, 5.0))
+    pvd = plotfiles_to_vtk([p1, p2], ["b", "h", "hu", "hv"], tmp_path, 2)
+    assert pvd == str(tmp_path / "simulation.pvd")
+    sets = read_pvd(pvd)
+    assert [(t, part) for t, part, _ in sets] == [(0.0, 0), (0.5, 0)]
+    v = read_vtu(sets[1][2])
+    assert v["Points"].shape == (6 * 8, 3) and v["Points"][9, 0] == 1.0 and v["Points"][9, 1] == 1.0
+    assert np.array_equal(v["h"].reshape(5, 7), 2 * Q[1])
+    assert np.array_equal(v["var6"].reshape(5, 7), A[2])
+    assert np.array_equal(v["connectivity"][:4], [0, 1, 9, 8])

@@ -10,6 +10,7 @@ to the library; ``cached_variant`` looks it up.
 """
 from __future__ import annotations
 
+import fcntl
 import json
 import os
 import pathlib
@@ -49,17 +50,24 @@ def cached_variant(n_q: int, precision: str, cells_per_instance: float,
 
 def record(n_q: int, precision: str, cells_per_instance: float, variant: int, times_ms: dict,
            shapes: list, path: pathlib.Path = CACHE) -> None:
-    data = _load(path)
-    data[_key(n_q, precision, size_class(cells_per_instance))] = dict(
-        variant=int(variant), shape=list(shapes[variant]),
-        ms_per_step={str(k): float(v) for k, v in times_ms.items()})
-    # one temporary file per process, then an atomic rename: processes that
-    # tune at the same time (one per GPU) never write the same file, and the
-    # cache is whichever complete version was renamed last
+    entry = dict(variant=int(variant), shape=list(shapes[variant]),
+                 ms_per_step={str(k): float(v) for k, v in times_ms.items()})
+    # Read-modify-write under an exclusive lock on a sidecar file, so that
+    # processes tuning different keys at the same time (one per GPU) each add
+    # their key to the latest cache; the new version is written to a
+    # per-process temporary file and renamed over the cache atomically, so a
+    # reader never sees a partial document.
     tmp = path.with_suffix(f".json.{os.getpid()}.tmp")
     try:
-        tmp.write_text(json.dumps(data, indent=1, sort_keys=True))
-        tmp.replace(path)
+        with open(path.with_suffix(".json.lock"), "a") as lk:
+            fcntl.flock(lk, fcntl.LOCK_EX)
+            try:
+                data = _load(path)
+                data[_key(n_q, precision, size_class(cells_per_instance))] = entry
+                tmp.write_text(json.dumps(data, indent=1, sort_keys=True))
+                tmp.replace(path)
+            finally:
+                fcntl.flock(lk, fcntl.LOCK_UN)
     except OSError:   # the cache is an optimisation: a read-only install just re-tunes
         tmp.unlink(missing_ok=True)
 

@@ -179,6 +179,10 @@ k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
     constexpr int G = Sh::G, GY = Sh::GY, RW = Sh::RW, RH = Sh::RH, NFC = Sh::NFC, NT = Sh::NT;
     constexpr bool pure = aux_pure<Model>::value;
     static_assert(pure, "the fused stage kernel needs Model::zb_aux_pure");
+    // make_rhs.H:166-229 (add_diffusive_flux, compiled in when
+    // Model::has_diffusion) is not part of these kernels: refuse such a model
+    // at compile time rather than drop its viscous term.
+    static_assert(!Model::has_diffusion, "diffusive models (Model::has_diffusion) are not built here");
 
     extern __shared__ __align__(16) double smem[];
     double* sQ = smem;                                  // [nq][RH][RW]

@@ -56,6 +56,10 @@ class SWE:
     def info(self) -> dict:
         return MODELS[self.model_id]
 
+    def state_names(self) -> list[str]:
+        """Names of the state rows, in the order Q stores them."""
+        return ["b", "h", "hu", "hv"][:2 + self.dimension]
+
     def side_kinds(self) -> tuple:
         """BC kind per side in (x_lo, x_hi, y_lo, y_hi) order ('' = unused side)."""
         sides = SIDES_1D if self.dimension == 1 else SIDES_2D

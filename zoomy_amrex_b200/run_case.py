@@ -2,16 +2,20 @@
 AMR hierarchy when ``max_level > 0``).
 
 Same entry shape as zoomy_amrex.run_case.run_case (zoomy_amrex/run_case.py:346-426):
-``run_case(model, settings, output_dir)``. The reference generates C++,
-compiles it, runs it as a subprocess and converts AMReX plotfiles to VTK; here
-the model family is precompiled into libzoomyfv.so and the march runs
-in-process on PyTorch CUDA tensors. The final state is returned. When
-``output_dir`` is given, AMReX plotfiles of (Q, aux) are written there as the
-reference's Evolve writes them (ZoomyAmr.cpp:782-812, 821-882): at the start
-of the first step with time >= next plot time, next plot time advancing by
-time_end / output_snapshots, and once more after the last step, named
-plt_<identifier><plot index:05d>; plus ``final.npz`` with the per-step
-dt/time/mass log.
+``run_case(model, settings, output_dir)`` returning the path of the run's
+ParaView collection ``<output_dir>/simulation.pvd``. The reference generates
+C++, compiles it, runs it as a subprocess and converts AMReX plotfiles to VTK;
+here the model family is precompiled into libzoomyfv.so and the march runs
+in-process on PyTorch CUDA tensors. AMReX plotfiles of (Q, aux) are written
+into ``output_dir`` as the reference's Evolve writes them
+(ZoomyAmr.cpp:782-812, 821-882): at the start of the first step with
+time >= next plot time, next plot time advancing by time_end /
+output_snapshots, and once more after the last step, named
+plt_<identifier><plot index:05d>; they are converted to ``simulation.pvd`` +
+``vtk/*.vtu`` like the reference's ``_plotfiles_to_vtk``
+(run_case.py:128-178), and ``final.npz`` holds the final state and the
+per-step dt/time/mass log. ``return_result=True`` returns the in-memory
+``CaseResult`` instead (then ``output_dir`` may be None: nothing is written).
 """
 from __future__ import annotations
 
@@ -41,13 +45,32 @@ class CaseResult:
     time: float
     steps: int
     log: np.ndarray        # (steps, 3): dt, time, mass per step
-    path: str | None = None
+    path: str | None = None      # the .pvd written into output_dir (None without one)
     plotfiles: list | None = None
 
 
-def run_case(model: SWE, settings: dict, output_dir: str | None = None, on_progress=None,
-             device: str = "cuda:0", use_graph: bool = True, chunk: int = 64) -> CaseResult:
-    """March ``model`` to settings['time_end'] (or settings['max_step'] steps)."""
+def run_case(model: SWE, settings: dict, output_dir: str | None = None, on_progress=None, *,
+             return_result: bool = False, device: str = "cuda:0", use_graph: bool = True,
+             chunk: int = 64):
+    """March ``model`` to settings['time_end'] (or settings['max_step'] steps).
+
+    Returns the ``.pvd`` path (a str), as the reference does, or the
+    ``CaseResult`` when ``return_result`` is set."""
+    if output_dir is None and not return_result:
+        raise ValueError("run_case: output_dir is required (the run's .pvd and plotfiles are written there); "
+                         "pass return_result=True for the in-memory result only")
+    res = _run(model, settings, output_dir, on_progress, device, use_graph, chunk)
+    if output_dir is not None:
+        res.path = _to_vtk(model, res, output_dir)
+    return res if return_result else res.path
+
+
+def _to_vtk(model, res: CaseResult, output_dir) -> str:
+    from .vtk import plotfiles_to_vtk
+    return plotfiles_to_vtk(res.plotfiles, model.state_names(), output_dir, model.dimension)
+
+
+def _run(model, settings, output_dir, on_progress, device, use_graph, chunk) -> CaseResult:
     from .level import Level   # needs torch + the CUDA library
 
     if settings.get("mpi_ranks", 1) not in (None, 1):
@@ -116,9 +139,7 @@ def run_case(model: SWE, settings: dict, output_dir: str | None = None, on_progr
     res = CaseResult(Q=Q, Qaux=A, time=st["time"], steps=st["step"], log=log)
     res.plotfiles = plots
     if out is not None:
-        p = out / "final.npz"
-        np.savez(p, Q=Q, Qaux=A, time=res.time, steps=res.steps, log=log)
-        res.path = str(p)
+        np.savez(out / "final.npz", Q=Q, Qaux=A, time=res.time, steps=res.steps, log=log)
     return res
 
 
@@ -183,7 +204,5 @@ def _run_case_amr(model: SWE, settings: dict, output_dir, on_progress, device) -
     res = CaseResult(Q=Q, Qaux=A, time=t, steps=steps, log=np.zeros((0, 3)))
     res.plotfiles = plots
     if out is not None:
-        p = out / "final.npz"
-        np.savez(p, Q=Q, Qaux=A, time=t, steps=steps)
-        res.path = str(p)
+        np.savez(out / "final.npz", Q=Q, Qaux=A, time=t, steps=steps)
     return res

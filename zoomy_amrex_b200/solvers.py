@@ -1,12 +1,15 @@
 """``HyperbolicSolver`` — the reference's solver front end, on the GPU.
 
-Mirrors zoomy_amrex.solvers.HyperbolicSolver (zoomy_amrex/solvers.py:199-219):
+Mirrors zoomy_amrex.solvers.HyperbolicSolver (zoomy_amrex/solvers.py:104-124):
 the same parameters (CFL, order, well_balanced, positivity) and the same
 ``solve(model, mesh, settings)`` call, where ``mesh`` is a descriptor
 ``{"domain": [...], "n_cells": [...]}`` and ``settings`` is structured
-(``time_end``, ``output.directory``, ``max_level``). The reference's
-``param.Parameterized`` base is replaced by a dataclass (``param`` is not a
-dependency here); bounds are checked the same way.
+(``time_end``, ``output.directory`` (required, as in the reference's
+``_output_dir``, solvers.py:96-100), ``max_level``). ``solve`` returns the
+run's ``.pvd`` path like the reference; ``run`` takes the same arguments and
+returns the in-memory ``CaseResult`` (``output.directory`` optional there).
+The reference's ``param.Parameterized`` base is replaced by a dataclass
+(``param`` is not a dependency here); bounds are checked the same way.
 """
 from __future__ import annotations
 
@@ -33,7 +36,7 @@ def _mesh_domain_ncells(mesh, settings):
 
 @dataclass
 class HyperbolicSolver:
-    """Explicit finite-volume march for hyperbolic models (SWE)."""
+    """Explicit finite-volume march for hyperbolic models (SWE / SME)."""
 
     CFL: float = 0.45
     order: int = 1
@@ -63,8 +66,20 @@ class HyperbolicSolver:
                 s[k] = v
         return s
 
-    def solve(self, model, mesh, settings, on_progress=None) -> CaseResult:
+    def _settings(self, mesh, settings) -> dict:
         s = self._legacy_settings(mesh, settings)
         s.update(cfl=self.CFL, spatial_order=self.order, well_balanced=self.well_balanced,
                  positivity=self.positivity)
-        return run_case(model, s, _get(settings, "output.directory"), on_progress=on_progress)
+        return s
+
+    def solve(self, model, mesh, settings, on_progress=None) -> str:
+        """Run and return the path of the run's ``.pvd`` (solvers.py:120-124)."""
+        d = _get(settings, "output.directory")
+        if d is None:
+            raise ValueError("solve: settings['output']['directory'] is required")
+        return run_case(model, self._settings(mesh, settings), d, on_progress=on_progress)
+
+    def run(self, model, mesh, settings, on_progress=None) -> CaseResult:
+        """``solve`` returning the final state, time, step count and log in memory."""
+        return run_case(model, self._settings(mesh, settings), _get(settings, "output.directory"),
+                        on_progress=on_progress, return_result=True)
