@@ -155,27 +155,75 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def cpu_sample(kind: str, n: int, rows: int = 256, min_seconds: float = 10.0, max_steps: int = 40):
-    """The CPU implementation on a strip of the same workload (first `rows` rows
-    of the n x n grid, same cells and data, walls on the strip edges)."""
+_CPU_THREADS_ALL = None
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def cpu_oracle(kind: str, threads: int | None = None):
+    """The CPU implementation with `threads` OpenMP threads (None = all the
+    host's threads, as OpenMP starts with)."""
+    global _CPU_THREADS_ALL
     from oracle.oracle import Oracle
     o = Oracle(kind)
-    threads = o.max_threads()
-    Q0, A0 = workload_fields(n, rows=slice(0, rows))
-    cfg = workload_config(n, ny=rows, y_extent=DOMAIN * rows / n)
+    if _CPU_THREADS_ALL is None:
+        _CPU_THREADS_ALL = o.max_threads()
+    o._fn("set_threads")(int(threads or _CPU_THREADS_ALL))
+    return o, int(threads or _CPU_THREADS_ALL)
+
+
+def cpu_time(kind: str, n: int, rows: int | None, threads: int | None, warmup: int, steps: int,
+             budget_s: float):
+    """`warmup` untimed then up to `steps` timed SSP-RK2 steps of the CPU
+    implementation on the workload's first `rows` rows (all rows: the whole
+    n x n level; a strip has walls on its edges), as few as the time budget
+    allows after a one-step calibration. Returns (cell-updates/s, steps timed,
+    threads, cells)."""
+    o, nt = cpu_oracle(kind, threads)
+    ny = n if rows is None else rows
+    Q0, A0 = workload_fields(n, rows=None if rows is None else slice(0, rows))
+    cfg = workload_config(n, ny=ny, y_extent=DOMAIN * ny / n)
     cfg.max_step = 1
     t0 = time.perf_counter()
-    Q, A, _, _, _, _ = o.run(cfg, Q0, A0)          # warm-up + calibration step
+    Q, A, _, _, _, _ = o.run(cfg, Q0, A0)                # calibration step (counts as warm-up)
     one = time.perf_counter() - t0
-    steps = int(max(1, min(max_steps, min_seconds / max(one, 1e-6))))
-    cfg.max_step = steps
+    if warmup > 1:
+        cfg.max_step = warmup - 1
+        Q, A, _, _, _, _ = o.run(cfg, Q, A)
+    k = int(max(1, min(steps, budget_s / max(one, 1e-6))))
+    cfg.max_step = k
     t0 = time.perf_counter()
-    Q, A, _, _, _, _ = o.run(cfg, Q, A)            # `steps` steps in one Evolve call
+    Q, A, _, _, _, _ = o.run(cfg, Q, A)                  # k steps in one Evolve call
     el = time.perf_counter() - t0
-    return {"value": n * rows * steps / el, "unit": UNIT, "cores": threads,
+    return n * ny * k / el, k, nt, n * ny
+
+
+def cpu_sample(kind: str, n: int):
+    """The CPU baseline on the host cores: all threads on the whole n x n
+    level (the reference arm's configuration) and one thread on a 64-row
+    strip of it, each about 10 s of work."""
+    label = "reference make_rhs.H" if kind == "ref" else "oracle restatement"
+    v_all, k_all, nt, cells = cpu_time(kind, n, None, None, 1, 20, 10.0)
+    v_one, k_one, _, cells1 = cpu_time(kind, n, 64, 1, 1, 60, 10.0)
+    cpu_oracle(kind, None)
+    return {"value": v_all, "unit": UNIT, "cores": nt,
             "kind": "reference" if kind == "ref" else "port",
-            "sample": f"{steps} SSP-RK2 steps on rows 0..{rows - 1} of the {n}x{n} grid "
-                      f"({n * rows} cells), OpenMP over rows, FP64"}
+            "sample": f"{k_all} SSP-RK2 steps on the whole {n}x{n} level ({cells} cells), {label}, FP64, "
+                      f"OpenMP over rows, {nt} threads",
+            "one_thread": {"value": v_one, "unit": UNIT, "cores": 1,
+                           "sample": f"{k_one} SSP-RK2 steps on rows 0..63 of the {n}x{n} level "
+                                     f"({cells1} cells, walls on the strip edges), 1 thread"},
+            "nproc": os.cpu_count(), "cpu_model": cpu_model()}
 
 
 def dist_setup(args):
@@ -190,32 +238,27 @@ def dist_setup(args):
 
 
 def run_reference(args, ws, rank):
-    """Reference arm: the reference's CPU path (make_rhs.H via oracle/_ref, or
-    the restatement when the reference build is absent) on the host cores."""
+    """Reference arm: the reference's CPU path (its own make_rhs.H under the
+    oracle's driver, oracle/_ref; the restatement when that build is absent)
+    on the host cores, all threads, on the same n x n level as the GPU arm.
+    Each step is one SSP-RK2 step of the whole level; at most about 4 minutes
+    of timed steps are run (steps_timed says how many)."""
     if rank != 0:
         return
     from oracle.oracle import LIB_REF
     kind = "ref" if LIB_REF.exists() else "oracle"
-    from oracle.oracle import Oracle
-    o = Oracle(kind)
-    n, rows = args.n, 64
-    Q0, A0 = workload_fields(n, rows=slice(0, rows))
-    cfg = workload_config(n, ny=rows, y_extent=DOMAIN * rows / n)
-    cfg.max_step = max(1, args.warmup)
-    Q, A, _, _, _, _ = o.run(cfg, Q0, A0)          # warm-up steps
-    cfg.max_step = args.steps
-    t0 = time.perf_counter()
-    Q, A, _, _, _, _ = o.run(cfg, Q, A)            # K steps in one Evolve call
-    el = time.perf_counter() - t0
-    v = n * rows * args.steps / el
-    sample = (f"each step: 1 SSP-RK2 step on rows 0..{rows - 1} of the {n}x{n} grid ({n * rows} cells), "
-              f"{'reference make_rhs.H' if kind == 'ref' else 'oracle restatement'}, FP64, OpenMP")
+    n = args.n
+    v, k, nt, cells = cpu_time(kind, n, None, None, max(1, args.warmup), args.steps, 240.0)
+    sample = (f"{k} timed SSP-RK2 steps of the whole {n}x{n} level ({cells} cells) after {max(1, args.warmup)} "
+              f"warm-up steps, {'reference make_rhs.H' if kind == 'ref' else 'oracle restatement'}, FP64, "
+              f"OpenMP over rows, {nt} threads")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "steps": args.steps, "steps_timed": k, "warmup": args.warmup, "ms_per_step": 1e3 * cells / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": config_desc(n, args.steps),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": o.max_threads(),
-                             "kind": "reference" if kind == "ref" else "port", "sample": sample},
+            "data": "synthetic", "config": dict(config_desc(n, k), form="FP64 (the reference's arithmetic)"),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nt,
+                             "kind": "reference" if kind == "ref" else "port", "sample": sample,
+                             "nproc": os.cpu_count(), "cpu_model": cpu_model()},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -670,7 +713,10 @@ def main():
                 "config": dict(config_desc(n, K), parallelism=f"replicas x{ws}" if ws > 1 else "single GPU",
                                form="FP32 chosen (compensated, eta storage)"),
                 "forms": {"fp32_chosen": v32, "fp64_plain": v64, "fp32_over_fp64": v32 / v64,
-                          "ms_per_step_fp32": ms32 / K, "ms_per_step_fp64": ms64 / K},
+                          "ms_per_step_fp32": ms32 / K, "ms_per_step_fp64": ms64 / K,
+                          "fp64_over_reference": (v64 / cpu["value"]) if cpu and cpu.get("value") else None,
+                          "fp64_over_reference_note": "same-precision ratio: FP64 GPU form over the "
+                                                      "reference's FP64 CPU path on all host threads"},
                 "depth_error_fp32_vs_fp64": err,
                 "autotune": tuning, "ensemble": ens, "adjoint": adj, "amr": amr,
                 "hbm_gbs": achieved32,
