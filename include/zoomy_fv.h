@@ -43,7 +43,11 @@ extern "C" {
 /* Compiled model families (the Model::/Numerics:: pair a handle runs). */
 enum {
     ZFV_MODEL_SWE1D = 1,   /* shallow water, 1 horizontal dim: Q=[b,h,hu],    aux 4 */
-    ZFV_MODEL_SWE2D = 2    /* shallow water, 2 horizontal dims: Q=[b,h,hu,hv], aux 7 */
+    ZFV_MODEL_SWE2D = 2,   /* shallow water, 2 horizontal dims: Q=[b,h,hu,hv], aux 7 */
+    ZFV_MODEL_SME2D_L2 = 3,/* shallow-moment equations, level 2, 2 horizontal dims:
+                              Q=[b,h,hu,hv,h*alpha1,h*alpha2,h*beta1,h*beta2], aux 1 (hinv);
+                              Navier-slip bed friction (csrc/models/sme.H) */
+    ZFV_MODEL_SME1D_L2 = 4 /* the same, 1 horizontal dim: Q=[b,h,hu,h*alpha1,h*alpha2], aux 1 */
 };
 
 /* Arithmetic form. */

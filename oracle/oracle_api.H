@@ -7,6 +7,7 @@
 #include <omp.h>
 #include "fv_oracle.H"
 #include "swe.H"
+#include "sme.H"
 
 #define ZO_CAT2(a, b) a##b
 #define ZO_CAT(a, b) ZO_CAT2(a, b)
@@ -24,6 +25,16 @@ int dispatch(const zfv_config* cfg, F&& f) {
     }
     case ZFV_MODEL_SWE2D: {
         using M = zb::SWE<double, 2>; using N = zb::SWENumerics<double, 2>;
+        Level<M, N, Kern<M, N>> L(*cfg);
+        return f(L);
+    }
+    case ZFV_MODEL_SME2D_L2: {
+        using M = zb::SME<double, 2, 2>; using N = zb::SMENumerics<double, 2, 2>;
+        Level<M, N, Kern<M, N>> L(*cfg);
+        return f(L);
+    }
+    case ZFV_MODEL_SME1D_L2: {
+        using M = zb::SME<double, 1, 2>; using N = zb::SMENumerics<double, 1, 2>;
         Level<M, N, Kern<M, N>> L(*cfg);
         return f(L);
     }

@@ -4,13 +4,15 @@
 // make_rhs.H is header-only C++ against AMReX's Array4/SmallMatrix and the
 // generated Model::/Numerics:: functions. It is compiled here unmodified,
 // from where it lies in the reference tree, against the AMReX API shim in
-// zoomy_amrex_b200/csrc/amrex_compat and the SWE Model/Numerics restatement,
-// once per model in its own namespace (ref_swe1d.cpp, ref_swe2d.cpp). The
+// zoomy_amrex_b200/csrc/amrex_compat and the model headers (csrc/models),
+// once per model in its own namespace (ref_swe1d.cpp, ref_swe2d.cpp,
+// ref_sme1d.cpp, ref_sme2d.cpp). The
 // reference's driver (ZoomyAmr.cpp) needs AMReX, MPI and generated headers and
 // is not buildable here; the oracle's restated driver stands in for it.
 #pragma once
 #include "fv_oracle.H"
 #include "swe.H"
+#include "sme.H"
 
 namespace zoracle {
 
@@ -39,11 +41,17 @@ struct NAME {                                                                   
 
 using RefModelSWE1D = zb::SWE<double, 1>;
 using RefModelSWE2D = zb::SWE<double, 2>;
+using RefModelSME2D = zb::SME<double, 2, 2>;
+using RefModelSME1D = zb::SME<double, 1, 2>;
 ZREF_DECLARE_KERNELS(RefSWE1D, RefModelSWE1D)
 ZREF_DECLARE_KERNELS(RefSWE2D, RefModelSWE2D)
+ZREF_DECLARE_KERNELS(RefSME2D, RefModelSME2D)
+ZREF_DECLARE_KERNELS(RefSME1D, RefModelSME1D)
 
 template <> struct RefKernels<zb::SWE<double, 1>, zb::SWENumerics<double, 1>> : RefSWE1D {};
 template <> struct RefKernels<zb::SWE<double, 2>, zb::SWENumerics<double, 2>> : RefSWE2D {};
+template <> struct RefKernels<zb::SME<double, 2, 2>, zb::SMENumerics<double, 2, 2>> : RefSME2D {};
+template <> struct RefKernels<zb::SME<double, 1, 2>, zb::SMENumerics<double, 1, 2>> : RefSME1D {};
 
 }  // namespace zoracle
 

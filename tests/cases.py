@@ -8,7 +8,7 @@ functions of tests/cases.py:195-227 and the CFL law of tests/conftest.py:37
 """
 import numpy as np
 
-from zoomy_amrex_b200.models import SWE, initial_state
+from zoomy_amrex_b200.models import SME, SWE, initial_state
 from zoomy_amrex_b200.settings import config_from_settings, grid
 
 CFL_1D, CFL_2D = 0.9, 0.9
@@ -171,5 +171,64 @@ def config2_strip_setup(steps: int = 20, rows: int = 64):
     n = 4096
     Q0, A0 = bump_workload_fields(n, rows=slice(0, rows))
     cfg = bump_workload_config(n, ny=rows, y_extent=BUMP_DOMAIN * rows / n)
+    cfg.max_step = steps
+    return cfg, Q0, A0
+
+
+# ---------------------------------------------------------------------------
+# Shallow-moment level-2 cases (csrc/models/sme.H): moments seeded as
+# h U(-0.05, 0.05) m/s. The reference driver's well-balancing rescales only
+# the mean momenta at a face (make_rhs.H:91-94), not the moments, so a
+# well-balanced case starts at rest in the mean (a moving one with moments
+# near wet/dry fronts is unstable under the reference scheme).
+
+def sme_ic(seed, u0=0.0, dim=2):
+    def ic(x):
+        rng = np.random.default_rng(seed + 2)
+        if dim == 2:
+            b = _bumps(x, seed)
+            cx, cy = rng.uniform(2, 8, 2)
+            eta = 1.0 + 0.3 * np.exp(-((x[0] - cx) ** 2 + (x[1] - cy) ** 2) / 2.0)
+        else:
+            b = 0.3 * np.exp(-((x[0] - 4.0) ** 2)) + 0.8 * np.exp(-((x[0] - 7.0) ** 2) * 4)
+            eta = 0.9 + 0.2 * np.exp(-((x[0] - 2.0) ** 2))
+        h = np.maximum(eta - b, 0.0)
+        nm = 4 if dim == 2 else 2
+        mom = [h * rng.uniform(-0.05, 0.05, h.shape) for _ in range(nm)]
+        if dim == 2:
+            return np.array([b, h, u0 * h, -0.5 * u0 * h, *mom])
+        return np.array([b, h, u0 * h, *mom])
+    return ic
+
+
+CASES_SME = {
+    "sme2d_wetdry_wb_impl_o2": (SME(level=2, dimension=3, bc="wall", initial_conditions=sme_ic(3)),
+                                dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[48, 40], spatial_order=2,
+                                     cfl=0.45, time_end=1e30, max_step=40, well_balanced=True,
+                                     implicit_source=True)),
+    "sme2d_moving_mixed_bc_o2": (SME(level=2, dimension=3,
+                                     bc={"West": "wall", "East": "extrapolation", "South": "extrapolation",
+                                         "North": "wall"},
+                                     initial_conditions=sme_ic(5, u0=0.1)),
+                                 dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[33, 17], spatial_order=2,
+                                      cfl=0.45, time_end=1e30, max_step=30, implicit_source=True)),
+    "sme2d_o1_impl_wb": (SME(level=2, dimension=3, bc="wall", initial_conditions=sme_ic(7)),
+                         dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[37, 29], spatial_order=1,
+                              cfl=0.45, time_end=1e30, max_step=25, well_balanced=True, implicit_source=True)),
+    "sme2d_tiny_7x5_o2": (SME(level=2, dimension=3, bc="wall", initial_conditions=sme_ic(11, u0=0.05)),
+                          dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[7, 5], spatial_order=2,
+                               cfl=0.45, time_end=1e30, max_step=20, implicit_source=True)),
+    "sme1d_wb_impl_o2": (SME(level=2, dimension=2, bc="wall", initial_conditions=sme_ic(13, dim=1)),
+                         dict(dimension=1, domain=[0, 10], n_cells=200, spatial_order=2, cfl=0.45,
+                              time_end=1e30, max_step=60, well_balanced=True, implicit_source=True)),
+}
+
+
+def sme_strip_setup(steps: int = 20, rows: int = 32, n: int = 2048):
+    """A strip of the shallow-moment benchmark level (n^2 over [0,50]^2 m):
+    rows 0..rows-1 of its fields, walls on the strip's four sides."""
+    from zoomy_amrex_b200.workloads import SME_DOMAIN, sme_workload_config, sme_workload_fields
+    Q0, A0 = sme_workload_fields(n, rows=slice(0, rows))
+    cfg = sme_workload_config(n, ny=rows, y_extent=SME_DOMAIN * rows / n)
     cfg.max_step = steps
     return cfg, Q0, A0

@@ -72,11 +72,13 @@ def test_decomposition_free_two_rank_golden(oracle):
 
 
 def _all_parity_setups():
-    from cases import CASES_1D, CASES_2D, config2_strip_setup, setup
+    from cases import CASES_1D, CASES_2D, CASES_SME, config2_strip_setup, setup, sme_strip_setup
     out = {f"golden/{n}": (lambda n=n: golden_setup(n)) for n in sorted(GOLDEN_CASES)}
     out.update({f"2d/{n}": (lambda n=n: setup(*CASES_2D[n])) for n in sorted(CASES_2D)})
     out.update({f"1d/{n}": (lambda n=n: setup(*CASES_1D[n])) for n in sorted(CASES_1D)})
     out["config2_strip_4096x64_20steps"] = lambda: config2_strip_setup(steps=20)
+    out.update({f"sme/{n}": (lambda n=n: setup(*CASES_SME[n])) for n in sorted(CASES_SME)})
+    out["sme_strip_2048x32_10steps"] = lambda: sme_strip_setup(steps=10)
     return out
 
 
@@ -96,6 +98,7 @@ def test_oracle_equals_reference_make_rhs(oracle, ref_oracle, name):
     a = oracle.run(cfg, Q0, A0)
     b = ref_oracle.run(cfg, Q0, A0)
     assert a[2] == b[2] and a[3] == b[3], "step count / final time differ"
+    assert np.isfinite(a[0]).all(), "the case should stay finite"
     assert np.array_equal(a[0], b[0], equal_nan=True), f"state max diff {np.nanmax(np.abs(a[0] - b[0])):.3e}"
     assert np.array_equal(a[1], b[1], equal_nan=True)
     assert np.array_equal(a[4][:, :2], b[4][:, :2]), "dt / time sequences differ"

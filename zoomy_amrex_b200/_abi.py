@@ -11,6 +11,8 @@ ZFV_MAX_PARAMS = 16
 
 ZFV_MODEL_SWE1D = 1
 ZFV_MODEL_SWE2D = 2
+ZFV_MODEL_SME2D_L2 = 3
+ZFV_MODEL_SME1D_L2 = 4
 
 ZFV_PREC_FP64 = 0
 ZFV_PREC_FP32 = 1
@@ -21,16 +23,22 @@ ZFV_FLAG_DONE = 4
 
 # Model registry: id -> (n_q, n_aux, n_params, dimension, parameter names,
 # default parameters, boundary tags). Mirrors the compiled Model::
-# constants (zoomy_amrex_b200/csrc/models/swe.H).
+# constants (zoomy_amrex_b200/csrc/models/swe.H, sme.H).
 SWE_PARAM_NAMES = ("g", "ex", "ey", "n_m", "h_floor", "eps")
 SWE_DEFAULTS = (9.81, 0.0, 0.0, 0.0, 1.0e-6, 1.0e-24)
 SWE_TAGS = ("extrapolation", "wall")
+SME_PARAM_NAMES = ("g", "ex", "ey", "nu", "lambda", "eps")
+SME_DEFAULTS = (9.81, 0.0, 0.0, 1.0e-3, 0.1, 1.0e-24)
 
 MODELS = {
     ZFV_MODEL_SWE1D: dict(name="swe1d", n_q=3, n_aux=4, n_params=6, dimension=1,
                           param_names=SWE_PARAM_NAMES, defaults=SWE_DEFAULTS, tags=SWE_TAGS),
     ZFV_MODEL_SWE2D: dict(name="swe2d", n_q=4, n_aux=7, n_params=6, dimension=2,
                           param_names=SWE_PARAM_NAMES, defaults=SWE_DEFAULTS, tags=SWE_TAGS),
+    ZFV_MODEL_SME2D_L2: dict(name="sme2d_l2", n_q=8, n_aux=1, n_params=6, dimension=2, level=2,
+                             param_names=SME_PARAM_NAMES, defaults=SME_DEFAULTS, tags=SWE_TAGS),
+    ZFV_MODEL_SME1D_L2: dict(name="sme1d_l2", n_q=5, n_aux=1, n_params=6, dimension=1, level=2,
+                             param_names=SME_PARAM_NAMES, defaults=SME_DEFAULTS, tags=SWE_TAGS),
 }
 
 

@@ -32,6 +32,8 @@ N_FP32_SHAPES = 13   # kNumVariants in csrc/fv32_shapes.H
 # (source, extra flags, object stem). The FP32 strip shapes are one source
 # compiled once per shape (-DZFV32_SHAPE=k) so that they build in parallel.
 SOURCES = ([("zoomy_fv.cu", ["--fmad=false"], "zoomy_fv"),
+            ("zoomy_fv64_swe.cu", ["--fmad=false"], "zoomy_fv64_swe"),
+            ("zoomy_fv64_sme.cu", ["--fmad=false"], "zoomy_fv64_sme"),
             ("zoomy_fv32.cu", FP32_FLAGS, "zoomy_fv32"),
             ("zoomy_adj.cu", ["--fmad=true"], "zoomy_adj")]
            + [("zoomy_fv32_shape.cu", FP32_FLAGS + [f"-DZFV32_SHAPE={k}"], f"zoomy_fv32_shape{k}")

@@ -124,7 +124,7 @@ k_jvp(const double* __restrict__ Qbase, const double* __restrict__ qbed, const d
 // partials[k * nblk + block] = sum over the block of w . V_k for k <
 // gridDim.y (blockIdx.y = k; V_k = V + k * vstride); with self_last the last
 // k is w . w instead.
-__global__ void __launch_bounds__(kNT)
+static __global__ void __launch_bounds__(kNT)
 k_dots(const double* __restrict__ w, const double* __restrict__ V, long long vstride, long long N,
        double* __restrict__ partials, int self_last) {
     __shared__ double red[kNT / 32];
@@ -137,7 +137,7 @@ k_dots(const double* __restrict__ w, const double* __restrict__ V, long long vst
 }
 
 // out[k] = sum of partials[k * nblk + b] over b in order (one block per k).
-__global__ void __launch_bounds__(kNT)
+static __global__ void __launch_bounds__(kNT)
 k_sum_partials(const double* __restrict__ partials, int nblk, double* __restrict__ out) {
     __shared__ double red[kNT / 32];
     const double* p = partials + (long long)blockIdx.x * nblk;
@@ -152,7 +152,7 @@ struct Coefs {
 };
 
 // y = a y + sum_k coef_k V_k (k < nv; a = 1: accumulate).
-__global__ void __launch_bounds__(kNT)
+static __global__ void __launch_bounds__(kNT)
 k_combine(double* __restrict__ y, double a, const double* __restrict__ V, long long vstride, int nv, Coefs cf,
           long long N) {
     for (long long e = (long long)blockIdx.x * kNT + threadIdx.x; e < N; e += (long long)gridDim.x * kNT) {
@@ -163,7 +163,7 @@ k_combine(double* __restrict__ y, double a, const double* __restrict__ V, long l
 }
 
 // dst = s * src
-__global__ void __launch_bounds__(kNT)
+static __global__ void __launch_bounds__(kNT)
 k_scale(double* __restrict__ dst, const double* __restrict__ src, double s, long long N) {
     for (long long e = (long long)blockIdx.x * kNT + threadIdx.x; e < N; e += (long long)gridDim.x * kNT)
         dst[e] = s * src[e];

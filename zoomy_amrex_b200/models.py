@@ -18,7 +18,7 @@ from typing import Callable, Mapping
 
 import numpy as np
 
-from ._abi import MODELS, ZFV_MODEL_SWE1D, ZFV_MODEL_SWE2D
+from ._abi import MODELS, ZFV_MODEL_SME1D_L2, ZFV_MODEL_SME2D_L2, ZFV_MODEL_SWE1D, ZFV_MODEL_SWE2D
 
 SIDES_2D = ("West", "East", "South", "North")   # run_case.py:281-283
 SIDES_1D = ("West", "East")
@@ -82,11 +82,40 @@ class SWE:
         return tuple(out)
 
 
+@dataclass
+class ShallowMoments(SWE):
+    """Shallow-moment equations of level ``level`` (csrc/models/sme.H): state
+    [b, h, hu, (hv), h alpha_1..h alpha_L, (h beta_1..h beta_L)], Navier-slip
+    bed friction with viscosity ``nu`` and slip length ``lambda`` (parameters
+    g, ex, ey, nu, lambda, eps). Same bc / initial_conditions / parameters
+    contract as SWE; initial_conditions return all n_q rows."""
+
+    level: int = 2
+
+    @property
+    def model_id(self) -> int:
+        if self.level != 2:
+            raise NotImplementedError(f"shallow-moment level {self.level} is not compiled (levels 0 and 2 are)")
+        if self.dimension not in (1, 2):
+            raise ValueError(f"SME dimension must be 1 or 2 horizontal directions, got {self.dimension}")
+        return ZFV_MODEL_SME1D_L2 if self.dimension == 1 else ZFV_MODEL_SME2D_L2
+
+    def state_names(self) -> list[str]:
+        names = ["b", "h", "hu", "hv"][:2 + self.dimension]
+        names += [f"halpha_{j}" for j in range(1, self.level + 1)]
+        if self.dimension == 2:
+            names += [f"hbeta_{j}" for j in range(1, self.level + 1)]
+        return names
+
+
 def SME(level: int = 0, dimension: int = 3, **kw) -> SWE:
-    """zoomy_core-style constructor: SME level 0 is the shallow-water model."""
-    if level != 0:
-        raise NotImplementedError("only shallow-moment level 0 (SWE) is compiled")
-    return SWE(dimension=dimension - 1, **kw)
+    """zoomy_core-style constructor (dimension counts the vertical too): level
+    0 is the shallow-water model, level 2 the two-moment shallow-moment model."""
+    if level == 0:
+        return SWE(dimension=dimension - 1, **kw)
+    if level == 2:
+        return ShallowMoments(dimension=dimension - 1, level=level, **kw)
+    raise NotImplementedError(f"shallow-moment level {level} is not compiled (levels 0 and 2 are)")
 
 
 def cell_centres(nx: int, ny: int, prob_lo, prob_hi, dimension: int) -> np.ndarray:

@@ -9,6 +9,10 @@ the shapes and value distributions of its scenarios:
 * ``bump_field``: Gaussian-bump bathymetry (centres uniform in the box,
   amplitudes U(0.2, 1.5) m, widths U(2, 10) m) under still water at eta0 plus
   an optional Gaussian hump;
+* ``sme_workload_fields`` / ``sme_workload_config``: the shallow-moment
+  level-2 scenario on [0,50]^2 m: the same bump generator, the same surface
+  (1 m plus a 0.3 m hump), fluid at rest in the mean with seeded moments
+  h alpha_j, h beta_j = h U(-0.05, 0.05) m/s;
 * ``dam_break_ensemble``: independent shallow-water boxes of uneven size
   (sides log-uniform per axis), each with its own bumps and a dam-break ratio
   drawn U(1.2, 3.0), as a list of (config, Q0, aux0) for the FP32 batch engine.
@@ -17,7 +21,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from ._abi import ZFV_MODEL_SWE2D, ZFV_PREC_FP32, ZFV_PREC_FP64, make_config
+from ._abi import ZFV_MODEL_SME2D_L2, ZFV_MODEL_SWE2D, ZFV_PREC_FP32, ZFV_PREC_FP64, make_config
 
 BUMP_SEED = 2026
 BUMP_DOMAIN = 100.0
@@ -142,3 +146,58 @@ def fp64_twin(cfg):
     C.memmove(C.byref(c), C.byref(cfg), C.sizeof(cfg))
     c.precision = ZFV_PREC_FP64
     return c
+
+
+SME_SEED = 2030
+SME_DOMAIN = 50.0
+
+
+def sme_workload_fields(n: int, seed: int = SME_SEED, rows: slice | None = None):
+    """Shallow-moment level-2 state on n x n cells over [0,50]^2 m: 16 seeded
+    Gaussian bumps (centres U(domain), amplitudes U(0.2,1.5) m, widths
+    U(2,10) m), eta = 1 m plus a 0.3 m Gaussian hump, h = max(eta - b, 0),
+    zero mean velocity, moments h alpha_1, h alpha_2, h beta_1, h beta_2 =
+    h U(-0.05, 0.05) m/s (seeded per cell). ``rows`` selects a strip of rows
+    of the same grid (the moments of those rows are the full grid's). Returns
+    Q0 (8, ny, n), aux0 (1, ny, n)."""
+    rng = np.random.default_rng(seed)
+    cx, cy = rng.uniform(0, SME_DOMAIN, 16), rng.uniform(0, SME_DOMAIN, 16)
+    amp, wid = rng.uniform(0.2, 1.5, 16), rng.uniform(2.0, 10.0, 16)
+    hx, hy, hw = rng.uniform(0, SME_DOMAIN), rng.uniform(0, SME_DOMAIN), rng.uniform(2.0, 10.0)
+    dx = SME_DOMAIN / n
+    x = (np.arange(n) + 0.5) * dx
+    sel = slice(0, n) if rows is None else rows
+    ys = x[sel]
+    ny = len(ys)
+    b = np.zeros((ny, n))
+    for k in range(16):
+        gx = np.exp(-((x - cx[k]) ** 2) / (2 * wid[k] ** 2))
+        gy = np.exp(-((ys - cy[k]) ** 2) / (2 * wid[k] ** 2))
+        b += amp[k] * np.outer(gy, gx)
+    eta = 1.0 + 0.3 * np.outer(np.exp(-((ys - hy) ** 2) / (2 * hw ** 2)),
+                               np.exp(-((x - hx) ** 2) / (2 * hw ** 2)))
+    h = np.maximum(eta - b, 0.0)
+    Q0 = np.zeros((8, ny, n))
+    Q0[0], Q0[1] = b, h
+    # per-cell moment draws of the whole grid, row-major, so that a strip of
+    # rows sees the same values as the full grid
+    mrng = np.random.default_rng(seed + 1)
+    start = 0 if rows is None else (rows.start or 0)
+    mrng.uniform(-0.05, 0.05, (start, 4, n)) if start else None
+    m = mrng.uniform(-0.05, 0.05, (ny, 4, n))
+    for k in range(4):
+        Q0[4 + k] = h * m[:, k, :]
+    return Q0, np.zeros((1, ny, n))
+
+
+def sme_workload_config(n: int, ny: int | None = None, y_extent: float | None = None,
+                        well_balanced: bool = True):
+    """The matching configuration: SME level 2 (2-D), order 2, point-implicit
+    Navier-slip friction (viscosity 1e-3, slip length 0.1), walls, cfl 0.45,
+    no stop time (callers set max_step / time_end)."""
+    ny = n if ny is None else ny
+    ye = SME_DOMAIN if y_extent is None else y_extent
+    return make_config(ZFV_MODEL_SME2D_L2, n, ny, (0.0, 0.0), (SME_DOMAIN, ye), spatial_order=2,
+                       well_balanced=well_balanced, implicit_source=True, cfl=0.45, dtmin=1e-7, dtmax=1.0,
+                       time_end=1e30, max_step=-1, bc=("wall",) * 4,
+                       params={"nu": 1.0e-3, "lambda": 0.1, "eps": 1e-24})
