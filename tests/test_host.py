@@ -113,10 +113,15 @@ def test_unknown_bc_and_param_are_errors():
 
 
 def test_sme_level0_dimension_convention():
+    from zoomy_amrex_b200._abi import ZFV_MODEL_SME1D_L2, ZFV_MODEL_SME2D_L2
     assert SME(level=0, dimension=3).dimension == 2
     assert SME(level=0, dimension=2).dimension == 1
-    with pytest.raises(NotImplementedError):
-        SME(level=2)
+    assert SME(level=2, dimension=3).model_id == ZFV_MODEL_SME2D_L2
+    assert SME(level=2, dimension=2).model_id == ZFV_MODEL_SME1D_L2
+    assert SME(level=2).state_names() == ["b", "h", "hu", "hv", "halpha_1", "halpha_2", "hbeta_1", "hbeta_2"]
+    for level in (1, 3):
+        with pytest.raises(NotImplementedError):
+            SME(level=level)
 
 
 def test_default_fields_are_init_solution():
