@@ -75,6 +75,8 @@ def parse():
                     help="skip the adjoint timing / gradient checks (1024^2, 200 steps)")
     ap.add_argument("--err-steps", type=int, default=1000,
                     help="steps of the FP32-vs-FP64 depth-error study (0 = skip)")
+    ap.add_argument("--sme-steps", type=int, default=500,
+                    help="steps of the shallow-moment level-2 (2048^2) error study (0 = skip that section)")
     return ap.parse_args()
 
 
@@ -551,6 +553,96 @@ def adjoint_bench(local, n=1024, steps=200, every=20, n_dirs=32, eps=1e-6, seed=
                                "rel_err_n_m": ag_nm}}
 
 
+# Shallow-moment level 2 (config 3): algorithmic HBM bytes per cell-update.
+# FP64 plain: stage 1 reads the 8 state rows and writes the 7 evolved ones;
+# stage 2 reads 8 + Q^n's 7 and writes 7 -> (15 + 22) x 8 B.
+BYTES_PER_CELL_STEP_SME_FP64 = 296
+# FP32 chosen: stage 1 reads 8 rows, writes inc1 (7); stage 2 reads 8 rows,
+# inc1 (7) and lo (7), writes 7 rows and lo (7) -> (15 + 36) x 4 B
+# (148 B without the compensation planes + 56 B for them).
+BYTES_PER_CELL_STEP_SME_FP32 = 204
+
+
+def sme_bench(local, n=2048, steps=500, timed=100, warm=5):
+    """Config 3: the shallow-moment model at level 2 on n^2 over [0,50]^2 m
+    (16 seeded bumps, eta = 1 m + 0.3 m hump, at rest in the mean, moments
+    h U(-0.05, 0.05) m/s, Navier-slip friction nu = 1e-3, slip length 0.1,
+    point-implicit, well-balanced, walls, order 2). Times `timed` steps of the
+    FP64 plain and FP32 chosen forms (the FP32 tile shape picked by the
+    autotuner, cached per n_dof_q = 8), then runs `steps` steps of both from
+    the same start and reports the FP32 error against FP64 (the FP64 GPU
+    form equals the CPU oracle bit for bit, tests/test_gpu_sme.py)."""
+    import torch
+    from zoomy_amrex_b200._abi import ZFV_PREC_FP32, ZFV_PREC_FP64
+    from zoomy_amrex_b200.autotune import record
+    from zoomy_amrex_b200.level import Level
+    from zoomy_amrex_b200.workloads import sme_workload_config, sme_workload_fields
+    dev = f"cuda:{local}"
+    Q0, A0 = sme_workload_fields(n)
+    cells = n * n
+
+    def timed_run(prec, variant=None, k=timed):
+        cfg = sme_workload_config(n)
+        cfg.precision = prec
+        lev = Level(cfg, Q0, A0, device=dev, variant=variant)
+        lev.begin()
+        lev.evolve(warm)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(lev.stream):
+            e0.record(lev.stream)
+            lev.evolve(k)
+            e1.record(lev.stream)
+        torch.cuda.synchronize()
+        st = lev.status()
+        lev.close()
+        assert np.isfinite(st["dt"]) and not st["done"], st
+        return e0.elapsed_time(e1) / k
+
+    ms64 = timed_run(ZFV_PREC_FP64)
+    shape_ms = {v: timed_run(ZFV_PREC_FP32, variant=v, k=max(10, timed // 5)) for v in range(3)}
+    best = min(shape_ms, key=shape_ms.get)
+    shapes = [(32, 8), (16, 8), (32, 4)]
+    record(8, "fp32", float(cells), best, shape_ms, shapes)
+    ms32 = timed_run(ZFV_PREC_FP32, variant=best)
+    # error after `steps` steps from the same start
+    out = {}
+    for prec in (ZFV_PREC_FP64, ZFV_PREC_FP32):
+        cfg = sme_workload_config(n)
+        cfg.precision = prec
+        cfg.max_step = steps
+        lev = Level(cfg, Q0, A0, device=dev, variant=best if prec == ZFV_PREC_FP32 else None)
+        st = lev.run(chunk=100)
+        out[prec] = (lev.state64().clone(), st)
+        lev.close()
+    q64, st64 = out[ZFV_PREC_FP64]
+    q32, st32 = out[ZFV_PREC_FP32]
+    dh = (q32[1] - q64[1]).abs()
+    dm = (q32[4:] - q64[4:]).abs()
+    peak, peak_kind = measured_peak()
+    a32 = cells * BYTES_PER_CELL_STEP_SME_FP32 / (ms32 * 1e-3) / 1e9
+    a64 = cells * BYTES_PER_CELL_STEP_SME_FP64 / (ms64 * 1e-3) / 1e9
+    return {"workload": f"sme2d_level2_{n}x{n} over [0,50]^2: 16 seeded bumps, eta = 1 m + 0.3 m hump, "
+                        "moments h U(-0.05,0.05), Navier slip nu 1e-3 lambda 0.1 (point-implicit 8x8), "
+                        "WB, walls, order 2, cfl 0.45",
+            "n_dof_q": 8, "cells": cells, "steps_timed": timed,
+            "fp64_plain": {"value": cells / (ms64 * 1e-3), "ms_per_step": ms64,
+                           "hbm_gbs": a64, "frac": a64 / peak,
+                           "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_SME_FP64},
+            "fp32_chosen": {"value": cells / (ms32 * 1e-3), "ms_per_step": ms32,
+                            "hbm_gbs": a32, "frac": a32 / peak,
+                            "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_SME_FP32,
+                            "tile_shape": shapes[best],
+                            "tile_shape_ms_per_step": {f"{shapes[v][0]}x{shapes[v][1]}": t
+                                                       for v, t in shape_ms.items()}},
+            "fp32_over_fp64": ms64 / ms32, "peak_source": peak_kind,
+            "error_fp32_vs_fp64": {"steps": steps, "time_fp64": st64["time"], "time_fp32": st32["time"],
+                                   "l1_depth": float(dh.mean()), "linf_depth": float(dh.max()),
+                                   "l1_moments": float(dm.mean()), "linf_moments": float(dm.max()),
+                                   "mass_rel_diff": abs(st32["mass"] - st64["mass"]) / st64["mass"],
+                                   "reference": "FP64 plain form on the GPU (bitwise equal to the CPU oracle)"}}
+
+
 def depth_error(n, Q0, A0, steps, local):
     """FP32 chosen form vs FP64 plain form after `steps` steps from the same
     state. The FP64 GPU form equals the CPU oracle bitwise (tests/test_gpu_parity.py),
@@ -655,6 +747,9 @@ def main():
     err = None
     if args.err_steps > 0 and rank == 0:
         err = depth_error(n, Q0, A0, args.err_steps, local)
+    sme = None
+    if args.sme_steps > 0 and rank == 0:
+        sme = sme_bench(local, steps=args.sme_steps)
 
     # end to end through the public Level API with host buffers (FP32 form):
     # pinned H2D of the FP64 state, aux0 by init_solution on the device (as
@@ -718,7 +813,7 @@ def main():
                           "fp64_over_reference_note": "same-precision ratio: FP64 GPU form over the "
                                                       "reference's FP64 CPU path on all host threads"},
                 "depth_error_fp32_vs_fp64": err,
-                "autotune": tuning, "ensemble": ens, "adjoint": adj, "amr": amr,
+                "autotune": tuning, "ensemble": ens, "adjoint": adj, "amr": amr, "sme_level2": sme,
                 "hbm_gbs": achieved32,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 2 * K, "clocks": clk.summary()}

@@ -109,3 +109,85 @@ def test_sme_lake_at_rest_is_exact(cuda):
     assert st["step"] == 200
     assert np.abs(Q[2:]).max() < 1e-12
     assert np.abs((Q[0] + Q[1]) - (Q0[0] + Q0[1])).max() < 1e-12
+
+
+# --- the FP32 chosen form of the shallow-moment model (generic tile kernels) ---
+
+def run_fp32(cfg64, Q0, A0, variant=None, chunk=25):
+    from zoomy_amrex_b200._abi import ZFV_PREC_FP32
+    from zoomy_amrex_b200.level import Level
+    from zoomy_amrex_b200.workloads import fp64_twin
+    cfg = fp64_twin(cfg64)
+    cfg.precision = ZFV_PREC_FP32
+    lev = Level(cfg, Q0, A0, variant=variant)
+    try:
+        st = lev.run(chunk=chunk)
+        return lev.state64().cpu().numpy(), lev.aux.cpu().numpy(), st, lev.log()
+    finally:
+        lev.close()
+
+
+@pytest.mark.parametrize("name", ["sme2d_wetdry_wb_impl_o2", "sme2d_moving_mixed_bc_o2"])
+def test_sme_fp32_error_vs_fp64_oracle(cuda, oracle, name):
+    """L1 / Linf error of the FP32 chosen form against the FP64 oracle, depth
+    and moments (the FP32 form has no bitwise target)."""
+    cfg, Q0, A0 = setup(*CASES_SME[name])
+    Q32, A32, st, _ = run_fp32(cfg, Q0, A0)
+    Qo, Ao, n, t, _, _ = oracle.run(cfg, Q0, A0)
+    assert st["step"] == n
+    assert abs(st["time"] - t) <= 1e-6 * t
+    dh = np.abs(Q32[1] - Qo[1])
+    dm = np.abs(Q32[2:] - Qo[2:])
+    print(f"[sme fp32 vs fp64 oracle] {name}: depth L1 {dh.mean():.3e} Linf {dh.max():.3e}, "
+          f"momenta/moments Linf {dm.max():.3e}")
+    assert dh.mean() <= 1e-6 and dh.max() <= 1e-4
+    assert dm.max() <= 1e-4
+    # export refreshes aux with the model's FP64 hinv of the exported depth
+    h4 = Q32[1] ** 4
+    np.testing.assert_allclose(A32[0], np.sqrt(2.0) * Q32[1] / np.sqrt(h4 + np.maximum(h4, 1e-24)), rtol=1e-14)
+
+
+def test_sme_fp32_benchmark_strip_error(cuda, oracle):
+    """Rows 0..31 of the 2048^2 shallow-moment benchmark level, 100 steps."""
+    cfg, Q0, A0 = sme_strip_setup(steps=100)
+    Q32, _, st, _ = run_fp32(cfg, Q0, A0)
+    Qo, _, n, _, _, _ = oracle.run(cfg, Q0, A0)
+    assert st["step"] == n == 100
+    dh = np.abs(Q32[1] - Qo[1])
+    print(f"[sme fp32 vs fp64 oracle, benchmark strip] depth L1 {dh.mean():.3e} Linf {dh.max():.3e} "
+          f"moments Linf {np.abs(Q32[4:] - Qo[4:]).max():.3e}")
+    assert dh.mean() <= 1e-6 and dh.max() <= 1e-4
+
+
+def test_sme_fp32_lake_at_rest_is_exact(cuda):
+    """Fully wet still water over bumps, no moments, order 2, WB, implicit:
+    the FP32 form keeps every momentum and moment exactly zero."""
+    from zoomy_amrex_b200.models import SME
+    from cases import _bumps
+
+    def ic(x):
+        b = _bumps(x, 19)
+        h = b.max() + 0.5 - b
+        z = np.zeros_like(h)
+        return np.array([b, h, z, z, z, z, z, z])
+    model = SME(level=2, dimension=3, bc="wall", initial_conditions=ic)
+    s = dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[64, 48], spatial_order=2, cfl=0.45, time_end=1e30,
+             max_step=200, well_balanced=True, implicit_source=True)
+    cfg, Q0, A0 = setup(model, s)
+    Q, _, st, _ = run_fp32(cfg, Q0, A0)
+    assert st["step"] == 200
+    assert np.abs(Q[2:]).max() == 0.0
+    assert np.abs((Q[0] + Q[1]) - (Q0[0] + Q0[1])).max() < 1e-12
+
+
+def test_sme_fp32_tile_shapes_agree_and_mass_is_conserved(cuda):
+    """Every tile shape computes the same faces in the same order: identical
+    results. With walls the FP64 mass of the compensated state is conserved."""
+    cfg, Q0, A0 = setup(*CASES_SME["sme2d_wetdry_wb_impl_o2"])
+    outs = [run_fp32(cfg, Q0, A0, variant=v) for v in range(3)]
+    for o in outs[1:]:
+        assert np.array_equal(o[0], outs[0][0])
+    log = outs[0][3]
+    b32 = Q0[0].astype(np.float32).astype(np.float64)
+    m0 = ((Q0[1] + Q0[0]) - b32).sum() * (10.0 / 48) * (10.0 / 40)
+    assert np.abs(log[:, 2] - m0).max() / m0 < 1e-10

@@ -35,6 +35,7 @@ SOURCES = ([("zoomy_fv.cu", ["--fmad=false"], "zoomy_fv"),
             ("zoomy_fv64_swe.cu", ["--fmad=false"], "zoomy_fv64_swe"),
             ("zoomy_fv64_sme.cu", ["--fmad=false"], "zoomy_fv64_sme"),
             ("zoomy_fv32.cu", FP32_FLAGS, "zoomy_fv32"),
+            ("zoomy_fv32_tile.cu", FP32_FLAGS, "zoomy_fv32_tile"),
             ("zoomy_adj.cu", ["--fmad=true"], "zoomy_adj")]
            + [("zoomy_fv32_shape.cu", FP32_FLAGS + [f"-DZFV32_SHAPE={k}"], f"zoomy_fv32_shape{k}")
               for k in range(N_FP32_SHAPES)])

@@ -1,0 +1,594 @@
+// The FP32 chosen form for any compiled model family: fused tile kernels
+// generic in Model::n_dof_q (the shallow-moment model at level 2 runs here;
+// the 2-D shallow-water model has its own hand-tuned column sweep,
+// fv32_sweep*.cuh).
+//
+// Same scheme as the FP64 plain form (make_rhs.H + the ZoomyAmr driver),
+// evaluated with FP32 storage and arithmetic the way the shallow-water
+// chosen form does it:
+//  * the state is stored as float planes [b, eta = h + b, q_2 .. q_{n-1}]:
+//    the depth's slopes are taken as d(eta) - d(b), so a lake at rest
+//    reconstructs eta at every face bit for bit, and the well-balancing bed
+//    source uses the hydrostatic pressure P(h*) = (g/2) h*^2 evaluated as
+//    the model's flux evaluates it, so that at rest the flux difference and
+//    the bed source cancel exactly;
+//  * compensated update: stage 1 stores its increment inc1 = dt RHS(q) +
+//    (implicit source step); stage 2 forms t = lo + (inc1 + inc2)/2 and adds
+//    it to the stored value by an exact two-sum, keeping the FP32 remainder
+//    lo in scratch;
+//  * FP64 only in the point-implicit source solve of near-dry cells
+//    (h < 1e-3, with the model's FP64 instance), in the reductions (CFL max
+//    and mass) and in the run record (time, dt).
+// One CTA owns a TX x TY tile: it loads the tile and its two-cell halo into
+// shared memory (stage 2: X + inc1), rebuilds out-of-domain ghost cells from
+// mirrored interior cells and Model::boundary_conditions (ZoomyAmr.cpp:342-443),
+// evaluates every face once into shared memory, and assembles, updates and
+// writes each cell. The state ping-pongs between the caller's Q rows 1..n-1
+// and an `alt` buffer; which one holds it is the run record's parity,
+// flipped by the block that finishes a step, so one step is always the same
+// two launches (one captured CUDA graph replays any number of steps).
+#pragma once
+#include <cuda_runtime.h>
+#include "fv_kernels.cuh"
+
+namespace zfv32t {
+
+// A model family in both precisions.
+template <class M64_, class N64_, class M32_, class N32_>
+struct Fam {
+    using M64 = M64_;
+    using N64 = N64_;
+    using M32 = M32_;
+    using N32 = N32_;
+    static constexpr int nq = M32::n_dof_q;
+    static constexpr int ne = nq - 1;            // evolved rows (the bed is static)
+    static constexpr int dim = M32::dimension;
+    static constexpr int np = M32::n_parameters;
+    static_assert(M64::n_dof_q == M32::n_dof_q, "one family, two precisions");
+    static_assert(M32::dimension == 2, "the generic FP32 tile kernels are 2-D");
+    static_assert(zfv::static_bed<M32>::value && zfv::aux_pure<M32>::value,
+                  "the FP32 form needs a static bed and a pure aux");
+    static_assert(!M32::has_diffusion, "diffusive models (Model::has_diffusion) are not built here");
+};
+
+// Level constants (FP64 for reductions and the run record, FP32 copies for
+// the stage arithmetic).
+template <int NP>
+struct TileParams {
+    int nx, ny;
+    long long plane;
+    double dx, dy, plox, ploy;
+    float fdx, fdy, rdx, rdy;
+    double p[NP];
+    float pf[NP];
+    int bc_tag[4];
+    double cfl, dtmin, dtmax, time_end;
+    int max_step, cfl_dimension, cfl_degree_factor;
+};
+
+struct TileBufs {
+    const float* bed;       // Q row 0
+    float* Qs;              // Q rows 1..n-1: state buffer 0
+    float* alt;             // state buffer 1 (n-1 planes)
+    float* inc;             // stage-1 increment (n-1 planes)
+    float* lo;              // compensation remainders (n-1 planes)
+    zfv::DevState* st;
+    double* partials;
+    double* log3;
+    int log_cap;
+};
+
+enum TMode : int { T_S1 = 1, T_S2 = 2 };
+constexpr float kNearDry = 1.0e-3f;
+
+template <class F, int TX, int TY>
+struct TShape {
+    static constexpr int G = 2, RW = TX + 2 * G, RH = TY + 2 * G;
+    static constexpr int NFC = 3 * F::ne + 2;     // flux, D+, D- of the evolved rows, h*_L, h*_R
+    static constexpr int NT = TX * TY;
+    static constexpr size_t q_elems = size_t(F::nq) * RH * RW;
+    static constexpr size_t fx_elems = size_t(TY) * (TX + 1) * NFC;
+    static constexpr size_t fy_elems = size_t(TY + 1) * TX * NFC;
+    static constexpr size_t smem_bytes = (q_elems + fx_elems + fy_elems) * sizeof(float);
+};
+
+__device__ __forceinline__ float mmf(float a, float b) {
+    if (a * b <= 0.0f) return 0.0f;
+    return (fabsf(a) < fabsf(b)) ? a : b;
+}
+
+// Knuth's two-sum: s + e == a + b exactly (no contraction: _rn intrinsics).
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = __fadd_rn(a, b);
+    const float bp = __fsub_rn(s, a);
+    const float ap = __fsub_rn(s, bp);
+    e = __fadd_rn(__fsub_rn(a, ap), __fsub_rn(b, bp));
+}
+
+// make_rhs.H:429-509 for one cell, returning the increment dq instead of
+// updating q: (I - dt J(q0)) dq = dt S(q0) with J = dS/dQ + dS/dA dA/dQ,
+// Gaussian elimination with partial pivoting, explicit fallback.
+template <class M, class R>
+__device__ __forceinline__ void implicit_increment(typename M::VQ const& q0, typename M::VA const& a, R dt,
+                                                   typename M::VP const& p, typename M::VX const& X,
+                                                   typename M::VQ& dq) {
+    constexpr int nq = M::n_dof_q, na = M::n_dof_qaux;
+    const auto S = M::source(q0, a, p, R(0), X);
+    const auto JQ = M::source_jacobian_wrt_variables(q0, a, p);
+    const auto JA = M::source_jacobian_wrt_aux_variables(q0, a, p);
+    const auto AQ = M::update_aux_variables_jacobian_wrt_variables(q0, a, p, R(0), X);
+    R A[nq][nq], b[nq];
+#pragma unroll
+    for (int r = 0; r < nq; ++r) {
+        b[r] = dt * S(r, 0);
+#pragma unroll
+        for (int c = 0; c < nq; ++c) {
+            R t = JQ(r * nq + c, 0);
+#pragma unroll
+            for (int k = 0; k < na; ++k) t += JA(r * na + k, 0) * AQ(k * nq + c, 0);
+            A[r][c] = (r == c ? R(1) : R(0)) - dt * t;
+        }
+    }
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < nq; ++k) {
+        if (!ok) break;
+        int piv = k;
+        R best = fabs(A[k][k]);
+#pragma unroll
+        for (int r = k + 1; r < nq; ++r)
+            if (fabs(A[r][k]) > best) { best = fabs(A[r][k]); piv = r; }
+        if (!(best > R(0)) || !isfinite(best)) { ok = false; break; }
+        if (piv != k) {
+#pragma unroll
+            for (int r = k + 1; r < nq; ++r) {
+                if (r == piv) {
+#pragma unroll
+                    for (int c = k; c < nq; ++c) { R t = A[k][c]; A[k][c] = A[r][c]; A[r][c] = t; }
+                    R t = b[k]; b[k] = b[r]; b[r] = t;
+                }
+            }
+        }
+#pragma unroll
+        for (int r = k + 1; r < nq; ++r) {
+            const R f = A[r][k] / A[k][k];
+#pragma unroll
+            for (int c = k; c < nq; ++c) A[r][c] -= f * A[k][c];
+            b[r] -= f * b[k];
+        }
+    }
+    if (ok) {
+        R x[nq];
+#pragma unroll
+        for (int r = nq - 1; r >= 0; --r) {
+            R s = R(0);
+#pragma unroll
+            for (int c = r + 1; c < nq; ++c) s += A[r][c] * x[c];
+            x[r] = (b[r] - s) / A[r][r];
+            if (!isfinite(x[r])) { ok = false; break; }
+        }
+        if (ok) {
+#pragma unroll
+            for (int n = 0; n < nq; ++n) dq(n, 0) = x[n];
+            return;
+        }
+    }
+#pragma unroll
+    for (int n = 0; n < nq; ++n) dq(n, 0) = isfinite(b[n]) ? b[n] : R(0);
+}
+
+// One RK stage of the generic FP32 form over a TX x TY tile.
+template <class F, int MODE, bool WB, bool IMPL, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY)
+k32t_stage(TileParams<F::np> L, TileBufs B, int order2)
+{
+    using Sh = TShape<F, TX, TY>;
+    using M = typename F::M32;
+    using N = typename F::N32;
+    using VQ = typename M::VQ;
+    using VA = typename M::VA;
+    using VP = typename M::VP;
+    using VN = typename M::VN;
+    using VX = typename M::VX;
+    constexpr int nq = F::nq, ne = F::ne;
+    constexpr int G = Sh::G, RW = Sh::RW, RH = Sh::RH, NFC = Sh::NFC, NT = Sh::NT;
+
+    extern __shared__ __align__(16) float tsm[];
+    float* sQ = tsm;                                  // [nq][RH][RW]: b, eta, q_2..
+    float* sFx = sQ + Sh::q_elems;                    // [TY][TX+1][NFC]
+    float* sFy = sFx + Sh::fx_elems;                  // [TY+1][TX][NFC]
+    __shared__ double red[2 * ((NT + 31) / 32)];
+
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int nx = L.nx, ny = L.ny;
+    const long long plane = L.plane;
+    zfv::DevState* st = B.st;
+    if (*(volatile unsigned*)&st->flags & zfv::kFlagDone) return;   // stopped: the state stays put
+    const unsigned parity = *(volatile unsigned*)&st->parity;
+    const float* X = parity ? B.alt : B.Qs;
+    float* Y = parity ? B.Qs : B.alt;
+    const double dtd = *(volatile double*)&st->dt;
+    const double time = *(volatile double*)&st->time;
+    const float dt = float(dtd);
+
+    VP p;
+#pragma unroll
+    for (int k = 0; k < F::np; ++k) p(k, 0) = L.pf[k];
+    const float g = L.pf[0];
+    VA azero{};
+
+    // 1. tile + halo: b, eta, rest (stage 2: the stage state X + inc1)
+    for (int k = tid; k < RW * RH; k += NT) {
+        const int lx = k % RW, ly = k / RW;
+        const int gi = x0 - G + lx, gj = y0 - G + ly;
+        if (gi >= 0 && gi < nx && gj >= 0 && gj < ny) {
+            const long long c = (long long)gj * nx + gi;
+            sQ[ly * RW + lx] = B.bed[c];
+#pragma unroll
+            for (int n = 1; n < nq; ++n) {
+                float v = X[(n - 1) * plane + c];
+                if constexpr (MODE == T_S2) v = v + B.inc[(n - 1) * plane + c];
+                sQ[(n * RH + ly) * RW + lx] = v;
+            }
+        }
+    }
+    __syncthreads();
+
+    // 2. ghost cells: mirrored interior cells through Model::boundary_conditions
+    const bool edge_tile = (x0 - G < 0) || (x0 + TX + G > nx) || (y0 - G < 0) || (y0 + TY + G > ny);
+    if (edge_tile) {
+        for (int k = tid; k < RW * RH; k += NT) {
+            const int lx = k % RW, ly = k / RW;
+            const int gi = x0 - G + lx, gj = y0 - G + ly;
+            if (gi >= 0 && gi < nx && gj >= 0 && gj < ny) continue;
+            if (gi < -G || gi > nx - 1 + G || gj < -G || gj > ny - 1 + G) continue;
+            const zfv::GhostMap<2> gm = zfv::ghost_map<2>(gi, gj, nx, ny);
+            if (gm.bc_side < 0) continue;
+            const int mx = gm.ii - x0 + G, my = gm.jj - y0 + G;
+            if (mx < 0 || mx >= RW || my < 0 || my >= RH) continue;   // excluded by zfv_create
+            VQ qi;
+#pragma unroll
+            for (int n = 0; n < nq; ++n) qi(n, 0) = sQ[(n * RH + my) * RW + mx];
+            const float eta_i = qi(1, 0);
+            qi(1, 0) = eta_i - qi(0, 0);
+            VX Xi{}, Xg{};
+            Xi(0, 0) = float(L.plox + (gm.ii + 0.5) * L.dx);
+            Xi(1, 0) = float(L.ploy + (gm.jj + 0.5) * L.dy);
+            Xg(0, 0) = float(L.plox + (gi + 0.5) * L.dx);
+            Xg(1, 0) = float(L.ploy + (gj + 0.5) * L.dy);
+            const VA ai = M::update_aux_variables(qi, azero, p, float(time), Xi);
+            VN nh{};
+            nh(gm.normal_dir, 0) = float(gm.normal_sign);
+            const VQ qg = M::boundary_conditions(L.bc_tag[gm.bc_side], qi, ai, nh, Xg, float(time), L.fdx);
+            // keep the mirrored eta bit for bit when the BC keeps depth and bed
+            const float eta_g = (qg(1, 0) == qi(1, 0) && qg(0, 0) == qi(0, 0)) ? eta_i : qg(1, 0) + qg(0, 0);
+            sQ[ly * RW + lx] = qg(0, 0);
+            sQ[(RH + ly) * RW + lx] = eta_g;
+#pragma unroll
+            for (int n = 2; n < nq; ++n) sQ[(n * RH + ly) * RW + lx] = qg(n, 0);
+        }
+        __syncthreads();
+    }
+
+    auto at = [&](int n, int lx, int ly) { return sQ[(n * RH + ly) * RW + lx]; };
+
+    // reconstruction of cell (lx, ly) at its face on side s (+1 high, -1 low)
+    // along direction D: b and eta with eta's slope = slope(h) + slope(b),
+    // slope(h) from the differences d(eta) - d(b); the other rows by minmod
+    auto recon = [&](int D, int lx, int ly, float sgn, VQ& q, float& eta) {
+        const int ax = (D == 0) ? 1 : 0, ay = 1 - ax;
+        const float b0 = at(0, lx, ly), e0 = at(1, lx, ly);
+        if (order2) {
+            const float bm = at(0, lx - ax, ly - ay), bp = at(0, lx + ax, ly + ay);
+            const float em = at(1, lx - ax, ly - ay), ep = at(1, lx + ax, ly + ay);
+            const float dbl = b0 - bm, dbr = bp - b0;
+            const float sb = mmf(dbl, dbr);
+            const float sh = mmf((e0 - em) - dbl, (ep - e0) - dbr);
+            q(0, 0) = b0 + 0.5f * sgn * sb;
+            eta = e0 + 0.5f * sgn * (sh + sb);
+#pragma unroll
+            for (int n = 2; n < nq; ++n) {
+                const float v0 = at(n, lx, ly);
+                const float s = mmf(v0 - at(n, lx - ax, ly - ay), at(n, lx + ax, ly + ay) - v0);
+                q(n, 0) = v0 + 0.5f * sgn * s;
+            }
+        } else {
+            q(0, 0) = b0;
+            eta = e0;
+#pragma unroll
+            for (int n = 2; n < nq; ++n) q(n, 0) = at(n, lx, ly);
+        }
+        q(1, 0) = eta - q(0, 0);
+    };
+
+    // face between cells (lx-ax, ly-ay) and (lx, ly) along D -> record F
+    auto face = [&](int D, int lx, int ly, float* Fr) {
+        const int ax = (D == 0) ? 1 : 0, ay = 1 - ax;
+        VQ qL, qR;
+        float eL, eR;
+        recon(D, lx - ax, ly - ay, 1.0f, qL, eL);
+        recon(D, lx, ly, -1.0f, qR, eR);
+        float hLs = qL(1, 0), hRs = qR(1, 0);
+        if constexpr (WB) {   // Audusse (make_rhs.H:84-98) with h* = max(0, eta - b_face)
+            const float bf = fmaxf(qL(0, 0), qR(0, 0));
+            hLs = fmaxf(0.0f, eL - bf);
+            hRs = fmaxf(0.0f, eR - bf);
+            const float sL = (qL(1, 0) > 0.0f) ? hLs / qL(1, 0) : 0.0f;
+            const float sR = (qR(1, 0) > 0.0f) ? hRs / qR(1, 0) : 0.0f;
+#pragma unroll
+            for (int d = 0; d < 2; ++d) {
+                qL(2 + d, 0) *= sL;
+                qR(2 + d, 0) *= sR;
+            }
+            qL(1, 0) = hLs; qR(1, 0) = hRs;
+            qL(0, 0) = bf; qR(0, 0) = bf;
+        }
+        VX Xz{};
+        const VA aL = M::update_aux_variables(qL, azero, p, float(time), Xz);
+        const VA aR = M::update_aux_variables(qR, azero, p, float(time), Xz);
+        VN nh{};
+        nh(D, 0) = 1.0f;
+        const VQ fl = N::numerical_flux(qL, qR, aL, aR, p, nh);
+        const auto fc = N::numerical_fluctuations(qL, qR, aL, aR, p, nh);
+#pragma unroll
+        for (int n = 1; n < nq; ++n) {
+            Fr[n - 1] = fl(n, 0);
+            Fr[ne + n - 1] = fc(n, 0);
+            Fr[2 * ne + n - 1] = fc(nq + n, 0);
+        }
+        Fr[3 * ne] = hLs;
+        Fr[3 * ne + 1] = hRs;
+    };
+
+    const int tx = tid % TX, ty = tid / TX;
+    const int i = x0 + tx, j = y0 + ty;
+    const int iend = min(x0 + TX, nx), jend = min(y0 + TY, ny);
+
+    // 3. faces, each once
+    if (j < jend) {
+        if (i <= iend) face(0, tx + G, ty + G, sFx + (ty * (TX + 1) + tx) * NFC);
+        if (tx == TX - 1 && x0 + TX <= iend) face(0, TX + G, ty + G, sFx + (ty * (TX + 1) + TX) * NFC);
+    }
+    if (i < iend) {
+        if (j <= jend) face(1, tx + G, ty + G, sFy + (ty * TX + tx) * NFC);
+        if (ty == TY - 1 && y0 + TY <= jend) face(1, tx + G, TY + G, sFy + (TY * TX + tx) * NFC);
+    }
+    __syncthreads();
+
+    // 4. assemble, update, implicit source, write
+    double m_loc = 0.0, s_loc = 0.0;
+    if (i < nx && j < ny) {
+        const long long c = (long long)j * nx + i;
+        const float* FxL = sFx + (ty * (TX + 1) + tx) * NFC;
+        const float* FxR = FxL + NFC;
+        const float* FyL = sFy + (ty * TX + tx) * NFC;
+        const float* FyR = FyL + TX * NFC;
+        float d[ne];
+#pragma unroll
+        for (int k = 0; k < ne; ++k) {
+            float fx = -(FxR[k] - FxL[k]) - FxR[2 * ne + k] - FxL[ne + k];
+            float fy = -(FyR[k] - FyL[k]) - FyR[2 * ne + k] - FyL[ne + k];
+            if constexpr (WB) {
+                // the bed source (make_rhs.H:154-163) as a difference of the
+                // same FP32 pressures the flux carries: zero at rest, exactly
+                if (k == 1) {
+                    const float pr = 0.5f * g * FxR[3 * ne] * FxR[3 * ne];
+                    const float pl = 0.5f * g * FxL[3 * ne + 1] * FxL[3 * ne + 1];
+                    fx = fx + (pr - pl);
+                } else if (k == 2) {
+                    const float pr = 0.5f * g * FyR[3 * ne] * FyR[3 * ne];
+                    const float pl = 0.5f * g * FyL[3 * ne + 1] * FyL[3 * ne + 1];
+                    fy = fy + (pr - pl);
+                }
+            }
+            d[k] = dt * (fx * L.rdx + fy * L.rdy);
+        }
+        const int lx = tx + G, ly = ty + G;
+        const float bc = at(0, lx, ly);
+        if constexpr (IMPL) {
+            // state after the explicit update, with the depth h = eta - b
+            VQ q0;
+            q0(0, 0) = bc;
+            q0(1, 0) = (at(1, lx, ly) + d[0]) - bc;
+#pragma unroll
+            for (int n = 2; n < nq; ++n) q0(n, 0) = at(n, lx, ly) + d[n - 1];
+            if (q0(1, 0) < kNearDry) {   // FP64 solve of the near-dry cell
+                using M64 = typename F::M64;
+                typename M64::VQ q64, dq64;
+                typename M64::VP p64;
+                typename M64::VA a64{};
+                typename M64::VX X64{};
+#pragma unroll
+                for (int k = 0; k < F::np; ++k) p64(k, 0) = L.p[k];
+                q64(0, 0) = double(bc);
+                q64(1, 0) = (double(at(1, lx, ly)) + double(d[0])) - double(bc);
+#pragma unroll
+                for (int n = 2; n < nq; ++n) q64(n, 0) = double(at(n, lx, ly)) + double(d[n - 1]);
+                a64 = M64::update_aux_variables(q64, a64, p64, time, X64);
+                implicit_increment<M64, double>(q64, a64, dtd, p64, X64, dq64);
+#pragma unroll
+                for (int n = 1; n < nq; ++n) d[n - 1] = float(double(d[n - 1]) + dq64(n, 0));
+            } else {
+                VQ dq;
+                VX Xz{};
+                const VA a0 = M::update_aux_variables(q0, azero, p, float(time), Xz);
+                implicit_increment<M, float>(q0, a0, dt, p, Xz, dq);
+#pragma unroll
+                for (int n = 1; n < nq; ++n) d[n - 1] = d[n - 1] + dq(n, 0);
+            }
+        }
+        if constexpr (MODE == T_S1) {
+#pragma unroll
+            for (int k = 0; k < ne; ++k) B.inc[k * plane + c] = d[k];
+        } else {
+            // Heun on the compensated state: Q^{n+1} = X + lo + (inc1 + inc2)/2
+            VQ qn;
+            qn(0, 0) = bc;
+#pragma unroll
+            for (int k = 0; k < ne; ++k) {
+                const float hi = X[k * plane + c];
+                const float t = B.lo[k * plane + c] + 0.5f * (B.inc[k * plane + c] + d[k]);
+                float s, e;
+                two_sum(hi, t, s, e);
+                Y[k * plane + c] = s;
+                B.lo[k * plane + c] = e;
+                qn(k + 1, 0) = s;
+            }
+            // this cell's CFL quantity (ZoomyAmr.cpp:472-487) and mass
+            const float etan = qn(1, 0);
+            qn(1, 0) = etan - bc;
+            VX Xz{};
+            const VA an = M::update_aux_variables(qn, azero, p, float(time), Xz);
+            float mm = 0.0f;
+#pragma unroll
+            for (int dd = 0; dd < 2; ++dd) {
+                VN nh{};
+                nh(dd, 0) = 1.0f;
+                const float inv = N::local_max_abs_eigenvalue(qn, an, p, nh)(0, 0) * (dd == 0 ? L.rdx : L.rdy);
+                if (inv > mm) mm = inv;
+            }
+            m_loc = double(mm);
+            s_loc = (double(etan) + double(B.lo[c])) - double(bc);
+        }
+    }
+    if constexpr (MODE == T_S2) {
+        const bool last = zfv::finish_step_units<NT>(m_loc, s_loc, red, B.partials, B.log3, B.log_cap, st, L,
+                                                      dtd, time, false, gridDim.x * gridDim.y,
+                                                      blockIdx.y * gridDim.x + blockIdx.x);
+        if (last && threadIdx.x == 0) {   // every block of the step has read parity by now
+            st->parity = parity ^ 1u;
+            __threadfence();
+        }
+    }
+}
+
+// FP64 reference layout [b, h, q_2..] -> FP32 [b, eta, q_2..] + remainders.
+// eta = h + b is formed in FP64 and split, so a lake at rest imports as a
+// constant eta. The state is left in Q (parity 0).
+template <class F>
+__global__ void k32t_import(const double* __restrict__ q64, float* __restrict__ Q, float* __restrict__ lo,
+                            long long plane) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < plane;
+         c += (long long)gridDim.x * blockDim.x) {
+        const double b = q64[c];
+        Q[c] = float(b);
+#pragma unroll
+        for (int n = 1; n < F::nq; ++n) {
+            const double v = (n == 1) ? q64[plane + c] + b : q64[n * plane + c];
+            const float hi = float(v);
+            Q[n * plane + c] = hi;
+            lo[(n - 1) * plane + c] = float(v - double(hi));
+        }
+    }
+}
+
+// FP32 state (wherever the parity says it is) -> FP64 reference layout, and
+// the aux refreshed from it with the model's FP64 update_aux_variables.
+template <class F>
+__global__ void k32t_export(const float* __restrict__ bed, const float* __restrict__ Qs, const float* __restrict__ alt,
+                            const float* __restrict__ lo, const zfv::DevState* st, double* __restrict__ q64,
+                            double* __restrict__ aux, typename F::M64::VP p, long long plane) {
+    using M64 = typename F::M64;
+    const float* X = (*(volatile const unsigned*)&st->parity) ? alt : Qs;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < plane;
+         c += (long long)gridDim.x * blockDim.x) {
+        typename M64::VQ q;
+        const double b = double(bed[c]);
+        q(0, 0) = b;
+#pragma unroll
+        for (int n = 1; n < F::nq; ++n) {
+            const double v = double(X[(n - 1) * plane + c]) + double(lo[(n - 1) * plane + c]);
+            q(n, 0) = (n == 1) ? v - b : v;
+        }
+#pragma unroll
+        for (int n = 0; n < F::nq; ++n) q64[n * plane + c] = q(n, 0);
+        if (aux) {
+            typename M64::VA a;
+#pragma unroll
+            for (int k = 0; k < M64::n_dof_qaux; ++k) a(k, 0) = aux[k * plane + c];
+            typename M64::VX X0{};
+            a = M64::update_aux_variables(q, a, p, 0.0, X0);
+#pragma unroll
+            for (int k = 0; k < M64::n_dof_qaux; ++k) aux[k * plane + c] = a(k, 0);
+        }
+    }
+}
+
+// First ComputeDt (WHAT 0: from the stored FP64 aux, as the reference's first
+// ComputeDt reads the aux InitData wrote) or the FP64 mass (WHAT 1), over the
+// compensated state; last-block-done reduction into the run record.
+template <class F, int NT, int WHAT>
+__global__ void __launch_bounds__(NT)
+k32t_reduce(TileParams<F::np> L, TileBufs B, const double* __restrict__ aux) {
+    using M64 = typename F::M64;
+    using N64 = typename F::N64;
+    __shared__ double red[2 * ((NT + 31) / 32)];
+    __shared__ unsigned s_last;
+    zfv::DevState* st = B.st;
+    const float* X = (*(volatile unsigned*)&st->parity) ? B.alt : B.Qs;
+    const long long plane = L.plane;
+    typename M64::VP p;
+#pragma unroll
+    for (int k = 0; k < F::np; ++k) p(k, 0) = L.p[k];
+    double m = 0.0, s = 0.0;
+    for (long long c = (long long)blockIdx.x * NT + threadIdx.x; c < plane; c += (long long)gridDim.x * NT) {
+        const double b = double(B.bed[c]);
+        typename M64::VQ q;
+        q(0, 0) = b;
+#pragma unroll
+        for (int n = 1; n < F::nq; ++n) {
+            const double v = double(X[(n - 1) * plane + c]) + double(B.lo[(n - 1) * plane + c]);
+            q(n, 0) = (n == 1) ? v - b : v;
+        }
+        if constexpr (WHAT == 0) {
+            typename M64::VA a;
+#pragma unroll
+            for (int k = 0; k < M64::n_dof_qaux; ++k) a(k, 0) = aux[k * plane + c];
+            const double inv = zfv::cell_max_inv<M64, N64, double>(q, a, p, L);
+            if (inv > m) m = inv;
+        } else {
+            s = s + q(1, 0);
+        }
+    }
+    zfv::block_reduce_max_sum<NT>(m, s, red);
+    const unsigned nblk = gridDim.x, blk = blockIdx.x;
+    if (threadIdx.x == 0) {
+        B.partials[2 * blk] = m;
+        B.partials[2 * blk + 1] = s;
+        __threadfence();
+        s_last = (atomicAdd(&st->counter, 1u) == nblk - 1) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double gm = 0.0, gs = 0.0;
+    for (unsigned b = threadIdx.x; b < nblk; b += NT) {
+        const double pm = __ldcg(&B.partials[2 * b]), ps = __ldcg(&B.partials[2 * b + 1]);
+        if (pm > gm) gm = pm;
+        gs = gs + ps;
+    }
+    zfv::block_reduce_max_sum<NT>(gm, gs, red);
+    if (threadIdx.x == 0) {
+        if constexpr (WHAT == 0) {
+            const double dt = zfv::dt_from_max(gm, st->time, L);
+            st->max_inv = gm;
+            st->dt = dt;
+            if (!isfinite(dt)) st->flags |= zfv::kFlagNonfiniteDt;
+        } else {
+            st->mass = gs * (L.dx * L.dy);
+        }
+        st->counter = 0u;
+        __threadfence();
+    }
+}
+
+// Start of a run: time 0, step 0, state in Q, stop flag.
+template <int NP>
+__global__ void k32t_init(zfv::DevState* st, TileParams<NP> L) {
+    st->time = 0.0; st->dt = 0.0; st->mass = 0.0; st->max_inv = 0.0;
+    st->step = 0; st->flags = zfv::run_done(0.0, 0, L) ? zfv::kFlagDone : 0u; st->mood_redos = 0;
+    st->counter = 0u; st->troubled = 0u; st->parity = 0u;
+}
+
+}  // namespace zfv32t

@@ -98,6 +98,7 @@ Runner* make_runner_fp32_swe2d(zfv_handle* h);
 // FP32 chosen-form runner of the generic tile kernels (zoomy_fv32_tile.cu):
 // any compiled model family; ZFV_MODEL_SME2D_L2.
 Runner* make_runner_fp32_generic(zfv_handle* h);
+int fp32_tile_variants();
 // FP64 plain-form runners (zoomy_fv64_swe.cu, zoomy_fv64_sme.cu).
 Runner* make_runner_fp64_swe1d(zfv_handle* h);
 Runner* make_runner_fp64_swe2d(zfv_handle* h);

@@ -131,8 +131,8 @@ int zfv_create(const zfv_config* cfg, zfv_handle** out) {
     if (cfg->precision != ZFV_PREC_FP64 && cfg->precision != ZFV_PREC_FP32)
         return fail(-1, "zfv_create: unsupported precision %d", cfg->precision);
     if (cfg->precision == ZFV_PREC_FP32) {
-        if (cfg->model != ZFV_MODEL_SWE2D)
-            return fail(-1, "zfv_create: the FP32 form is built for ZFV_MODEL_SWE2D only");
+        if (cfg->model != ZFV_MODEL_SWE2D && cfg->model != ZFV_MODEL_SME2D_L2)
+            return fail(-1, "zfv_create: the FP32 form is built for ZFV_MODEL_SWE2D and ZFV_MODEL_SME2D_L2");
         if (cfg->clamp_positivity)
             return fail(-1, "zfv_create: the FP32 form does not implement clamp_positivity");
     }
@@ -171,7 +171,8 @@ int zfv_create(const zfv_config* cfg, zfv_handle** out) {
     if (!h) return fail(-4, "zfv_create: out of host memory");
     h->cfg = *cfg;
     if (cfg->precision == ZFV_PREC_FP32) {
-        h->run.reset(make_runner_fp32_swe2d(h));
+        if (cfg->model == ZFV_MODEL_SWE2D) h->run.reset(make_runner_fp32_swe2d(h));
+        else h->run.reset(make_runner_fp32_generic(h));
     } else {
         switch (cfg->model) {
         case ZFV_MODEL_SWE1D: h->run.reset(make_runner_fp64_swe1d(h)); break;
