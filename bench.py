@@ -521,9 +521,29 @@ def adjoint_bench(local, n=1024, steps=200, every=20, n_dirs=32, eps=1e-6, seed=
     # the scheme is piecewise smooth (minmod switches, wet/dry): the gap to the
     # derivative comes from switches crossed inside +-eps and shrinks with eps
     sweep = {f"{e:.0e}": float(np.median(fd_errors(8, e))) for e in (1e-8, 1e-10)}
-    # torch autograd of the tensor restatement (small case)
+    # Taylor test on the same seeded directions: the remainder
+    # |L(x + e d) - L(x) - e g.d| of a continuous piecewise-smooth map falls as
+    # e^2 (a kink inside +-e adds at most e times its slope jump and is
+    # crossed with probability ~e); its slope over e = 1e-2 .. 1e-5
+    L0 = float(loss_of(forward_only(base, A, cfg, steps)))
+    epss = [1e-2, 1e-3, 1e-4, 1e-5, 1e-6, 1e-7]
+    trng = np.random.default_rng(seed + 1)
+    rem = np.zeros((n_dirs, len(epss)))
+    for k in range(n_dirs):
+        V = torch.from_numpy(trng.standard_normal(Q0.shape) * 1e-2).to(dev)
+        V[1:] *= wet
+        v_nm = float(trng.standard_normal() * 1e-3)
+        gd = float((gq * V).sum()) + gnm * v_nm
+        for e, ee in enumerate(epss):
+            Le = float(loss_of(forward_only(base + ee * V, A, cfg, steps, n_m=0.03 + ee * v_nm)))
+            rem[k, e] = abs(Le - L0 - ee * gd)
+    med = np.median(rem, axis=0)
+    taylor_slope = float(np.polyfit(np.log10(epss[:4]), np.log10(med[:4]), 1)[0])
+    # torch autograd of the tensor restatement (whose forward is the CUDA
+    # forward bit for bit, so both differentiate the same branches) at 256^2,
+    # 200 steps, checkpointed
     from oracle import torch_swe as T
-    m = 128
+    m, ms = 256, 200
     Qs, As = workload_fields(m)
     cfg_s = workload_config(m)
     cfg_s.time_end = 1e30
@@ -531,12 +551,13 @@ def adjoint_bench(local, n=1024, steps=200, every=20, n_dirs=32, eps=1e-6, seed=
     obs = (torch.from_numpy(Qs[0] + Qs[1]) + 0.01).to(dev)
     qa = torch.from_numpy(Qs).to(dev).requires_grad_(True)
     nma = torch.tensor(0.03, dtype=torch.float64, device=dev, requires_grad=True)
-    QTa = evolve_differentiable(qa, nma, As_t, cfg_s, 40, checkpoint_every=every)
+    QTa = evolve_differentiable(qa, nma, As_t, cfg_s, ms, checkpoint_every=every)
     (0.5 * ((QTa[0] + QTa[1] - obs) ** 2).sum()).backward()
     qt = torch.from_numpy(Qs).to(dev).requires_grad_(True)
     nmt = torch.tensor(0.03, dtype=torch.float64, device=dev, requires_grad=True)
     p = dict(g=9.81, ex=0.0, ey=0.0, h_floor=1e-6, eps=1e-24)
-    QTt, _ = T.run(qt, As_t[6], nmt, 40, p, DOMAIN / m, DOMAIN / m, (1, 1, 1, 1))
+    QTt, _ = T.run(qt, As_t[6], nmt, ms, p, DOMAIN / m, DOMAIN / m, (1, 1, 1, 1), checkpoint=True)
+    fwd_bitwise = bool(torch.equal(QTt.detach(), QTa.detach()))
     (0.5 * ((QTt[0] + QTt[1] - obs) ** 2).sum()).backward()
     ag_err = float((qa.grad - qt.grad).abs().max() / qt.grad.abs().max())
     ag_nm = abs(float(nma.grad) - float(nmt.grad)) / abs(float(nmt.grad))
@@ -549,7 +570,12 @@ def adjoint_bench(local, n=1024, steps=200, every=20, n_dirs=32, eps=1e-6, seed=
                    "median_rel_err": float(np.median(errs)),
                    "median_rel_err_smaller_eps": sweep,
                    "note": "directions over (b, h, hu, hv, n_m); h, hu, hv perturbed on wet cells"},
-            "torch_autograd": {"case": f"{m}x{m}, 40 steps", "max_rel_err_state": ag_err,
+            "taylor": {"directions": n_dirs, "eps": epss, "median_remainder": [float(v) for v in med],
+                       "slope_1e-2_to_1e-5": taylor_slope,
+                       "note": "|L(x+e d) - L(x) - e g.d| on seeded directions; slope 2 = the gradient is the "
+                               "derivative of the piecewise-smooth map"},
+            "torch_autograd": {"case": f"{m}x{m}, {ms} steps, checkpoints every {every}",
+                               "forward_bitwise": fwd_bitwise, "max_rel_err_state": ag_err,
                                "rel_err_n_m": ag_nm}}
 
 

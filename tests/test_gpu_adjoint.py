@@ -162,3 +162,77 @@ def test_adjoint_tile_shapes_agree(cuda):
     for v, (g, n) in enumerate(grads):
         assert float((g - g0).abs().max()) <= 1e-12 * scale, v
         assert abs(n - n0) <= 1e-12 * abs(n0), v
+
+
+def _bench_case(m):
+    from zoomy_amrex_b200.workloads import bump_workload_config, bump_workload_fields
+    Q0, A0 = bump_workload_fields(m)
+    cfg = bump_workload_config(m)
+    cfg.time_end = 1e30
+    return cfg, Q0, A0
+
+
+def test_adjoint_equals_torch_autograd_at_benchmark_scale(cuda):
+    """The benchmark's wet/dry bump level at 256^2 (Manning implicit, WB,
+    walls), 200 steps, checkpoints every 20: the tensor restatement's forward
+    is the CUDA forward bit for bit (same IEEE operations in the same order),
+    so torch autograd of it takes the same minmod / max / wet-dry branches as
+    the hand-written reverse, and the two gradients agree to 1e-10."""
+    import torch
+    from oracle import torch_swe as T
+    from zoomy_amrex_b200.adjoint import evolve_differentiable
+    m, steps = 256, 200
+    cfg, Q0, A0 = _bench_case(m)
+    rng = np.random.default_rng(11)
+    eta_obs = torch.from_numpy(Q0[0] + Q0[1] + 0.01 * rng.standard_normal((m, m))).cuda()
+    A = torch.from_numpy(A0).cuda()
+    q = torch.from_numpy(Q0).cuda().requires_grad_(True)
+    nm = torch.tensor(0.03, dtype=torch.float64, device="cuda", requires_grad=True)
+    QT = evolve_differentiable(q, nm, A, cfg, steps, checkpoint_every=20)
+    _loss(QT, eta_obs).backward()
+    qt = torch.from_numpy(Q0).cuda().requires_grad_(True)
+    nmt = torch.tensor(0.03, dtype=torch.float64, device="cuda", requires_grad=True)
+    QTt, _ = T.run(qt, A[6], nmt, steps, PAR, 100.0 / m, 100.0 / m, (1, 1, 1, 1), checkpoint=True)
+    assert torch.equal(QTt.detach(), QT.detach()), float((QTt - QT).abs().max())
+    _loss(QTt, eta_obs).backward()
+    for r in range(4):
+        err = float((q.grad[r] - qt.grad[r]).abs().max() / qt.grad[r].abs().max())
+        print(f"[adjoint vs autograd, 256^2 x 200] row {r}: max rel {err:.2e}")
+        assert err <= 1e-10, (r, err)
+    e_nm = abs(float(nm.grad) - float(nmt.grad)) / abs(float(nmt.grad))
+    print(f"[adjoint vs autograd, 256^2 x 200] n_m: rel {e_nm:.2e}")
+    assert e_nm <= 1e-10
+
+
+def test_adjoint_taylor_remainder_is_second_order(cuda):
+    """Taylor test of the piecewise-smooth map x -> L(Q_T(x)): the remainder
+    |L(x + eps d) - L(x) - eps g.d| falls as eps^2 (a kink crossed inside
+    +-eps adds at most eps times the slope jump, and is crossed with
+    probability ~eps), on seeded directions over (b, h, hu, hv) with the
+    depth and momenta perturbed on wet cells."""
+    import torch
+    from zoomy_amrex_b200.adjoint import evolve_differentiable, forward_only
+    m, steps = 128, 100
+    cfg, Q0, A0 = _bench_case(m)
+    rng = np.random.default_rng(12)
+    eta_obs = torch.from_numpy(Q0[0] + Q0[1] + 0.01 * rng.standard_normal((m, m))).cuda()
+    A = torch.from_numpy(A0).cuda()
+    q = torch.from_numpy(Q0).cuda().requires_grad_(True)
+    nm = torch.tensor(0.03, dtype=torch.float64, device="cuda", requires_grad=True)
+    L0 = _loss(evolve_differentiable(q, nm, A, cfg, steps, checkpoint_every=20), eta_obs)
+    L0.backward()
+    base = torch.from_numpy(Q0).cuda()
+    wet = torch.from_numpy((Q0[1] > 0).astype(np.float64)).cuda()
+    epss = [1e-2, 1e-3, 1e-4, 1e-5]
+    rem = np.zeros((8, len(epss)))
+    for k in range(8):
+        V = torch.from_numpy(rng.standard_normal(Q0.shape) * 1e-2).cuda()
+        V[1:] *= wet
+        gd = float((q.grad * V).sum())
+        for e, eps in enumerate(epss):
+            Le = float(_loss(forward_only(base + eps * V, A, cfg, steps), eta_obs))
+            rem[k, e] = abs(Le - float(L0) - eps * gd)
+    med = np.median(rem, axis=0)
+    slope = np.polyfit(np.log10(epss), np.log10(med), 1)[0]
+    print(f"[adjoint Taylor test 128^2 x 100] median remainders {med}, slope {slope:.2f}")
+    assert slope >= 1.8

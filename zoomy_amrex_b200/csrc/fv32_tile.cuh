@@ -371,15 +371,17 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2)
             float fy = -(FyR[k] - FyL[k]) - FyR[2 * ne + k] - FyL[ne + k];
             if constexpr (WB) {
                 // the bed source (make_rhs.H:154-163) as a difference of the
-                // same FP32 pressures the flux carries: zero at rest, exactly
+                // same FP32 pressures (g/2) h* h* the flux carries, each
+                // rounded once (the _rn products are never fused into an
+                // FMA with the difference): zero at rest, exactly
                 if (k == 1) {
-                    const float pr = 0.5f * g * FxR[3 * ne] * FxR[3 * ne];
-                    const float pl = 0.5f * g * FxL[3 * ne + 1] * FxL[3 * ne + 1];
-                    fx = fx + (pr - pl);
+                    const float pr = __fmul_rn(__fmul_rn(0.5f * g, FxR[3 * ne]), FxR[3 * ne]);
+                    const float pl = __fmul_rn(__fmul_rn(0.5f * g, FxL[3 * ne + 1]), FxL[3 * ne + 1]);
+                    fx = fx + __fsub_rn(pr, pl);
                 } else if (k == 2) {
-                    const float pr = 0.5f * g * FyR[3 * ne] * FyR[3 * ne];
-                    const float pl = 0.5f * g * FyL[3 * ne + 1] * FyL[3 * ne + 1];
-                    fy = fy + (pr - pl);
+                    const float pr = __fmul_rn(__fmul_rn(0.5f * g, FyR[3 * ne]), FyR[3 * ne]);
+                    const float pl = __fmul_rn(__fmul_rn(0.5f * g, FyL[3 * ne + 1]), FyL[3 * ne + 1]);
+                    fy = fy + __fsub_rn(pr, pl);
                 }
             }
             d[k] = dt * (fx * L.rdx + fy * L.rdy);
