@@ -304,6 +304,11 @@ int zfv_batch_set_frames(zfv_batch* b, const float* const* frames, void* stream)
 /* Set each instance's next dt from dts (device, one per instance; enqueued,
  * no synchronization). AMR levels step with dt_0 / 2^l. */
 int zfv_batch_set_dt(zfv_batch* b, const double* dts, void* stream);
+/* ComputeDt of every run record's current state (ZoomyAmr::ComputeDt,
+ * ZoomyAmr.cpp:448-515, over the record's instances, hinv from the state),
+ * written as the record's next dt (enqueued, no synchronization): the
+ * reference's per-level step law, ZoomyAmr.cpp:739. */
+int zfv_batch_compute_dt(zfv_batch* b, void* stream);
 /* One stage (1 or 2) of one SSP-RK2 step of every instance, so that ghost
  * frames can be refilled between the stages (Advance's per-stage FillPatch,
  * ZoomyAmr.cpp:561-572). */
@@ -361,6 +366,11 @@ int zfv_amr_tag(const zfv_amr_level* level, const int* patches, int n_patches, i
 int zfv_amr_set_dt(const void* const* level_descs, double* const* dts, const int* n_inst, int n_levels,
                    double cfl, double cfl_divisor, double dtmin, double dtmax, double time_end, double* time,
                    void* stream);
+/* The base level's step under the reference's per-level law
+ * (ZoomyAmr.cpp:739-749): the dt in its run record (zfv_batch_compute_dt)
+ * clamped to land on time_end (0 once *time >= time_end), added to *time
+ * (device). level_desc: zfv_batch_descriptors() of the base level. */
+int zfv_amr_level_dt(const void* level_desc, double time_end, double* time, void* stream);
 /* Fill freshly created patches from the old patches of the level (where
  * present) or from the coarser level. */
 int zfv_amr_regrid_fill(const zfv_amr_level* level, const zfv_amr_level* old_level, const zfv_amr_level* coarse,

@@ -523,9 +523,13 @@ struct Level {
     }
 
     // One stage of ZoomyAmr::Advance (do_stage, ZoomyAmr.cpp:561-662)
+    // set by a multi-level driver that fills this box's ghost cells itself
+    // (from its neighbours and the coarser level) before each stage
+    bool own_ghosts = false;
+
     void stage(int order, Real t, Real dt, bool face_based) {
         update_state(t);
-        fill_physical_bc(t);          // FillPatch + FillBoundary for one box
+        if (!own_ghosts) fill_physical_bc(t);   // FillPatch + FillBoundary for one box
         rhs(order, t, face_based);
         auto q4 = aQ(); auto a4 = aA(); auto r4 = arr(Rhs, nq);
 #pragma omp parallel for schedule(static)

@@ -65,6 +65,8 @@ def _load(kind: str):
     getattr(lib, prefix + "set_threads").argtypes = [C.c_int]
     if kind == "oracle":
         lib.oracle_init_solution.argtypes = [C.c_int, C.c_int, C.c_int, _D, _D, _D]
+        lib.oracle_amr2_run.argtypes = [cfgp, _D, C.POINTER(C.c_int), C.c_int, C.c_int, C.c_double, C.c_int, _D,
+                                        _D]
     _libs[kind] = (lib, prefix)
     return _libs[kind]
 
@@ -159,3 +161,26 @@ class Oracle:
         if self._fn("advance")(C.byref(cfg), _p(Q), _p(A), time, dt, int(face_based)) != 0:
             raise RuntimeError("advance failed")
         return Q, A
+
+
+def amr2_run(cfg: zfv_config, Q0, rects, n_steps: int, dt: float | None, return_time: bool = False):
+    """Two-level AMR run of the restatement (oracle/fv_oracle_amr.H): base
+    state Q0 (4, ny, nx), fine patches ``rects`` = [(i0, j0, nx, ny)] in fine
+    cells (started as the interpolation of the base state), ``n_steps``
+    coarse steps of ``dt`` (None: the reference's per-level CFL law).
+    Returns (base state, [fine patch states]) (and the final time)."""
+    lib, _ = _load("oracle")
+    Q = np.ascontiguousarray(Q0, dtype=np.float64).copy()
+    r = np.ascontiguousarray(np.asarray(rects, dtype=np.int32).reshape(-1, 4))
+    out = np.zeros(int(sum(4 * int(w) * int(h) for _, _, w, h in r)))
+    t = C.c_double(0.0)
+    rc = lib.oracle_amr2_run(C.byref(cfg), _p(Q), r.ctypes.data_as(C.POINTER(C.c_int)), len(r), int(n_steps),
+                             0.0 if dt is None else float(dt), 1 if dt is None else 0, _p(out), C.byref(t))
+    if rc != 0:
+        raise RuntimeError(f"oracle_amr2_run failed ({rc})")
+    fine, off = [], 0
+    for _, _, w, h in r:
+        n = 4 * int(w) * int(h)
+        fine.append(out[off:off + n].reshape(4, int(h), int(w)))
+        off += n
+    return (Q, fine, float(t.value)) if return_time else (Q, fine)

@@ -204,3 +204,65 @@ def test_amr_levels_come_and_go(cuda):
     assert n_start == 3 and n_mid == 1 and n_end == 3
     assert np.isfinite(q).all()
     assert abs(m1 - m0) / m0 < 1e-3
+
+
+@pytest.mark.parametrize("dt_mode", ["fixed", "level"])
+def test_two_levels_with_refinement_match_the_multilevel_oracle(cuda, dt_mode):
+    """A base level of 128^2 with a fine level around a moving hump (eta
+    gradient tags, 16^2 blocks, never regridded), 30 coarse steps: the FP32
+    hierarchy against the FP64 two-level oracle (oracle/fv_oracle_amr.H: the
+    same subcycling, coarse-fine ghost interpolation and average-down) by
+    L1 / Linf on both levels, and the fine level's initial interpolation.
+    dt_mode "fixed": a dt below both levels' CFL steps (the time-aligned law
+    then takes it); "level": the reference's per-level CFL law
+    (ZoomyAmr.cpp:739-749), each level's dt from its own current state."""
+    from oracle.oracle import amr2_run
+    from zoomy_amrex_b200.amr import AmrHierarchy
+    n, L, steps, B = 128, 10.0, 30, 16
+    x = (np.arange(n) + 0.5) * (L / n)
+    X, Y = np.meshgrid(x, x)
+    b = 0.4 * np.exp(-((X - 4.0) ** 2 + (Y - 6.5) ** 2) / 1.5) + 0.2 * np.exp(-((X - 7.0) ** 2 + (Y - 3.0) ** 2))
+    eta = 1.0 + 0.25 * np.exp(-((X - 6.0) ** 2 + (Y - 5.0) ** 2) / 0.8)
+    h = np.maximum(eta - b, 0.0)
+    Q0 = np.array([b, h, 0 * h, 0 * h])
+    # below both levels' CFL steps (base: 0.45 / 6 * dx / (|u| + sqrt(g h)) >= 1.3e-3
+    # for |u| + sqrt(g h) < 4.5 m/s; the fine level allows twice its half step)
+    dt = 1.0e-3 if dt_mode == "fixed" else 1.0
+    cfg = make_config(ZFV_MODEL_SWE2D, n, n, (0.0, 0.0), (L, L), spatial_order=2, well_balanced=True,
+                      implicit_source=True, cfl=0.45, dtmax=dt, time_end=1e30, max_step=-1,
+                      bc=("wall",) * 4, params={"n_m": 0.03})
+    hier = AmrHierarchy(cfg, Q0, max_level=1, B=B, threshold=0.02, regrid_int=0,
+                        dt_mode="aligned" if dt_mode == "fixed" else "level")
+    try:
+        assert len(hier.levels) == 2
+        patches = hier.levels[1].patches
+        nblk = sum(nbx * nby for _, _, nbx, nby in patches)
+        assert 0 < nblk < (2 * n // B) ** 2, nblk       # refined somewhere, not everywhere
+        rects = [(bx * B, by * B, nbx * B, nby * B) for bx, by, nbx, nby in patches]
+        F0 = hier.level_state(1)
+        _, fine0 = amr2_run(cfg, Q0, rects, 0, dt)
+        for (i0, j0, w, hh), f in zip(rects, fine0):
+            d = np.abs(F0[:, j0:j0 + hh, i0:i0 + w] - f)
+            assert d[1].max() < 1e-6 and d[0].max() < 1e-6
+        hier.run(steps)
+        t_gpu = hier.time
+        G0, G1 = hier.level_state(0), hier.level_state(1)
+    finally:
+        hier.close()
+    Qo, fine, t_or = amr2_run(cfg, Q0, rects, steps, dt if dt_mode == "fixed" else None, return_time=True)
+    print(f"[amr 2 levels vs oracle, {dt_mode}] time gpu {t_gpu:.9f} oracle {t_or:.9f}")
+    assert abs(t_gpu - t_or) <= 1e-6 * t_or
+    d0 = np.abs(G0[1] - Qo[1])
+    m0 = np.abs(G0[2:] - Qo[2:])
+    print(f"[amr 2 levels vs oracle, {dt_mode}] base: depth L1 {d0.mean():.2e} Linf {d0.max():.2e}, "
+          f"momenta Linf {m0.max():.2e}")
+    assert d0.mean() < 1e-6 and d0.max() < 1e-4 and m0.max() < 1e-4
+    worst = 0.0
+    for (i0, j0, w, hh), f in zip(rects, fine):
+        g = G1[:, j0:j0 + hh, i0:i0 + w]
+        assert np.isfinite(g).all()
+        d1 = np.abs(g[1] - f[1])
+        worst = max(worst, d1.max())
+        assert d1.mean() < 1e-6 and np.abs(g[2:] - f[2:]).max() < 1e-4
+    print(f"[amr 2 levels vs oracle, {dt_mode}] fine patches {len(rects)}: depth Linf {worst:.2e}")
+    assert worst < 1e-4

@@ -26,6 +26,7 @@ SYMBOLS = ("zfv_last_error", "zfv_version", "zfv_sizeof_config", "zfv_sizeof_sta
            "zfv_adj_set_variant", "zfv_batch_create_grouped", "zfv_batch_set_frames", "zfv_batch_set_dt",
            "zfv_batch_stage", "zfv_batch_descriptors", "zfv_amr_fill", "zfv_amr_average_down", "zfv_amr_tag",
            "zfv_amr_regrid_fill", "zfv_amr_set_dt", "zfv_implicit_global_stats",
+           "zfv_batch_compute_dt", "zfv_amr_level_dt",
            "zfv_init_solution", "zfv_set_variant", "zfv_get_variant")
 
 
@@ -94,6 +95,8 @@ def lib():
     L.zfv_batch_create_grouped.argtypes = [C.POINTER(zfv_config), i, C.POINTER(i), C.POINTER(vp)]
     L.zfv_batch_set_frames.argtypes = [vp, pp, vp]
     L.zfv_batch_set_dt.argtypes = [vp, vp, vp]
+    L.zfv_batch_compute_dt.argtypes = [vp, vp]
+    L.zfv_amr_level_dt.argtypes = [vp, d, vp, vp]
     L.zfv_batch_stage.argtypes = [vp, i, vp]
     L.zfv_batch_descriptors.argtypes = [vp]
     L.zfv_batch_descriptors.restype = vp

@@ -18,10 +18,13 @@ one launch per RK stage advances all patches of a level, the patches of a
 level share one run record, and a patch's ghost ring is a small frame array
 the stage kernels read in place of the physical mirror.
 
-Two choices differ from the reference, which steps each level with its own
-CFL dt (so fine levels need not land on the coarse time) and regrids at every
-coarse step: here dt_l = dt_0 / 2^l with dt_0 the largest step every level's
-CFL law allows, and regridding happens every ``regrid_int`` coarse steps.
+The step law is a choice (``dt_mode``): "aligned" (the default) steps level
+l with dt_0 / 2^l, dt_0 the largest step every level's CFL law allows, so the
+levels stay time-aligned; "level" is the reference's law (ZoomyAmr.cpp:739-749):
+before each of its steps a level takes its own CFL dt from its current
+state (level 0 clamped to land on time_end), so a fine level's two substeps
+need not add up to the coarse step. Regridding happens every ``regrid_int``
+coarse steps (the reference regrids at every coarse step).
 """
 from __future__ import annotations
 
@@ -139,7 +142,7 @@ class AmrHierarchy:
 
     def __init__(self, cfg: zfv_config, Q0, max_level: int = 2, B: int = 64, threshold: float = 0.01,
                  regrid_int: int = 2, device="cuda:0", variant: int = 9, patch_blocks: int = 16,
-                 tag: str = "eta_gradient", tag_b_max: float = 1.0e30):
+                 tag: str = "eta_gradient", tag_b_max: float = 1.0e30, dt_mode: str = "aligned"):
         if cfg.nx % B or cfg.ny % B or B % 2:
             raise ValueError("the base grid must be a multiple of the (even) box side B in both directions")
         self.cfg = _cfg_copy(cfg)
@@ -151,6 +154,9 @@ class AmrHierarchy:
             raise ValueError("patch_blocks must be in 1 .. 32")
         if tag not in self.TAGS:
             raise ValueError(f"tag must be one of {sorted(self.TAGS)}")
+        if dt_mode not in ("aligned", "level"):
+            raise ValueError("dt_mode must be 'aligned' or 'level'")
+        self.dt_mode = dt_mode
         self.criterion, self.tag_b_max = self.TAGS[tag], float(tag_b_max)
         self.patch_blocks = patch_blocks
         self.nbx0, self.nby0 = cfg.nx // B, cfg.ny // B
@@ -293,7 +299,13 @@ class AmrHierarchy:
 
     def _advance(self, lev: int):
         L = self.levels[lev]
-        L.batch.set_dt(L.dts)
+        if self.dt_mode == "level":
+            L.batch.compute_dt()
+            if lev == 0:
+                _lib.check(_lib.lib().zfv_amr_level_dt(C.c_void_p(L.batch.descriptors), self.cfg.time_end,
+                                                       self._time.data_ptr(), self._s()), "zfv_amr_level_dt")
+        else:
+            L.batch.set_dt(L.dts)
         self.fill(lev, 1)
         L.batch.stage(1)
         self.fill(lev, 2)
@@ -307,7 +319,8 @@ class AmrHierarchy:
             self.average_down(lev + 1)
 
     def _coarse_step(self):
-        self._set_dt()
+        if self.dt_mode == "aligned":
+            self._set_dt()
         self._time_step(0)
 
     def step(self):

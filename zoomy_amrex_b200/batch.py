@@ -145,6 +145,11 @@ class Batch:
         """Next dt of every instance from a device float64 tensor (enqueued)."""
         _lib.check(_lib.lib().zfv_batch_set_dt(self._h, dts.data_ptr(), self._s()), "zfv_batch_set_dt")
 
+    def compute_dt(self):
+        """Next dt of every run record from the CFL law on its current state
+        (ZoomyAmr::ComputeDt; enqueued)."""
+        _lib.check(_lib.lib().zfv_batch_compute_dt(self._h, self._s()), "zfv_batch_compute_dt")
+
     def stage(self, k: int):
         """Stage k (1 or 2) of one step of every instance (enqueued)."""
         _lib.check(_lib.lib().zfv_batch_stage(self._h, int(k), self._s()), "zfv_batch_stage")

@@ -296,5 +296,18 @@ __global__ void k32a_set_dt(DtArgs a) {
     }
 }
 
+// The reference's per-level step law (ZoomyAmr.cpp:739-749) for the base
+// level: its run record's dt (ComputeDt of its current state) clamped to land
+// on time_end (0 once time_end is reached), and the hierarchy time advanced
+// by it. One thread.
+__global__ void k32a_level_dt(const BInst* __restrict__ lev, double time_end, double* time) {
+    zfv::DevState* st = lev[0].st;
+    const double remaining = time_end - *time;
+    double dt = *(volatile double*)&st->dt;
+    dt = remaining > 0.0 ? fmin(dt, remaining) : 0.0;
+    st->dt = dt;
+    *time += dt;
+}
+
 }  // namespace amr
 }  // namespace zfv32

@@ -214,7 +214,8 @@ static __global__ void k32b_init(const BInst* __restrict__ insts, int n) {
 }
 
 // ComputeDt (WHAT 0, clamped to time_end, from the stored aux as the
-// reference's first ComputeDt) or the FP64 mass (WHAT 1), per instance.
+// reference's first ComputeDt; WHAT 2 the same with hinv taken from the
+// current state) or the FP64 mass (WHAT 1), per instance.
 template <int NW, int CPT, int PK, int WHAT>
 __global__ void __launch_bounds__(32 * NW)
 k32b_reduce(const BInst* __restrict__ insts, const int2* __restrict__ units, int n_aux) {
@@ -231,8 +232,8 @@ k32b_reduce(const BInst* __restrict__ insts, const int2* __restrict__ units, int
     for_strip_cells<NW, CPT, PK>(sD, u, [&](long long c) {
         const double b = double(sD.bed[c]);
         const double h = (double(X[c]) + double(sD.lo[c])) - b;
-        if constexpr (WHAT == 0) {
-            const double hinv = sD.aux[(n_aux - 1) * pl + c];
+        if constexpr (WHAT != 1) {
+            const double hinv = (WHAT == 0) ? sD.aux[(n_aux - 1) * pl + c] : kp_hinv_d(h, L.epsd);
             const double c0 = sqrt(L.gd * fmax(h, 0.0));
             const double hu = double(X[pl + c]) + double(sD.lo[pl + c]);
             const double hv = double(X[2 * pl + c]) + double(sD.lo[2 * pl + c]);
@@ -265,7 +266,7 @@ k32b_reduce(const BInst* __restrict__ insts, const int2* __restrict__ units, int
     }
     zfv::block_reduce_max_sum<NT>(gm, gs, red);
     if (threadIdx.x == 0) {
-        if constexpr (WHAT == 0) {
+        if constexpr (WHAT != 1) {
             const double dt = zfv::dt_from_max(gm, st->time, L);
             st->max_inv = gm;
             st->dt = dt;

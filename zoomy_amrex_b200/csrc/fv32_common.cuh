@@ -16,6 +16,7 @@ struct Params {
     double dx, dy, plox, ploy;       // FP64 (reductions, dt)
     float fdx, fdy, rdx, rdy, rfdx, rfdy;
     float g, ex, ey, nm, hfloor, eps;
+    float hwet;                      // above this depth h^4 > eps: the KP hinv is 1/h
     double gd, exd, eyd, nmd, hfloord, epsd;
     int bc_tag[4];
     double cfl, dtmin, dtmax, time_end;
@@ -31,9 +32,11 @@ struct C4 { float b, e, u, v; };   // bed, surface eta = h + b, hu, hv
 
 constexpr float kNearDry = 1.0e-3f;   // FP64 implicit solve below this depth
 
+// minmod (make_rhs.H:9-13) as the median of (a, b, 0): 0 when the signs
+// differ or either is 0, else the one of smaller magnitude; four min/max
+// operations and no multiply or compare-and-select.
 __device__ __forceinline__ float mm(float a, float b) {
-    if (a * b <= 0.0f) return 0.0f;
-    return (fabsf(a) < fabsf(b)) ? a : b;
+    return fmaxf(fminf(a, b), fminf(fmaxf(a, b), 0.0f));
 }
 
 // Knuth's two-sum: s + e == a + b exactly (round-to-nearest, no contraction:
@@ -50,6 +53,12 @@ __device__ __forceinline__ float kp_hinv(float h, float eps) {
     const float h2 = h * h;
     const float x0 = h2 * h2;
     return 1.41421356237f * h * rsqrtf(x0 + fmaxf(x0, eps));
+}
+// The same, 1/h (one reciprocal) where every active lane's depth exceeds
+// hwet (h^4 > eps), decided by a warp vote.
+__device__ __forceinline__ float kp_hinv_w(float h, float eps, float hwet) {
+    if (__all_sync(__activemask(), h > hwet)) return 1.0f / h;
+    return kp_hinv(h, eps);
 }
 __device__ __forceinline__ double kp_hinv_d(double h, double eps) {
     const double h2 = h * h;

@@ -36,7 +36,8 @@ constexpr int kDefaultVariant = 9;
 struct ShapeOps {
     // FP64 reference layout -> FP32 state (exp == false) or back (exp == true)
     void (*convert)(int n_units, cudaStream_t s, const BInst* d, const int2* u, int n_aux, bool exp);
-    // grid reduction per instance: what 0 = ComputeDt from the stored aux, 1 = mass
+    // grid reduction per instance: what 0 = ComputeDt from the stored aux, 1 = mass,
+    // 2 = ComputeDt of the current state
     void (*reduce)(int n_units, cudaStream_t s, const BInst* d, const int2* u, int n_aux, int what);
     // stages 3 = both stages of n_steps steps; 1 or 2 = that stage alone, once
     void (*step)(int n_units, cudaStream_t s, const BInst* d, const int2* u, bool wb, bool impl,

@@ -85,7 +85,7 @@ __device__ __forceinline__ FaceR face_rs(RS a, RS c, const Params& L) {
         db = c.b - a.b;
     }
     const float g = L.g, hg = 0.5f * L.g;
-    const float hiL = kp_hinv(a.h, L.eps), hiR = kp_hinv(c.h, L.eps);
+    const float hiL = kp_hinv_w(a.h, L.eps, L.hwet), hiR = kp_hinv_w(c.h, L.eps, L.hwet);
     const float unL = (DIR == 0) ? a.u : a.v, unR = (DIR == 0) ? c.u : c.v;
     const float pL = hg * a.h * a.h, pR = hg * c.h * c.h;
     const float qL = unL * hiL, qR = unR * hiR;          // normal velocities
@@ -263,7 +263,7 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
             const float r1 = Ax1 * L.rdx + Ay1 * L.rdy;
             const float r2 = Ax2 * L.rdx + Ay2 * L.rdy;
             const float h = w1.e - w1.b;
-            const float hinv = kp_hinv(h, L.eps);
+            const float hinv = kp_hinv_w(h, L.eps, L.hwet);
             float inc_e = dt * r0, inc_u = dt * r1, inc_v = dt * r2;
             if constexpr (!IMPL) {
                 const float mh = fmaxf(h, L.hfloor);
@@ -311,7 +311,7 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
                 lo[c] = le; lo[pl + c] = lu; lo[2 * pl + c] = lv;
                 // CFL terms of the new state (ZoomyAmr.cpp:472-487) and its FP64 mass
                 const float hn = he - w1.b;
-                const float hin = kp_hinv(hn, L.eps);
+                const float hin = kp_hinv_w(hn, L.eps, L.hwet);
                 const float c0 = sqrtf(L.g * fmaxf(hn, 0.0f));
                 const float evx = (fabsf(hu * hin) + c0) * L.rfdx;
                 const float evy = (fabsf(hv * hin) + c0) * L.rfdy;

@@ -40,11 +40,14 @@ __device__ __forceinline__ float2 rsqrt2(float2 a) { return f2(rsqrtf(a.x), rsqr
 struct C42 { float2 b, e, u, v; };          // cells A, B: bed, eta, hu, hv
 struct RS2 { float2 b, h, e, u, v; };       // reconstructed face states of A, B
 
-// KP desingularised 1/h (the model's update_aux_variables), packed.
-__device__ __forceinline__ float2 kp_hinv2(float2 h, float eps) {
+// KP desingularised 1/h (the model's update_aux_variables), packed. Where
+// every active lane's depths exceed hwet (h^4 > eps) the formula is 1/h:
+// one reciprocal each, decided by a warp vote.
+__device__ __forceinline__ float2 kp_hinv2(float2 h, const Params& L) {
+    if (__all_sync(__activemask(), fminf(h.x, h.y) > L.hwet)) return f2(1.0f / h.x, 1.0f / h.y);
     const float2 h2 = mul(h, h);
     const float2 x0 = mul(h2, h2);
-    return mul(mul(s2(1.41421356237f), h), rsqrt2(add(x0, fmax2(x0, s2(eps)))));
+    return mul(mul(s2(1.41421356237f), h), rsqrt2(add(x0, fmax2(x0, s2(L.eps)))));
 }
 
 __device__ __forceinline__ void reconstruct2(const C42& m, const C42& c, const C42& p, RS2& lo, RS2& hi) {
@@ -90,7 +93,7 @@ __device__ __forceinline__ FaceLR face2(RS2 a, RS2 c, const Params& L) {
         db = sub(c.b, a.b);
     }
     const float2 g = s2(L.g), hg = s2(0.5f * L.g), half = s2(0.5f);
-    const float2 hiL = kp_hinv2(a.h, L.eps), hiR = kp_hinv2(c.h, L.eps);
+    const float2 hiL = kp_hinv2(a.h, L), hiR = kp_hinv2(c.h, L);
     const float2 unL = (DIR == 0) ? a.u : a.v, unR = (DIR == 0) ? c.u : c.v;
     const float2 pL = mul(mul(hg, a.h), a.h), pR = mul(mul(hg, c.h), c.h);
     const float2 qL = mul(unL, hiL), qR = mul(unR, hiR);
@@ -173,8 +176,9 @@ __device__ __forceinline__ void manning_implicit2(float2 h, float2 u, float2 v, 
     const float2 rdet = f2(__frcp_rn(det.x), __frcp_rn(det.y));
     const float2 x0 = mul(sub(mul(r0, d), mul(b, r1)), rdet);
     const float2 x1 = mul(sub(mul(a, r1), mul(c, r0)), rdet);
-    const bool okx = fabsf(det.x) > 0.0f && isfinite(det.x) && isfinite(x0.x) && isfinite(x1.x);
-    const bool oky = fabsf(det.y) > 0.0f && isfinite(det.y) && isfinite(x0.y) && isfinite(x1.y);
+    // a zero, infinite or NaN determinant makes the solution non-finite
+    const float2 xs = add(x0, x1);
+    const bool okx = isfinite(xs.x), oky = isfinite(xs.y);
     du = f2(okx ? x0.x : (isfinite(r0.x) ? r0.x : 0.0f), oky ? x0.y : (isfinite(r0.y) ? r0.y : 0.0f));
     dv = f2(okx ? x1.x : (isfinite(r1.x) ? r1.x : 0.0f), oky ? x1.y : (isfinite(r1.y) ? r1.y : 0.0f));
 }
@@ -301,7 +305,7 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
             const float2 r1 = fma(Ax1, rdx, mul(Ay1, rdy));
             const float2 r2 = fma(Ax2, rdx, mul(Ay2, rdy));
             const float2 h = sub(w1.e, w1.b);
-            const float2 hinv = kp_hinv2(h, L.eps);
+            const float2 hinv = kp_hinv2(h, L);
             float2 inc_e = mul(vdt, r0), inc_u = mul(vdt, r1), inc_v = mul(vdt, r2);
             if constexpr (!IMPL) {
                 const float2 mh = fmax2(h, s2(L.hfloor));
@@ -379,21 +383,20 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
                     nf[0][q] = nf2[q].x; nf[1][q] = nf2[q].y;
                     nl[0][q] = nl2[q].x; nl[1][q] = nl2[q].y;
                 }
-                const float bb[2] = {w1.b.x, w1.b.y};
-#pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    const bool own = k == 0 ? ownA : ownB;
-                    if (own) {
-                        // CFL terms of the new state (ZoomyAmr.cpp:472-487) and its FP64 mass
-                        const float hn = nf[k][0] - bb[k];
-                        const float hin = kp_hinv(hn, L.eps);
-                        const float c0 = sqrtf(L.g * fmaxf(hn, 0.0f));
-                        const float evx = (fabsf(nf[k][1] * hin) + c0) * L.rfdx;
-                        const float evy = (fabsf(nf[k][2] * hin) + c0) * L.rfdy;
-                        const float mm_ = fmaxf(fmaxf(evx, evy), 0.0f);
-                        m_f = fmaxf(m_f, mm_);
-                        s_loc = s_loc + ((double(nf[k][0]) - double(bb[k])) + double(nl[k][0]));
-                    }
+                // CFL terms of the new state (ZoomyAmr.cpp:472-487), packed, and its FP64 mass
+                const float2 hn = sub(nf2[0], w1.b);
+                const float2 hin = kp_hinv2(hn, L);
+                const float2 c0 = sqrt2(mul(s2(L.g), fmax2(hn, s2(0.0f))));
+                const float2 evx = mul(add(fabs2(mul(nf2[1], hin)), c0), s2(L.rfdx));
+                const float2 evy = mul(add(fabs2(mul(nf2[2], hin)), c0), s2(L.rfdy));
+                const float2 ev = fmax2(fmax2(evx, evy), s2(0.0f));
+                if (ownA) {
+                    m_f = fmaxf(m_f, ev.x);
+                    s_loc = s_loc + ((double(nf[0][0]) - double(w1.b.x)) + double(nl[0][0]));
+                }
+                if (ownB) {
+                    m_f = fmaxf(m_f, ev.y);
+                    s_loc = s_loc + ((double(nf[1][0]) - double(w1.b.y)) + double(nl[1][0]));
                 }
                 if (vec_io) {
 #pragma unroll

@@ -21,6 +21,7 @@
 //    (h < 1e-3) and in the mass sum.
 // Kernels are compiled with FMA contraction on (this file only).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -57,6 +58,7 @@ Params make_params(const zfv_config& c) {
     L.nmd = c.params[zb::swe_n_m]; L.hfloord = c.params[zb::swe_h_floor]; L.epsd = c.params[zb::swe_eps];
     L.g = float(L.gd); L.ex = float(L.exd); L.ey = float(L.eyd); L.nm = float(L.nmd);
     L.hfloor = float(L.hfloord); L.eps = float(L.epsd);
+    L.hwet = float(std::pow(L.epsd, 0.25) * 1.001);
     for (int s = 0; s < 4; ++s) L.bc_tag[s] = c.bc_tag[s];
     L.cfl = c.cfl; L.dtmin = c.dtmin; L.dtmax = c.dtmax; L.time_end = c.time_end;
     L.max_step = c.max_step; L.cfl_dimension = c.cfl_dimension; L.cfl_degree_factor = c.cfl_degree_factor;
@@ -248,6 +250,11 @@ struct BatchCore {
         return cuda_check(cudaGetLastError(), "zfv_batch mass launch");
     }
 
+    int compute_dt(cudaStream_t s) {
+        ops().reduce(nunits(), s, d_desc(), d_units(), n_aux, 2);
+        return cuda_check(cudaGetLastError(), "zfv_batch_compute_dt launch");
+    }
+
     // stages: 3 = both stages of `nsteps` steps; 1 or 2 = that stage alone,
     // once (AMR boxes refill their ghost frames between the stages)
     int evolve(int nsteps, cudaStream_t s, int stages = 3) {
@@ -395,6 +402,11 @@ int zfv_batch_set_frames(zfv_batch* b, const float* const* frames, void* stream)
     return b->core.set_frames(frames, (cudaStream_t)stream);
 }
 
+int zfv_batch_compute_dt(zfv_batch* b, void* stream) {
+    if (!b || !b->core.bound) return fail(-1, "zfv_batch_compute_dt: bind the batch first");
+    return b->core.compute_dt((cudaStream_t)stream);
+}
+
 int zfv_batch_set_dt(zfv_batch* b, const double* dts, void* stream) {
     if (!b || !dts || !b->core.bound) return fail(-1, "zfv_batch_set_dt: bind the batch first");
     return b->core.set_dt(dts, (cudaStream_t)stream);
@@ -489,6 +501,13 @@ int zfv_amr_set_dt(const void* const* level_descs, double* const* dts, const int
     a.time = time;
     zfv32::amr::k32a_set_dt<<<1, 256, 0, (cudaStream_t)stream>>>(a);
     return cuda_check(cudaGetLastError(), "zfv_amr_set_dt launch");
+}
+
+int zfv_amr_level_dt(const void* level_desc, double time_end, double* time, void* stream) {
+    if (!level_desc || !time) return fail(-1, "zfv_amr_level_dt: null argument");
+    zfv32::amr::k32a_level_dt<<<1, 1, 0, (cudaStream_t)stream>>>(static_cast<const zfv32::BInst*>(level_desc),
+                                                                  time_end, time);
+    return cuda_check(cudaGetLastError(), "zfv_amr_level_dt launch");
 }
 
 int zfv_amr_regrid_fill(const zfv_amr_level* level, const zfv_amr_level* old_level, const zfv_amr_level* coarse,

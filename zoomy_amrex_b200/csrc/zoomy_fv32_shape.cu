@@ -28,6 +28,7 @@ void convert(int nu, cudaStream_t s, const BInst* d, const int2* u, int n_aux, b
 
 void reduce(int nu, cudaStream_t s, const BInst* d, const int2* u, int n_aux, int what) {
     if (what == 0) k32b_reduce<NW, CPT, PK, 0><<<nu, 32 * NW, 0, s>>>(d, u, n_aux);
+    else if (what == 2) k32b_reduce<NW, CPT, PK, 2><<<nu, 32 * NW, 0, s>>>(d, u, n_aux);
     else k32b_reduce<NW, CPT, PK, 1><<<nu, 32 * NW, 0, s>>>(d, u, n_aux);
 }
 
