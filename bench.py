@@ -626,9 +626,10 @@ def sme_bench(local, n=2048, steps=500, timed=100, warm=5):
         return e0.elapsed_time(e1) / k
 
     ms64 = timed_run(ZFV_PREC_FP64)
-    shape_ms = {v: timed_run(ZFV_PREC_FP32, variant=v, k=max(10, timed // 5)) for v in range(3)}
+    from zoomy_amrex_b200.batch import generic_tile_variants
+    shapes = generic_tile_variants()
+    shape_ms = {v: timed_run(ZFV_PREC_FP32, variant=v, k=max(10, timed // 5)) for v in range(len(shapes))}
     best = min(shape_ms, key=shape_ms.get)
-    shapes = [(32, 8), (16, 8), (32, 4)]
     record(8, "fp32", float(cells), best, shape_ms, shapes)
     ms32 = timed_run(ZFV_PREC_FP32, variant=best)
     # error after `steps` steps from the same start
@@ -659,7 +660,8 @@ def sme_bench(local, n=2048, steps=500, timed=100, warm=5):
                             "hbm_gbs": a32, "frac": a32 / peak,
                             "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_SME_FP32,
                             "tile_shape": shapes[best],
-                            "tile_shape_ms_per_step": {f"{shapes[v][0]}x{shapes[v][1]}": t
+                            "tile_shape_ms_per_step": {f"{shapes[v][0]}x{shapes[v][1]}"
+                                                       + ("-tma" if shapes[v][2] else ""): t
                                                        for v, t in shape_ms.items()}},
             "fp32_over_fp64": ms64 / ms32, "peak_source": peak_kind,
             "error_fp32_vs_fp64": {"steps": steps, "time_fp64": st64["time"], "time_fp32": st32["time"],

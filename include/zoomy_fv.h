@@ -63,7 +63,9 @@ enum {
 enum {
     ZFV_FLAG_NONFINITE_DT   = 1,   /* the CFL reduction produced a non-finite dt            */
     ZFV_FLAG_MOOD_REDO      = 2,   /* a step was redone at order 1 (positivity = mood)      */
-    ZFV_FLAG_DONE           = 4    /* time >= time_end or step >= max_step: kernels idle   */
+    ZFV_FLAG_DONE           = 4,   /* time >= time_end or step >= max_step: kernels idle   */
+    ZFV_FLAG_DEVICE_WAIT    = 8    /* a bounded device-side wait (a TMA copy's barrier) ran
+                                      out: the run was stopped and its last step is invalid */
 };
 
 /*
@@ -286,6 +288,15 @@ int zfv_batch_units(const zfv_batch* b);
  * zfv_get_variant returns -1.
  */
 int zfv_tile_variants(int* nw, int* cpt, int* cols, int* flags, int max_n);
+/*
+ * Tile variants of the generic FP32 kernels (the FP32 form of the
+ * shallow-moment model, ZFV_MODEL_SME2D_L2): tile width and height in cells
+ * and the staging (0 = plain coalesced loads, 1 = TMA boxes completing on an
+ * mbarrier; needs nx % 4 == 0 and a 16-byte aligned state). Writes up to
+ * max_n of them and returns how many exist; zfv_set_variant selects one for
+ * such a level (default 0). Every variant gives the same bits.
+ */
+int zfv_generic_tile_variants(int* tx, int* ty, int* tma, int max_n);
 int zfv_set_variant(zfv_handle* h, int variant, void* stream);
 int zfv_get_variant(const zfv_handle* h);
 

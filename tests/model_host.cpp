@@ -36,7 +36,7 @@ typename M::VA aux_of(typename M::VQ const& q, typename M::VP const& p) {
 // what: 0 flux along D, 1 moment rows of B_D(q) dq, 2 source, 3 dS/dq (row-major),
 //       4 dS/dhinv, 5 Gershgorin bound along D (out[0]), 6 numerical flux (qL = q, qR = dq),
 //       7 numerical fluctuations (qL = q, qR = dq; 2 n values), 8 path product Btilde (qR - qL),
-//       9 wall ghost state for the face normal e_D
+//       9 wall ghost state for the face normal e_D, 10 the block point-implicit increment (dt = dq[0])
 template <class M, class N>
 int eval(int what, int D, const double* q, const double* dq, const double* pp, double* out) {
     constexpr int n = M::n_dof_q;
@@ -93,6 +93,15 @@ int eval(int what, int D, const double* q, const double* dq, const double* pp, d
         const auto F = N::numerical_fluctuations(Q, QR, a, aux_of<M>(QR, p), p, nh);
         for (int k = 0; k < 2 * n; ++k) out[k] = F(k, 0);
         return 0;
+    }
+    case 10: {
+        if constexpr (requires_ncp<M>::value) {   // the block point-implicit step, dt = dq[0]
+            typename M::VQ d{};
+            M::zb_implicit_increment(Q, a, p, dq[0], d);
+            for (int k = 0; k < n; ++k) out[k] = d(k, 0);
+            return 0;
+        }
+        return -1;
     }
     case 9: {
         const auto G = M::boundary_conditions(1, Q, a, nh, X, 0.0, 1.0);

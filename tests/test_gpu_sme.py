@@ -181,10 +181,15 @@ def test_sme_fp32_lake_at_rest_is_exact(cuda):
 
 
 def test_sme_fp32_tile_shapes_agree_and_mass_is_conserved(cuda):
-    """Every tile shape computes the same faces in the same order: identical
-    results. With walls the FP64 mass of the compensated state is conserved."""
+    """Every tile shape, staged by plain loads or by TMA boxes, computes the
+    same faces in the same order: identical results. With walls the FP64
+    mass of the compensated state is conserved."""
+    from zoomy_amrex_b200.batch import generic_tile_variants
     cfg, Q0, A0 = setup(*CASES_SME["sme2d_wetdry_wb_impl_o2"])
-    outs = [run_fp32(cfg, Q0, A0, variant=v) for v in range(3)]
+    variants = generic_tile_variants()
+    assert len(variants) == 6 and [v[2] for v in variants] == [0, 0, 0, 1, 1, 1]
+    assert cfg.nx % 4 == 0
+    outs = [run_fp32(cfg, Q0, A0, variant=v) for v in range(len(variants))]
     for o in outs[1:]:
         assert np.array_equal(o[0], outs[0][0])
     log = outs[0][3]

@@ -162,3 +162,28 @@ def test_wall_reflects_the_whole_velocity_profile(host):
             first = 2 + dim + D * level
             want[first:first + level] *= -1
             assert np.array_equal(g, want)
+
+
+@pytest.mark.parametrize("dim,level", CASES)
+def test_block_point_implicit_step_solves_the_linear_system(host, dim, level):
+    """zb_implicit_increment (the FP32 kernels' structured solve) returns
+    the solution of (I - dt J) dq = dt S with J = dS/dQ at fixed hinv
+    (make_rhs.H:429-509's system), J and S from the symbolic derivation."""
+    from sme_sympy import numeric
+    f = numeric(level, dim)
+    rng = np.random.default_rng(300 + 10 * dim + level)
+    for _ in range(20):
+        q = rand_state(rng, dim, level)
+        par = np.array([9.81, rng.uniform(-0.1, 0.1), rng.uniform(-0.1, 0.1), rng.uniform(1e-4, 1e-2),
+                        rng.uniform(0.01, 1.0), 1e-24])
+        dt = float(rng.uniform(1e-4, 5e-2))
+        n = len(q)
+        d = np.zeros(n); d[0] = dt
+        got = ev(host, 1, dim, level, 10, 0, q, d, par=par)[:n]
+        ps = tuple(par[:5])
+        J = np.asarray(f["dSdq"](q, ps), float)
+        S = np.asarray(f["S"](q, ps), float).ravel()
+        want = np.linalg.solve(np.eye(n) - dt * J, dt * S)
+        # the bed and depth rows have no source: their increment is exactly zero
+        assert got[0] == 0.0 and got[1] == 0.0
+        np.testing.assert_allclose(got[2:], want[2:], rtol=1e-11, atol=1e-15)

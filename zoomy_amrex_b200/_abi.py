@@ -20,6 +20,7 @@ ZFV_PREC_FP32 = 1
 ZFV_FLAG_NONFINITE_DT = 1
 ZFV_FLAG_MOOD_REDO = 2
 ZFV_FLAG_DONE = 4
+ZFV_FLAG_DEVICE_WAIT = 8
 
 # Model registry: id -> (n_q, n_aux, n_params, dimension, parameter names,
 # default parameters, boundary tags). Mirrors the compiled Model::

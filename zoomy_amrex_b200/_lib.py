@@ -27,7 +27,7 @@ SYMBOLS = ("zfv_last_error", "zfv_version", "zfv_sizeof_config", "zfv_sizeof_sta
            "zfv_batch_stage", "zfv_batch_descriptors", "zfv_amr_fill", "zfv_amr_average_down", "zfv_amr_tag",
            "zfv_amr_regrid_fill", "zfv_amr_set_dt", "zfv_implicit_global_stats",
            "zfv_batch_compute_dt", "zfv_amr_level_dt",
-           "zfv_init_solution", "zfv_set_variant", "zfv_get_variant")
+           "zfv_init_solution", "zfv_set_variant", "zfv_get_variant", "zfv_generic_tile_variants")
 
 
 class ZfvError(RuntimeError):
@@ -80,6 +80,7 @@ def lib():
     L.zfv_batch_status.argtypes = [vp, C.POINTER(zfv_status), vp]
     L.zfv_batch_units.argtypes = [vp]
     L.zfv_tile_variants.argtypes = [C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i), i]
+    L.zfv_generic_tile_variants.argtypes = [C.POINTER(i), C.POINTER(i), C.POINTER(i), i]
     L.zfv_batch_set_variant.argtypes = [vp, i, vp]
     L.zfv_evolve_static.argtypes = [vp, vp, vp, i, i, C.POINTER(zfv_status), vp]
     L.zfv_run_state_bytes.restype = C.c_size_t

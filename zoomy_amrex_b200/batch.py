@@ -38,6 +38,17 @@ def tile_variants() -> list[tuple[int, int, int, int]]:
     return [(nw[k], cpt[k], cols[k], pf[k]) for k in range(n)]
 
 
+def generic_tile_variants() -> list[tuple[int, int, int]]:
+    """Tile variants of the generic FP32 kernels (the shallow-moment model's
+    FP32 form) as (tile width, tile height, staging: 0 plain loads, 1 TMA)."""
+    L = _lib.lib()
+    tx = (C.c_int * 32)()
+    ty = (C.c_int * 32)()
+    tma = (C.c_int * 32)()
+    n = int(L.zfv_generic_tile_variants(tx, ty, tma, 32))
+    return [(tx[k], ty[k], tma[k]) for k in range(n)]
+
+
 class Batch:
     """A batch of FP32 SWE2D instances on one device.
 

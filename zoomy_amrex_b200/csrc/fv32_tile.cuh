@@ -28,6 +28,9 @@
 // flipped by the block that finishes a step, so one step is always the same
 // two launches (one captured CUDA graph replays any number of steps).
 #pragma once
+#include <cstdint>
+#include <type_traits>
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "fv_kernels.cuh"
 
@@ -78,19 +81,85 @@ struct TileBufs {
     int log_cap;
 };
 
+// Tensor maps of the TMA-staged tiles: 3-D (x, y, plane) views of the bed,
+// the two state buffers (Q rows 1.. and alt) and the stage-1 increment.
+struct TileMaps {
+    CUtensorMap bed, qs, alt, inc;
+};
+
 enum TMode : int { T_S1 = 1, T_S2 = 2 };
 constexpr float kNearDry = 1.0e-3f;
+// try_wait polls of an mbarrier before a stage gives up (each poll may block
+// for a hardware-defined interval): a bound, so that a copy that never
+// completes ends in an error flag instead of a hang
+constexpr int kMaxBarrierPolls = 1 << 22;
 
-template <class F, int TX, int TY>
+// Shared-memory layout of a tile. Plain loads stage the tile and its 2-cell
+// halo as (TX + 4) x (TY + 4) per row; TMA boxes start 4 columns to the
+// left (a box's first x coordinate must be a multiple of 16 bytes) and are
+// TX + 8 wide, so a halo cell lx sits at column lx + XO.
+template <class F, int TX, int TY, bool TMA = false>
 struct TShape {
-    static constexpr int G = 2, RW = TX + 2 * G, RH = TY + 2 * G;
+    static constexpr int G = 2, RH = TY + 2 * G;
+    static constexpr int RWS = TMA ? TX + 8 : TX + 2 * G;    // stored row width
+    static constexpr int XO = TMA ? 2 : 0;                    // column of halo cell 0
+    static constexpr int RW = TX + 2 * G;                     // halo cells per row
     static constexpr int NFC = 3 * F::ne + 2;     // flux, D+, D- of the evolved rows, h*_L, h*_R
     static constexpr int NT = TX * TY;
-    static constexpr size_t q_elems = size_t(F::nq) * RH * RW;
+    static constexpr size_t pad32(size_t n) { return (n + 31) / 32 * 32; }   // 128-byte blocks
+    static constexpr size_t q_elems = pad32(size_t(F::nq) * RH * RWS);
+    static constexpr size_t inc_elems = TMA ? pad32(size_t(F::ne) * RH * RWS) : 0;   // stage-2 TMA staging
     static constexpr size_t fx_elems = size_t(TY) * (TX + 1) * NFC;
     static constexpr size_t fy_elems = size_t(TY + 1) * TX * NFC;
-    static constexpr size_t smem_bytes = (q_elems + fx_elems + fy_elems) * sizeof(float);
+    // TMA boxes land on 128-byte boundaries: the kernel rounds the dynamic
+    // shared-memory base up, which the extra 128 bytes cover
+    static constexpr size_t smem_bytes = (q_elems + inc_elems + fx_elems + fy_elems) * sizeof(float) + (TMA ? 128 : 0);
+    __host__ __device__ static constexpr unsigned box_bytes(int planes) { return unsigned(planes) * RH * RWS * sizeof(float); }
 };
+
+// --- TMA (cp.async.bulk.tensor) and mbarrier helpers, this CTA only -------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n"
+        " .reg .pred p;\n"
+        " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the barrier's phase; false when the polls ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
+    for (int it = 0; it < kMaxBarrierPolls; ++it)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+// One 3-D box of a tensor map (x, y, plane) into this CTA's shared memory,
+// completing on `bar`. x must be a multiple of 4 floats (16 bytes).
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
 
 __device__ __forceinline__ float mmf(float a, float b) {
     if (a * b <= 0.0f) return 0.0f;
@@ -177,12 +246,22 @@ __device__ __forceinline__ void implicit_increment(typename M::VQ const& q0, typ
     for (int n = 0; n < nq; ++n) dq(n, 0) = isfinite(b[n]) ? b[n] : R(0);
 }
 
-// One RK stage of the generic FP32 form over a TX x TY tile.
-template <class F, int MODE, bool WB, bool IMPL, int TX, int TY>
+// Models that provide a structured point-implicit solve (the same linear
+// system, solved by blocks) use it in the FP32 kernels.
+template <class M, class = void> struct has_block_implicit : std::false_type {};
+template <class M>
+struct has_block_implicit<M, std::void_t<decltype(&M::zb_implicit_increment)>> : std::true_type {};
+
+// One RK stage of the generic FP32 form over a TX x TY tile. TMA: the tile
+// and its halo are staged by one thread with cp.async.bulk.tensor copies of
+// the bed, state and (stage 2) increment boxes, completing on an mbarrier
+// (the tensor maps cover this GPU's own buffers only); otherwise by plain
+// coalesced loads of every thread.
+template <class F, int MODE, bool WB, bool IMPL, int TX, int TY, bool TMA>
 __global__ void __launch_bounds__(TX * TY)
-k32t_stage(TileParams<F::np> L, TileBufs B, int order2)
+k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ TileMaps maps)
 {
-    using Sh = TShape<F, TX, TY>;
+    using Sh = TShape<F, TX, TY, TMA>;
     using M = typename F::M32;
     using N = typename F::N32;
     using VQ = typename M::VQ;
@@ -191,13 +270,19 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2)
     using VN = typename M::VN;
     using VX = typename M::VX;
     constexpr int nq = F::nq, ne = F::ne;
-    constexpr int G = Sh::G, RW = Sh::RW, RH = Sh::RH, NFC = Sh::NFC, NT = Sh::NT;
+    constexpr int G = Sh::G, RW = Sh::RW, RWS = Sh::RWS, XO = Sh::XO, RH = Sh::RH, NFC = Sh::NFC, NT = Sh::NT;
 
-    extern __shared__ __align__(16) float tsm[];
-    float* sQ = tsm;                                  // [nq][RH][RW]: b, eta, q_2..
-    float* sFx = sQ + Sh::q_elems;                    // [TY][TX+1][NFC]
+    extern __shared__ __align__(128) float tsm_raw[];
+    float* tsm = TMA ? reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(tsm_raw) + 127) & ~uintptr_t(127))
+                     : tsm_raw;
+    float* sQ = tsm;                                  // [nq][RH][RWS]: b, eta, q_2..
+    float* sI = sQ + Sh::q_elems;                     // TMA, stage 2: [ne][RH][RWS] increment
+    float* sFx = sI + Sh::inc_elems;                  // [TY][TX+1][NFC]
     float* sFy = sFx + Sh::fx_elems;                  // [TY+1][TX][NFC]
     __shared__ double red[2 * ((NT + 31) / 32)];
+    __shared__ __align__(8) uint64_t tbar;
+    // halo-local cell (lx, ly) of row n
+    auto sq = [&](int n, int lx, int ly) -> float& { return sQ[(n * RH + ly) * RWS + lx + XO]; };
 
     const int tid = threadIdx.x;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -219,17 +304,44 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2)
     VA azero{};
 
     // 1. tile + halo: b, eta, rest (stage 2: the stage state X + inc1)
-    for (int k = tid; k < RW * RH; k += NT) {
-        const int lx = k % RW, ly = k / RW;
-        const int gi = x0 - G + lx, gj = y0 - G + ly;
-        if (gi >= 0 && gi < nx && gj >= 0 && gj < ny) {
-            const long long c = (long long)gj * nx + gi;
-            sQ[ly * RW + lx] = B.bed[c];
+    if constexpr (TMA) {
+        if (tid == 0) {
+            mbar_init(&tbar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            constexpr unsigned bytes = Sh::box_bytes(nq) + (MODE == T_S2 ? Sh::box_bytes(ne) : 0u);
+            mbar_expect_tx(&tbar, bytes);
+            const int bx = x0 - G - XO, by = y0 - G;        // bx is a multiple of 4 (TX is)
+            tma_load_3d(sQ, &maps.bed, bx, by, 0, &tbar);
+            tma_load_3d(sQ + RH * RWS, parity ? &maps.alt : &maps.qs, bx, by, 0, &tbar);
+            if constexpr (MODE == T_S2) tma_load_3d(sI, &maps.inc, bx, by, 0, &tbar);
+        }
+        const bool done = mbar_wait(&tbar, 0);
+        if (__syncthreads_or(!done)) {
+            // the copies never completed: flag the run (its results are
+            // invalid), stop it, wait (bounded) for copies still in flight
+            if (tid == 0) atomicOr(&st->flags, zfv::kFlagDeviceWait | zfv::kFlagDone);
+            mbar_wait(&tbar, 0);
+            return;
+        }
+        if constexpr (MODE == T_S2) {
+            for (int k = tid; k < ne * RH * RWS; k += NT) sQ[RH * RWS + k] += sI[k];
+        }
+    } else {
+        for (int k = tid; k < RW * RH; k += NT) {
+            const int lx = k % RW, ly = k / RW;
+            const int gi = x0 - G + lx, gj = y0 - G + ly;
+            if (gi >= 0 && gi < nx && gj >= 0 && gj < ny) {
+                const long long c = (long long)gj * nx + gi;
+                sq(0, lx, ly) = B.bed[c];
 #pragma unroll
-            for (int n = 1; n < nq; ++n) {
-                float v = X[(n - 1) * plane + c];
-                if constexpr (MODE == T_S2) v = v + B.inc[(n - 1) * plane + c];
-                sQ[(n * RH + ly) * RW + lx] = v;
+                for (int n = 1; n < nq; ++n) {
+                    float v = X[(n - 1) * plane + c];
+                    if constexpr (MODE == T_S2) v = v + B.inc[(n - 1) * plane + c];
+                    sq(n, lx, ly) = v;
+                }
             }
         }
     }
@@ -249,7 +361,7 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2)
             if (mx < 0 || mx >= RW || my < 0 || my >= RH) continue;   // excluded by zfv_create
             VQ qi;
 #pragma unroll
-            for (int n = 0; n < nq; ++n) qi(n, 0) = sQ[(n * RH + my) * RW + mx];
+            for (int n = 0; n < nq; ++n) qi(n, 0) = sq(n, mx, my);
             const float eta_i = qi(1, 0);
             qi(1, 0) = eta_i - qi(0, 0);
             VX Xi{}, Xg{};
@@ -263,15 +375,15 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2)
             const VQ qg = M::boundary_conditions(L.bc_tag[gm.bc_side], qi, ai, nh, Xg, float(time), L.fdx);
             // keep the mirrored eta bit for bit when the BC keeps depth and bed
             const float eta_g = (qg(1, 0) == qi(1, 0) && qg(0, 0) == qi(0, 0)) ? eta_i : qg(1, 0) + qg(0, 0);
-            sQ[ly * RW + lx] = qg(0, 0);
-            sQ[(RH + ly) * RW + lx] = eta_g;
+            sq(0, lx, ly) = qg(0, 0);
+            sq(1, lx, ly) = eta_g;
 #pragma unroll
-            for (int n = 2; n < nq; ++n) sQ[(n * RH + ly) * RW + lx] = qg(n, 0);
+            for (int n = 2; n < nq; ++n) sq(n, lx, ly) = qg(n, 0);
         }
         __syncthreads();
     }
 
-    auto at = [&](int n, int lx, int ly) { return sQ[(n * RH + ly) * RW + lx]; };
+    auto at = [&](int n, int lx, int ly) { return sq(n, lx, ly); };
 
     // reconstruction of cell (lx, ly) at its face on side s (+1 high, -1 low)
     // along direction D: b and eta with eta's slope = slope(h) + slope(b),
@@ -415,7 +527,8 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2)
                 VQ dq;
                 VX Xz{};
                 const VA a0 = M::update_aux_variables(q0, azero, p, float(time), Xz);
-                implicit_increment<M, float>(q0, a0, dt, p, Xz, dq);
+                if constexpr (has_block_implicit<M>::value) M::zb_implicit_increment(q0, a0, p, dt, dq);
+                else implicit_increment<M, float>(q0, a0, dt, p, Xz, dq);
 #pragma unroll
                 for (int n = 1; n < nq; ++n) d[n - 1] = d[n - 1] + dq(n, 0);
             }

@@ -46,6 +46,7 @@ static_assert(sizeof(DevState) == 128, "DevState layout");
 constexpr unsigned kFlagNonfiniteDt = 1u;
 constexpr unsigned kFlagMoodRedo = 2u;
 constexpr unsigned kFlagDone = 4u;
+constexpr unsigned kFlagDeviceWait = 8u;   // a bounded device-side wait gave up: the step is invalid
 
 // ZoomyAmr::UpdateState's per-cell body (ZoomyAmr.cpp:310-331).
 template <class Model, class R, class PL>

@@ -213,7 +213,8 @@ struct SME
             S(mom(d), 0) = g * e * h - fb;
             for (int i = 1; i <= LEVEL; ++i) {
                 R cs = R(0);
-                for (int j = 1; j <= LEVEL; ++j) cs = cs + R(K::C(i, j)) * Q(mnt(d, j), 0);
+                for (int j = 1; j <= LEVEL; ++j)
+                    if (K::C(i, j) != 0.0) cs = cs + R(K::C(i, j)) * Q(mnt(d, j), 0);
                 S(mnt(d, i), 0) = -R(2 * i + 1) * (fb + nu * (hinv * hinv) * cs);
             }
         }
@@ -260,11 +261,73 @@ struct SME
             J(mom(d) * na + i_hinv, 0) = -kb * ub;
             for (int i = 1; i <= LEVEL; ++i) {
                 R cs = R(0);
-                for (int j = 1; j <= LEVEL; ++j) cs = cs + R(K::C(i, j)) * Q(mnt(d, j), 0);
+                for (int j = 1; j <= LEVEL; ++j)
+                    if (K::C(i, j) != 0.0) cs = cs + R(K::C(i, j)) * Q(mnt(d, j), 0);
                 J(mnt(d, i) * na + i_hinv, 0) = -R(2 * i + 1) * (kb * ub + R(2) * nu * hinv * cs);
             }
         }
         return J;
+    }
+
+    // Build-side shortcut (not part of the printer's interface): the
+    // point-implicit step of make_rhs.H:429-509, (I - dt J) dq = dt S with
+    // J = dS/dQ at fixed aux, solved block by block. The bed and depth rows of
+    // J and S are zero (dq = 0 there) and the friction couples only the mean
+    // momentum and the moments of one direction, so the system splits into
+    // DIM blocks of 1 + LEVEL unknowns, each solved by elimination with
+    // partial pivoting. Non-finite results fall back to the explicit step
+    // dt S (or 0), as make_rhs.H:501-508. The FP32 kernels use it; the FP64
+    // form keeps the reference's full elimination for bitwise parity.
+    static PORTABLE_FN AMREX_FORCE_INLINE void zb_implicit_increment(VQ const& Q, VA const& Qaux, VP const& p,
+                                                                    R dt, VQ& dq) {
+        constexpr int nb = 1 + LEVEL;
+        const auto S = source(Q, Qaux, p, R(0), VX{});
+        const R nu = p(sme_nu, 0);
+        const R kh = (nu / p(sme_lambda, 0)) * Qaux(i_hinv, 0);
+        const R hh = Qaux(i_hinv, 0) * Qaux(i_hinv, 0);
+        dq(0, 0) = R(0);
+        dq(1, 0) = R(0);
+        for (int d = 0; d < DIM; ++d) {
+            R A[nb][nb], b[nb];
+            int row[nb];
+            for (int r = 0; r < nb; ++r) {
+                row[r] = (r == 0) ? mom(d) : mnt(d, r);
+                b[r] = dt * S(row[r], 0);
+                const R cr = R(2 * r + 1);
+                for (int c = 0; c < nb; ++c) {
+                    R j = -kh;
+                    if (r > 0 && c > 0 && K::C(r, c) != 0.0) j = j - nu * hh * R(K::C(r, c));
+                    A[r][c] = (r == c ? R(1) : R(0)) - dt * (cr * j);
+                }
+            }
+            bool ok = true;
+            for (int k = 0; k < nb && ok; ++k) {
+                int piv = k;
+                for (int r = k + 1; r < nb; ++r)
+                    if (std::abs(A[r][k]) > std::abs(A[piv][k])) piv = r;
+                if (!(std::abs(A[piv][k]) > R(0))) { ok = false; break; }
+                if (piv != k) {
+                    for (int c = 0; c < nb; ++c) { const R t = A[k][c]; A[k][c] = A[piv][c]; A[piv][c] = t; }
+                    const R t = b[k]; b[k] = b[piv]; b[piv] = t;
+                }
+                for (int r = k + 1; r < nb; ++r) {
+                    const R f = A[r][k] / A[k][k];
+                    for (int c = k; c < nb; ++c) A[r][c] = A[r][c] - f * A[k][c];
+                    b[r] = b[r] - f * b[k];
+                }
+            }
+            R x[nb];
+            for (int r = nb - 1; r >= 0 && ok; --r) {
+                R s = b[r];
+                for (int c = r + 1; c < nb; ++c) s = s - A[r][c] * x[c];
+                x[r] = s / A[r][r];
+                ok = ok && std::isfinite(x[r]);
+            }
+            for (int r = 0; r < nb; ++r) {
+                const R e = dt * S(row[r], 0);
+                dq(row[r], 0) = ok ? x[r] : (std::isfinite(e) ? e : R(0));
+            }
+        }
     }
 
     static PORTABLE_FN AMREX_FORCE_INLINE amrex::SmallMatrix<R, n_dof_q * DIM, 1>
@@ -411,8 +474,10 @@ struct SME
             for (int j = 1; j <= LEVEL; ++j) {
                 R c = (i == j) ? w : R(0);
                 for (int k = 1; k <= LEVEL; ++k) {
-                    d0 = d0 - R(K::A(i, j, k)) * (ga[j] * ga[k]);
-                    c = c + (R(2) * R(K::A(i, j, k)) + R(K::B(i, j, k))) * ga[k];
+                    // (the tables are compile-time constants: zero terms fold away)
+                    if (K::A(i, j, k) != 0.0) d0 = d0 - R(K::A(i, j, k)) * (ga[j] * ga[k]);
+                    if (2.0 * K::A(i, j, k) + K::B(i, j, k) != 0.0)
+                        c = c + R(2.0 * K::A(i, j, k) + K::B(i, j, k)) * ga[k];
                 }
                 r = r + std::abs(c);
             }
@@ -425,9 +490,10 @@ struct SME
                 for (int j = 1; j <= LEVEL; ++j) {
                     R cg = R(0), ct = (i == j) ? w : R(0);
                     for (int k = 1; k <= LEVEL; ++k) {
-                        e0 = e0 - R(K::A(i, j, k)) * (ga[j] * ta[k]);
-                        cg = cg + (R(K::A(i, j, k)) + R(K::B(i, j, k))) * ta[k];
-                        ct = ct + R(K::A(i, k, j)) * ga[k];
+                        if (K::A(i, j, k) != 0.0) e0 = e0 - R(K::A(i, j, k)) * (ga[j] * ta[k]);
+                        if (K::A(i, j, k) + K::B(i, j, k) != 0.0)
+                            cg = cg + R(K::A(i, j, k) + K::B(i, j, k)) * ta[k];
+                        if (K::A(i, k, j) != 0.0) ct = ct + R(K::A(i, k, j)) * ga[k];
                     }
                     s = s + std::abs(cg) + std::abs(ct);
                 }

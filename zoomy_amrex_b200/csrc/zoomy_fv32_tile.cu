@@ -4,11 +4,17 @@
 // and the hardware's approximate FP32 division and square root, like
 // zoomy_fv32.cu.
 //
-// Tile shapes (zfv_set_variant): 0 = 32 x 8 cells, 1 = 16 x 8, 2 = 32 x 4.
-// The shape changes the launch grid only; every shape computes the same
-// faces and updates in the same order, so results are identical.
+// Tile shapes (zfv_set_variant): 0 = 32 x 8 cells, 1 = 16 x 8, 2 = 32 x 4,
+// staged by plain loads; 3, 4, 5 = the same shapes staged by TMA
+// (cp.async.bulk.tensor boxes of the bed, state and increment planes, which
+// needs nx a multiple of 4 and 16-byte aligned buffers). The shape and the
+// staging change the launch grid and the copy engine only; every variant
+// computes the same faces and updates in the same order, so results are
+// identical.
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "zfv_internal.H"
@@ -19,9 +25,44 @@ using namespace zfvi;
 
 namespace zfv32t {
 
-constexpr int kTileVariants = 3;
-constexpr int kTileTX[kTileVariants] = {32, 16, 32};
-constexpr int kTileTY[kTileVariants] = {8, 8, 4};
+constexpr int kTileShapes = 3;
+constexpr int kTileVariants = 2 * kTileShapes;
+constexpr int kTileTX[kTileShapes] = {32, 16, 32};
+constexpr int kTileTY[kTileShapes] = {8, 8, 4};
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links the CUDA runtime only).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    return fn;
+}
+
+// A 3-D (nx, ny, planes) FP32 view with a (box_x, box_y, planes) box;
+// cells outside the view read as zero.
+int encode_planes(CUtensorMap* m, const float* base, int nx, int ny, int planes, int box_x, int box_y) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return fail(-3, "zfv_set_variant: cuTensorMapEncodeTiled is not available");
+    const cuuint64_t dims[3] = {cuuint64_t(nx), cuuint64_t(ny), cuuint64_t(planes)};
+    const cuuint64_t strides[2] = {cuuint64_t(nx) * sizeof(float), cuuint64_t(nx) * ny * sizeof(float)};
+    const cuuint32_t box[3] = {cuuint32_t(box_x), cuuint32_t(box_y), cuuint32_t(planes)};
+    const cuuint32_t elem[3] = {1, 1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, elem,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(-3, "cuTensorMapEncodeTiled failed (%d)", int(r));
+    return 0;
+}
 
 template <class F>
 struct RunnerTile final : Runner {
@@ -46,28 +87,56 @@ struct RunnerTile final : Runner {
         L.max_step = c.max_step; L.cfl_dimension = c.cfl_dimension; L.cfl_degree_factor = c.cfl_degree_factor;
     }
 
-    template <int V> using ShapeV = TShape<F, kTileTX[V], kTileTY[V]>;
+    template <int V, bool TMA> using ShapeV = TShape<F, kTileTX[V], kTileTY[V], TMA>;
+
+    // tensor maps of the last (Q, scratch) pair the TMA variants ran on
+    TileMaps maps{};
+    const void* maps_q = nullptr;
+    const char* maps_scratch = nullptr;
 
     int max_blocks() const {
         int m = 0;
-        for (int v = 0; v < kTileVariants; ++v)
+        for (int v = 0; v < kTileShapes; ++v)
             m = std::max(m, ((L.nx + kTileTX[v] - 1) / kTileTX[v]) * ((L.ny + kTileTY[v] - 1) / kTileTY[v]));
         return std::max(m, kReduceBlocksMax);
     }
 
-    template <int V, int MODE, bool WB, bool IMPL>
+    template <int V, int MODE, bool WB, bool IMPL, bool TMA>
     int set_smem1() {
-        return cuda_check(cudaFuncSetAttribute(k32t_stage<F, MODE, WB, IMPL, kTileTX[V], kTileTY[V]>,
+        return cuda_check(cudaFuncSetAttribute(k32t_stage<F, MODE, WB, IMPL, kTileTX[V], kTileTY[V], TMA>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               int(ShapeV<V>::smem_bytes)),
+                                               int(ShapeV<V, TMA>::smem_bytes)),
                           "cudaFuncSetAttribute (FP32 tile)");
     }
     template <int V, bool WB, bool IMPL>
-    int set_smem2() { return set_smem1<V, T_S1, WB, IMPL>() | set_smem1<V, T_S2, WB, IMPL>(); }
+    int set_smem2() {
+        return set_smem1<V, T_S1, WB, IMPL, false>() | set_smem1<V, T_S2, WB, IMPL, false>() |
+               set_smem1<V, T_S1, WB, IMPL, true>() | set_smem1<V, T_S2, WB, IMPL, true>();
+    }
     template <int V>
     int set_smem_v() {
         return set_smem2<V, false, false>() | set_smem2<V, false, true>() | set_smem2<V, true, false>() |
                set_smem2<V, true, true>();
+    }
+
+    // TMA needs 16-byte row and plane strides and 16-byte aligned planes
+    bool tma_ok(const void* Q) const {
+        return L.nx % 4 == 0 && (reinterpret_cast<uintptr_t>(Q) & 15) == 0;
+    }
+    int ensure_maps(const void* Q, const char* scratch) {
+        if (Q == maps_q && scratch == maps_scratch) return 0;
+        if (!tma_ok(Q)) return fail(-1, "zfv: the TMA tile variants need nx %% 4 == 0 and a 16-byte aligned state");
+        const int v = var - kTileShapes;
+        const int bw = kTileTX[v] + 8, bh = kTileTY[v] + 4;
+        const TileBufs B = bufs(Q, const_cast<char*>(scratch));
+        int rc = encode_planes(&maps.bed, B.bed, L.nx, L.ny, 1, bw, bh);
+        if (!rc) rc = encode_planes(&maps.qs, B.Qs, L.nx, L.ny, ne, bw, bh);
+        if (!rc) rc = encode_planes(&maps.alt, B.alt, L.nx, L.ny, ne, bw, bh);
+        if (!rc) rc = encode_planes(&maps.inc, B.inc, L.nx, L.ny, ne, bw, bh);
+        if (rc) { maps_q = nullptr; maps_scratch = nullptr; return rc; }
+        maps_q = Q;
+        maps_scratch = scratch;
+        return 0;
     }
 
     int setup() override {
@@ -125,30 +194,37 @@ struct RunnerTile final : Runner {
         return cuda_check(cudaGetLastError(), "zfv_total_mass launch (FP32 tile)");
     }
 
-    template <int V, bool WB, bool IMPL>
+    template <int V, bool WB, bool IMPL, bool TMA>
     void step_v(const TileBufs& B, int n, cudaStream_t s) {
         constexpr int TX = kTileTX[V], TY = kTileTY[V];
         const dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, 1);
-        const size_t sm = ShapeV<V>::smem_bytes;
+        const size_t sm = ShapeV<V, TMA>::smem_bytes;
         for (int k = 0; k < n; ++k) {
-            k32t_stage<F, T_S1, WB, IMPL, TX, TY><<<grid, TX * TY, sm, s>>>(L, B, 1);
-            k32t_stage<F, T_S2, WB, IMPL, TX, TY><<<grid, TX * TY, sm, s>>>(L, B, 1);
+            k32t_stage<F, T_S1, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 1, maps);
+            k32t_stage<F, T_S2, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 1, maps);
         }
     }
-    template <int V>
+    template <int V, bool TMA>
     void step_flags(const TileBufs& B, int n, cudaStream_t s) {
         const bool wb = h->cfg.well_balanced != 0, im = h->cfg.implicit_source != 0;
-        if (wb) { if (im) step_v<V, true, true>(B, n, s); else step_v<V, true, false>(B, n, s); }
-        else { if (im) step_v<V, false, true>(B, n, s); else step_v<V, false, false>(B, n, s); }
+        if (wb) { if (im) step_v<V, true, true, TMA>(B, n, s); else step_v<V, true, false, TMA>(B, n, s); }
+        else { if (im) step_v<V, false, true, TMA>(B, n, s); else step_v<V, false, false, TMA>(B, n, s); }
     }
 
     int evolve(void* Q, void* A, char* scratch, int n, cudaStream_t s) override {
         if (A) aux_bound = static_cast<double*>(A);
+        if (var >= kTileShapes) {
+            const int rc = ensure_maps(Q, scratch);
+            if (rc) return rc;
+        }
         const TileBufs B = bufs(Q, scratch);
         switch (var) {
-        case 0: step_flags<0>(B, n, s); break;
-        case 1: step_flags<1>(B, n, s); break;
-        default: step_flags<2>(B, n, s); break;
+        case 0: step_flags<0, false>(B, n, s); break;
+        case 1: step_flags<1, false>(B, n, s); break;
+        case 2: step_flags<2, false>(B, n, s); break;
+        case 3: step_flags<0, true>(B, n, s); break;
+        case 4: step_flags<1, true>(B, n, s); break;
+        default: step_flags<2, true>(B, n, s); break;
         }
         return cuda_check(cudaGetLastError(), "zfv_evolve launch (FP32 tile)");
     }
@@ -189,7 +265,11 @@ struct RunnerTile final : Runner {
     }
     int set_variant(int v, cudaStream_t) override {
         if (v < 0 || v >= kTileVariants) return fail(-1, "zfv_set_variant: unknown tile shape %d", v);
+        if (v >= kTileShapes && L.nx % 4 != 0)
+            return fail(-1, "zfv_set_variant: the TMA tile variants need nx %% 4 == 0 (nx = %d)", L.nx);
         var = v;
+        maps_q = nullptr;      // re-encode for the new box
+        maps_scratch = nullptr;
         return 0;
     }
     int variant() const override { return var; }
@@ -208,3 +288,13 @@ Runner* make_runner_fp32_generic(zfv_handle* h) {
 }
 int fp32_tile_variants() { return zfv32t::kTileVariants; }
 }  // namespace zfvi
+
+extern "C" int zfv_generic_tile_variants(int* tx, int* ty, int* tma, int max_n) {
+    for (int v = 0; v < zfv32t::kTileVariants && v < max_n; ++v) {
+        const int s = v % zfv32t::kTileShapes;
+        if (tx) tx[v] = zfv32t::kTileTX[s];
+        if (ty) ty[v] = zfv32t::kTileTY[s];
+        if (tma) tma[v] = v >= zfv32t::kTileShapes;
+    }
+    return zfv32t::kTileVariants;
+}

@@ -4,13 +4,17 @@
     python -m zoomy_amrex_b200.profile_case fp64    [--n 3072] [--steps 3]
     python -m zoomy_amrex_b200.profile_case adjoint [--n 512]  [--steps 20] [--variant V]
     python -m zoomy_amrex_b200.profile_case amr     [--n 1024] [--steps 4]  [--variant V]
+    python -m zoomy_amrex_b200.profile_case sme64   [--n 1024] [--steps 3]
+    python -m zoomy_amrex_b200.profile_case sme32   [--n 1024] [--steps 3]  [--variant V]
 
 Each runs the benchmark's wet/dry bump level (``workloads.bump_workload_*``)
 on an n x n grid: the FP32 form as a batch of one with the given strip shape,
 the FP64 form through a Level, or the forward + backward of the FP64 adjoint
 with checkpoints every 20 steps, or (amr) the 3-level AMR hierarchy of a dam
 break over bumps on an n x n base grid (boxes 64^2, one CUDA graph per coarse
-step). The launches are the product's own; a
+step), or (sme64 / sme32) the shallow-moment level-2 benchmark level
+(``workloads.sme_workload_*``) on n x n in the FP64 plain form or the FP32
+chosen form (tile shape V). The launches are the product's own; a
 profiler selects them by kernel name (k32b_stage, k_stage, k_adj_face, ...).
 """
 from __future__ import annotations
@@ -20,7 +24,7 @@ import argparse
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("form", choices=["fp32", "fp64", "adjoint", "amr"])
+    ap.add_argument("form", choices=["fp32", "fp64", "adjoint", "amr", "sme64", "sme32"])
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--variant", type=int, default=None)
@@ -47,6 +51,19 @@ def main(argv=None):
         n, steps = a.n or 3072, a.steps or 3
         Q0, A0 = bump_workload_fields(n)
         lev = Level(bump_workload_config(n), Q0, A0)
+        lev.begin()
+        lev.evolve(steps)
+        st = lev.status()
+        lev.close()
+    elif a.form in ("sme64", "sme32"):
+        from .level import Level
+        from .workloads import sme_workload_config, sme_workload_fields
+        n, steps = a.n or 1024, a.steps or 3
+        Q0, A0 = sme_workload_fields(n)
+        cfg = sme_workload_config(n)
+        if a.form == "sme32":
+            cfg.precision = ZFV_PREC_FP32
+        lev = Level(cfg, Q0, A0, variant=a.variant if a.form == "sme32" else None)
         lev.begin()
         lev.evolve(steps)
         st = lev.status()
