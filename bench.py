@@ -499,46 +499,67 @@ def adjoint_bench(local, n=1024, steps=200, every=20, n_dirs=32, eps=1e-6, seed=
     torch.cuda.synchronize()
     ms_bwd = b0.elapsed_time(b1)
     gc.enable()
-    gq, gnm = q.grad.detach(), float(nm.grad)
-    # central differences on seeded directions (wet cells only for h, hu, hv:
-    # a dry cell's depth cannot be perturbed both ways)
-    wet = torch.from_numpy((Q0[1] > 0).astype(np.float64)).to(dev)
 
-    def fd_errors(n, e):
-        out = []
-        for k in range(n):
-            V = torch.from_numpy(rng.standard_normal(Q0.shape) * 1e-2).to(dev)
+    def checks(x0, gq, gnm, wet, n, crng):
+        """Central differences and the Taylor remainder of L at x0 along
+        seeded directions over (b, h, hu, hv, n_m); h, hu, hv perturbed on
+        wet cells only (a dry cell's depth cannot be perturbed both ways)."""
+        def direction():
+            V = torch.from_numpy(crng.standard_normal(Q0.shape) * 1e-2).to(dev)
             V[1:] *= wet
-            v_nm = float(rng.standard_normal() * 1e-3)
-            lp = float(loss_of(forward_only(base + e * V, A, cfg, steps, n_m=0.03 + e * v_nm)))
-            lm = float(loss_of(forward_only(base - e * V, A, cfg, steps, n_m=0.03 - e * v_nm)))
-            fd = (lp - lm) / (2 * e)
-            an = float((gq * V).sum()) + gnm * v_nm
-            out.append(abs(fd - an) / max(abs(fd), abs(an), 1e-300))
-        return out
+            return V, float(crng.standard_normal() * 1e-3)
 
-    errs = fd_errors(n_dirs, eps)
-    # the scheme is piecewise smooth (minmod switches, wet/dry): the gap to the
-    # derivative comes from switches crossed inside +-eps and shrinks with eps
-    sweep = {f"{e:.0e}": float(np.median(fd_errors(8, e))) for e in (1e-8, 1e-10)}
-    # Taylor test on the same seeded directions: the remainder
-    # |L(x + e d) - L(x) - e g.d| of a continuous piecewise-smooth map falls as
-    # e^2 (a kink inside +-e adds at most e times its slope jump and is
-    # crossed with probability ~e); its slope over e = 1e-2 .. 1e-5
-    L0 = float(loss_of(forward_only(base, A, cfg, steps)))
-    epss = [1e-2, 1e-3, 1e-4, 1e-5, 1e-6, 1e-7]
-    trng = np.random.default_rng(seed + 1)
-    rem = np.zeros((n_dirs, len(epss)))
-    for k in range(n_dirs):
-        V = torch.from_numpy(trng.standard_normal(Q0.shape) * 1e-2).to(dev)
-        V[1:] *= wet
-        v_nm = float(trng.standard_normal() * 1e-3)
-        gd = float((gq * V).sum()) + gnm * v_nm
-        for e, ee in enumerate(epss):
-            Le = float(loss_of(forward_only(base + ee * V, A, cfg, steps, n_m=0.03 + ee * v_nm)))
-            rem[k, e] = abs(Le - L0 - ee * gd)
-    med = np.median(rem, axis=0)
-    taylor_slope = float(np.polyfit(np.log10(epss[:4]), np.log10(med[:4]), 1)[0])
+        def fd_errors(k, e):
+            out = []
+            for _ in range(k):
+                V, v_nm = direction()
+                lp = float(loss_of(forward_only(x0 + e * V, A, cfg, steps, n_m=0.03 + e * v_nm)))
+                lm = float(loss_of(forward_only(x0 - e * V, A, cfg, steps, n_m=0.03 - e * v_nm)))
+                fd = (lp - lm) / (2 * e)
+                an = float((gq * V).sum()) + gnm * v_nm
+                out.append(abs(fd - an) / max(abs(fd), abs(an), 1e-300))
+            return out
+
+        errs = fd_errors(n, eps)
+        sweep = {f"{e:.0e}": float(np.median(fd_errors(8, e))) for e in (1e-8, 1e-10)}
+        # Taylor remainder |L(x + e d) - L(x) - e g.d|: e^2 for a continuous
+        # piecewise-smooth map at a point off its kinks (a kink inside +-e adds
+        # at most e times its slope jump and is crossed with probability ~e)
+        L0 = float(loss_of(forward_only(x0, A, cfg, steps)))
+        epss = [1e-2, 1e-3, 1e-4, 1e-5, 1e-6, 1e-7]
+        rem = np.zeros((n, len(epss)))
+        for k in range(n):
+            V, v_nm = direction()
+            gd = float((gq * V).sum()) + gnm * v_nm
+            for e, ee in enumerate(epss):
+                Le = float(loss_of(forward_only(x0 + ee * V, A, cfg, steps, n_m=0.03 + ee * v_nm)))
+                rem[k, e] = abs(Le - L0 - ee * gd)
+        med = np.median(rem, axis=0)
+        slope = float(np.polyfit(np.log10(epss[:4]), np.log10(med[:4]), 1)[0])
+        return ({"directions": n, "eps": eps, "max_rel_err": max(errs), "median_rel_err": float(np.median(errs)),
+                 "median_rel_err_smaller_eps": sweep},
+                {"directions": n, "eps": epss, "median_remainder": [float(v) for v in med],
+                 "slope_1e-2_to_1e-5": slope})
+
+    # at the benchmark's own start (a lake at rest over wet and dry cells):
+    # its zero momenta and near-flat bed stretches sit on minmod kinks, and
+    # the wet/dry switches are jumps, so differences converge slowly there
+    fd_wd, taylor_wd = checks(base, q.grad.detach(), float(nm.grad),
+                              torch.from_numpy((Q0[1] > 0).astype(np.float64)).to(dev), 8,
+                              np.random.default_rng(seed + 1))
+    # at a generic point of a fully wet level (0.6 m more depth, N(0, 1e-3^2)
+    # noise on b, h, hu, hv): off the kinks, where the map is differentiable
+    nrng = np.random.default_rng(seed + 2)
+    Qg = Q0.copy()
+    Qg[1] += 0.6
+    for r in range(4):
+        Qg[r] += 1e-3 * nrng.standard_normal(Q0[0].shape)
+    xg = torch.from_numpy(Qg).to(dev)
+    qg = xg.clone().requires_grad_(True)
+    nmg = torch.tensor(0.03, dtype=torch.float64, device=dev, requires_grad=True)
+    loss_of(evolve_differentiable(qg, nmg, A, cfg, steps, checkpoint_every=every)).backward()
+    fd_g, taylor_g = checks(xg, qg.grad.detach(), float(nmg.grad), torch.ones_like(xg[0]), n_dirs,
+                            np.random.default_rng(seed + 3))
     # torch autograd of the tensor restatement (whose forward is the CUDA
     # forward bit for bit, so both differentiate the same branches) at 256^2,
     # 200 steps, checkpointed
@@ -566,14 +587,13 @@ def adjoint_bench(local, n=1024, steps=200, every=20, n_dirs=32, eps=1e-6, seed=
             "steps": steps, "checkpoint_every": every,
             "ms_forward": ms_fwd, "ms_forward_with_checkpoints": ms_fwd_ck, "ms_backward": ms_bwd,
             "adj_over_fwd": ms_bwd / ms_fwd,
-            "fd": {"directions": n_dirs, "eps": eps, "max_rel_err": max(errs),
-                   "median_rel_err": float(np.median(errs)),
-                   "median_rel_err_smaller_eps": sweep,
-                   "note": "directions over (b, h, hu, hv, n_m); h, hu, hv perturbed on wet cells"},
-            "taylor": {"directions": n_dirs, "eps": epss, "median_remainder": [float(v) for v in med],
-                       "slope_1e-2_to_1e-5": taylor_slope,
-                       "note": "|L(x+e d) - L(x) - e g.d| on seeded directions; slope 2 = the gradient is the "
-                               "derivative of the piecewise-smooth map"},
+            "fd": dict(fd_g, point="fully wet level (+0.6 m), N(0, 1e-3^2) noise on b, h, hu, hv"),
+            "taylor": dict(taylor_g, point="fully wet level (+0.6 m), N(0, 1e-3^2) noise on b, h, hu, hv",
+                           note="|L(x+e d) - L(x) - e g.d| on seeded directions over (b, h, hu, hv, n_m); "
+                                "slope 2 = the gradient is the derivative of the piecewise-smooth map"),
+            "fd_lake_at_rest_wetdry": dict(fd_wd, note="the benchmark's start: on minmod kinks, wet/dry jumps"),
+            "taylor_lake_at_rest_wetdry": dict(taylor_wd, note="the benchmark's start: on minmod kinks, "
+                                                               "wet/dry jumps"),
             "torch_autograd": {"case": f"{m}x{m}, {ms} steps, checkpoints every {every}",
                                "forward_bitwise": fwd_bitwise, "max_rel_err_state": ag_err,
                                "rel_err_n_m": ag_nm}}

@@ -205,21 +205,30 @@ def test_adjoint_equals_torch_autograd_at_benchmark_scale(cuda):
 
 
 def test_adjoint_taylor_remainder_is_second_order(cuda):
-    """Taylor test of x -> L(Q_T(x)) on a fully wet level (the benchmark's
-    bumps and hump with 0.6 m more depth everywhere, Manning implicit, WB, walls): the remainder
-    |L(x + eps d) - L(x) - eps g.d| falls as eps^2 on seeded directions over
-    (b, h, hu, hv). The map is piecewise smooth (minmod, the max wave speed),
-    and a kink crossed inside +-eps adds at most eps times its slope jump
-    with probability ~eps, so the slope stays 2. (With dry cells the discrete
-    map also has jumps, e.g. the friction Jacobian's Heaviside at
-    h = h_floor, and the remainder falls more slowly.)"""
+    """Taylor test of x -> L(Q_T(x)) at a generic point of a fully wet level
+    (the benchmark's bumps and hump with 0.6 m more depth everywhere,
+    N(0, 1e-3^2) seeded noise on b, h, hu and hv; Manning implicit, WB,
+    walls): the remainder |L(x + eps d) - L(x) - eps g.d| falls as eps^2 on
+    seeded directions over (b, h, hu, hv). The map is continuous and
+    piecewise smooth (minmod, the hydrostatic max(b_L, b_R), the Rusanov and
+    CFL maxima); a kink crossed inside +-eps adds at most eps times its slope
+    jump and is crossed with probability ~eps, so the slope stays 2 -- as
+    long as the base point is not itself on kinks. A lake at rest is: zero
+    momentum and near-flat stretches of the smooth bed put the minmod
+    arguments at (or within rounding of) zero, where no derivative exists
+    and the remainder falls only as eps; hence the noise. (With dry cells
+    the discrete map also has jumps, e.g. the friction Jacobian's Heaviside
+    at h = h_floor.)"""
     import torch
     from zoomy_amrex_b200.adjoint import evolve_differentiable, forward_only
     m, steps = 128, 100
     cfg, Q0, A0 = _bench_case(m)
     Q0 = Q0.copy()
     Q0[1] = Q0[1] + 0.6                                  # every cell wet, the hump kept
-    assert Q0[1].min() >= 0.6
+    nrng = np.random.default_rng(13)
+    for r in range(4):                                   # off the kinks of the lake at rest
+        Q0[r] += 1e-3 * nrng.standard_normal((m, m))
+    assert Q0[1].min() >= 0.59
     rng = np.random.default_rng(12)
     eta_obs = torch.from_numpy(Q0[0] + Q0[1] + 0.01 * rng.standard_normal((m, m))).cuda()
     A = torch.from_numpy(A0).cuda()

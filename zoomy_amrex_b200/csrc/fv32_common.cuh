@@ -101,6 +101,15 @@ __device__ __forceinline__ void manning_implicit(T h, T u, T v, T hinv, T dt, T 
     dv = x1;
 }
 
+// A near-dry cell at rest with no source: u = v = 0 and no slope forcing
+// (ex = ey = 0) or no depth. manning_implicit then returns exactly +0 in
+// both rows (ux = uy = 0, sp = 0, det = 1 and x0 = 0 - (+-0) = +0), so the
+// FP64 solve can be skipped: dry cells are a tenth of a wet/dry level, and a
+// warp with one of them would otherwise run the FP64 path.
+__device__ __forceinline__ bool rest_without_source(float h, float u, float v, const Params& L) {
+    return u == 0.0f && v == 0.0f && (h == 0.0f || (L.exd == 0.0 && L.eyd == 0.0));
+}
+
 enum Mode { S1 = 1, S2 = 2 };
 
 }  // namespace zfv32

@@ -11,6 +11,9 @@
 //      asynchronous copies issued at the top of each row;
 //   2  the stage-2 kernel is capped at 128 registers (4 blocks of 128
 //      threads per SM instead of 3, at the cost of some spilling).
+// (Holding both stages to 5 or 6 blocks per SM, at most 102 / 85
+// registers, and unrolling the paired row loop by 4 were measured slower at
+// 4096^2 -- spilling and instruction-cache misses -- and are not compiled.)
 // Short strips (4 or 2 rows per warp) spend more on the y halo but finish a
 // unit sooner: levels of a few million cells (AMR levels, ensemble boxes)
 // fill the GPU for about one wave, so a launch there lasts about as long as

@@ -275,9 +275,10 @@ __device__ __forceinline__ void sweep_strip(const float* __restrict__ bed, const
             } else {
                 const float he = h + inc_e, ue = w1.u + inc_u, ve = w1.v + inc_v;
                 if (he < kNearDry) {
-                    double du, dv;
-                    manning_implicit<double>(double(he), double(ue), double(ve), double(hinv), dtd,
-                                             L.gd, L.exd, L.eyd, L.nmd, L.hfloord, du, dv);
+                    double du = 0.0, dv = 0.0;
+                    if (!rest_without_source(he, ue, ve, L))
+                        manning_implicit<double>(double(he), double(ue), double(ve), double(hinv), dtd,
+                                                 L.gd, L.exd, L.eyd, L.nmd, L.hfloord, du, dv);
                     inc_u += float(du); inc_v += float(dv);
                 } else {
                     float du, dv;

@@ -324,9 +324,11 @@ __device__ __forceinline__ void sweep_strip2(const float* __restrict__ bed, cons
 #pragma unroll
                     for (int k = 0; k < 2; ++k) {
                         if (hh[k] < kNearDry) {
-                            double a, b;
-                            manning_implicit<double>(double(hh[k]), double(uu[k]), double(vv[k]), double(hi[k]),
-                                                     dtd, L.gd, L.exd, L.eyd, L.nmd, L.hfloord, a, b);
+                            double a = 0.0, b = 0.0;
+                            if (!rest_without_source(hh[k], uu[k], vv[k], L))
+                                manning_implicit<double>(double(hh[k]), double(uu[k]), double(vv[k]),
+                                                         double(hi[k]), dtd, L.gd, L.exd, L.eyd, L.nmd,
+                                                         L.hfloord, a, b);
                             du[k] = float(a); dv[k] = float(b);
                         } else {
                             manning_implicit<float>(hh[k], uu[k], vv[k], hi[k], dt, L.g, L.ex, L.ey, L.nm,
