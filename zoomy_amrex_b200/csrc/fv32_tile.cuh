@@ -198,31 +198,34 @@ __device__ __forceinline__ void implicit_increment(typename M::VQ const& q0, typ
             A[r][c] = (r == c ? R(1) : R(0)) - dt * t;
         }
     }
+    // Constant trip counts (ranges are guards), selects for row swaps and no
+    // early exit keep the matrix in registers (see implicit_source_cell);
+    // after a failed pivot the values are discarded for the fallback.
     bool ok = true;
 #pragma unroll
     for (int k = 0; k < nq; ++k) {
-        if (!ok) break;
         int piv = k;
         R best = fabs(A[k][k]);
 #pragma unroll
-        for (int r = k + 1; r < nq; ++r)
-            if (fabs(A[r][k]) > best) { best = fabs(A[r][k]); piv = r; }
-        if (!(best > R(0)) || !isfinite(best)) { ok = false; break; }
-        if (piv != k) {
+        for (int r = 0; r < nq; ++r)
+            if (r > k && fabs(A[r][k]) > best) { best = fabs(A[r][k]); piv = r; }
+        ok = ok && (best > R(0)) && isfinite(best);
 #pragma unroll
-            for (int r = k + 1; r < nq; ++r) {
-                if (r == piv) {
+        for (int r = 0; r < nq; ++r) {
+            if (r > k && r == piv) {
 #pragma unroll
-                    for (int c = k; c < nq; ++c) { R t = A[k][c]; A[k][c] = A[r][c]; A[r][c] = t; }
-                    R t = b[k]; b[k] = b[r]; b[r] = t;
-                }
+                for (int c = 0; c < nq; ++c)
+                    if (c >= k) { R t = A[k][c]; A[k][c] = A[r][c]; A[r][c] = t; }
+                R t = b[k]; b[k] = b[r]; b[r] = t;
             }
         }
 #pragma unroll
-        for (int r = k + 1; r < nq; ++r) {
+        for (int r = 0; r < nq; ++r) {
+            if (r <= k) continue;
             const R f = A[r][k] / A[k][k];
 #pragma unroll
-            for (int c = k; c < nq; ++c) A[r][c] -= f * A[k][c];
+            for (int c = 0; c < nq; ++c)
+                if (c >= k) A[r][c] -= f * A[k][c];
             b[r] -= f * b[k];
         }
     }
@@ -232,9 +235,10 @@ __device__ __forceinline__ void implicit_increment(typename M::VQ const& q0, typ
         for (int r = nq - 1; r >= 0; --r) {
             R s = R(0);
 #pragma unroll
-            for (int c = r + 1; c < nq; ++c) s += A[r][c] * x[c];
+            for (int c = 0; c < nq; ++c)
+                if (c > r) s += A[r][c] * x[c];
             x[r] = (b[r] - s) / A[r][r];
-            if (!isfinite(x[r])) { ok = false; break; }
+            ok = ok && isfinite(x[r]);
         }
         if (ok) {
 #pragma unroll
@@ -520,7 +524,9 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
 #pragma unroll
                 for (int n = 2; n < nq; ++n) q64(n, 0) = double(at(n, lx, ly)) + double(d[n - 1]);
                 a64 = M64::update_aux_variables(q64, a64, p64, time, X64);
-                implicit_increment<M64, double>(q64, a64, dtd, p64, X64, dq64);
+                // the structured solve keeps this rare branch's registers small
+                if constexpr (has_block_implicit<M64>::value) M64::zb_implicit_increment(q64, a64, p64, dtd, dq64);
+                else implicit_increment<M64, double>(q64, a64, dtd, p64, X64, dq64);
 #pragma unroll
                 for (int n = 1; n < nq; ++n) d[n - 1] = float(double(d[n - 1]) + dq64(n, 0));
             } else {

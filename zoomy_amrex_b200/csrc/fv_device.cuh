@@ -185,32 +185,39 @@ __device__ __forceinline__ void implicit_source_cell(typename ModelTypes<Model>:
             M[r][c] = (r == c ? R(1.0) : R(0.0)) - dt * t;
         }
     }
+    // Register-resident elimination: every loop has a constant trip count
+    // (inner ranges such as c >= k are guards, not bounds, so the compiler
+    // unrolls inner loops before outer ones and every index is a constant),
+    // rows are swapped by selecting through the unrolled rows, and there is
+    // no early exit: once a pivot fails, the remaining arithmetic runs on
+    // values that are then discarded for the explicit fallback, as the
+    // reference's early exit discards them. The operations on the kept
+    // values are the reference's, in its order.
     bool ok = true;
 #pragma unroll
     for (int k = 0; k < nq; ++k) {
-        if (!ok) break;
         int piv = k;
         R best = fabs(M[k][k]);
 #pragma unroll
-        for (int r = k + 1; r < nq; ++r)
-            if (fabs(M[r][k]) > best) { best = fabs(M[r][k]); piv = r; }
-        if (!(best > R(0.0)) || !isfinite(best)) { ok = false; break; }
-        if (piv != k) {
-            // register-resident row swap: select through the unrolled rows
+        for (int r = 0; r < nq; ++r)
+            if (r > k && fabs(M[r][k]) > best) { best = fabs(M[r][k]); piv = r; }
+        ok = ok && (best > R(0.0)) && isfinite(best);
 #pragma unroll
-            for (int r = k + 1; r < nq; ++r) {
-                if (r == piv) {
+        for (int r = 0; r < nq; ++r) {
+            if (r > k && r == piv) {
 #pragma unroll
-                    for (int c = k; c < nq; ++c) { R t = M[k][c]; M[k][c] = M[r][c]; M[r][c] = t; }
-                    R t = b[k]; b[k] = b[r]; b[r] = t;
-                }
+                for (int c = 0; c < nq; ++c)
+                    if (c >= k) { R t = M[k][c]; M[k][c] = M[r][c]; M[r][c] = t; }
+                R t = b[k]; b[k] = b[r]; b[r] = t;
             }
         }
 #pragma unroll
-        for (int r = k + 1; r < nq; ++r) {
+        for (int r = 0; r < nq; ++r) {
+            if (r <= k) continue;
             const R f = M[r][k] / M[k][k];
 #pragma unroll
-            for (int c = k; c < nq; ++c) M[r][c] -= f * M[k][c];
+            for (int c = 0; c < nq; ++c)
+                if (c >= k) M[r][c] -= f * M[k][c];
             b[r] -= f * b[k];
         }
     }
@@ -220,9 +227,10 @@ __device__ __forceinline__ void implicit_source_cell(typename ModelTypes<Model>:
         for (int r = nq - 1; r >= 0; --r) {
             R s = R(0.0);
 #pragma unroll
-            for (int c = r + 1; c < nq; ++c) s += M[r][c] * dq[c];
+            for (int c = 0; c < nq; ++c)
+                if (c > r) s += M[r][c] * dq[c];
             dq[r] = (b[r] - s) / M[r][r];
-            if (!isfinite(dq[r])) { ok = false; break; }
+            ok = ok && isfinite(dq[r]);
         }
         if (ok) {
 #pragma unroll

@@ -163,8 +163,14 @@ __device__ __forceinline__ bool finish_step_units(double m, double s, double* re
     return true;
 }
 
+// Blocks per SM the register budget aims at: 3 for the 2-D shallow-water
+// tile; 2 for 1-D rows and for models with more than 4 unknowns, whose
+// point-implicit elimination (n^2 doubles) must stay in registers.
+template <class Model>
+constexpr int stage_min_blocks() { return (Model::dimension == 2 && Model::n_dof_q <= 4) ? 3 : 2; }
+
 template <class Model, class Numerics, int ORDER, int MODE, bool WB, bool IMPL, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY, (Model::dimension == 2) ? 3 : 2)
+__global__ void __launch_bounds__(TX * TY, stage_min_blocks<Model>())
 k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
         const double* __restrict__ qold, double* __restrict__ qout,
         LevelParams<double, Model::n_parameters> L, DevState* st,

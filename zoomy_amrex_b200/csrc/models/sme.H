@@ -196,6 +196,7 @@ struct SME
     // h times the bed velocity along d: h u(zeta = 0) = h w + sum_j h gamma_j.
     static PORTABLE_FN AMREX_FORCE_INLINE R bed_flux(VQ const& Q, int d) {
         R ub = Q(mom(d), 0);
+#pragma unroll
         for (int j = 1; j <= LEVEL; ++j) ub = ub + Q(mnt(d, j), 0);
         return ub;
     }
@@ -207,12 +208,15 @@ struct SME
         const R kb = nu / p(sme_lambda, 0);
         const R hinv = Qaux(i_hinv, 0);
         const R h = Q(1, 0);
+#pragma unroll
         for (int d = 0; d < DIM; ++d) {
             const R e = (d == 0) ? p(sme_ex, 0) : p(sme_ey, 0);
             const R fb = kb * (hinv * bed_flux(Q, d));
             S(mom(d), 0) = g * e * h - fb;
+#pragma unroll
             for (int i = 1; i <= LEVEL; ++i) {
                 R cs = R(0);
+#pragma unroll
                 for (int j = 1; j <= LEVEL; ++j)
                     if (K::C(i, j) != 0.0) cs = cs + R(K::C(i, j)) * Q(mnt(d, j), 0);
                 S(mnt(d, i), 0) = -R(2 * i + 1) * (fb + nu * (hinv * hinv) * cs);
@@ -231,16 +235,20 @@ struct SME
         const R kb = nu / p(sme_lambda, 0);
         const R hinv = Qaux(i_hinv, 0);
         const R kh = kb * hinv;
+#pragma unroll
         for (int d = 0; d < DIM; ++d) {
             const R e = (d == 0) ? p(sme_ex, 0) : p(sme_ey, 0);
             const int w = mom(d);
             J(w * n + 1, 0) = g * e;
             J(w * n + w, 0) = -kh;
+#pragma unroll
             for (int j = 1; j <= LEVEL; ++j) J(w * n + mnt(d, j), 0) = -kh;
+#pragma unroll
             for (int i = 1; i <= LEVEL; ++i) {
                 const int r = mnt(d, i);
                 const R ci = R(2 * i + 1);
                 J(r * n + w, 0) = -ci * kh;
+#pragma unroll
                 for (int j = 1; j <= LEVEL; ++j)
                     J(r * n + mnt(d, j), 0) = -ci * (kh + nu * (hinv * hinv) * R(K::C(i, j)));
             }
@@ -256,11 +264,14 @@ struct SME
         const R nu = p(sme_nu, 0);
         const R kb = nu / p(sme_lambda, 0);
         const R hinv = Qaux(i_hinv, 0);
+#pragma unroll
         for (int d = 0; d < DIM; ++d) {
             const R ub = bed_flux(Q, d);
             J(mom(d) * na + i_hinv, 0) = -kb * ub;
+#pragma unroll
             for (int i = 1; i <= LEVEL; ++i) {
                 R cs = R(0);
+#pragma unroll
                 for (int j = 1; j <= LEVEL; ++j)
                     if (K::C(i, j) != 0.0) cs = cs + R(K::C(i, j)) * Q(mnt(d, j), 0);
                 J(mnt(d, i) * na + i_hinv, 0) = -R(2 * i + 1) * (kb * ub + R(2) * nu * hinv * cs);
@@ -287,13 +298,19 @@ struct SME
         const R hh = Qaux(i_hinv, 0) * Qaux(i_hinv, 0);
         dq(0, 0) = R(0);
         dq(1, 0) = R(0);
+        // Every loop has a constant trip count (ranges are guards) and no
+        // early exit (after a failed pivot the values are discarded for the
+        // fallback), and rows are swapped by selecting through the unrolled
+        // rows, so the blocks stay in registers.
+#pragma unroll
         for (int d = 0; d < DIM; ++d) {
             R A[nb][nb], b[nb];
-            int row[nb];
+#pragma unroll
             for (int r = 0; r < nb; ++r) {
-                row[r] = (r == 0) ? mom(d) : mnt(d, r);
-                b[r] = dt * S(row[r], 0);
+                const int row = (r == 0) ? mom(d) : mnt(d, r);
+                b[r] = dt * S(row, 0);
                 const R cr = R(2 * r + 1);
+#pragma unroll
                 for (int c = 0; c < nb; ++c) {
                     R j = -kh;
                     if (r > 0 && c > 0 && K::C(r, c) != 0.0) j = j - nu * hh * R(K::C(r, c));
@@ -301,31 +318,47 @@ struct SME
                 }
             }
             bool ok = true;
-            for (int k = 0; k < nb && ok; ++k) {
+#pragma unroll
+            for (int k = 0; k < nb; ++k) {
                 int piv = k;
-                for (int r = k + 1; r < nb; ++r)
-                    if (std::abs(A[r][k]) > std::abs(A[piv][k])) piv = r;
-                if (!(std::abs(A[piv][k]) > R(0))) { ok = false; break; }
-                if (piv != k) {
-                    for (int c = 0; c < nb; ++c) { const R t = A[k][c]; A[k][c] = A[piv][c]; A[piv][c] = t; }
-                    const R t = b[k]; b[k] = b[piv]; b[piv] = t;
+                R best = std::abs(A[k][k]);
+#pragma unroll
+                for (int r = 0; r < nb; ++r)
+                    if (r > k && std::abs(A[r][k]) > best) { best = std::abs(A[r][k]); piv = r; }
+                ok = ok && (best > R(0));
+#pragma unroll
+                for (int r = 0; r < nb; ++r) {
+                    if (r > k && r == piv) {
+#pragma unroll
+                        for (int c = 0; c < nb; ++c) { const R t = A[k][c]; A[k][c] = A[r][c]; A[r][c] = t; }
+                        const R t = b[k]; b[k] = b[r]; b[r] = t;
+                    }
                 }
-                for (int r = k + 1; r < nb; ++r) {
+#pragma unroll
+                for (int r = 0; r < nb; ++r) {
+                    if (r <= k) continue;
                     const R f = A[r][k] / A[k][k];
-                    for (int c = k; c < nb; ++c) A[r][c] = A[r][c] - f * A[k][c];
+#pragma unroll
+                    for (int c = 0; c < nb; ++c)
+                        if (c >= k) A[r][c] = A[r][c] - f * A[k][c];
                     b[r] = b[r] - f * b[k];
                 }
             }
             R x[nb];
-            for (int r = nb - 1; r >= 0 && ok; --r) {
+#pragma unroll
+            for (int r = nb - 1; r >= 0; --r) {
                 R s = b[r];
-                for (int c = r + 1; c < nb; ++c) s = s - A[r][c] * x[c];
+#pragma unroll
+                for (int c = 0; c < nb; ++c)
+                    if (c > r) s = s - A[r][c] * x[c];
                 x[r] = s / A[r][r];
                 ok = ok && std::isfinite(x[r]);
             }
+#pragma unroll
             for (int r = 0; r < nb; ++r) {
-                const R e = dt * S(row[r], 0);
-                dq(row[r], 0) = ok ? x[r] : (std::isfinite(e) ? e : R(0));
+                const int row = (r == 0) ? mom(d) : mnt(d, r);
+                const R e = dt * S(row, 0);
+                dq(row, 0) = ok ? x[r] : (std::isfinite(e) ? e : R(0));
             }
         }
     }
@@ -345,9 +378,11 @@ struct SME
         R const /*time*/, R const /*dX*/) {
         VQ g = Q;
         if (bc_idx == 1) {
+#pragma unroll
             for (int j = 0; j <= LEVEL; ++j) {
                 R qn = Q(j == 0 ? mom(0) : mnt(0, j), 0) * n(0, 0);
                 if constexpr (DIM == 2) qn = qn + Q(j == 0 ? mom(1) : mnt(1, j), 0) * n(1, 0);
+#pragma unroll
                 for (int d = 0; d < DIM; ++d) {
                     const int r = (j == 0) ? mom(d) : mnt(d, j);
                     g(r, 0) = Q(r, 0) - R(2) * qn * n(d, 0);
@@ -374,18 +409,23 @@ struct SME
         F(1, 0) = qw;
         // mean momenta: the shallow-water terms, then the moments' share
         R sw = R(0);
+#pragma unroll
         for (int j = 1; j <= LEVEL; ++j) sw = sw + R(K::N(j)) * (Q(mnt(D, j), 0) * Q(mnt(D, j), 0));
         F(mom(D), 0) = (qw * qw * hinv + R(0.5) * g * h * h) + hinv * sw;
         if constexpr (DIM == 2) {
             const R qt = Q(mom(E), 0);
             R st = R(0);
+#pragma unroll
             for (int j = 1; j <= LEVEL; ++j) st = st + R(K::N(j)) * (Q(mnt(D, j), 0) * Q(mnt(E, j), 0));
             F(mom(E), 0) = qt * qw * hinv + hinv * st;
         }
         // moments along D (normal) and across it (transverse)
+#pragma unroll
         for (int i = 1; i <= LEVEL; ++i) {
             R an = R(0), at = R(0);
+#pragma unroll
             for (int j = 1; j <= LEVEL; ++j)
+#pragma unroll
                 for (int k = 1; k <= LEVEL; ++k) {
                     const R a = R(K::A(i, j, k));
                     if (a == R(0)) continue;
@@ -409,10 +449,13 @@ struct SME
         const R wm = Q(mom(D), 0) * hinv;
         R tm = R(0);
         if constexpr (DIM == 2) tm = Q(mom(E), 0) * hinv;
+#pragma unroll
         for (int i = 1; i <= LEVEL; ++i) {
             R rn = -wm * dq(mnt(D, i), 0), rt = -tm * dq(mnt(D, i), 0);
+#pragma unroll
             for (int j = 1; j <= LEVEL; ++j) {
                 R cn = R(0), ct = R(0);
+#pragma unroll
                 for (int k = 1; k <= LEVEL; ++k) {
                     const R bc = R(K::B(i, j, k));
                     if (bc == R(0)) continue;
@@ -438,18 +481,22 @@ struct SME
         const R w = Q(mom(D), 0) * hinv;
         R ga[LEVEL + 1], ta[LEVEL + 1];
         ga[0] = R(0); ta[0] = R(0);
+#pragma unroll
         for (int j = 1; j <= LEVEL; ++j) ga[j] = Q(mnt(D, j), 0) * hinv;
         R t = R(0);
         if constexpr (DIM == 2) {
             t = Q(mom(E), 0) * hinv;
+#pragma unroll
             for (int j = 1; j <= LEVEL; ++j) ta[j] = Q(mnt(E, j), 0) * hinv;
         } else {
+#pragma unroll
             for (int j = 1; j <= LEVEL; ++j) ta[j] = R(0);
         }
         R best = R(1);   // the depth row: dF_h/dq_w = 1
         {   // normal mean momentum: columns h, q_w, h gamma_j
             R d0 = g * h - w * w;
             R r = std::abs(R(2) * w);
+#pragma unroll
             for (int j = 1; j <= LEVEL; ++j) {
                 d0 = d0 - R(K::N(j)) * (ga[j] * ga[j]);
                 r = r + std::abs(R(2) * R(K::N(j)) * ga[j]);
@@ -460,6 +507,7 @@ struct SME
         if constexpr (DIM == 2) {   // transverse mean momentum: h, q_w, q_t, h gamma_j, h tau_j
             R d0 = -w * t;
             R r = std::abs(t) + std::abs(w);
+#pragma unroll
             for (int j = 1; j <= LEVEL; ++j) {
                 d0 = d0 - R(K::N(j)) * (ga[j] * ta[j]);
                 r = r + std::abs(R(K::N(j)) * ta[j]) + std::abs(R(K::N(j)) * ga[j]);
@@ -467,12 +515,15 @@ struct SME
             r = r + std::abs(d0);
             best = amrex::max(best, r);
         }
+#pragma unroll
         for (int i = 1; i <= LEVEL; ++i) {
             // normal moment i: h, q_w, h gamma_j (flux + non-conservative)
             R d0 = R(-2) * w * ga[i];
             R r = std::abs(R(2) * ga[i]);
+#pragma unroll
             for (int j = 1; j <= LEVEL; ++j) {
                 R c = (i == j) ? w : R(0);
+#pragma unroll
                 for (int k = 1; k <= LEVEL; ++k) {
                     // (the tables are compile-time constants: zero terms fold away)
                     if (K::A(i, j, k) != 0.0) d0 = d0 - R(K::A(i, j, k)) * (ga[j] * ga[k]);
@@ -487,8 +538,10 @@ struct SME
                 // transverse moment i: h, q_w, q_t, h gamma_j, h tau_k
                 R e0 = -w * ta[i] - t * ga[i];
                 R s = std::abs(ta[i]) + std::abs(ga[i]);
+#pragma unroll
                 for (int j = 1; j <= LEVEL; ++j) {
                     R cg = R(0), ct = (i == j) ? w : R(0);
+#pragma unroll
                     for (int k = 1; k <= LEVEL; ++k) {
                         if (K::A(i, j, k) != 0.0) e0 = e0 - R(K::A(i, j, k)) * (ga[j] * ta[k]);
                         if (K::A(i, j, k) + K::B(i, j, k) != 0.0)
@@ -530,6 +583,7 @@ struct SMENumerics
         VQ fL = M::template flux_dir<D>(qL, aL, p);
         VQ fR = M::template flux_dir<D>(qR, aR, p);
         VQ F;
+#pragma unroll
         for (int n = 0; n < nq; ++n) F(n, 0) = R(0.5) * (fL(n, 0) + fR(n, 0));
         return F;
     }
@@ -539,15 +593,19 @@ struct SMENumerics
     template <int D>
     static PORTABLE_FN AMREX_FORCE_INLINE VQ path_product(VQ const& qL, VQ const& qR, VP const& p) {
         VQ dq, bdq{};
+#pragma unroll
         for (int n = 0; n < nq; ++n) dq(n, 0) = qR(n, 0) - qL(n, 0);
         bdq(M::mom(D), 0) = p(sme_g, 0) * (R(0.5) * (qL(1, 0) + qR(1, 0))) * dq(0, 0);
         if constexpr (LEVEL > 0) {
             const R eps = p(sme_eps, 0);
+#pragma unroll
             for (int q = 0; q < 3; ++q) {
                 const R s = R(K::gl_s(q));
                 VQ ps, part;
+#pragma unroll
                 for (int n = 1; n < nq; ++n) ps(n, 0) = qL(n, 0) + s * dq(n, 0);
                 M::template ncp_moments<D>(ps, M::hinv_of(ps(1, 0), eps), dq, part);
+#pragma unroll
                 for (int j = 1; j <= LEVEL; ++j) {
                     bdq(M::mnt(D, j), 0) = bdq(M::mnt(D, j), 0) + R(K::gl_w(q)) * part(M::mnt(D, j), 0);
                     if constexpr (DIM == 2) {
@@ -569,6 +627,7 @@ struct SMENumerics
         V2Q D2;
         D2(0, 0) = R(0);
         D2(nq, 0) = R(0);
+#pragma unroll
         for (int n = 1; n < nq; ++n) {
             const R dq = qR(n, 0) - qL(n, 0);
             D2(n, 0) = R(0.5) * bdq(n, 0) + R(0.5) * s * dq;        // D+
