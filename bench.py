@@ -650,7 +650,7 @@ def sme_bench(local, n=2048, steps=500, timed=100, warm=5):
     shapes = generic_tile_variants()
     shape_ms = {v: timed_run(ZFV_PREC_FP32, variant=v, k=max(10, timed // 5)) for v in range(len(shapes))}
     best = min(shape_ms, key=shape_ms.get)
-    record(8, "fp32", float(cells), best, shape_ms, shapes)
+    record(8, "fp32-tile", float(cells), best, shape_ms, shapes)
     ms32 = timed_run(ZFV_PREC_FP32, variant=best)
     # error after `steps` steps from the same start
     out = {}

@@ -75,19 +75,61 @@ def test_lake_at_rest_is_exact_in_fp32(cuda):
 
 def test_lake_at_rest_with_dry_islands_order1(cuda):
     """With emerging bumps (dry islands) the reference scheme is exactly
-    well-balanced at order 1 (Audusse); so is the FP32 form."""
+    well-balanced at order 1 (Audusse); so is the FP32 form at order 1 (the
+    generic tile kernels' forward-Euler stage): the momenta stay exactly
+    zero and eta does not move."""
     model = SWE(2, "wall", bumps(5, hump=0.0), parameters={"n_m": 0.03})
     s = _settings(64, 100, spatial_order=1)
     from zoomy_amrex_b200.level import Level
     cfg64, Q0, A0 = setup(model, s)
     assert (Q0[1] == 0).any()
-    # the FP32 form runs the SSP-RK2 path only: check the FP64 form here and the
-    # FP32 form at order 2 on the fully wet lake above
     lev = Level(cfg64, Q0, A0)
     lev.run(chunk=50)
     Q = lev.Q.cpu().numpy()
     lev.close()
     assert np.abs(Q[2:]).max() < 1e-12
+    Q32, _, st, _, _ = run_fp32(model, s)
+    assert st["step"] == 100
+    assert np.abs(Q32[2:]).max() == 0.0
+    wet = Q0[1] > 0
+    assert np.abs((Q32[0] + Q32[1]) - (Q0[0] + Q0[1]))[wet].max() < 1e-12
+    assert (Q32[1][~wet] == 0.0).all()
+
+
+@pytest.mark.parametrize("moving", [False, True])
+def test_fp32_order1_error_vs_fp64_oracle(cuda, oracle, moving):
+    """Order 1 (one forward-Euler stage per step) of the chosen form: L1 /
+    Linf depth error after 150 steps of the wet/dry hump over bumps against
+    the FP64 reference (Manning implicit, WB, walls), every tile variant
+    giving the same bits."""
+    from zoomy_amrex_b200.batch import generic_tile_variants
+    from zoomy_amrex_b200.level import Level
+    model = SWE(2, "wall", bumps(7, moving=moving), parameters={"n_m": 0.03})
+    s = _settings(80, 150, spatial_order=1)
+    cfg64, Q0, A0 = setup(model, s)
+    cfg = config_from_settings(model, s, precision=ZFV_PREC_FP32)
+    outs = []
+    for v in range(len(generic_tile_variants())):
+        lev = Level(cfg, Q0, A0, variant=v)
+        try:
+            st = lev.run(chunk=50)
+            outs.append((lev.state64().cpu().numpy(), st))
+        finally:
+            lev.close()
+    for Q, _ in outs[1:]:
+        assert np.array_equal(Q, outs[0][0])
+    Q32, st = outs[0]
+    Qo, Ao, n, t, logo, _ = oracle.run(cfg64, Q0, A0)
+    assert st["step"] == n == 150
+    assert abs(st["time"] - t) <= 1e-6 * t
+    dh = np.abs(Q32[1] - Qo[1])
+    l1, linf = dh.mean(), dh.max()
+    print(f"[fp32 order 1 vs fp64 oracle] moving={moving}: L1 {l1:.3e} Linf {linf:.3e} "
+          f"mom {np.abs(Q32[2:] - Qo[2:]).max():.3e}")
+    assert l1 <= 1e-6, l1
+    assert linf <= 1e-4, linf
+    assert np.abs(Q32[2:] - Qo[2:]).max() <= 1e-4
+    assert ((Q32[1] <= 1e-6) == (Qo[1] <= 1e-6)).mean() > 0.999
 
 
 @pytest.mark.parametrize("moving", [False, True])

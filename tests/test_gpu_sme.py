@@ -127,7 +127,7 @@ def run_fp32(cfg64, Q0, A0, variant=None, chunk=25):
         lev.close()
 
 
-@pytest.mark.parametrize("name", ["sme2d_wetdry_wb_impl_o2", "sme2d_moving_mixed_bc_o2"])
+@pytest.mark.parametrize("name", ["sme2d_wetdry_wb_impl_o2", "sme2d_moving_mixed_bc_o2", "sme2d_o1_impl_wb"])
 def test_sme_fp32_error_vs_fp64_oracle(cuda, oracle, name):
     """L1 / Linf error of the FP32 chosen form against the FP64 oracle, depth
     and moments (the FP32 form has no bitwise target)."""

@@ -9,7 +9,9 @@ zfv_adj_record / zfv_adj_step): gradients with respect to the initial state
 Memory: the forward keeps one checkpoint (Q and the 128-byte device run
 record) every ``checkpoint_every`` steps; the backward re-runs each segment
 from its checkpoint, recording the tape of that segment only (about 14 state
-planes per step), then walks it backwards. The map differentiated is the one
+planes per step), then walks it backwards. The last segment is recorded by
+the forward itself (its tape is kept until the backward), so the backward
+re-runs all segments but that one. The map differentiated is the one
 the solver applies, including dt_n = cfl / (d (2k+1) max_inv(Q^n)); the
 forward recomputation is bitwise identical to the original run.
 """
@@ -90,21 +92,32 @@ class SWEEvolve(torch.autograd.Function):
         sol.stream.wait_stream(torch.cuda.current_stream(device))
         _lib.check(L.zfv_begin(sol.h, Q.data_ptr(), A.data_ptr(), sol.scratch.data_ptr(), sol.s()), "zfv_begin")
         ckpts = []
+        last = None       # (start, n, tape) of the segment the forward recorded
         done = 0
         with torch.cuda.stream(sol.stream):
             while done < n_steps:
-                rs = torch.empty(sol.rs_bytes, dtype=torch.uint8, device=device)
-                _lib.check(L.zfv_save_run_state(sol.h, sol.scratch.data_ptr(), rs.data_ptr(), sol.s()),
-                           "zfv_save_run_state")
-                ckpts.append((done, Q.clone(), rs))
                 n = min(checkpoint_every, n_steps - done)
-                _lib.check(L.zfv_evolve(sol.h, Q.data_ptr(), A.data_ptr(), sol.scratch.data_ptr(), n, sol.s()),
-                           "zfv_evolve")
+                if done + n == n_steps:
+                    # the last segment: record its tape now (the same launches
+                    # as zfv_evolve plus the tape writes) instead of re-running
+                    # it in the backward
+                    tape = torch.empty(int(L.zfv_adj_tape_bytes(sol.h, n)), dtype=torch.uint8, device=device)
+                    _lib.check(L.zfv_adj_record(sol.h, Q.data_ptr(), A.data_ptr(), sol.scratch.data_ptr(),
+                                                tape.data_ptr(), n, sol.s()), "zfv_adj_record")
+                    last = (done, n, tape)
+                else:
+                    rs = torch.empty(sol.rs_bytes, dtype=torch.uint8, device=device)
+                    _lib.check(L.zfv_save_run_state(sol.h, sol.scratch.data_ptr(), rs.data_ptr(), sol.s()),
+                               "zfv_save_run_state")
+                    ckpts.append((done, Q.clone(), rs))
+                    _lib.check(L.zfv_evolve(sol.h, Q.data_ptr(), A.data_ptr(), sol.scratch.data_ptr(), n,
+                                            sol.s()), "zfv_evolve")
                 done += n
         _check_steps(sol, n_steps)
         torch.cuda.current_stream(device).wait_stream(sol.stream)
         ctx.sol = sol
         ctx.ckpts = ckpts
+        ctx.last = last
         ctx.aux0 = aux0.detach().to(torch.float64).contiguous()
         ctx.n_steps = n_steps
         ctx.every = checkpoint_every
@@ -117,12 +130,23 @@ class SWEEvolve(torch.autograd.Function):
         device = gQ.device
         lam = gQ.detach().to(torch.float64).contiguous().clone()
         grad = torch.zeros(2, dtype=torch.float64, device=device)
-        tape = torch.empty(int(L.zfv_adj_tape_bytes(sol.h, ctx.every)), dtype=torch.uint8, device=device)
         work = torch.zeros(int(L.zfv_adj_work_bytes(sol.h)), dtype=torch.uint8, device=device)
-        Q = torch.empty_like(ctx.ckpts[0][1])
-        A = ctx.aux0.clone()
         sol.stream.wait_stream(torch.cuda.current_stream(device))
+
+        def reverse(start, n, tape):
+            for k in reversed(range(n)):
+                aux0 = ctx.aux0.data_ptr() if start + k == 0 else None
+                _lib.check(L.zfv_adj_step(sol.h, tape.data_ptr(), k, lam.data_ptr(), grad.data_ptr(), aux0,
+                                          work.data_ptr(), sol.s()), "zfv_adj_step")
+
         with torch.cuda.stream(sol.stream):
+            if ctx.last is not None:
+                start, n, tape_last = ctx.last
+                reverse(start, n, tape_last)
+            if ctx.ckpts:
+                tape = torch.empty(int(L.zfv_adj_tape_bytes(sol.h, ctx.every)), dtype=torch.uint8, device=device)
+                Q = torch.empty_like(ctx.ckpts[0][1])
+                A = ctx.aux0.clone()
             for start, Qc, rs in reversed(ctx.ckpts):
                 n = min(ctx.every, ctx.n_steps - start)
                 Q.copy_(Qc)
@@ -130,14 +154,11 @@ class SWEEvolve(torch.autograd.Function):
                            "zfv_load_run_state")
                 _lib.check(L.zfv_adj_record(sol.h, Q.data_ptr(), A.data_ptr(), sol.scratch.data_ptr(),
                                             tape.data_ptr(), n, sol.s()), "zfv_adj_record")
-                for k in reversed(range(n)):
-                    aux0 = ctx.aux0.data_ptr() if start + k == 0 else None
-                    _lib.check(L.zfv_adj_step(sol.h, tape.data_ptr(), k, lam.data_ptr(),
-                                              grad.data_ptr(), aux0,
-                                              work.data_ptr(), sol.s()), "zfv_adj_step")
+                reverse(start, n, tape)
         torch.cuda.current_stream(device).wait_stream(sol.stream)
         sol.stream.synchronize()
         ctx.sol = None
+        ctx.last = None
         sol.close()
         g_nm = grad[0].reshape(()).to(gQ.dtype)
         return lam, g_nm, None, None, None, None

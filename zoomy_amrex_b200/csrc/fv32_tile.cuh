@@ -87,7 +87,10 @@ struct TileMaps {
     CUtensorMap bed, qs, alt, inc;
 };
 
-enum TMode : int { T_S1 = 1, T_S2 = 2 };
+// T_S1 / T_S2: the two SSP-RK2 stages (spatial order 2); T_ONE: the single
+// forward-Euler stage of spatial order 1 (Q^{n+1} = Q^n + dt RHS, then the
+// step's reduction), as the reference's order-1 Advance.
+enum TMode : int { T_S1 = 1, T_S2 = 2, T_ONE = 3 };
 constexpr float kNearDry = 1.0e-3f;
 // try_wait polls of an mbarrier before a stage gives up (each poll may block
 // for a hardware-defined interval): a bound, so that a copy that never
@@ -544,12 +547,14 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
             for (int k = 0; k < ne; ++k) B.inc[k * plane + c] = d[k];
         } else {
             // Heun on the compensated state: Q^{n+1} = X + lo + (inc1 + inc2)/2
+            // (order 1: X + lo + inc)
             VQ qn;
             qn(0, 0) = bc;
 #pragma unroll
             for (int k = 0; k < ne; ++k) {
                 const float hi = X[k * plane + c];
-                const float t = B.lo[k * plane + c] + 0.5f * (B.inc[k * plane + c] + d[k]);
+                const float t = (MODE == T_ONE) ? B.lo[k * plane + c] + d[k]
+                                                : B.lo[k * plane + c] + 0.5f * (B.inc[k * plane + c] + d[k]);
                 float s, e;
                 two_sum(hi, t, s, e);
                 Y[k * plane + c] = s;
@@ -573,7 +578,7 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
             s_loc = (double(etan) + double(B.lo[c])) - double(bc);
         }
     }
-    if constexpr (MODE == T_S2) {
+    if constexpr (MODE == T_S2 || MODE == T_ONE) {
         const bool last = zfv::finish_step_units<NT>(m_loc, s_loc, red, B.partials, B.log3, B.log_cap, st, L,
                                                       dtd, time, false, gridDim.x * gridDim.y,
                                                       blockIdx.y * gridDim.x + blockIdx.x);

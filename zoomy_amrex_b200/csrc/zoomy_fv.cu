@@ -171,7 +171,8 @@ int zfv_create(const zfv_config* cfg, zfv_handle** out) {
     if (!h) return fail(-4, "zfv_create: out of host memory");
     h->cfg = *cfg;
     if (cfg->precision == ZFV_PREC_FP32) {
-        if (cfg->model == ZFV_MODEL_SWE2D) h->run.reset(make_runner_fp32_swe2d(h));
+        // the shallow-water sweep is order 2; order 1 runs on the generic tile kernels
+        if (cfg->model == ZFV_MODEL_SWE2D && cfg->spatial_order == 2) h->run.reset(make_runner_fp32_swe2d(h));
         else h->run.reset(make_runner_fp32_generic(h));
     } else {
         switch (cfg->model) {
@@ -180,6 +181,10 @@ int zfv_create(const zfv_config* cfg, zfv_handle** out) {
         case ZFV_MODEL_SME2D_L2: h->run.reset(make_runner_fp64_sme2d_l2(h)); break;
         case ZFV_MODEL_SME1D_L2: h->run.reset(make_runner_fp64_sme1d_l2(h)); break;
         }
+    }
+    if (!h->run) {
+        delete h;
+        return fail(-2, "zfv_create: precision %d is not built for model %d", cfg->precision, cfg->model);
     }
     int rc = h->run->setup();
     if (rc) { delete h; return rc; }

@@ -1,6 +1,8 @@
 // FP32 chosen form of the families without a hand-tuned sweep
-// (ZFV_PREC_FP32 with ZFV_MODEL_SME2D_L2): the generic tile kernels of
-// fv32_tile.cuh behind the Runner interface. Compiled with FMA contraction
+// (ZFV_PREC_FP32 with ZFV_MODEL_SME2D_L2, and ZFV_MODEL_SWE2D at spatial
+// order 1, which the shallow-water sweep does not implement): the generic
+// tile kernels of fv32_tile.cuh behind the Runner interface. Order 2 runs
+// the two SSP-RK2 stages, order 1 one forward-Euler stage per step. Compiled with FMA contraction
 // and the hardware's approximate FP32 division and square root, like
 // zoomy_fv32.cu.
 //
@@ -19,6 +21,7 @@
 
 #include "zfv_internal.H"
 #include "sme.H"
+#include "swe.H"
 #include "fv32_tile.cuh"
 
 using namespace zfvi;
@@ -70,6 +73,7 @@ struct RunnerTile final : Runner {
     zfv_handle* h;
     TileParams<NP> L;
     int var = 0;
+    bool order1 = false;
 
     explicit RunnerTile(zfv_handle* hh) : h(hh) {
         const zfv_config& c = h->cfg;
@@ -111,7 +115,8 @@ struct RunnerTile final : Runner {
     template <int V, bool WB, bool IMPL>
     int set_smem2() {
         return set_smem1<V, T_S1, WB, IMPL, false>() | set_smem1<V, T_S2, WB, IMPL, false>() |
-               set_smem1<V, T_S1, WB, IMPL, true>() | set_smem1<V, T_S2, WB, IMPL, true>();
+               set_smem1<V, T_ONE, WB, IMPL, false>() | set_smem1<V, T_S1, WB, IMPL, true>() |
+               set_smem1<V, T_S2, WB, IMPL, true>() | set_smem1<V, T_ONE, WB, IMPL, true>();
     }
     template <int V>
     int set_smem_v() {
@@ -141,7 +146,9 @@ struct RunnerTile final : Runner {
 
     int setup() override {
         const zfv_config& c = h->cfg;
-        if (c.spatial_order != 2) return fail(-2, "zfv_create: the FP32 form implements spatial_order 2 only");
+        if (c.spatial_order != 1 && c.spatial_order != 2)
+            return fail(-2, "zfv_create: the FP32 form implements spatial_order 1 and 2");
+        order1 = c.spatial_order == 1;
         if (c.positivity_mood) return fail(-2, "zfv_create: the FP32 form does not implement MOOD");
         if (c.implicit_global && c.implicit_source)
             return fail(-1, "zfv_create: implicit_global is built for the FP64 form");
@@ -200,8 +207,12 @@ struct RunnerTile final : Runner {
         const dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, 1);
         const size_t sm = ShapeV<V, TMA>::smem_bytes;
         for (int k = 0; k < n; ++k) {
-            k32t_stage<F, T_S1, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 1, maps);
-            k32t_stage<F, T_S2, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 1, maps);
+            if (order1) {
+                k32t_stage<F, T_ONE, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 0, maps);
+            } else {
+                k32t_stage<F, T_S1, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 1, maps);
+                k32t_stage<F, T_S2, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 1, maps);
+            }
         }
     }
     template <int V, bool TMA>
@@ -281,8 +292,11 @@ namespace zfvi {
 Runner* make_runner_fp32_generic(zfv_handle* h) {
     using F = zfv32t::Fam<zb::SME<double, 2, 2>, zb::SMENumerics<double, 2, 2>, zb::SME<float, 2, 2>,
                           zb::SMENumerics<float, 2, 2>>;
+    using FS = zfv32t::Fam<zb::SWE<double, 2>, zb::SWENumerics<double, 2>, zb::SWE<float, 2>,
+                           zb::SWENumerics<float, 2>>;
     switch (h->cfg.model) {
     case ZFV_MODEL_SME2D_L2: return new zfv32t::RunnerTile<F>(h);
+    case ZFV_MODEL_SWE2D: return new zfv32t::RunnerTile<FS>(h);
     default: return nullptr;
     }
 }

@@ -15,7 +15,16 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._abi import MODELS, ZFV_PREC_FP32, zfv_config, zfv_status
+from ._abi import MODELS, ZFV_MODEL_SWE2D, ZFV_PREC_FP32, zfv_config, zfv_status
+
+
+def fp32_kernel_family(cfg: zfv_config) -> str:
+    """Which FP32 kernels run a level, and so which shapes its variant
+    indexes: "fp32" = the shallow-water column sweep (2-D SWE, order 2;
+    batch.tile_variants()), "fp32-tile" = the generic tile kernels (every
+    other FP32 case; batch.generic_tile_variants()). The autotuner caches
+    the two under these names."""
+    return "fp32" if (cfg.model == ZFV_MODEL_SWE2D and cfg.spatial_order == 2) else "fp32-tile"
 
 _DTYPE = torch.float64
 
@@ -80,7 +89,7 @@ class Level:
         if self.fp32:
             if variant is None:   # the autotuner's pick for this size, if one was measured
                 from .autotune import cached_variant
-                variant = cached_variant(nq, "fp32", cfg.nx * cfg.ny)
+                variant = cached_variant(nq, fp32_kernel_family(cfg), cfg.nx * cfg.ny)
             if variant is not None:
                 self.set_variant(variant)
         elif variant is not None:
@@ -97,7 +106,9 @@ class Level:
 
     @property
     def variant(self) -> int:
-        """Strip shape of the FP32 stage kernels (index into batch.tile_variants()); -1 for FP64."""
+        """Shape of the FP32 stage kernels (index into batch.tile_variants() for the
+        shallow-water sweep, batch.generic_tile_variants() otherwise, see
+        fp32_kernel_family); -1 for FP64."""
         return int(_lib.lib().zfv_get_variant(self._h))
 
     def set_variant(self, variant: int):

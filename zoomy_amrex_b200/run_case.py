@@ -30,7 +30,7 @@ from .settings import config_from_settings, grid
 
 def _precision(settings: dict) -> int:
     """settings['precision']: "fp64" (default; the reference's arithmetic) or
-    "fp32" (the FP32 chosen form: SWE2D, order 2)."""
+    "fp32" (the FP32 chosen form: 2-D SWE at order 1 or 2, 2-D SME level 2)."""
     from ._abi import ZFV_PREC_FP32, ZFV_PREC_FP64
     p = str(settings.get("precision", "fp64")).lower()
     if p not in ("fp64", "fp32"):
