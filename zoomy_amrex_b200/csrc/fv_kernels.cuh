@@ -57,7 +57,12 @@ struct TileShape {
     static constexpr size_t q_elems = size_t(nq) * RH * RW;
     static constexpr size_t fx_elems = size_t(TY) * (TX + 1) * NFC;
     static constexpr size_t fy_elems = (dim == 2) ? size_t(TY + 1) * TX * NFC : 0;
-    static constexpr size_t smem_bytes = (q_elems + fx_elems + fy_elems) * sizeof(double);
+    // the x faces and then the y faces use one buffer; between the two
+    // passes each cell keeps its x part of the balance (NQE values and the
+    // WB x pressure term) in xp
+    static constexpr size_t f_elems = fx_elems > fy_elems ? fx_elems : fy_elems;
+    static constexpr size_t xp_elems = (dim == 2) ? size_t(NQE + 1) * NT : 0;
+    static constexpr size_t smem_bytes = (q_elems + f_elems + xp_elems) * sizeof(double);
 };
 
 // Deterministic block reduction: max of m (NaN-ignoring, as the reference's
@@ -163,11 +168,13 @@ __device__ __forceinline__ bool finish_step_units(double m, double s, double* re
     return true;
 }
 
-// Blocks per SM the register budget aims at: 3 for the 2-D shallow-water
-// tile; 2 for 1-D rows and for models with more than 4 unknowns, whose
-// point-implicit elimination (n^2 doubles) must stay in registers.
+// Blocks per SM the register budget aims at: 4 for the 2-D shallow-water
+// tile (64 registers; its shared memory, with the one face buffer, fits 4
+// blocks too), so that 32 warps hide the FP64 latency; 2 for 1-D rows and
+// for models with more than 4 unknowns, whose point-implicit elimination
+// (n^2 doubles) must stay in registers.
 template <class Model>
-constexpr int stage_min_blocks() { return (Model::dimension == 2 && Model::n_dof_q <= 4) ? 3 : 2; }
+constexpr int stage_min_blocks() { return (Model::dimension == 2 && Model::n_dof_q <= 4) ? 4 : 2; }
 
 template <class Model, class Numerics, int ORDER, int MODE, bool WB, bool IMPL, int TX, int TY>
 __global__ void __launch_bounds__(TX * TY, stage_min_blocks<Model>())
@@ -192,8 +199,8 @@ k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
 
     extern __shared__ __align__(16) double smem[];
     double* sQ = smem;                                  // [nq][RH][RW]
-    double* sFx = sQ + Sh::q_elems;                     // [TY][TX+1][NFC]
-    double* sFy = sFx + Sh::fx_elems;                   // [TY+1][TX][NFC]
+    double* sF = sQ + Sh::q_elems;                      // x faces [TY][TX+1][NFC], then y faces [TY+1][TX][NFC]
+    double* sXp = sF + Sh::f_elems;                     // 2-D: [NQE+1][NT] x parts of the cells' balances
     __shared__ double red[2 * ((NT + 31) / 32)];
 
     const int tid = threadIdx.x;
@@ -322,30 +329,55 @@ k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
         store_face(F, fl, fc, hl, hr);
     };
 
-    // 3. faces, each once
+    // 3. faces, each once: the x faces, each cell's x part of its balance,
+    // then the y faces in the same buffer. The x part is Fx / dx and the WB
+    // x pressure term, each formed exactly as the one-pass assembly forms
+    // it, so the balance below is the same IEEE arithmetic in the same order.
+    const bool valid = (i < nx) && (j < ny);
     if (j < jend) {
         const int ly = ty + GY;
-        if (i <= iend) x_face(i, j, ly, sFx + (ty * (TX + 1) + tx) * NFC);
+        if (i <= iend) x_face(i, j, ly, sF + (ty * (TX + 1) + tx) * NFC);
         if (tx == TX - 1 && x0 + TX <= iend)
-            x_face(x0 + TX, j, ly, sFx + (ty * (TX + 1) + TX) * NFC);
-    }
-    if constexpr (dim == 2) {
-        if (i < iend) {
-            const int lx = tx + G;
-            if (j <= jend) y_face(i, j, lx, sFy + (ty * TX + tx) * NFC);
-            if (ty == TY - 1 && y0 + TY <= jend)
-                y_face(i, y0 + TY, lx, sFy + (TY * TX + tx) * NFC);
-        }
+            x_face(x0 + TX, j, ly, sF + (ty * (TX + 1) + TX) * NFC);
     }
     __syncthreads();
+    R xdiv[NQE], xwb = R(0.0);
+    if (valid) {
+        const double* FxL = sF + (ty * (TX + 1) + tx) * NFC;
+        const double* FxR = FxL + NFC;
+#pragma unroll
+        for (int k = 0; k < NQE; ++k) {
+            const R Fx = -(FxR[k] - FxL[k]) - FxR[2 * NQE + k] - FxL[NQE + k];
+            xdiv[k] = Fx / L.dx;
+        }
+        if constexpr (WB)
+            xwb = R(0.5) * p(0, 0) * (FxR[3 * NQE] * FxR[3 * NQE] - FxL[3 * NQE + 1] * FxL[3 * NQE + 1]) / L.dx;
+    }
+    if constexpr (dim == 2) {
+        if (valid) {
+#pragma unroll
+            for (int k = 0; k < NQE; ++k) sXp[k * NT + tid] = xdiv[k];
+            sXp[NQE * NT + tid] = xwb;
+        }
+        __syncthreads();   // every x face read: the buffer takes the y faces
+        if (i < iend) {
+            const int lx = tx + G;
+            if (j <= jend) y_face(i, j, lx, sF + (ty * TX + tx) * NFC);
+            if (ty == TY - 1 && y0 + TY <= jend)
+                y_face(i, y0 + TY, lx, sF + (TY * TX + tx) * NFC);
+        }
+        __syncthreads();
+        if (valid) {
+#pragma unroll
+            for (int k = 0; k < NQE; ++k) xdiv[k] = sXp[k * NT + tid];
+            xwb = sXp[NQE * NT + tid];
+        }
+    }
 
     // 4. assemble (make_rhs.H:346-399), update, implicit source, epilogue
-    const bool valid = (i < nx) && (j < ny);
     double m_loc = 0.0, s_loc = 0.0;
     if (valid) {
-        const double* FxL = sFx + (ty * (TX + 1) + tx) * NFC;
-        const double* FxR = FxL + NFC;
-        const double* FyL = (dim == 2) ? sFy + (ty * TX + tx) * NFC : nullptr;
+        const double* FyL = (dim == 2) ? sF + (ty * TX + tx) * NFC : nullptr;
         const double* FyR = (dim == 2) ? FyL + TX * NFC : nullptr;
         const typename T::VQ qc = loadq(tx + G, ty + GY);
         const auto X = cell_centre<Model, R>(L, i, j);
@@ -359,15 +391,14 @@ k_stage(const double* __restrict__ qin, const double* __restrict__ qbed,
 #pragma unroll
         for (int n = n0; n < nq; ++n) {
             const int k = n - n0;
-            const R Fx = -(FxR[k] - FxL[k]) - FxR[2 * NQE + k] - FxL[NQE + k];
             R Fy = R(0.0);
             if constexpr (dim == 2) Fy = -(FyR[k] - FyL[k]) - FyR[2 * NQE + k] - FyL[NQE + k];
-            rhs(n, 0) = Fx / L.dx + Fy / L.dy;
+            rhs(n, 0) = xdiv[k] + Fy / L.dy;
             if constexpr (!IMPL) rhs(n, 0) += S(n, 0);
         }
         if constexpr (WB) {
             const R g = p(0, 0);
-            rhs(kIdxH + 1, 0) += R(0.5) * g * (FxR[3 * NQE] * FxR[3 * NQE] - FxL[3 * NQE + 1] * FxL[3 * NQE + 1]) / L.dx;
+            rhs(kIdxH + 1, 0) += xwb;
             if constexpr (dim == 2)
                 rhs(kIdxH + 2, 0) += R(0.5) * g * (FyR[3 * NQE] * FyR[3 * NQE] - FyL[3 * NQE + 1] * FyL[3 * NQE + 1]) / L.dy;
         }
