@@ -187,3 +187,33 @@ def test_block_point_implicit_step_solves_the_linear_system(host, dim, level):
         # the bed and depth rows have no source: their increment is exactly zero
         assert got[0] == 0.0 and got[1] == 0.0
         np.testing.assert_allclose(got[2:], want[2:], rtol=1e-11, atol=1e-15)
+
+
+@pytest.mark.parametrize("dim,level", CASES)
+def test_implicit_system_block_structure(host, dim, level):
+    """The structure the FP64 kernels' block elimination relies on
+    (zb_implicit_blocks): the source and its Jacobian vanish in rows b and h,
+    column b is zero, and no entry couples the blocks {mean momentum and
+    moments of direction d}. Checked exactly on the header's Jacobian and
+    against the symbolic derivation's sparsity."""
+    from sme_sympy import numeric
+    f = numeric(level, dim)
+    n = 2 + dim * (1 + level)
+    block = np.full(n, -1)
+    for d in range(dim):
+        block[2 + d] = d
+        block[2 + dim + d * level: 2 + dim + (d + 1) * level] = d
+    rng = np.random.default_rng(400 + 10 * dim + level)
+    for _ in range(20):
+        q = rand_state(rng, dim, level)
+        par = np.array([9.81, rng.uniform(-0.1, 0.1), rng.uniform(-0.1, 0.1), rng.uniform(1e-4, 1e-2),
+                        rng.uniform(0.01, 1.0), 1e-24])
+        S = ev(host, 1, dim, level, 2, 0, q, par=par)[:n]
+        J = ev(host, 1, dim, level, 3, 0, q, par=par)[:n * n].reshape(n, n)
+        Js = np.asarray(f["dSdq"](q, tuple(par[:5])), float)
+        assert S[0] == 0.0 and S[1] == 0.0
+        assert not J[0].any() and not J[1].any() and not J[:, 0].any()
+        for r in range(2, n):
+            for c in range(2, n):
+                if block[r] != block[c]:
+                    assert J[r, c] == 0.0 and Js[r, c] == 0.0, (r, c)

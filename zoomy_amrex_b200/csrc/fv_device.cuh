@@ -159,9 +159,10 @@ __device__ __forceinline__ void eval_face(typename ModelTypes<Model>::VQ const& 
     fluct = Numerics::numerical_fluctuations(qL, qR, aL, aR, p, nh);
 }
 
-// make_rhs.H:429-509 on one cell: q0 (post-explicit-update state, in/out), a (stage aux).
+// make_rhs.H:429-509 on one cell: q0 (post-explicit-update state, in/out),
+// a (stage aux). The dense elimination, register-resident.
 template <class Model, class R>
-__device__ __forceinline__ void implicit_source_cell(typename ModelTypes<Model>::VQ& q,
+__device__ __forceinline__ void implicit_source_dense(typename ModelTypes<Model>::VQ& q,
                                                      typename ModelTypes<Model>::VA const& a,
                                                      R dt, typename ModelTypes<Model>::VP const& p,
                                                      R time,
@@ -243,6 +244,203 @@ __device__ __forceinline__ void implicit_source_cell(typename ModelTypes<Model>:
         const R v = q0(n, 0) + dt * S(n, 0);
         q(n, 0) = isfinite(v) ? v : q0(n, 0);
     }
+}
+
+// The same elimination out of line, its matrix in local memory (runtime
+// loops): the structured path below falls back to it for the rare cells
+// whose system does not have the declared structure, without raising the
+// calling kernel's register count. The operations are the reference's, in
+// its order.
+template <class Model, class R>
+__device__ __noinline__ void implicit_source_outline(typename ModelTypes<Model>::VQ& q,
+                                                     typename ModelTypes<Model>::VA const& a,
+                                                     R dt, typename ModelTypes<Model>::VP const& p,
+                                                     R time,
+                                                     typename ModelTypes<Model>::VX const& X) {
+    constexpr int nq = Model::n_dof_q;
+    constexpr int na = Model::n_dof_qaux;
+    const typename ModelTypes<Model>::VQ q0 = q;
+    const auto S = Model::source(q0, a, p, time, X);
+    const auto JQ = Model::source_jacobian_wrt_variables(q0, a, p);
+    const auto JA = Model::source_jacobian_wrt_aux_variables(q0, a, p);
+    const auto AQ = Model::update_aux_variables_jacobian_wrt_variables(q0, a, p, time, X);
+    R M[nq][nq], b[nq], dq[nq];
+#pragma unroll 1
+    for (int r = 0; r < nq; ++r) {
+        b[r] = dt * S(r, 0);
+#pragma unroll 1
+        for (int c = 0; c < nq; ++c) {
+            R t = JQ(r * nq + c, 0);
+#pragma unroll 1
+            for (int k = 0; k < na; ++k) t += JA(r * na + k, 0) * AQ(k * nq + c, 0);
+            M[r][c] = (r == c ? R(1.0) : R(0.0)) - dt * t;
+        }
+    }
+    bool ok = true;
+#pragma unroll 1
+    for (int k = 0; k < nq && ok; ++k) {
+        int piv = k;
+        R best = fabs(M[k][k]);
+#pragma unroll 1
+        for (int r = k + 1; r < nq; ++r)
+            if (fabs(M[r][k]) > best) { best = fabs(M[r][k]); piv = r; }
+        if (!(best > R(0.0)) || !isfinite(best)) { ok = false; break; }
+        if (piv != k) {
+#pragma unroll 1
+            for (int c = k; c < nq; ++c) { const R t = M[k][c]; M[k][c] = M[piv][c]; M[piv][c] = t; }
+            const R t = b[k]; b[k] = b[piv]; b[piv] = t;
+        }
+#pragma unroll 1
+        for (int r = k + 1; r < nq; ++r) {
+            const R f = M[r][k] / M[k][k];
+#pragma unroll 1
+            for (int c = k; c < nq; ++c) M[r][c] -= f * M[k][c];
+            b[r] -= f * b[k];
+        }
+    }
+#pragma unroll 1
+    for (int r = nq - 1; r >= 0 && ok; --r) {
+        R s = R(0.0);
+#pragma unroll 1
+        for (int c = r + 1; c < nq; ++c) s += M[r][c] * dq[c];
+        dq[r] = (b[r] - s) / M[r][r];
+        if (!isfinite(dq[r])) ok = false;
+    }
+    if (ok) {
+#pragma unroll 1
+        for (int n = 0; n < nq; ++n) q(n, 0) = q0(n, 0) + dq[n];
+        return;
+    }
+#pragma unroll 1
+    for (int n = 0; n < nq; ++n) {
+        const R v = q0(n, 0) + dt * S(n, 0);
+        q(n, 0) = isfinite(v) ? v : q0(n, 0);
+    }
+}
+
+// The same system solved block by block, for models that declare the
+// structure (zb_implicit_blocks, fv_model_traits.H). With rows 0 and 1 of
+// the system the identity (zero source, zero off-diagonal entries in their
+// rows and in column 0, no pivot in column 1), the reference's first two
+// elimination steps change no nonzero value; with no entry coupling two
+// blocks, every later step's pivot search, row swaps, eliminations and the
+// back substitution touch other blocks' rows only through products with
+// zeros. So solving each block with the reference's operations in the
+// reference's order gives the reference's result (up to the sign of zero
+// entries), with n_b small matrices in registers instead of one n x n. A
+// cell whose system breaks the preconditions takes the full elimination.
+template <class Model, class R>
+__device__ __forceinline__ void implicit_source_blocks(typename ModelTypes<Model>::VQ& q,
+                                                       typename ModelTypes<Model>::VA const& a,
+                                                       R dt, typename ModelTypes<Model>::VP const& p,
+                                                       R time,
+                                                       typename ModelTypes<Model>::VX const& X) {
+    constexpr int nq = Model::n_dof_q;
+    constexpr int na = Model::n_dof_qaux;
+    constexpr int NB = Model::zb_implicit_blocks, BS = Model::zb_implicit_block_size;
+    static_assert(2 + NB * BS == nq, "the blocks and rows 0, 1 cover the state");
+    const typename ModelTypes<Model>::VQ q0 = q;
+    const auto S = Model::source(q0, a, p, time, X);
+    const auto JQ = Model::source_jacobian_wrt_variables(q0, a, p);
+    const auto JA = Model::source_jacobian_wrt_aux_variables(q0, a, p);
+    const auto AQ = Model::update_aux_variables_jacobian_wrt_variables(q0, a, p, time, X);
+    // an entry of I - dt J, formed as the reference forms it
+    auto m = [&](int r, int c) -> R {
+        R t = JQ(r * nq + c, 0);
+#pragma unroll
+        for (int k = 0; k < na; ++k) t += JA(r * na + k, 0) * AQ(k * nq + c, 0);
+        return (r == c ? R(1.0) : R(0.0)) - dt * t;
+    };
+    const R m00 = m(0, 0), m11 = m(1, 1);
+    bool pre = (m00 > R(0.0)) && isfinite(m00) && (m11 > R(0.0)) && isfinite(m11) &&
+               (dt * S(0, 0) == R(0.0)) && (dt * S(1, 0) == R(0.0));
+#pragma unroll
+    for (int c = 1; c < nq; ++c) pre = pre && (m(c, 0) == R(0.0)) && (m(0, c) == R(0.0));
+#pragma unroll
+    for (int c = 2; c < nq; ++c) pre = pre && (m(1, c) == R(0.0)) && !(fabs(m(c, 1)) > m11);
+    if (!pre) {
+        implicit_source_outline<Model, R>(q, a, dt, p, time, X);
+        return;
+    }
+    R dq[NB][BS];
+    bool ok = true;
+#pragma unroll
+    for (int bi = 0; bi < NB; ++bi) {
+        R A[BS][BS], b[BS];
+#pragma unroll
+        for (int r = 0; r < BS; ++r) {
+            const int rr = Model::zb_implicit_row(bi, r);
+            b[r] = dt * S(rr, 0);
+#pragma unroll
+            for (int c = 0; c < BS; ++c) A[r][c] = m(rr, Model::zb_implicit_row(bi, c));
+        }
+#pragma unroll
+        for (int k = 0; k < BS; ++k) {
+            int piv = k;
+            R best = fabs(A[k][k]);
+#pragma unroll
+            for (int r = 0; r < BS; ++r)
+                if (r > k && fabs(A[r][k]) > best) { best = fabs(A[r][k]); piv = r; }
+            ok = ok && (best > R(0.0)) && isfinite(best);
+#pragma unroll
+            for (int r = 0; r < BS; ++r) {
+                if (r > k && r == piv) {
+#pragma unroll
+                    for (int c = 0; c < BS; ++c)
+                        if (c >= k) { const R t = A[k][c]; A[k][c] = A[r][c]; A[r][c] = t; }
+                    const R t = b[k]; b[k] = b[r]; b[r] = t;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < BS; ++r) {
+                if (r <= k) continue;
+                const R f = A[r][k] / A[k][k];
+#pragma unroll
+                for (int c = 0; c < BS; ++c)
+                    if (c >= k) A[r][c] -= f * A[k][c];
+                b[r] -= f * b[k];
+            }
+        }
+#pragma unroll
+        for (int r = BS - 1; r >= 0; --r) {
+            R s = R(0.0);
+#pragma unroll
+            for (int c = 0; c < BS; ++c)
+                if (c > r) s += A[r][c] * dq[bi][c];
+            dq[bi][r] = (b[r] - s) / A[r][r];
+            ok = ok && isfinite(dq[bi][r]);
+        }
+    }
+    if (ok) {
+        // rows 0 and 1: (0 - 0) / 1 = +0 in the reference
+        q(0, 0) = q0(0, 0) + R(0.0);
+        q(1, 0) = q0(1, 0) + R(0.0);
+#pragma unroll
+        for (int bi = 0; bi < NB; ++bi)
+#pragma unroll
+            for (int r = 0; r < BS; ++r) {
+                const int rr = Model::zb_implicit_row(bi, r);
+                q(rr, 0) = q0(rr, 0) + dq[bi][r];
+            }
+        return;
+    }
+#pragma unroll
+    for (int n = 0; n < nq; ++n) {
+        const R v = q0(n, 0) + dt * S(n, 0);
+        q(n, 0) = isfinite(v) ? v : q0(n, 0);
+    }
+}
+
+// make_rhs.H:429-509 on one cell: the structured elimination where the model
+// declares its blocks, the dense one otherwise.
+template <class Model, class R>
+__device__ __forceinline__ void implicit_source_cell(typename ModelTypes<Model>::VQ& q,
+                                                     typename ModelTypes<Model>::VA const& a,
+                                                     R dt, typename ModelTypes<Model>::VP const& p,
+                                                     R time,
+                                                     typename ModelTypes<Model>::VX const& X) {
+    if constexpr (implicit_blocks<Model>::value) implicit_source_blocks<Model, R>(q, a, dt, p, time, X);
+    else implicit_source_dense<Model, R>(q, a, dt, p, time, X);
 }
 
 // Per-cell CFL quantity of ZoomyAmr::ComputeDt (ZoomyAmr.cpp:472-487).

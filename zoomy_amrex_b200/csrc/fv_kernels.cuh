@@ -170,11 +170,15 @@ __device__ __forceinline__ bool finish_step_units(double m, double s, double* re
 
 // Blocks per SM the register budget aims at: 4 for the 2-D shallow-water
 // tile (64 registers; its shared memory, with the one face buffer, fits 4
-// blocks too), so that 32 warps hide the FP64 latency; 2 for 1-D rows and
-// for models with more than 4 unknowns, whose point-implicit elimination
-// (n^2 doubles) must stay in registers.
+// blocks too), so that 32 warps hide the FP64 latency; 3 for 2-D models
+// with more unknowns whose point-implicit system is solved by blocks; 2 for
+// 1-D rows and for dense n x n eliminations, which must stay in registers.
 template <class Model>
-constexpr int stage_min_blocks() { return (Model::dimension == 2 && Model::n_dof_q <= 4) ? 4 : 2; }
+constexpr int stage_min_blocks() {
+    if constexpr (Model::dimension == 2 && Model::n_dof_q <= 4) return 4;
+    else if constexpr (Model::dimension == 2 && implicit_blocks<Model>::value) return 3;
+    else return 2;
+}
 
 template <class Model, class Numerics, int ORDER, int MODE, bool WB, bool IMPL, int TX, int TY>
 __global__ void __launch_bounds__(TX * TY, stage_min_blocks<Model>())

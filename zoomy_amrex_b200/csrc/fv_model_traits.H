@@ -11,6 +11,13 @@
 //                   they recompute it from Q where the reference reads it.
 //   zb_static_bed — state row 0 (the bed) never changes in a step, so it is
 //                   read but never written back.
+//   zb_implicit_blocks, zb_implicit_block_size, zb_implicit_row(b, i) — the
+//                   point-implicit system's structure: rows 0 and 1 (bed,
+//                   depth) have a zero source and zero Jacobian rows, the
+//                   other rows fall into blocks (row indices ascending within
+//                   a block), and the Jacobian couples no two blocks. The FP64
+//                   elimination then runs block by block with the reference's
+//                   operations on every nonzero value (implicit_source_cell).
 #pragma once
 #include <type_traits>
 #include "AMReX_SmallMatrix.H"
@@ -35,5 +42,8 @@ template <class M> struct aux_pure<M, std::void_t<decltype(M::zb_aux_pure)>>
 template <class M, class = void> struct static_bed : std::false_type {};
 template <class M> struct static_bed<M, std::void_t<decltype(M::zb_static_bed)>>
     : std::integral_constant<bool, M::zb_static_bed> {};
+
+template <class M, class = void> struct implicit_blocks : std::false_type {};
+template <class M> struct implicit_blocks<M, std::void_t<decltype(M::zb_implicit_blocks)>> : std::true_type {};
 
 }  // namespace zfv

@@ -153,6 +153,12 @@ struct SME
     static constexpr bool zb_static_bed = true;
 
     // Row of the mean momentum along direction d, and of moment j (1-based) along d.
+    // The point-implicit system's blocks (see fv_model_traits.H): per
+    // direction d the mean momentum and its LEVEL moments.
+    static constexpr int zb_implicit_blocks = DIM;
+    static constexpr int zb_implicit_block_size = 1 + LEVEL;
+    static constexpr PORTABLE_FN int zb_implicit_row(int b, int i) { return i == 0 ? mom(b) : mnt(b, i); }
+
     static constexpr PORTABLE_FN int mom(int d) { return 2 + d; }
     static constexpr PORTABLE_FN int mnt(int d, int j) { return 2 + DIM + d * LEVEL + (j - 1); }
 
