@@ -31,6 +31,7 @@
 #include <cstdint>
 #include <type_traits>
 #include <cuda.h>
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 #include "fv_kernels.cuh"
 
@@ -116,7 +117,11 @@ struct TShape {
     static constexpr size_t fy_elems = size_t(TY + 1) * TX * NFC;
     // TMA boxes land on 128-byte boundaries: the kernel rounds the dynamic
     // shared-memory base up, which the extra 128 bytes cover
-    static constexpr size_t smem_bytes = (q_elems + inc_elems + fx_elems + fy_elems) * sizeof(float) + (TMA ? 128 : 0);
+    // the update's own inputs of each owned cell (X, lo, inc1: 3 x ne),
+    // copied asynchronously at the start of the update stages
+    static constexpr size_t epi_elems = size_t(3) * F::ne * NT;
+    static constexpr size_t smem_bytes =
+        (q_elems + inc_elems + fx_elems + fy_elems + epi_elems) * sizeof(float) + (TMA ? 128 : 0);
     __host__ __device__ static constexpr unsigned box_bytes(int planes) { return unsigned(planes) * RH * RWS * sizeof(float); }
 };
 
@@ -286,6 +291,7 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
     float* sI = sQ + Sh::q_elems;                     // TMA, stage 2: [ne][RH][RWS] increment
     float* sFx = sI + Sh::inc_elems;                  // [TY][TX+1][NFC]
     float* sFy = sFx + Sh::fx_elems;                  // [TY+1][TX][NFC]
+    float* sE = sFy + Sh::fy_elems;                   // [3][ne][NT]: X, lo, inc1 of the owned cell
     __shared__ double red[2 * ((NT + 31) / 32)];
     __shared__ __align__(8) uint64_t tbar;
     // halo-local cell (lx, ly) of row n
@@ -303,6 +309,24 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
     const double dtd = *(volatile double*)&st->dt;
     const double time = *(volatile double*)&st->time;
     const float dt = float(dtd);
+
+    // the update's own inputs of this thread's cell (X and lo; stage 2 also
+    // inc1) start loading now and arrive while the faces are computed
+    const int tx = tid % TX, ty = tid / TX;
+    const int i = x0 + tx, j = y0 + ty;
+    if constexpr (MODE != T_S1) {
+        if (i < nx && j < ny) {
+            const long long cc = (long long)j * nx + i;
+#pragma unroll
+            for (int k = 0; k < ne; ++k) {
+                __pipeline_memcpy_async(sE + k * NT + tid, X + k * plane + cc, sizeof(float));
+                __pipeline_memcpy_async(sE + (ne + k) * NT + tid, B.lo + k * plane + cc, sizeof(float));
+                if constexpr (MODE == T_S2)
+                    __pipeline_memcpy_async(sE + (2 * ne + k) * NT + tid, B.inc + k * plane + cc, sizeof(float));
+            }
+        }
+        __pipeline_commit();
+    }
 
     VP p;
 #pragma unroll
@@ -331,6 +355,7 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
             // invalid), stop it, wait (bounded) for copies still in flight
             if (tid == 0) atomicOr(&st->flags, zfv::kFlagDeviceWait | zfv::kFlagDone);
             mbar_wait(&tbar, 0);
+            if constexpr (MODE != T_S1) __pipeline_wait_prior(0);
             return;
         }
         if constexpr (MODE == T_S2) {
@@ -460,8 +485,6 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
         Fr[3 * ne + 1] = hRs;
     };
 
-    const int tx = tid % TX, ty = tid / TX;
-    const int i = x0 + tx, j = y0 + ty;
     const int iend = min(x0 + TX, nx), jend = min(y0 + TY, ny);
 
     // 3. faces, each once
@@ -548,18 +571,21 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
         } else {
             // Heun on the compensated state: Q^{n+1} = X + lo + (inc1 + inc2)/2
             // (order 1: X + lo + inc)
+            __pipeline_wait_prior(0);
             VQ qn;
             qn(0, 0) = bc;
+            float lo0 = 0.0f;
 #pragma unroll
             for (int k = 0; k < ne; ++k) {
-                const float hi = X[k * plane + c];
-                const float t = (MODE == T_ONE) ? B.lo[k * plane + c] + d[k]
-                                                : B.lo[k * plane + c] + 0.5f * (B.inc[k * plane + c] + d[k]);
+                const float hi = sE[k * NT + tid];
+                const float lo = sE[(ne + k) * NT + tid];
+                const float t = (MODE == T_ONE) ? lo + d[k] : lo + 0.5f * (sE[(2 * ne + k) * NT + tid] + d[k]);
                 float s, e;
                 two_sum(hi, t, s, e);
                 Y[k * plane + c] = s;
                 B.lo[k * plane + c] = e;
                 qn(k + 1, 0) = s;
+                if (k == 0) lo0 = e;
             }
             // this cell's CFL quantity (ZoomyAmr.cpp:472-487) and mass
             const float etan = qn(1, 0);
@@ -575,7 +601,7 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
                 if (inv > mm) mm = inv;
             }
             m_loc = double(mm);
-            s_loc = (double(etan) + double(B.lo[c])) - double(bc);
+            s_loc = (double(etan) + double(lo0)) - double(bc);
         }
     }
     if constexpr (MODE == T_S2 || MODE == T_ONE) {
