@@ -273,3 +273,70 @@ def test_fp32_level_with_device_made_aux(cuda):
     (Qa, Aa, na, ta), (Qb, Ab, nb, tb) = out
     assert na == nb == 30 and ta == tb
     assert np.array_equal(Qa, Qb) and np.array_equal(Aa, Ab)
+
+
+def _dry_dam(x):
+    r = np.sqrt((x[0] - 3.0) ** 2 + (x[1] - 5.0) ** 2)
+    h = np.where(r < 2.0, 1.0, 0.0)
+    z = np.zeros_like(h)
+    b = 0.1 * np.sin(x[0]) * np.cos(x[1])
+    return np.array([b, h, z, z])
+
+
+def test_fp32_mood_whole_step_redo(cuda, oracle):
+    """positivity = "mood" in the FP32 form (generic tile kernels): order-2
+    candidates with a negative or non-finite depth are discarded and the
+    step is redone at order 1 from Q^n (ZoomyAmr.cpp:685-720). A circular
+    dam break onto a dry bed (cfl 1, WB, walls) troubles about half of the
+    FP64 reference's steps; the FP32 form redoes steps too (which ones can
+    differ: a candidate depth of -1e-17 in FP64 can be exactly 0 in the
+    FP32 form's eta storage), stays finite and close to the reference, and
+    gives the same bits on a plain and a TMA-staged tile."""
+    from zoomy_amrex_b200.level import Level
+    model = SWE(2, "wall", _dry_dam)
+    s = dict(dimension=2, domain=[0, 10, 0, 10], n_cells=[40, 32], spatial_order=2, cfl=1.0,
+             time_end=1e30, max_step=60, positivity="mood", well_balanced=True)
+    cfg64, Q0, A0 = setup(model, s)
+    Qo, Ao, n, t, logo, redos = oracle.run(cfg64, Q0, A0)
+    assert redos > 0
+    cfg = config_from_settings(model, s, precision=ZFV_PREC_FP32)
+    outs = []
+    for v in (0, 3):
+        lev = Level(cfg, Q0, A0, variant=v)
+        try:
+            st = lev.run(chunk=20)
+            outs.append((lev.state64().cpu().numpy(), st))
+        finally:
+            lev.close()
+    assert np.array_equal(outs[0][0], outs[1][0])
+    Q32, st = outs[0]
+    dh = np.abs(Q32[1] - Qo[1])
+    print(f"[fp32 mood] redos {st['mood_redos']} (fp64 {redos}), time {st['time']:.4f} (fp64 {t:.4f}), "
+          f"depth L1 {dh.mean():.3e} Linf {dh.max():.3e}, min h {Q32[1].min():.3e} (fp64 {Qo[1].min():.3e})")
+    assert st["step"] == n and st["mood_redos"] > 0 and st["flags"] & 2
+    assert np.isfinite(Q32).all()
+
+
+def test_fp32_mood_untroubled_steps_equal_plain_steps(cuda):
+    """The MOOD candidate + commit path of the FP32 tile kernels gives the
+    plain SSP-RK2 step's bits when no step is troubled (a shallow-moment
+    case made fully wet, 0.5 m more depth everywhere, cfl 0.45)."""
+    from cases import CASES_SME
+    from zoomy_amrex_b200.level import Level
+    from zoomy_amrex_b200.workloads import fp64_twin
+    cfg64, Q0, A0 = setup(*CASES_SME["sme2d_wetdry_wb_impl_o2"])
+    Q0 = Q0.copy()
+    Q0[1] += 0.5
+    res = []
+    for mood in (0, 1):
+        cfg = fp64_twin(cfg64)
+        cfg.precision = ZFV_PREC_FP32
+        cfg.positivity_mood = mood
+        lev = Level(cfg, Q0, A0, variant=1)
+        try:
+            st = lev.run(chunk=25)
+            res.append((lev.state64().cpu().numpy(), st))
+        finally:
+            lev.close()
+    assert res[1][1]["mood_redos"] == 0 and res[0][1]["step"] == res[1][1]["step"]
+    assert np.array_equal(res[0][0], res[1][0])

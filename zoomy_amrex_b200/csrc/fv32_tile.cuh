@@ -76,6 +76,7 @@ struct TileBufs {
     float* alt;             // state buffer 1 (n-1 planes)
     float* inc;             // stage-1 increment (n-1 planes)
     float* lo;              // compensation remainders (n-1 planes)
+    float* lo2;             // MOOD: the order-2 candidate's remainders (n-1 planes), else null
     zfv::DevState* st;
     double* partials;
     double* log3;
@@ -90,8 +91,14 @@ struct TileMaps {
 
 // T_S1 / T_S2: the two SSP-RK2 stages (spatial order 2); T_ONE: the single
 // forward-Euler stage of spatial order 1 (Q^{n+1} = Q^n + dt RHS, then the
-// step's reduction), as the reference's order-1 Advance.
-enum TMode : int { T_S1 = 1, T_S2 = 2, T_ONE = 3 };
+// step's reduction), as the reference's order-1 Advance. MOOD (positivity
+// "mood", ZoomyAmr.cpp:699-730): T_S2M writes the order-2 Heun candidate
+// (its remainders to lo2) and flags a troubled step, k32t_mood_commit takes
+// an untroubled candidate, and T_R1 / T_R2 redo a troubled step at order 1
+// from Q^n (both run only for a troubled step).
+enum TMode : int { T_S1 = 1, T_S2 = 2, T_ONE = 3, T_S2M = 4, T_R1 = 5, T_R2 = 6 };
+template <int MODE> __host__ __device__ constexpr bool t_stage1() { return MODE == T_S1 || MODE == T_R1; }
+template <int MODE> __host__ __device__ constexpr bool t_stage2() { return MODE == T_S2 || MODE == T_S2M || MODE == T_R2; }
 constexpr float kNearDry = 1.0e-3f;
 // try_wait polls of an mbarrier before a stage gives up (each poll may block
 // for a hardware-defined interval): a bound, so that a copy that never
@@ -303,6 +310,9 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
     const long long plane = L.plane;
     zfv::DevState* st = B.st;
     if (*(volatile unsigned*)&st->flags & zfv::kFlagDone) return;   // stopped: the state stays put
+    if constexpr (MODE == T_R1 || MODE == T_R2) {                     // the redo runs for a troubled step only
+        if (*(volatile unsigned*)&st->troubled == 0u) return;
+    }
     const unsigned parity = *(volatile unsigned*)&st->parity;
     const float* X = parity ? B.alt : B.Qs;
     float* Y = parity ? B.Qs : B.alt;
@@ -314,14 +324,14 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
     // inc1) start loading now and arrive while the faces are computed
     const int tx = tid % TX, ty = tid / TX;
     const int i = x0 + tx, j = y0 + ty;
-    if constexpr (MODE != T_S1) {
+    if constexpr (!t_stage1<MODE>()) {
         if (i < nx && j < ny) {
             const long long cc = (long long)j * nx + i;
 #pragma unroll
             for (int k = 0; k < ne; ++k) {
                 __pipeline_memcpy_async(sE + k * NT + tid, X + k * plane + cc, sizeof(float));
                 __pipeline_memcpy_async(sE + (ne + k) * NT + tid, B.lo + k * plane + cc, sizeof(float));
-                if constexpr (MODE == T_S2)
+                if constexpr (t_stage2<MODE>())
                     __pipeline_memcpy_async(sE + (2 * ne + k) * NT + tid, B.inc + k * plane + cc, sizeof(float));
             }
         }
@@ -342,12 +352,12 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
         }
         __syncthreads();
         if (tid == 0) {
-            constexpr unsigned bytes = Sh::box_bytes(nq) + (MODE == T_S2 ? Sh::box_bytes(ne) : 0u);
+            constexpr unsigned bytes = Sh::box_bytes(nq) + (t_stage2<MODE>() ? Sh::box_bytes(ne) : 0u);
             mbar_expect_tx(&tbar, bytes);
             const int bx = x0 - G - XO, by = y0 - G;        // bx is a multiple of 4 (TX is)
             tma_load_3d(sQ, &maps.bed, bx, by, 0, &tbar);
             tma_load_3d(sQ + RH * RWS, parity ? &maps.alt : &maps.qs, bx, by, 0, &tbar);
-            if constexpr (MODE == T_S2) tma_load_3d(sI, &maps.inc, bx, by, 0, &tbar);
+            if constexpr (t_stage2<MODE>()) tma_load_3d(sI, &maps.inc, bx, by, 0, &tbar);
         }
         const bool done = mbar_wait(&tbar, 0);
         if (__syncthreads_or(!done)) {
@@ -355,10 +365,10 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
             // invalid), stop it, wait (bounded) for copies still in flight
             if (tid == 0) atomicOr(&st->flags, zfv::kFlagDeviceWait | zfv::kFlagDone);
             mbar_wait(&tbar, 0);
-            if constexpr (MODE != T_S1) __pipeline_wait_prior(0);
+            if constexpr (!t_stage1<MODE>()) __pipeline_wait_prior(0);
             return;
         }
-        if constexpr (MODE == T_S2) {
+        if constexpr (t_stage2<MODE>()) {
             for (int k = tid; k < ne * RH * RWS; k += NT) sQ[RH * RWS + k] += sI[k];
         }
     } else {
@@ -371,7 +381,7 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
 #pragma unroll
                 for (int n = 1; n < nq; ++n) {
                     float v = X[(n - 1) * plane + c];
-                    if constexpr (MODE == T_S2) v = v + B.inc[(n - 1) * plane + c];
+                    if constexpr (t_stage2<MODE>()) v = v + B.inc[(n - 1) * plane + c];
                     sq(n, lx, ly) = v;
                 }
             }
@@ -565,7 +575,7 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
                 for (int n = 1; n < nq; ++n) d[n - 1] = d[n - 1] + dq(n, 0);
             }
         }
-        if constexpr (MODE == T_S1) {
+        if constexpr (t_stage1<MODE>()) {
 #pragma unroll
             for (int k = 0; k < ne; ++k) B.inc[k * plane + c] = d[k];
         } else {
@@ -583,13 +593,22 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
                 float s, e;
                 two_sum(hi, t, s, e);
                 Y[k * plane + c] = s;
-                B.lo[k * plane + c] = e;
+                // the MOOD candidate keeps its remainders apart: a redo
+                // starts again from Q^n's
+                if constexpr (MODE == T_S2M) B.lo2[k * plane + c] = e;
+                else B.lo[k * plane + c] = e;
                 qn(k + 1, 0) = s;
                 if (k == 0) lo0 = e;
             }
             // this cell's CFL quantity (ZoomyAmr.cpp:472-487) and mass
             const float etan = qn(1, 0);
             qn(1, 0) = etan - bc;
+            if constexpr (MODE == T_S2M) {
+                // ZoomyAmr.cpp:706-708: a depth below zero or not finite
+                // troubles the whole step
+                const float hh = qn(1, 0);
+                if (!(hh >= 0.0f) || !(hh < 3.0e38f)) atomicOr(&st->troubled, 1u);
+            }
             VX Xz{};
             const VA an = M::update_aux_variables(qn, azero, p, float(time), Xz);
             float mm = 0.0f;
@@ -604,14 +623,76 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
             s_loc = (double(etan) + double(lo0)) - double(bc);
         }
     }
-    if constexpr (MODE == T_S2 || MODE == T_ONE) {
+    if constexpr (MODE == T_S2 || MODE == T_ONE || MODE == T_R2) {
         const bool last = zfv::finish_step_units<NT>(m_loc, s_loc, red, B.partials, B.log3, B.log_cap, st, L,
-                                                      dtd, time, false, gridDim.x * gridDim.y,
+                                                      dtd, time, MODE == T_R2, gridDim.x * gridDim.y,
                                                       blockIdx.y * gridDim.x + blockIdx.x);
         if (last && threadIdx.x == 0) {   // every block of the step has read parity by now
             st->parity = parity ^ 1u;
             __threadfence();
         }
+    }
+}
+
+// MOOD commit (ZoomyAmr.cpp:699-730): when no cell of the order-2 candidate
+// is troubled, the candidate (written by T_S2M to the other state buffer,
+// its remainders to lo2) becomes Q^{n+1}: its remainders move to lo, and
+// this kernel does the step's CFL / mass reduction and flips the state
+// buffers, as T_S2 does. For a troubled step it does nothing and the order-1
+// redo finishes the step.
+template <class F, int NT>
+__global__ void __launch_bounds__(NT)
+k32t_mood_commit(TileParams<F::np> L, TileBufs B) {
+    using M = typename F::M32;
+    using N = typename F::N32;
+    constexpr int nq = F::nq, ne = F::ne;
+    __shared__ double red[2 * ((NT + 31) / 32)];
+    zfv::DevState* st = B.st;
+    if (*(volatile unsigned*)&st->flags & zfv::kFlagDone) return;
+    if (*(volatile unsigned*)&st->troubled != 0u) return;
+    const unsigned parity = *(volatile unsigned*)&st->parity;
+    const float* Y = parity ? B.Qs : B.alt;            // the candidate
+    const double dtd = *(volatile double*)&st->dt;
+    const double time = *(volatile double*)&st->time;
+    const long long plane = L.plane;
+    typename M::VP p;
+#pragma unroll
+    for (int k = 0; k < F::np; ++k) p(k, 0) = L.pf[k];
+    const typename M::VA azero{};
+    double m_loc = 0.0, s_loc = 0.0;
+    for (long long c = (long long)blockIdx.x * NT + threadIdx.x; c < plane; c += (long long)gridDim.x * NT) {
+        const float bc = B.bed[c];
+        typename M::VQ qn;
+        qn(0, 0) = bc;
+        float lo0 = 0.0f;
+#pragma unroll
+        for (int k = 0; k < ne; ++k) {
+            const float e = B.lo2[k * plane + c];
+            B.lo[k * plane + c] = e;
+            qn(k + 1, 0) = Y[k * plane + c];
+            if (k == 0) lo0 = e;
+        }
+        const float etan = qn(1, 0);
+        qn(1, 0) = etan - bc;
+        typename M::VX Xz{};
+        const typename M::VA an = M::update_aux_variables(qn, azero, p, float(time), Xz);
+        float mm = 0.0f;
+#pragma unroll
+        for (int dd = 0; dd < 2; ++dd) {
+            typename M::VN nh{};
+            nh(dd, 0) = 1.0f;
+            const float inv = N::local_max_abs_eigenvalue(qn, an, p, nh)(0, 0) * (dd == 0 ? L.rdx : L.rdy);
+            if (inv > mm) mm = inv;
+        }
+        if (double(mm) > m_loc) m_loc = double(mm);
+        s_loc = s_loc + ((double(etan) + double(lo0)) - double(bc));
+    }
+    (void)nq;
+    const bool last = zfv::finish_step_units<NT>(m_loc, s_loc, red, B.partials, B.log3, B.log_cap, st, L, dtd,
+                                                  time, false, gridDim.x, blockIdx.x);
+    if (last && threadIdx.x == 0) {
+        st->parity = parity ^ 1u;
+        __threadfence();
     }
 }
 

@@ -27,6 +27,7 @@ struct ScratchLayout {
     size_t stage = 0;        // FP64: n_q stage planes; FP32: increment planes
     size_t alt = 0;          // FP32: ping-pong state planes
     size_t lo = 0;           // FP32: compensation planes
+    size_t lo2 = 0;          // FP32 with MOOD: the order-2 candidate's compensation planes
     size_t jfnk = 0;         // FP64 with implicit_global: the Newton-Krylov work area
     size_t total = 0;
 };

@@ -171,8 +171,10 @@ int zfv_create(const zfv_config* cfg, zfv_handle** out) {
     if (!h) return fail(-4, "zfv_create: out of host memory");
     h->cfg = *cfg;
     if (cfg->precision == ZFV_PREC_FP32) {
-        // the shallow-water sweep is order 2; order 1 runs on the generic tile kernels
-        if (cfg->model == ZFV_MODEL_SWE2D && cfg->spatial_order == 2) h->run.reset(make_runner_fp32_swe2d(h));
+        // the shallow-water sweep is order 2 without MOOD; order 1 and MOOD run on
+        // the generic tile kernels
+        if (cfg->model == ZFV_MODEL_SWE2D && cfg->spatial_order == 2 && !cfg->positivity_mood)
+            h->run.reset(make_runner_fp32_swe2d(h));
         else h->run.reset(make_runner_fp32_generic(h));
     } else {
         switch (cfg->model) {

@@ -1,8 +1,10 @@
 // FP32 chosen form of the families without a hand-tuned sweep
 // (ZFV_PREC_FP32 with ZFV_MODEL_SME2D_L2, and ZFV_MODEL_SWE2D at spatial
-// order 1, which the shallow-water sweep does not implement): the generic
-// tile kernels of fv32_tile.cuh behind the Runner interface. Order 2 runs
-// the two SSP-RK2 stages, order 1 one forward-Euler stage per step. Compiled with FMA contraction
+// order 1 or with positivity "mood", which the shallow-water sweep does not
+// implement): the generic tile kernels of fv32_tile.cuh behind the Runner
+// interface. Order 2 runs the two SSP-RK2 stages, order 1 one forward-Euler
+// stage per step; MOOD adds the candidate, commit and order-1 redo launches
+// (the redo stages return at once for an untroubled step). Compiled with FMA contraction
 // and the hardware's approximate FP32 division and square root, like
 // zoomy_fv32.cu.
 //
@@ -74,6 +76,7 @@ struct RunnerTile final : Runner {
     TileParams<NP> L;
     int var = 0;
     bool order1 = false;
+    bool mood = false;     // positivity "mood" at order 2
 
     explicit RunnerTile(zfv_handle* hh) : h(hh) {
         const zfv_config& c = h->cfg;
@@ -112,12 +115,14 @@ struct RunnerTile final : Runner {
                                                int(ShapeV<V, TMA>::smem_bytes)),
                           "cudaFuncSetAttribute (FP32 tile)");
     }
-    template <int V, bool WB, bool IMPL>
-    int set_smem2() {
-        return set_smem1<V, T_S1, WB, IMPL, false>() | set_smem1<V, T_S2, WB, IMPL, false>() |
-               set_smem1<V, T_ONE, WB, IMPL, false>() | set_smem1<V, T_S1, WB, IMPL, true>() |
-               set_smem1<V, T_S2, WB, IMPL, true>() | set_smem1<V, T_ONE, WB, IMPL, true>();
+    template <int V, bool WB, bool IMPL, bool TMA>
+    int set_smem_modes() {
+        return set_smem1<V, T_S1, WB, IMPL, TMA>() | set_smem1<V, T_S2, WB, IMPL, TMA>() |
+               set_smem1<V, T_ONE, WB, IMPL, TMA>() | set_smem1<V, T_S2M, WB, IMPL, TMA>() |
+               set_smem1<V, T_R1, WB, IMPL, TMA>() | set_smem1<V, T_R2, WB, IMPL, TMA>();
     }
+    template <int V, bool WB, bool IMPL>
+    int set_smem2() { return set_smem_modes<V, WB, IMPL, false>() | set_smem_modes<V, WB, IMPL, true>(); }
     template <int V>
     int set_smem_v() {
         return set_smem2<V, false, false>() | set_smem2<V, false, true>() | set_smem2<V, true, false>() |
@@ -149,7 +154,8 @@ struct RunnerTile final : Runner {
         if (c.spatial_order != 1 && c.spatial_order != 2)
             return fail(-2, "zfv_create: the FP32 form implements spatial_order 1 and 2");
         order1 = c.spatial_order == 1;
-        if (c.positivity_mood) return fail(-2, "zfv_create: the FP32 form does not implement MOOD");
+        if (c.clamp_positivity) return fail(-1, "zfv_create: the FP32 form does not implement clamp_positivity");
+        mood = c.positivity_mood && c.spatial_order == 2;   // as the FP64 form: MOOD redoes order-2 steps
         if (c.implicit_global && c.implicit_source)
             return fail(-1, "zfv_create: implicit_global is built for the FP64 form");
         return set_smem_v<0>() | set_smem_v<1>() | set_smem_v<2>();
@@ -164,7 +170,8 @@ struct RunnerTile final : Runner {
         S.alt = S.stage + align_up(pb * ne);
         S.lo = S.alt + align_up(pb * ne);
         S.jfnk = 0;
-        S.total = S.lo + align_up(pb * ne);
+        S.lo2 = mood ? S.lo + align_up(pb * ne) : 0;
+        S.total = (mood ? S.lo2 : S.lo) + align_up(pb * ne);
     }
 
     TileBufs bufs(const void* Q, char* scratch) const {
@@ -176,6 +183,7 @@ struct RunnerTile final : Runner {
         B.alt = reinterpret_cast<float*>(scratch + S.alt);
         B.inc = reinterpret_cast<float*>(scratch + S.stage);
         B.lo = reinterpret_cast<float*>(scratch + S.lo);
+        B.lo2 = mood ? reinterpret_cast<float*>(scratch + S.lo2) : nullptr;
         B.st = reinterpret_cast<zfv::DevState*>(scratch + S.state);
         B.partials = reinterpret_cast<double*>(scratch + S.partials);
         B.log3 = reinterpret_cast<double*>(scratch + S.log);
@@ -209,6 +217,13 @@ struct RunnerTile final : Runner {
         for (int k = 0; k < n; ++k) {
             if (order1) {
                 k32t_stage<F, T_ONE, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 0, maps);
+            } else if (mood) {
+                // ZoomyAmr.cpp:699-730: candidate, then commit or whole-step order-1 redo
+                k32t_stage<F, T_S1, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 1, maps);
+                k32t_stage<F, T_S2M, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 1, maps);
+                k32t_mood_commit<F, kReduceNT><<<reduce_blocks(), kReduceNT, 0, s>>>(L, B);
+                k32t_stage<F, T_R1, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 0, maps);
+                k32t_stage<F, T_R2, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 0, maps);
             } else {
                 k32t_stage<F, T_S1, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 1, maps);
                 k32t_stage<F, T_S2, WB, IMPL, TX, TY, TMA><<<grid, TX * TY, sm, s>>>(L, B, 1, maps);

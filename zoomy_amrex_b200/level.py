@@ -20,11 +20,12 @@ from ._abi import MODELS, ZFV_MODEL_SWE2D, ZFV_PREC_FP32, zfv_config, zfv_status
 
 def fp32_kernel_family(cfg: zfv_config) -> str:
     """Which FP32 kernels run a level, and so which shapes its variant
-    indexes: "fp32" = the shallow-water column sweep (2-D SWE, order 2;
-    batch.tile_variants()), "fp32-tile" = the generic tile kernels (every
+    indexes: "fp32" = the shallow-water column sweep (2-D SWE, order 2, no
+    MOOD; batch.tile_variants()), "fp32-tile" = the generic tile kernels (every
     other FP32 case; batch.generic_tile_variants()). The autotuner caches
     the two under these names."""
-    return "fp32" if (cfg.model == ZFV_MODEL_SWE2D and cfg.spatial_order == 2) else "fp32-tile"
+    sweep = cfg.model == ZFV_MODEL_SWE2D and cfg.spatial_order == 2 and not cfg.positivity_mood
+    return "fp32" if sweep else "fp32-tile"
 
 _DTYPE = torch.float64
 
