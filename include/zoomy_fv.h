@@ -53,10 +53,13 @@ enum {
 /* Arithmetic form. */
 enum {
     ZFV_PREC_FP64 = 0,     /* the plain form: FP64 everywhere, bit-compatible with the CPU path */
-    ZFV_PREC_FP32 = 1      /* the chosen form (ZFV_MODEL_SWE2D): FP32 state and flux arithmetic,
-                              Q = [b, eta = h + b, hu, hv] as float, compensation planes in
-                              scratch carry the low-order part of eta, hu, hv (compensated
-                              update); FP64 for near-dry implicit sources and the mass sum */
+    ZFV_PREC_FP32 = 1      /* the chosen form (ZFV_MODEL_SWE2D, ZFV_MODEL_SME2D_L2): FP32 state
+                              and flux arithmetic, Q = [b, eta = h + b, q_2, ...] as float,
+                              compensation planes in scratch carry the low-order part of the
+                              evolved rows (compensated update); FP64 for near-dry implicit
+                              sources and the mass sum. 2-D SWE at order 2 without MOOD runs
+                              on the column sweep (zfv_tile_variants); SME, order 1 and
+                              MOOD run on the generic tile kernels (zfv_generic_tile_variants) */
 };
 
 /* Status flags (bitwise OR) reported by zfv_get_status(). */
@@ -290,7 +293,8 @@ int zfv_batch_units(const zfv_batch* b);
 int zfv_tile_variants(int* nw, int* cpt, int* cols, int* flags, int max_n);
 /*
  * Tile variants of the generic FP32 kernels (the FP32 form of the
- * shallow-moment model, ZFV_MODEL_SME2D_L2): tile width and height in cells
+ * shallow-moment model, ZFV_MODEL_SME2D_L2, and of 2-D SWE at spatial order 1
+ * or with positivity_mood): tile width and height in cells
  * and the staging (0 = plain coalesced loads, 1 = TMA boxes completing on an
  * mbarrier; needs nx % 4 == 0 and a 16-byte aligned state). Writes up to
  * max_n of them and returns how many exist; zfv_set_variant selects one for
