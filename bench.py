@@ -444,6 +444,12 @@ def adjoint_bench(local, n=1024, steps=200, every=20, n_dirs=32, eps=1e-6, seed=
     import torch
     from zoomy_amrex_b200.adjoint import evolve_differentiable, forward_only
     dev = f"cuda:{local}"
+    # start from an empty allocator cache: the sections before leave blocks of
+    # other sizes behind, and the warm-up below should be what caches the
+    # checkpoints and tapes the timed run reuses
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     rng = np.random.default_rng(seed)
     Q0, A0 = workload_fields(n)
     cfg = workload_config(n)

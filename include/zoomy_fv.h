@@ -425,6 +425,10 @@ size_t zfv_adj_work_bytes(const zfv_handle* h);
 int zfv_adj_record(zfv_handle* h, void* Q, void* aux, void* scratch, void* tape, int n_steps, void* stream);
 int zfv_adj_step(zfv_handle* h, const void* tape, int k, void* lam, double* grad, const void* aux0,
                  void* work, void* stream);
+/* zfv_adj_step for recorded steps n_steps - 1 down to 0 of `tape`, in one
+ * call (aux0, or NULL, is passed for step 0 only). */
+int zfv_adj_steps(zfv_handle* h, const void* tape, int n_steps, void* lam, double* grad, const void* aux0,
+                  void* work, void* stream);
 /* Tile shapes compiled for the adjoint's face-reverse kernel (a process-wide
  * tuning choice; every shape gives the same gradient up to rounding). */
 int zfv_adj_variants(void);

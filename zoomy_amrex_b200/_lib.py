@@ -27,7 +27,8 @@ SYMBOLS = ("zfv_last_error", "zfv_version", "zfv_sizeof_config", "zfv_sizeof_sta
            "zfv_batch_stage", "zfv_batch_descriptors", "zfv_amr_fill", "zfv_amr_average_down", "zfv_amr_tag",
            "zfv_amr_regrid_fill", "zfv_amr_set_dt", "zfv_implicit_global_stats",
            "zfv_batch_compute_dt", "zfv_amr_level_dt",
-           "zfv_init_solution", "zfv_set_variant", "zfv_get_variant", "zfv_generic_tile_variants")
+           "zfv_init_solution", "zfv_set_variant", "zfv_get_variant", "zfv_generic_tile_variants",
+           "zfv_adj_steps")
 
 
 class ZfvError(RuntimeError):
@@ -92,6 +93,7 @@ def lib():
     L.zfv_adj_work_bytes.restype = C.c_size_t
     L.zfv_adj_record.argtypes = [vp, vp, vp, vp, vp, i, vp]
     L.zfv_adj_step.argtypes = [vp, vp, i, vp, vp, vp, vp, vp]
+    L.zfv_adj_steps.argtypes = [vp, vp, i, vp, vp, vp, vp, vp]
     L.zfv_adj_set_variant.argtypes = [i]
     L.zfv_batch_create_grouped.argtypes = [C.POINTER(zfv_config), i, C.POINTER(i), C.POINTER(vp)]
     L.zfv_batch_set_frames.argtypes = [vp, pp, vp]

@@ -134,10 +134,10 @@ class SWEEvolve(torch.autograd.Function):
         sol.stream.wait_stream(torch.cuda.current_stream(device))
 
         def reverse(start, n, tape):
-            for k in reversed(range(n)):
-                aux0 = ctx.aux0.data_ptr() if start + k == 0 else None
-                _lib.check(L.zfv_adj_step(sol.h, tape.data_ptr(), k, lam.data_ptr(), grad.data_ptr(), aux0,
-                                          work.data_ptr(), sol.s()), "zfv_adj_step")
+            # the segment's steps n-1 .. 0 in one call (no host round trip per step)
+            aux0 = ctx.aux0.data_ptr() if start == 0 else None
+            _lib.check(L.zfv_adj_steps(sol.h, tape.data_ptr(), n, lam.data_ptr(), grad.data_ptr(), aux0,
+                                       work.data_ptr(), sol.s()), "zfv_adj_steps")
 
         with torch.cuda.stream(sol.stream):
             if ctx.last is not None:

@@ -316,6 +316,19 @@ int zfv_adj_step(zfv_handle* h, const void* tape, int k, void* lam, double* grad
                             static_cast<const double*>(aux0), static_cast<char*>(work), (cudaStream_t)stream);
 }
 
+int zfv_adj_steps(zfv_handle* h, const void* tape, int n_steps, void* lam, double* grad, const void* aux0,
+                  void* work, void* stream) {
+    if (!h || !tape || !lam || !grad || !work) return fail(-1, "zfv_adj_steps: null argument");
+    if (n_steps < 0) return fail(-1, "zfv_adj_steps: negative step count");
+    for (int k = n_steps - 1; k >= 0; --k) {
+        const int rc = h->run->adj_step(static_cast<const char*>(tape), k, static_cast<double*>(lam), grad,
+                                        k == 0 ? static_cast<const double*>(aux0) : nullptr,
+                                        static_cast<char*>(work), (cudaStream_t)stream);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
 int zfv_adj_set_variant(int variant) { return adj_set_variant(variant); }
 
 int zfv_adj_variants(void) { return adj_variants(); }
