@@ -33,6 +33,22 @@ def _copy_cfg(cfg: zfv_config) -> zfv_config:
     return c
 
 
+# One side stream per device for every solver of this module: the caching
+# allocator keeps freed blocks per stream, so checkpoints and tapes of one
+# gradient computation are reused by the next one instead of being allocated
+# again (a 2 GB tape allocated inside a backward can cost more than the
+# backward's kernels).
+_STREAMS: dict = {}
+
+
+def _side_stream(device) -> "torch.cuda.Stream":
+    d = torch.device(device)
+    key = d.index if d.index is not None else torch.cuda.current_device()
+    if key not in _STREAMS:
+        _STREAMS[key] = torch.cuda.Stream(d)
+    return _STREAMS[key]
+
+
 class _Solver:
     """A handle plus the buffers the forward/backward share."""
 
@@ -45,7 +61,7 @@ class _Solver:
         _lib.check(L.zfv_create(C.byref(cfg), C.byref(h)), "zfv_create")
         self.h = h
         self.device = device
-        self.stream = torch.cuda.Stream(device)
+        self.stream = _side_stream(device)
         self.scratch = torch.zeros(int(L.zfv_scratch_bytes(h)), dtype=torch.uint8, device=device)
         self.rs_bytes = int(L.zfv_run_state_bytes())
         info = MODELS[cfg.model]

@@ -34,6 +34,7 @@
 #include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 #include "fv_kernels.cuh"
+#include "fv_async.cuh"
 
 namespace zfv32t {
 
@@ -100,10 +101,6 @@ enum TMode : int { T_S1 = 1, T_S2 = 2, T_ONE = 3, T_S2M = 4, T_R1 = 5, T_R2 = 6 
 template <int MODE> __host__ __device__ constexpr bool t_stage1() { return MODE == T_S1 || MODE == T_R1; }
 template <int MODE> __host__ __device__ constexpr bool t_stage2() { return MODE == T_S2 || MODE == T_S2M || MODE == T_R2; }
 constexpr float kNearDry = 1.0e-3f;
-// try_wait polls of an mbarrier before a stage gives up (each poll may block
-// for a hardware-defined interval): a bound, so that a copy that never
-// completes ends in an error flag instead of a hang
-constexpr int kMaxBarrierPolls = 1 << 22;
 
 // Shared-memory layout of a tile. Plain loads stage the tile and its 2-cell
 // halo as (TX + 4) x (TY + 4) per row; TMA boxes start 4 columns to the
@@ -132,49 +129,12 @@ struct TShape {
     __host__ __device__ static constexpr unsigned box_bytes(int planes) { return unsigned(planes) * RH * RWS * sizeof(float); }
 };
 
-// --- TMA (cp.async.bulk.tensor) and mbarrier helpers, this CTA only -------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() {
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
-    uint32_t ok;
-    asm volatile(
-        "{\n"
-        " .reg .pred p;\n"
-        " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n"
-        "}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(phase)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for the barrier's phase; false when the polls ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
-    for (int it = 0; it < kMaxBarrierPolls; ++it)
-        if (mbar_try_wait(bar, phase)) return true;
-    return false;
-}
-// One 3-D box of a tensor map (x, y, plane) into this CTA's shared memory,
-// completing on `bar`. x must be a multiple of 4 floats (16 bytes).
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
-                                            uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-        : "memory");
-}
+// TMA and mbarrier helpers (fv_async.cuh)
+using zfv::mbar_expect_tx;
+using zfv::mbar_fence_init;
+using zfv::mbar_init;
+using zfv::mbar_wait;
+using zfv::tma_load_3d;
 
 __device__ __forceinline__ float mmf(float a, float b) {
     if (a * b <= 0.0f) return 0.0f;
