@@ -772,7 +772,10 @@ def main():
                 "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_FP32, "traffic_per": "launch",
                 "fp64_plain": {"achieved": achieved64, "frac": achieved64 / peak,
                                "algorithmic_bytes_per_cell_step": BYTES_PER_CELL_STEP_FP64,
-                               "bound": "fp64 alu"}}
+                               "bound": "fp64 latency",
+                               "note": "ncu: FP64 pipe 49-52 % busy, issue active 66-68 %, "
+                                       "fixed-latency stalls on FP64 dependency chains; "
+                                       "DRAM 5-7 % of peak"}}
     sm_mhz = (clk.summary() or {}).get("sm_mhz") or 1965.0
     issue_peak = N_SM * SCHEDULERS_PER_SM * sm_mhz * 1e6
     issue = cells * NCU_WARP_INSTR_PER_CELL_STEP_FP32 / step32
