@@ -45,16 +45,17 @@ BYTES_PER_CELL_STEP_FP32 = 92
 
 # DRAM bytes per cell per step (both stage launches), from `ncu --set full`
 # of `python -m zoomy_amrex_b200.profile_case fp32 --n 3072 --variant 9
-# --steps 3` (the shape the autotuner picks for the 4096^2 level): stage 1
-# read 151.2 MB + wrote 79.4 MB, stage 2 read 378.5 MB + wrote 191.1 MB over
+# --steps 3` (4 warps x 8 rows, column pairs; the autotuner's pick for the
+# 4096^2 level is this shape or its 16-row twin, within 1 %): stage 1 read
+# 151.2 MB + wrote 78.9 MB, stage 2 read 378.5 MB + wrote 188.5 MB over
 # 3072^2 cells. The traffic scales with the cells, so it is scaled to the
 # benchmark grid per launch.
-NCU_TRAFFIC_PER_CELL_STEP_FP32 = 84.79
-# Warp instructions per cell per step of the same capture (stage 1 10.66 +
-# stage 2 14.37): the FP32 stages are bound by instruction issue, so the
+NCU_TRAFFIC_PER_CELL_STEP_FP32 = 84.45
+# Warp instructions per cell per step of the same capture (stage 1 10.12 +
+# stage 2 13.80): the FP32 stages are bound by instruction issue, so the
 # line also reports the issue rate they reach against the SMs' peak (148 SMs
 # x 4 schedulers x 1 warp instruction per cycle at the sampled SM clock).
-NCU_WARP_INSTR_PER_CELL_STEP_FP32 = 25.03
+NCU_WARP_INSTR_PER_CELL_STEP_FP32 = 23.92
 N_SM, SCHEDULERS_PER_SM = 148, 4
 
 
@@ -782,7 +783,7 @@ def main():
     roofline["issue"] = {"achieved": issue, "peak": issue_peak, "unit": "warp instructions/s",
                          "frac": issue / issue_peak,
                          "warp_instructions_per_cell_step": NCU_WARP_INSTR_PER_CELL_STEP_FP32,
-                         "note": "the bound the FP32 stages meet (ncu: issue active 56-63 %); "
+                         "note": "the bound the FP32 stages meet (ncu: issue active 55-63 %); "
                                  "instructions per cell from the ncu capture of the same kernels"}
 
     ens = None

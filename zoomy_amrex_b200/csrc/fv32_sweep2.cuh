@@ -80,23 +80,39 @@ struct FaceLR {
 template <int DIR, bool WB>
 __device__ __forceinline__ FaceLR face2(RS2 a, RS2 c, const Params& L) {
     float2 db = s2(0.0f);
+    float2 qL, qR;          // normal velocities of the face states
     if constexpr (WB) {
         const float2 bf = fmax2(a.b, c.b);
         const float2 hsL = fmax2(s2(0.0f), sub(a.e, bf)), hsR = fmax2(s2(0.0f), sub(c.e, bf));
-        const float2 sL = f2((a.h.x > 0.0f) ? __fdividef(hsL.x, a.h.x) : 0.0f,
-                             (a.h.y > 0.0f) ? __fdividef(hsL.y, a.h.y) : 0.0f);
-        const float2 sR = f2((c.h.x > 0.0f) ? __fdividef(hsR.x, c.h.x) : 0.0f,
-                             (c.h.y > 0.0f) ? __fdividef(hsR.y, c.h.y) : 0.0f);
-        a.u = mul(a.u, sL); a.v = mul(a.v, sL); c.u = mul(c.u, sR); c.v = mul(c.v, sR);
+        const float hs_min = fminf(fminf(hsL.x, hsL.y), fminf(hsR.x, hsR.y));
+        const float h_min = fminf(fminf(a.h.x, a.h.y), fminf(c.h.x, c.h.y));
+        if (__all_sync(__activemask(), hs_min > L.hwet && h_min > 0.0f)) {
+            // every face depth wet: with r = 1/h the Audusse factor is
+            // s = h* r and the normal velocity (s m_n) / h* is m_n r, so one
+            // reciprocal per side serves both
+            const float2 rL = f2(1.0f / a.h.x, 1.0f / a.h.y), rR = f2(1.0f / c.h.x, 1.0f / c.h.y);
+            const float2 sL = mul(hsL, rL), sR = mul(hsR, rR);
+            qL = mul((DIR == 0) ? a.u : a.v, rL);
+            qR = mul((DIR == 0) ? c.u : c.v, rR);
+            a.u = mul(a.u, sL); a.v = mul(a.v, sL); c.u = mul(c.u, sR); c.v = mul(c.v, sR);
+        } else {
+            const float2 sL = f2((a.h.x > 0.0f) ? __fdividef(hsL.x, a.h.x) : 0.0f,
+                                 (a.h.y > 0.0f) ? __fdividef(hsL.y, a.h.y) : 0.0f);
+            const float2 sR = f2((c.h.x > 0.0f) ? __fdividef(hsR.x, c.h.x) : 0.0f,
+                                 (c.h.y > 0.0f) ? __fdividef(hsR.y, c.h.y) : 0.0f);
+            a.u = mul(a.u, sL); a.v = mul(a.v, sL); c.u = mul(c.u, sR); c.v = mul(c.v, sR);
+            qL = mul((DIR == 0) ? a.u : a.v, kp_hinv2(hsL, L));
+            qR = mul((DIR == 0) ? c.u : c.v, kp_hinv2(hsR, L));
+        }
         a.h = hsL; c.h = hsR;
     } else {
         db = sub(c.b, a.b);
+        qL = mul((DIR == 0) ? a.u : a.v, kp_hinv2(a.h, L));
+        qR = mul((DIR == 0) ? c.u : c.v, kp_hinv2(c.h, L));
     }
     const float2 g = s2(L.g), hg = s2(0.5f * L.g), half = s2(0.5f);
-    const float2 hiL = kp_hinv2(a.h, L), hiR = kp_hinv2(c.h, L);
     const float2 unL = (DIR == 0) ? a.u : a.v, unR = (DIR == 0) ? c.u : c.v;
     const float2 pL = mul(mul(hg, a.h), a.h), pR = mul(mul(hg, c.h), c.h);
-    const float2 qL = mul(unL, hiL), qR = mul(unR, hiR);
     float2 fuL, fvL, fuR, fvR;
     if constexpr (DIR == 0) {
         fuL = fma(a.u, qL, pL);  fvL = mul(a.v, qL);
@@ -164,7 +180,9 @@ __device__ __forceinline__ void manning_implicit2(float2 h, float2 u, float2 v, 
     const float2 sp = sqrt2(fma(ux, ux, mul(uy, uy)));
     const float2 Su = sub(mul(s2(L.g * L.ex), h), mul(mul(k, ux), sp));
     const float2 Sv = sub(mul(s2(L.g * L.ey), h), mul(mul(k, uy), sp));
-    const float2 rsp = f2(sp.x > 0.0f ? __frcp_rn(sp.x) : 0.0f, sp.y > 0.0f ? __frcp_rn(sp.y) : 0.0f);
+    // the hardware reciprocal (1/x is approximate under -prec-div=false):
+    // rcp(0) = inf and rcp(inf) = 0 keep the non-finite test below exact
+    const float2 rsp = f2(sp.x > 0.0f ? 1.0f / sp.x : 0.0f, sp.y > 0.0f ? 1.0f / sp.y : 0.0f);
     const float2 dsx = mul(mul(ux, hinv), rsp), dsy = mul(mul(uy, hinv), rsp);
     const float2 nk = neg(k), vdt = s2(dt), one = s2(1.0f);
     const float2 J22 = mul(nk, fma(hinv, sp, mul(ux, dsx))), J23 = mul(nk, mul(ux, dsy));
@@ -173,7 +191,7 @@ __device__ __forceinline__ void manning_implicit2(float2 h, float2 u, float2 v, 
     const float2 c = mul(neg(vdt), J32), d = fma(neg(vdt), J33, one);
     const float2 det = sub(mul(a, d), mul(b, c));
     const float2 r0 = mul(vdt, Su), r1 = mul(vdt, Sv);
-    const float2 rdet = f2(__frcp_rn(det.x), __frcp_rn(det.y));
+    const float2 rdet = f2(1.0f / det.x, 1.0f / det.y);
     const float2 x0 = mul(sub(mul(r0, d), mul(b, r1)), rdet);
     const float2 x1 = mul(sub(mul(a, r1), mul(c, r0)), rdet);
     // a zero, infinite or NaN determinant makes the solution non-finite
