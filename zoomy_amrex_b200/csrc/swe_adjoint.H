@@ -88,8 +88,7 @@ PORTABLE_FN ZADJ_INLINE R rsqrt_of(R x) {
 }
 
 // dhinv from one reciprocal square root: with D = x0 + max(x0, eps),
-// dhinv = sqrt2 D^(-1/2) (1 - h D' / (2 D)). A derivative coefficient only:
-// values that decide a branch (hinv itself) are computed as the forward does.
+// dhinv = sqrt2 D^(-1/2) (1 - h D' / (2 D)). A derivative coefficient only.
 template <class R>
 PORTABLE_FN ZADJ_INLINE R dhinv_r(R h, R eps) {
     const R h2 = h * h;
@@ -100,6 +99,51 @@ PORTABLE_FN ZADJ_INLINE R dhinv_r(R h, R eps) {
     const R r = rsqrt_of(D);
     const R dD = R(4) * h * h2 * (big ? R(2) : R(1));
     return std::sqrt(R(2)) * r * (R(1) - R(0.5) * h * dD * (r * r));
+}
+
+// hinv from one reciprocal square root, sqrt2 h D^(-1/2) (within an ulp or
+// two of hinv): the face reverse's coefficient. The only branch it feeds is
+// the Rusanov speed's max(evL, evR), which it can turn only where the two
+// speeds agree to an ulp without being equal (equal inputs still give equal
+// speeds).
+template <class R>
+PORTABLE_FN ZADJ_INLINE R hinv_r(R h, R eps) {
+    const R h2 = h * h;
+    const R x0 = h2 * h2;
+    return std::sqrt(R(2)) * h * rsqrt_of(x0 + amrex::max(x0, eps));
+}
+
+// Rounded product and sum that the compiler may not fuse (the forward
+// kernels are built without contraction).
+template <class R>
+PORTABLE_FN ZADJ_INLINE R mul_rn(R a, R b) {
+#ifdef __CUDA_ARCH__
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+template <class R>
+PORTABLE_FN ZADJ_INLINE R add_rn(R a, R b) {
+#ifdef __CUDA_ARCH__
+    return __dadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+
+// A face side's Rusanov speed |m_n hinv(h)| + sqrt(g max(h, 0)) in the
+// forward's own operations (make_rhs.H:77-131 with the model's eigenvalue):
+// qh, qm the reconstructed depth and normal momentum, h the depth the flux
+// sees (h* with WB, where m = qm (h* / qh)).
+template <bool WB, class R>
+PORTABLE_FN ZADJ_INLINE R speed_fwd(R qh, R h, R qm, R g, R eps) {
+    R m = qm;
+    if constexpr (WB) m = mul_rn(qm, (qh > R(0)) ? h / qh : R(0));
+    const R h2 = mul_rn(h, h);
+    const R x0 = mul_rn(h2, h2);
+    const R hi = mul_rn(std::sqrt(R(2)), h) / std::sqrt(add_rn(x0, amrex::max(x0, eps)));
+    return add_rn(std::fabs(mul_rn(m, hi)), std::sqrt(mul_rn(g, amrex::max(h, R(0)))));
 }
 
 template <class R>
@@ -182,21 +226,47 @@ PORTABLE_FN ZADJ_INLINE void face_rev(const R c[4][4], SweP<R> const& p, const R
         tR = qR[1] + qR[0] - bf;
         hsL = amrex::max(R(0), tL);
         hsR = amrex::max(R(0), tR);
-        // the forward's values (they decide max / minmod branches below);
-        // iq = 1 / q_h serves the reverse only
-        sL = (qL[1] > R(0)) ? hsL / qL[1] : R(0);
-        sR = (qR[1] > R(0)) ? hsR / qR[1] : R(0);
+        // iq = 1 / q_h; s = h* iq (the forward divides: s is within an ulp
+        // of the forward's, and the branches below depend on it only through
+        // the Rusanov speed's max)
         iqL = (qL[1] > R(0)) ? R(1) / qL[1] : R(0);
         iqR = (qR[1] > R(0)) ? R(1) / qR[1] : R(0);
+        sL = hsL * iqL;
+        sR = hsR * iqR;
         mL[0] *= sL; mL[1] *= sL; mR[0] *= sR; mR[1] *= sR;
         hL = hsL; hR = hsR; bL = bf; bR = bf;
     }
     const R g = p.g;
-    const R hiL = hinv(hL, p.eps), hiR = hinv(hR, p.eps);
+    const R hiL = hinv_r(hL, p.eps), hiR = hinv_r(hR, p.eps);
     const R uL = mL[D] * hiL, uR = mR[D] * hiR;
-    const R cL = std::sqrt(g * amrex::max(hL, R(0))), cR = std::sqrt(g * amrex::max(hR, R(0)));
+    // c = sqrt(g h) exactly as the forward forms it; dc/dh = g r / 2 with
+    // r = (g h)^(-1/2)
+    const R ghL = mul_rn(g, amrex::max(hL, R(0))), ghR = mul_rn(g, amrex::max(hR, R(0)));
+    const R cL = std::sqrt(ghL), cR = std::sqrt(ghR);
+    const R rcL = (ghL > R(0)) ? rsqrt_of(ghL) : R(0), rcR = (ghR > R(0)) ? rsqrt_of(ghR) : R(0);
     const R evL = std::fabs(uL) + cL, evR = std::fabs(uR) + cR;
-    const bool pickR = evL < evR;          // amrex::max(evL, evR)
+    bool pickR = evL < evR;                // amrex::max(evL, evR)
+    const R aL = std::fabs(uL), aR = std::fabs(uR);
+    if (std::fabs(evL - evR) <= R(1e-13) * (aL + aR) + R(1e-15) * (evL + evR)) {
+        // Near a tie the branch is decided as the forward decides it. c is
+        // the forward's and |u| is within 1e-13 relative of the forward's
+        // |u| (a few ulps), so each forward speed fl(|u| + c) lies between
+        // the sums of c with |u| -+ 1e-13 |u|: where those agree (always for
+        // a side with |u| far below an ulp of c, as in water nearly at rest)
+        // it is known exactly.
+        const R loL = (aL - R(1e-13) * aL) + cL, upL = (aL + R(1e-13) * aL) + cL;
+        const R loR = (aR - R(1e-13) * aR) + cR, upR = (aR + R(1e-13) * aR) + cR;
+        if (loL == upL && loR == upR) {
+            pickR = loL < loR;
+        } else {
+            // else from the forward's own arithmetic: equal speeds where both
+            // sides' inputs agree (a mirrored wall face; the forward keeps
+            // evL), else the speeds recomputed as the forward computes them
+            const R nL = qL[2 + D], nR = qR[2 + D];
+            const bool same = hL == hR && qL[1] == qR[1] && std::fabs(nL) == std::fabs(nR);
+            pickR = !same && speed_fwd<WB>(qL[1], hL, nL, g, p.eps) < speed_fwd<WB>(qR[1], hR, nR, g, p.eps);
+        }
+    }
     const R s = pickR ? evR : evL;
     const R db = bR - bL;
     const R Bn = g * (R(0.5) * (hL + hR));
@@ -238,11 +308,11 @@ PORTABLE_FN ZADJ_INLINE void face_rev(const R c[4][4], SweP<R> const& p, const R
         if (pickR) {
             const R lu = sgn(uR) * lev;
             lmR[D] += lu * hiR; lhiR += lu * mR[D];
-            if (hR > R(0)) lhR += lev * g / (R(2) * cR);
+            if (hR > R(0)) lhR += lev * g * R(0.5) * rcR;
         } else {
             const R lu = sgn(uL) * lev;
             lmL[D] += lu * hiL; lhiL += lu * mL[D];
-            if (hL > R(0)) lhL += lev * g / (R(2) * cL);
+            if (hL > R(0)) lhL += lev * g * R(0.5) * rcL;
         }
     }
     lhL += lhiL * dhinv_r(hL, p.eps);
