@@ -20,14 +20,14 @@ BUILD = ROOT / "tests" / "_build"
 PAR = np.array([9.81, 0.0, 0.0, 0.03, 1e-6, 1e-24])
 
 
-@pytest.fixture(scope="module")
-def adj():
+def _host_lib(name, defines=()):
     BUILD.mkdir(exist_ok=True)
-    so = BUILD / "libadjhost.so"
+    so = BUILD / name
     src = ROOT / "tests" / "adjoint_host.cpp"
     deps = [src, CSRC / "swe_adjoint.H", CSRC / "models" / "zb_portable_math.H"]
     if not so.exists() or any(d.stat().st_mtime > so.stat().st_mtime for d in deps):
         subprocess.run(["g++", "-O2", "-ffp-contract=off", "-std=c++17", "-shared", "-fPIC",
+                        *[f"-D{d}" for d in defines],
                         "-I", str(CSRC), "-I", str(CSRC / "amrex_compat"), "-I", str(CSRC / "models"),
                         str(src), "-o", str(so)], check=True)
     L = C.CDLL(str(so))
@@ -37,6 +37,18 @@ def adj():
     L.adj_face_fwd.argtypes = [i, i, p, p, p]
     L.adj_face_rev.argtypes = [i, i, p, p, p, p]
     return L
+
+
+@pytest.fixture(scope="module")
+def adj():
+    return _host_lib("libadjhost.so")
+
+
+@pytest.fixture(scope="module")
+def adj_fwd_branches():
+    """The same reverse with every wave-speed max decided from speeds
+    recomputed with the forward's operations."""
+    return _host_lib("libadjhost_fwdbranch.so", ("ZADJ_FORWARD_BRANCHES",))
 
 
 def _p(a):
@@ -174,3 +186,39 @@ def test_stage_reverse_with_dry_cells(adj):
         fd = (lamY * (st.fwd(X + eps * V, dt) - st.fwd(X - eps * V, dt))).sum() / (2 * eps)
         an = (lamX * V).sum()
         assert abs(fd - an) <= 1e-5 * (abs(fd) + abs(an)), (k, fd, an)
+
+
+@pytest.mark.parametrize("wb", [0, 1])
+@pytest.mark.parametrize("dry", [False, True])
+def test_near_tie_branches_are_the_forwards(adj, adj_fwd_branches, wb, dry):
+    """The face reverse forms hinv and the Audusse ratio a few ulps off the
+    forward's, and decides the Rusanov max near ties by bracketing the
+    forward's speeds. A state whose velocities are constant along x (x-face
+    speeds tie to an ulp) and water at rest with ulp-level momenta (every
+    speed ties to an ulp) must give the reverse of the build that recomputes
+    every speed with the forward's operations, to rounding."""
+    nx, ny = 40, 32
+    rng = np.random.default_rng(2)
+    x = (np.arange(nx) + 0.5) / nx * 10.0
+    y = (np.arange(ny) + 0.5) / ny * 10.0
+    X, Y = np.meshgrid(x, y)
+    b = 0.3 * np.exp(-((X - 4) ** 2 + (Y - 6) ** 2) / 4.0) + 0.02 * rng.random((ny, nx))
+    if dry:
+        b = b + 1.3 * np.exp(-((X - 5) ** 2 + (Y - 5) ** 2) / 1.0)
+    eta = 1.0 + 0.2 * np.exp(-((X - 7) ** 2 + (Y - 3) ** 2) / 2.0)
+    h = np.maximum(eta - b, 0.0)
+    moving = np.array([b, h, h * (0.2 + 0.05 * np.sin(Y)), h * (-0.1 + 0.05 * np.cos(X))])
+    h1 = np.maximum(1.0 - b, 0.0)
+    at_rest = np.array([b, h1, 1e-15 * rng.standard_normal((ny, nx)) * h1,
+                        1e-15 * rng.standard_normal((ny, nx)) * h1])
+    lam = np.random.default_rng(5).standard_normal(moving.shape)
+    for Q in (moving, at_rest):
+        Q = np.ascontiguousarray(Q)
+        st, sf = (Stage(L, nx, ny, (1, 0, 1, 1), wb, True) for L in (adj, adj_fwd_branches))
+        for k in range(8):
+            ga, _, _ = st.rev(Q, 0.01, lam)
+            gb, _, _ = sf.rev(Q, 0.01, lam)
+            for r in range(4):
+                err = np.abs(ga[r] - gb[r]).max() / np.abs(gb[r]).max()
+                assert err <= 1e-14, (k, r, err)
+            Q = np.ascontiguousarray(st.fwd(Q, 0.01))

@@ -247,7 +247,15 @@ PORTABLE_FN ZADJ_INLINE void face_rev(const R c[4][4], SweP<R> const& p, const R
     const R evL = std::fabs(uL) + cL, evR = std::fabs(uR) + cR;
     bool pickR = evL < evR;                // amrex::max(evL, evR)
     const R aL = std::fabs(uL), aR = std::fabs(uR);
-    if (std::fabs(evL - evR) <= R(1e-13) * (aL + aR) + R(1e-15) * (evL + evR)) {
+#ifdef ZADJ_FORWARD_BRANCHES
+    // test build: every face recomputes both speeds with the forward's
+    // operations (the near-tie rule below must give the same branches)
+    constexpr bool kTieRule = false;
+    pickR = speed_fwd<WB>(qL[1], hL, qL[2 + D], g, p.eps) < speed_fwd<WB>(qR[1], hR, qR[2 + D], g, p.eps);
+#else
+    constexpr bool kTieRule = true;
+#endif
+    if (kTieRule && std::fabs(evL - evR) <= R(1e-13) * (aL + aR) + R(1e-15) * (evL + evR)) {
         // Near a tie the branch is decided as the forward decides it. c is
         // the forward's and |u| is within 1e-13 relative of the forward's
         // |u| (a few ulps), so each forward speed fl(|u| + c) lies between
