@@ -54,7 +54,7 @@ __device__ __forceinline__ void block_sum2(double& a, double& b, double* red) {
 // planes) and loc (the hinv(X.h) term of lam_X.h), partials[2 * block] =
 // (dL/dn_m, dL/ddt) of this block's cells.
 template <bool IMPL, int NT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 1024 / NT)
 k_adj_cell(const double* __restrict__ lam_in, double scale, const double* __restrict__ X,
            const double* __restrict__ qs, P6 L, const double* __restrict__ meta,
            double* __restrict__ lamq, double* __restrict__ loc, double* __restrict__ partials) {
