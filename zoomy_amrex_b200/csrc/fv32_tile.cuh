@@ -112,20 +112,30 @@ struct TShape {
     static constexpr int RWS = TMA ? TX + 8 : TX + 2 * G;    // stored row width
     static constexpr int XO = TMA ? 2 : 0;                    // column of halo cell 0
     static constexpr int RW = TX + 2 * G;                     // halo cells per row
-    static constexpr int NFC = 3 * F::ne + 2;     // flux, D+, D- of the evolved rows, h*_L, h*_R
+    // per face and evolved row: l = flux - D+ (what the cell on its high
+    // side gains) and r = flux + D- (what the cell on its low side loses);
+    // then h*_L, h*_R; an odd count, so that neighbouring threads' faces sit
+    // in different shared-memory banks
+    static constexpr int NFC = (2 * F::ne + 2) | 1;
     static constexpr int NT = TX * TY;
     static constexpr size_t pad32(size_t n) { return (n + 31) / 32 * 32; }   // 128-byte blocks
     static constexpr size_t q_elems = pad32(size_t(F::nq) * RH * RWS);
     static constexpr size_t inc_elems = TMA ? pad32(size_t(F::ne) * RH * RWS) : 0;   // stage-2 TMA staging
+    // the x faces ([TY][TX+1][NFC]) and, after their terms are taken, the y
+    // faces ([TY+1][TX][NFC]) in one buffer
     static constexpr size_t fx_elems = size_t(TY) * (TX + 1) * NFC;
     static constexpr size_t fy_elems = size_t(TY + 1) * TX * NFC;
+    static constexpr size_t f_elems = pad32(fx_elems > fy_elems ? fx_elems : fy_elems);
     // TMA boxes land on 128-byte boundaries: the kernel rounds the dynamic
     // shared-memory base up, which the extra 128 bytes cover
     // the update's own inputs of each owned cell (X, lo, inc1: 3 x ne),
     // copied asynchronously at the start of the update stages
     static constexpr size_t epi_elems = size_t(3) * F::ne * NT;
     static constexpr size_t smem_bytes =
-        (q_elems + inc_elems + fx_elems + fy_elems + epi_elems) * sizeof(float) + (TMA ? 128 : 0);
+        (q_elems + inc_elems + f_elems + epi_elems) * sizeof(float) + (TMA ? 128 : 0);
+    // blocks per SM that the shared memory allows (228 KB per SM, 1 KB of it
+    // reserved per block, a few hundred bytes of static shared memory)
+    static constexpr int smem_blocks = int((228 * 1024) / (smem_bytes + 1024 + 256));
     __host__ __device__ static constexpr unsigned box_bytes(int planes) { return unsigned(planes) * RH * RWS * sizeof(float); }
 };
 
@@ -236,8 +246,21 @@ struct has_block_implicit<M, std::void_t<decltype(&M::zb_implicit_increment)>> :
 // the bed, state and (stage 2) increment boxes, completing on an mbarrier
 // (the tensor maps cover this GPU's own buffers only); otherwise by plain
 // coalesced loads of every thread.
+// Blocks per SM the stage kernel's launch bounds ask for: what the shared
+// memory holds, so that registers do not limit the blocks below it, but
+// leaving each thread at least 64 registers where the model's point-implicit
+// system is solved by blocks and 80 where it takes a dense elimination
+// (which spills below that).
+template <class F, int TX, int TY, bool TMA>
+constexpr int tile_min_blocks() {
+    constexpr int regs = has_block_implicit<typename F::M64>::value ? 64 : 80;
+    constexpr int by_regs = 65536 / (TX * TY * regs);
+    constexpr int s = TShape<F, TX, TY, TMA>::smem_blocks;
+    return s < 1 ? 1 : (s > by_regs ? by_regs : s);
+}
+
 template <class F, int MODE, bool WB, bool IMPL, int TX, int TY, bool TMA>
-__global__ void __launch_bounds__(TX * TY)
+__global__ void __launch_bounds__(TX * TY, (tile_min_blocks<F, TX, TY, TMA>()))
 k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ TileMaps maps)
 {
     using Sh = TShape<F, TX, TY, TMA>;
@@ -256,9 +279,8 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
                      : tsm_raw;
     float* sQ = tsm;                                  // [nq][RH][RWS]: b, eta, q_2..
     float* sI = sQ + Sh::q_elems;                     // TMA, stage 2: [ne][RH][RWS] increment
-    float* sFx = sI + Sh::inc_elems;                  // [TY][TX+1][NFC]
-    float* sFy = sFx + Sh::fx_elems;                  // [TY+1][TX][NFC]
-    float* sE = sFy + Sh::fy_elems;                   // [3][ne][NT]: X, lo, inc1 of the owned cell
+    float* sF = sI + Sh::inc_elems;                   // x faces [TY][TX+1][NFC], then y faces [TY+1][TX][NFC]
+    float* sE = sF + Sh::f_elems;                     // [3][ne][NT]: X, lo, inc1 of the owned cell
     __shared__ double red[2 * ((NT + 31) / 32)];
     __shared__ __align__(8) uint64_t tbar;
     // halo-local cell (lx, ly) of row n
@@ -447,57 +469,64 @@ k32t_stage(TileParams<F::np> L, TileBufs B, int order2, const __grid_constant__ 
         const auto fc = N::numerical_fluctuations(qL, qR, aL, aR, p, nh);
 #pragma unroll
         for (int n = 1; n < nq; ++n) {
-            Fr[n - 1] = fl(n, 0);
-            Fr[ne + n - 1] = fc(n, 0);
-            Fr[2 * ne + n - 1] = fc(nq + n, 0);
+            Fr[n - 1] = fl(n, 0) - fc(n, 0);             // l = flux - D+
+            Fr[ne + n - 1] = fl(n, 0) + fc(nq + n, 0);   // r = flux + D-
         }
-        Fr[3 * ne] = hLs;
-        Fr[3 * ne + 1] = hRs;
+        Fr[2 * ne] = hLs;
+        Fr[2 * ne + 1] = hRs;
     };
 
     const int iend = min(x0 + TX, nx), jend = min(y0 + TY, ny);
 
-    // 3. faces, each once
+    // 3. faces, each once: the x faces, each owned cell's x terms, then the
+    // y faces in the same buffer
     if (j < jend) {
-        if (i <= iend) face(0, tx + G, ty + G, sFx + (ty * (TX + 1) + tx) * NFC);
-        if (tx == TX - 1 && x0 + TX <= iend) face(0, TX + G, ty + G, sFx + (ty * (TX + 1) + TX) * NFC);
+        if (i <= iend) face(0, tx + G, ty + G, sF + (ty * (TX + 1) + tx) * NFC);
+        if (tx == TX - 1 && x0 + TX <= iend) face(0, TX + G, ty + G, sF + (ty * (TX + 1) + TX) * NFC);
     }
+    __syncthreads();
+    const bool own = i < nx && j < ny;
+    // a cell's balance from a direction: l of its low face - r of its high
+    // face (make_rhs.H:346-399), with WB the bed source as a difference of
+    // the same FP32 pressures (g/2) h* h* the flux carries, each rounded once
+    // (the _rn products are never fused into an FMA with the difference):
+    // zero at rest, exactly
+    auto dir_terms = [&](const float* FL, const float* FH, int kwb, float* out) {
+#pragma unroll
+        for (int k = 0; k < ne; ++k) {
+            float f = FL[k] - FH[ne + k];
+            if constexpr (WB) {
+                if (k == kwb) {
+                    const float pr = __fmul_rn(__fmul_rn(0.5f * g, FH[2 * ne]), FH[2 * ne]);
+                    const float pl = __fmul_rn(__fmul_rn(0.5f * g, FL[2 * ne + 1]), FL[2 * ne + 1]);
+                    f = f + __fsub_rn(pr, pl);
+                }
+            }
+            out[k] = f;
+        }
+    };
+    float fxr[ne];
+    if (own) {
+        const float* FxL = sF + (ty * (TX + 1) + tx) * NFC;
+        dir_terms(FxL, FxL + NFC, 1, fxr);
+    }
+    __syncthreads();
     if (i < iend) {
-        if (j <= jend) face(1, tx + G, ty + G, sFy + (ty * TX + tx) * NFC);
-        if (ty == TY - 1 && y0 + TY <= jend) face(1, tx + G, TY + G, sFy + (TY * TX + tx) * NFC);
+        if (j <= jend) face(1, tx + G, ty + G, sF + (ty * TX + tx) * NFC);
+        if (ty == TY - 1 && y0 + TY <= jend) face(1, tx + G, TY + G, sF + (TY * TX + tx) * NFC);
     }
     __syncthreads();
 
     // 4. assemble, update, implicit source, write
     double m_loc = 0.0, s_loc = 0.0;
-    if (i < nx && j < ny) {
+    if (own) {
         const long long c = (long long)j * nx + i;
-        const float* FxL = sFx + (ty * (TX + 1) + tx) * NFC;
-        const float* FxR = FxL + NFC;
-        const float* FyL = sFy + (ty * TX + tx) * NFC;
-        const float* FyR = FyL + TX * NFC;
+        const float* FyL = sF + (ty * TX + tx) * NFC;
+        float fyr[ne];
+        dir_terms(FyL, FyL + TX * NFC, 2, fyr);
         float d[ne];
 #pragma unroll
-        for (int k = 0; k < ne; ++k) {
-            float fx = -(FxR[k] - FxL[k]) - FxR[2 * ne + k] - FxL[ne + k];
-            float fy = -(FyR[k] - FyL[k]) - FyR[2 * ne + k] - FyL[ne + k];
-            if constexpr (WB) {
-                // the bed source (make_rhs.H:154-163) as a difference of the
-                // same FP32 pressures (g/2) h* h* the flux carries, each
-                // rounded once (the _rn products are never fused into an
-                // FMA with the difference): zero at rest, exactly
-                if (k == 1) {
-                    const float pr = __fmul_rn(__fmul_rn(0.5f * g, FxR[3 * ne]), FxR[3 * ne]);
-                    const float pl = __fmul_rn(__fmul_rn(0.5f * g, FxL[3 * ne + 1]), FxL[3 * ne + 1]);
-                    fx = fx + __fsub_rn(pr, pl);
-                } else if (k == 2) {
-                    const float pr = __fmul_rn(__fmul_rn(0.5f * g, FyR[3 * ne]), FyR[3 * ne]);
-                    const float pl = __fmul_rn(__fmul_rn(0.5f * g, FyL[3 * ne + 1]), FyL[3 * ne + 1]);
-                    fy = fy + __fsub_rn(pr, pl);
-                }
-            }
-            d[k] = dt * (fx * L.rdx + fy * L.rdy);
-        }
+        for (int k = 0; k < ne; ++k) d[k] = dt * (fxr[k] * L.rdx + fyr[k] * L.rdy);
         const int lx = tx + G, ly = ty + G;
         const float bc = at(0, lx, ly);
         if constexpr (IMPL) {
