@@ -168,15 +168,15 @@ __device__ __forceinline__ bool finish_step_units(double m, double s, double* re
     return true;
 }
 
-// Blocks per SM the register budget aims at: 4 for the 2-D shallow-water
-// tile (64 registers; its shared memory, with the one face buffer, fits 4
-// blocks too), so that 32 warps hide the FP64 latency; 3 for 2-D models
-// with more unknowns whose point-implicit system is solved by blocks; 2 for
-// 1-D rows and for dense n x n eliminations, which must stay in registers.
+// Blocks per SM the register budget aims at: 4 for 2-D tiles, so that 32
+// warps (shallow water: 256 threads at 64 registers) or 16 (the models whose
+// point-implicit system is solved by blocks: 128 threads at 128 registers,
+// the dense fallback out of line) hide the FP64 latency; their shared
+// memory, with the one face buffer, fits 4 blocks too; 2 for 1-D rows and
+// for dense n x n eliminations, which must stay in registers.
 template <class Model>
 constexpr int stage_min_blocks() {
-    if constexpr (Model::dimension == 2 && Model::n_dof_q <= 4) return 4;
-    else if constexpr (Model::dimension == 2 && implicit_blocks<Model>::value) return 3;
+    if constexpr (Model::dimension == 2 && (Model::n_dof_q <= 4 || implicit_blocks<Model>::value)) return 4;
     else return 2;
 }
 
