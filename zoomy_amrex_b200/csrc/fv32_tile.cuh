@@ -249,8 +249,8 @@ struct has_block_implicit<M, std::void_t<decltype(&M::zb_implicit_increment)>> :
 // Blocks per SM the stage kernel's launch bounds ask for: what the shared
 // memory holds, so that registers do not limit the blocks below it, but
 // leaving each thread at least 64 registers where the model's point-implicit
-// system is solved by blocks and 80 where it takes a dense elimination
-// (which spills below that).
+// system is solved by blocks (no spill there) and 80 where its near-dry FP64
+// branch takes a dense elimination (a few bytes of spill at 80, more below).
 template <class F, int TX, int TY, bool TMA>
 constexpr int tile_min_blocks() {
     constexpr int regs = has_block_implicit<typename F::M64>::value ? 64 : 80;
